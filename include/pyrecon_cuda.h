@@ -1,0 +1,254 @@
+/*
+ * pyrecon_cuda.h -- C ABI of libpyrecon_cuda.so, the sm_100a (B200) implementation of
+ * pyrecon's reconstruction hot path.
+ *
+ * Every entry point:
+ *   - takes DEVICE pointers for meshes, particles and workspaces, and HOST pointers for the
+ *     small 3-vectors (nmesh, boxsize, boxcenter, los, radius);
+ *   - takes the CUDA stream as `void *stream` (a cudaStream_t; NULL = legacy default stream)
+ *     and only enqueues work on it (no host synchronisation, no device allocation: scratch
+ *     comes from the caller through `workspace`, sized by the matching *_workspace_bytes);
+ *   - returns a prc_status_t; argument checks happen before anything is enqueued.
+ * Conditions found while running (positions outside the box, NaN/inf) are OR-ed into the
+ * caller's device word `flags` (PRC_FLAG_*); kernels downstream of a raised flag in the same
+ * call skip their writes, so the output mesh is left untouched, as the reference leaves it
+ * when it raises MeshError (pyrecon/mesh.py:549-553).
+ *
+ * Meshes are C-ordered (n0, n1, n2); half spectra are (n0, n1, n2/2+1) interleaved complex;
+ * positions are (N, 3) row-major float32 or float64 (`pos_bytes` = 4 or 8).  `_f32` / `_f64`
+ * suffixes select the mesh precision, as the reference's mesh_float.so / mesh_double.so and
+ * multigrid_float.so / multigrid_double.so do (reference src/Makefile:11-21).
+ */
+#ifndef PYRECON_CUDA_H
+#define PYRECON_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int prc_status_t;
+
+#if defined(__GNUC__)
+#define PRC_API __attribute__((visibility("default")))
+#else
+#define PRC_API
+#endif
+
+#define PRC_OK 0
+#define PRC_ERR_ARG 1          /* invalid argument (null pointer, bad size, bad enum) */
+#define PRC_ERR_WORKSPACE 2    /* workspace smaller than *_workspace_bytes */
+#define PRC_ERR_CUDA 3         /* a kernel launch or CUDA runtime call failed */
+#define PRC_ERR_UNSUPPORTED 4  /* mesh size this build does not handle (FFT radix / limits) */
+#define PRC_ERR_TIMEOUT 5      /* a bounded device-side wait gave up */
+
+#define PRC_FLAG_OUT_OF_BOX 1  /* a position outside [boxcenter - boxsize/2, boxcenter + boxsize/2] */
+#define PRC_FLAG_NONFINITE 2   /* a NaN/inf position or weight */
+
+#define PRC_FIELD_DISP 0       /* Zeldovich displacement only */
+#define PRC_FIELD_RSD 1        /* RSD displacement f (s.l) l only */
+#define PRC_FIELD_DISP_RSD 2   /* both */
+
+/* Library version string. */
+PRC_API const char *prc_version(void);
+
+/* Human-readable name of a status code. */
+PRC_API const char *prc_status_string(prc_status_t status);
+
+/* 1 if every axis of nmesh is handled by the FFT kernels (n = 2^a 3^b 5^c 7^d, n2 even,
+ * n <= 1024), else 0. */
+PRC_API int prc_fft_supported(const int32_t nmesh[3]);
+
+/* ------------------------------------------------------------------------------------------
+ * Painting.  Replaces assign_cic (reference src/mesh.c:26-63) together with the index
+ * transform, wrap and box / NaN checks of RealMesh.assign_cic (pyrecon/mesh.py:529-568).
+ * Deterministic: particles are radix-sorted by base cell (stable), then each mesh column
+ * sums its contributions in a fixed order in FP64.  `mesh` is an FP64 accumulator that
+ * `accumulate` = 1 adds into (repeated assign_* calls), 0 overwrites.  `column_sums`
+ * (n0*n1 doubles, may be NULL) receives the sum of every final mesh column (z axis).
+ * `mesh_bytes` (4 or 8) is the reference mesh dtype that fixes the index-space precision;
+ * `weights` may be NULL (unit weights), else `weight_bytes` = 4 or 8.
+ * ------------------------------------------------------------------------------------------ */
+PRC_API size_t prc_assign_cic_workspace_bytes(const int32_t nmesh[3], int64_t npos, int mesh_bytes);
+PRC_API prc_status_t prc_assign_cic(double *mesh, double *column_sums, const int32_t nmesh[3],
+                            const double boxsize[3], const double boxcenter[3], int mesh_bytes,
+                            const void *positions, int pos_bytes, const void *weights,
+                            int weight_bytes, int64_t npos, int wrap, int accumulate,
+                            int32_t *flags, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Base-cell keys and the stable order that sorts them (the permutation the paint uses):
+ * keys_sorted[i] = key[order[i]], key = (ix * n1 + iy) * n2 + iz.  Exposed so the sort can be
+ * checked bit for bit against a stable argsort. Uses the paint workspace. */
+PRC_API prc_status_t prc_cic_cell_order(uint32_t *keys_sorted, uint32_t *order, const int32_t nmesh[3],
+                                const double boxsize[3], const double boxcenter[3], int mesh_bytes,
+                                const void *positions, int pos_bytes, int64_t npos, int wrap,
+                                int32_t *flags, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Deterministic FP64 sum of n doubles into *out (device).  Replaces np.sum of a mesh. */
+PRC_API size_t prc_sum_workspace_bytes(int64_t n);
+PRC_API prc_status_t prc_sum_f64(const double *x, int64_t n, double *out, void *workspace,
+                         size_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Gathers.  Output `out` has the positions' dtype (the reference casts back,
+ * pyrecon/mesh.py:610,653).
+ * ------------------------------------------------------------------------------------------ */
+/* Replaces read_cic (reference src/mesh.c:269-310) + RealMesh.read_cic (mesh.py:570-610). */
+PRC_API prc_status_t prc_read_cic_f32(const float *mesh, const int32_t nmesh[3], const double boxsize[3],
+                              const double boxcenter[3], const void *positions, int pos_bytes,
+                              int64_t npos, int wrap, void *out, int32_t *flags, void *stream);
+PRC_API prc_status_t prc_read_cic_f64(const double *mesh, const int32_t nmesh[3], const double boxsize[3],
+                              const double boxcenter[3], const void *positions, int pos_bytes,
+                              int64_t npos, int wrap, void *out, int32_t *flags, void *stream);
+
+/* Replaces read_finite_difference_cic (reference src/mesh.c:187-266) +
+ * RealMesh.read_finite_difference_cic (mesh.py:612-653); out is (npos, 3). */
+PRC_API prc_status_t prc_read_finite_difference_cic_f32(const float *mesh, const int32_t nmesh[3],
+                                                const double boxsize[3], const double boxcenter[3],
+                                                const void *positions, int pos_bytes, int64_t npos,
+                                                int wrap, void *out, int32_t *flags, void *stream);
+PRC_API prc_status_t prc_read_finite_difference_cic_f64(const double *mesh, const int32_t nmesh[3],
+                                                const double boxsize[3], const double boxcenter[3],
+                                                const void *positions, int pos_bytes, int64_t npos,
+                                                int wrap, void *out, int32_t *flags, void *stream);
+
+/* Fused shift read-out of the FFT algorithms: three CIC gathers of psi_x, psi_y, psi_z, the RSD
+ * term f (s.l) l with l = los (global, unit 3-vector) or p/|p| of the wrapped positions (los =
+ * NULL), field selection and, if `shifted`, positions - shifts wrapped when `wrap`.
+ * Replaces BaseReconstruction.read_shifts / read_shifted_positions (pyrecon/recon.py:255-325).
+ * out is (npos, 3) in `out_bytes` precision. */
+PRC_API prc_status_t prc_read_shifts_psi_f32(const float *psi_x, const float *psi_y, const float *psi_z,
+                                     const int32_t nmesh[3], const double boxsize[3],
+                                     const double boxcenter[3], const void *positions, int pos_bytes,
+                                     int64_t npos, double f, const double *los, int field, int shifted,
+                                     int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+PRC_API prc_status_t prc_read_shifts_psi_f64(const double *psi_x, const double *psi_y, const double *psi_z,
+                                     const int32_t nmesh[3], const double boxsize[3],
+                                     const double boxcenter[3], const void *positions, int pos_bytes,
+                                     int64_t npos, double f, const double *los, int field, int shifted,
+                                     int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+
+/* Same for the multigrid potential: finite-difference CIC gradient of phi, RSD direction from
+ * the UNWRAPPED positions (pyrecon/multigrid.py:137-158). */
+PRC_API prc_status_t prc_read_shifts_phi_f32(const float *phi, const int32_t nmesh[3], const double boxsize[3],
+                                     const double boxcenter[3], const void *positions, int pos_bytes,
+                                     int64_t npos, double f, const double *los, int field, int shifted,
+                                     int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+PRC_API prc_status_t prc_read_shifts_phi_f64(const double *phi, const int32_t nmesh[3], const double boxsize[3],
+                                     const double boxcenter[3], const void *positions, int pos_bytes,
+                                     int64_t npos, double f, const double *los, int field, int shifted,
+                                     int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * FFTs and the k-space steps (the numpy / pyfftw sites of pyrecon/mesh.py:974-1118 and the
+ * algorithm modules).  Forward transforms are unnormalised; inverse ones divide by n0*n1*n2,
+ * as numpy's fftn / ifftn.  Spectra are the r2c half; multipliers are applied in their
+ * Hermitian-symmetrised form so results equal the reference's c2c transform followed by .real.
+ * ------------------------------------------------------------------------------------------ */
+PRC_API size_t prc_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int nspectra);
+
+/* Forward r2c: in is a real mesh of `in_bytes` (4 or 8) precision, out the half spectrum. */
+PRC_API prc_status_t prc_rfft3d_f32(const void *in, int in_bytes, void *out, const int32_t nmesh[3], void *stream);
+PRC_API prc_status_t prc_rfft3d_f64(const void *in, int in_bytes, void *out, const int32_t nmesh[3], void *stream);
+/* Inverse c2r of a half spectrum (overwritten) into a real mesh. */
+PRC_API prc_status_t prc_irfft3d_f32(void *in, float *out, const int32_t nmesh[3], void *stream);
+PRC_API prc_status_t prc_irfft3d_f64(void *in, double *out, const int32_t nmesh[3], void *stream);
+
+/* Gaussian smoothing exp(-1/2 sum (r_a k_a)^2) of a real mesh (in: `in_bytes` precision,
+ * may equal out).  Replaces RealMesh.smooth_gaussian(method='fft') (mesh.py:655-680). */
+PRC_API prc_status_t prc_smooth_gaussian_f32(const void *in, int in_bytes, float *out, const int32_t nmesh[3],
+                                     const double boxsize[3], const double radius[3], void *workspace,
+                                     size_t workspace_bytes, void *stream);
+PRC_API prc_status_t prc_smooth_gaussian_f64(const void *in, int in_bytes, double *out, const int32_t nmesh[3],
+                                     const double boxsize[3], const double radius[3], void *workspace,
+                                     size_t workspace_bytes, void *stream);
+
+/* set_density_contrast of BaseReconstruction (pyrecon/recon.py:198-249): smooths the FP64 data
+ * (and randoms, may be NULL) meshes, then delta = (d - alpha r) / (bias alpha r) where
+ * r > ran_min * sum_r / size_randoms, else 0 (no randoms: d / mean(d) - 1, / bias).
+ * `sums` is a device pointer to {sum of data mesh, sum of randoms mesh} (FP64, e.g. from
+ * prc_sum_f64 on the paint's column sums); smoothing conserves the sum, so alpha = sums[0] /
+ * sums[1]. */
+PRC_API size_t prc_density_contrast_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int with_randoms);
+PRC_API prc_status_t prc_density_contrast_f32(const double *mesh_data, const double *mesh_randoms,
+                                      const double *sums, const int32_t nmesh[3], const double boxsize[3],
+                                      const double radius[3], double bias, double ran_min,
+                                      double size_randoms, float *delta, void *workspace,
+                                      size_t workspace_bytes, void *stream);
+PRC_API prc_status_t prc_density_contrast_f64(const double *mesh_data, const double *mesh_randoms,
+                                      const double *sums, const int32_t nmesh[3], const double boxsize[3],
+                                      const double radius[3], double bias, double ran_min,
+                                      double size_randoms, double *delta, void *workspace,
+                                      size_t workspace_bytes, void *stream);
+
+/* PlaneParallelFFTReconstruction.run (pyrecon/plane_parallel_fft.py:41-55):
+ * psi_a = IFFT(i k_a delta_k / (k^2 (1 + beta mu^2))), los a unit 3-vector. */
+PRC_API size_t prc_plane_parallel_workspace_bytes(const int32_t nmesh[3], int mesh_bytes);
+PRC_API prc_status_t prc_plane_parallel_fft_f32(const float *delta, const int32_t nmesh[3], const double boxsize[3],
+                                        double beta, const double los[3], float *psi_x, float *psi_y,
+                                        float *psi_z, void *workspace, size_t workspace_bytes, void *stream);
+PRC_API prc_status_t prc_plane_parallel_fft_f64(const double *delta, const int32_t nmesh[3], const double boxsize[3],
+                                        double beta, const double los[3], double *psi_x, double *psi_y,
+                                        double *psi_z, void *workspace, size_t workspace_bytes, void *stream);
+
+/* IterativeFFTReconstruction.run (pyrecon/iterative_fft.py:12-82), niterations of the
+ * Burden et al. 2015 field-level iteration then psi_a = IFFT(i k_a delta_k / k^2).
+ * los = NULL selects the local line of sight. */
+PRC_API size_t prc_iterative_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int local_los);
+PRC_API prc_status_t prc_iterative_fft_f32(const float *delta, const int32_t nmesh[3], const double boxsize[3],
+                                   const double boxcenter[3], double beta, const double *los,
+                                   int niterations, float *psi_x, float *psi_y, float *psi_z,
+                                   void *workspace, size_t workspace_bytes, void *stream);
+PRC_API prc_status_t prc_iterative_fft_f64(const double *delta, const int32_t nmesh[3], const double boxsize[3],
+                                   const double boxcenter[3], double beta, const double *los,
+                                   int niterations, double *psi_x, double *psi_y, double *psi_z,
+                                   void *workspace, size_t workspace_bytes, void *stream);
+
+/* Mirror of prod_sum (reference src/mesh.c:327-365): mesh *= (ax[i] + ay[j] + az[k])^exp on a
+ * real array of `shape`, coords = concatenation az, ay, ax (exp = -1, 1 or any integer). */
+PRC_API prc_status_t prc_prod_sum_f32(float *mesh, const int32_t shape[3], const float *coords, int exp, void *stream);
+PRC_API prc_status_t prc_prod_sum_f64(double *mesh, const int32_t shape[3], const double *coords, int exp, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Multigrid.  Replaces fmg (reference src/multigrid.c:303-328) and its components.
+ * los = NULL selects the local line of sight (19-point stencil with the first-derivative term).
+ * _f32 with mixed_precision = 1: every V-cycle is computed as v += V(0, f - A v) with the
+ * residual and v in FP64 and the V-cycle itself in FP32 (identical in exact arithmetic to the
+ * reference's fixed FMG schedule); mixed_precision = 0 runs the whole schedule in FP32.
+ * ------------------------------------------------------------------------------------------ */
+PRC_API size_t prc_multigrid_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int mixed_precision);
+PRC_API prc_status_t prc_multigrid_f32(const float *delta, float *phi, const int32_t nmesh[3], const double boxsize[3],
+                               const double boxcenter[3], double beta, double damping, int jacobi_niterations,
+                               int vcycle_niterations, const double *los, int mixed_precision, void *workspace,
+                               size_t workspace_bytes, void *stream);
+PRC_API prc_status_t prc_multigrid_f64(const double *delta, double *phi, const int32_t nmesh[3], const double boxsize[3],
+                               const double boxcenter[3], double beta, double damping, int jacobi_niterations,
+                               int vcycle_niterations, const double *los, void *workspace,
+                               size_t workspace_bytes, void *stream);
+
+/* Components, one level (jacobi: src/multigrid.c:44-104, residual :107-164, prolong :167-209,
+ * reduce :212-266).  jacobi runs `niterations` sweeps in place on v using `scratch` (one mesh). */
+PRC_API prc_status_t prc_mg_jacobi_f32(float *v, const float *f, float *scratch, const int32_t nmesh[3],
+                               const double boxsize[3], const double boxcenter[3], double beta, double damping,
+                               int niterations, const double *los, void *stream);
+PRC_API prc_status_t prc_mg_jacobi_f64(double *v, const double *f, double *scratch, const int32_t nmesh[3],
+                               const double boxsize[3], const double boxcenter[3], double beta, double damping,
+                               int niterations, const double *los, void *stream);
+PRC_API prc_status_t prc_mg_residual_f32(const float *v, const float *f, float *r, const int32_t nmesh[3],
+                                 const double boxsize[3], const double boxcenter[3], double beta,
+                                 const double *los, void *stream);
+PRC_API prc_status_t prc_mg_residual_f64(const double *v, const double *f, double *r, const int32_t nmesh[3],
+                                 const double boxsize[3], const double boxcenter[3], double beta,
+                                 const double *los, void *stream);
+PRC_API prc_status_t prc_mg_reduce_f32(const float *fine, float *coarse, const int32_t nmesh_fine[3], void *stream);
+PRC_API prc_status_t prc_mg_reduce_f64(const double *fine, double *coarse, const int32_t nmesh_fine[3], void *stream);
+PRC_API prc_status_t prc_mg_prolong_f32(const float *coarse, float *fine, const int32_t nmesh_coarse[3], void *stream);
+PRC_API prc_status_t prc_mg_prolong_f64(const double *coarse, double *fine, const int32_t nmesh_coarse[3], void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYRECON_CUDA_H */

@@ -1,0 +1,976 @@
+// Cloud-in-cell painting (deterministic, sort-by-cell) and the particle gathers.
+//
+// Paint pipeline for N particles on an n0 x n1 x n2 mesh (prc_assign_cic):
+//   1. keys:     per particle, wrap / box check / index transform exactly as numpy does it
+//                (pyrecon/mesh.py:546-555), base cell key = (ix*n1 + iy)*n2 + iz (mesh.c:35-37);
+//   2. sort:     stable LSD radix sort of (key, particle id), <= 9-bit digits;
+//   3. payload:  particles gathered in sorted order as (dx, dy, dz, w) in the mesh dtype, with
+//                the post-modulo fractional offsets of src/mesh.c:45-47;
+//   4. columns:  start offset of every (ix, iy) column in the sorted array;
+//   5. pull:     one warp per OUTPUT column (X, Y) sums, in a fixed order, the contributions of
+//                the four base columns (X-cx, Y-cy) in FP64 shared memory: per 32-particle chunk
+//                a segmented warp scan over equal iz, then two conflict-free phases add to
+//                z = iz and z = iz + 1.  Same inputs -> same bits, run after run.
+#include "common.cuh"
+
+#include <limits.h>
+
+#include <algorithm>
+
+namespace prc {
+
+// ---------------------------------------------------------------------------------------------
+// Radix sort of (uint32 key, uint32 value), stable
+// ---------------------------------------------------------------------------------------------
+namespace rsort {
+
+constexpr int THREADS = 256;
+constexpr int WARPS = THREADS / 32;
+constexpr int ITEMS = 16;                      // per thread
+constexpr int TILE = THREADS * ITEMS;          // 4096 items per tile
+constexpr int MAXBITS = 9;
+constexpr int MAXRADIX = 1 << MAXBITS;
+
+__global__ void __launch_bounds__(THREADS) upsweep(const uint32_t* __restrict__ keys, int64_t n, int shift,
+                                                   int radix, int ntiles, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t cnt[MAXRADIX];
+    const uint32_t mask = (uint32_t)radix - 1;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        for (int d = threadIdx.x; d < radix; d += THREADS) cnt[d] = 0;
+        __syncthreads();
+        int64_t base = (int64_t)tile * TILE;
+        for (int k = 0; k < ITEMS; k++) {
+            int64_t i = base + (int64_t)k * THREADS + threadIdx.x;
+            if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & mask], 1u);
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < radix; d += THREADS) hist[(int64_t)d * ntiles + tile] = cnt[d];
+        __syncthreads();
+    }
+}
+
+// Exclusive scan of `count` uint32 in place, by one block per SCAN_TILE chunk + one pass over
+// the chunk totals.  Sizes here stay below 2^32 (digit counts of < 2^32 items).
+constexpr int SCAN_THREADS = 512;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        s_warp[lane] = w;   // inclusive warp-total prefix
+    }
+    __syncthreads();
+    uint32_t before = warp > 0 ? s_warp[warp - 1] : 0u;
+    uint32_t res = before + x - v;
+    if (total) *total = s_warp[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return res;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) scan_tiles(uint32_t* __restrict__ data, int64_t count,
+                                                           uint32_t* __restrict__ tile_sums) {
+    __shared__ uint32_t s_warp[32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS], sum = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        v[k] = base + k < count ? data[base + k] : 0u;
+        sum += v[k];
+    }
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(sum, s_warp, &total);
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        if (base + k < count) data[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) scan_totals(uint32_t* __restrict__ sums, int count) {
+    __shared__ uint32_t s_warp[32];
+    uint32_t carry = 0;
+    for (int base = 0; base < count; base += SCAN_THREADS) {
+        int i = base + threadIdx.x;
+        uint32_t v = i < count ? sums[i] : 0u;
+        uint32_t total;
+        uint32_t ex = block_exclusive_scan(v, s_warp, &total);
+        if (i < count) sums[i] = carry + ex;
+        carry += total;
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) scan_add(uint32_t* __restrict__ data, int64_t count,
+                                                         const uint32_t* __restrict__ tile_sums) {
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+    uint32_t add = tile_sums[blockIdx.x];
+    for (int k = threadIdx.x; k < SCAN_TILE; k += SCAN_THREADS)
+        if (base + k < count) data[base + k] += add;
+}
+
+// Stable scatter of one tile: each warp ranks its contiguous 512-item slice chunk by chunk
+// (__match_any_sync groups equal digits; lanes keep input order), warps are then offset by the
+// counts of the warps before them, and the tile by the scanned histogram.
+__global__ void __launch_bounds__(THREADS) downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                     uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                     int64_t n, int shift, int radix, int ntiles,
+                                                     const uint32_t* __restrict__ offsets) {
+    extern __shared__ uint32_t smem[];
+    uint32_t* s_key = smem;                       // TILE
+    uint32_t* s_val = s_key + TILE;               // TILE
+    uint32_t* s_rank = s_val + TILE;              // TILE
+    uint32_t* s_cnt = s_rank + TILE;              // WARPS * radix
+    const uint32_t mask = (uint32_t)radix - 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    constexpr int SLICE = TILE / WARPS;
+
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int64_t base = (int64_t)tile * TILE;
+        int valid = (int)min((int64_t)TILE, n - base);
+        for (int k = threadIdx.x; k < TILE; k += THREADS) {
+            if (k < valid) {
+                s_key[k] = kin[base + k];
+                s_val[k] = vin[base + k];
+            }
+        }
+        for (int k = threadIdx.x; k < WARPS * radix; k += THREADS) s_cnt[k] = 0u;
+        __syncthreads();
+        uint32_t* cnt = s_cnt + warp * radix;
+        for (int c = 0; c < SLICE; c += 32) {
+            int k = warp * SLICE + c + lane;
+            bool ok = k < valid;
+            uint32_t d = ok ? (s_key[k] >> shift) & mask : 0xffffffffu;
+            uint32_t peers = __match_any_sync(0xffffffffu, d);
+            uint32_t before = ok ? cnt[d] : 0u;
+            __syncwarp();
+            if (ok) {
+                s_rank[k] = before + __popc(peers & lt);
+                if ((peers & lt) == 0u) cnt[d] = before + __popc(peers);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < radix; d += THREADS) {
+            uint32_t run = offsets[(int64_t)d * ntiles + tile];
+            for (int w = 0; w < WARPS; w++) {
+                uint32_t c = s_cnt[w * radix + d];
+                s_cnt[w * radix + d] = run;
+                run += c;
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < valid; k += THREADS) {
+            uint32_t key = s_key[k];
+            uint32_t d = (key >> shift) & mask;
+            uint32_t pos = s_cnt[(k / SLICE) * radix + d] + s_rank[k];
+            kout[pos] = key;
+            vout[pos] = s_val[k];
+        }
+        __syncthreads();
+    }
+}
+
+inline size_t downsweep_smem(int radix) { return (size_t)(3 * TILE + WARPS * radix) * sizeof(uint32_t); }
+
+inline int num_tiles(int64_t n) { return (int)((n + TILE - 1) / TILE); }
+
+inline int64_t scan_count(int64_t n, int radix) { return (int64_t)num_tiles(n) * radix; }
+
+inline int scan_blocks(int64_t count) { return (int)((count + SCAN_TILE - 1) / SCAN_TILE); }
+
+// Bytes of scratch for sorting n items with the largest digit (histogram + scan tile sums).
+inline size_t scratch_bytes(int64_t n) {
+    int64_t c = scan_count(n, MAXRADIX);
+    return (size_t)(c + scan_blocks(c) + 64) * sizeof(uint32_t);
+}
+
+// Sorts (k0, v0) by the low `bits` bits of the key.  Ping-pongs with (k1, v1); returns through
+// *kres / *vres which pair holds the result.
+int sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, int64_t n, int bits, uint32_t* scratch,
+               uint32_t** kres, uint32_t** vres, cudaStream_t st) {
+    *kres = k0;
+    *vres = v0;
+    if (n <= 1 || bits <= 0) return PRC_OK;
+    int npass = (bits + MAXBITS - 1) / MAXBITS;
+    int dbits = (bits + npass - 1) / npass;
+    int radix = 1 << dbits;
+    int ntiles = num_tiles(n);
+    int64_t count = (int64_t)ntiles * radix;
+    uint32_t* hist = scratch;
+    uint32_t* tsums = scratch + count;
+    int sms = device_sm_count();
+    int grid = min(ntiles, sms * 8);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(downsweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)downsweep_smem(MAXRADIX));
+        attr_set = true;
+    }
+    uint32_t *ka = k0, *va = v0, *kb = k1, *vb = v1;
+    for (int p = 0; p < npass; p++) {
+        int shift = p * dbits;
+        upsweep<<<grid, THREADS, 0, st>>>(ka, n, shift, radix, ntiles, hist);
+        int sb = scan_blocks(count);
+        scan_tiles<<<sb, SCAN_THREADS, 0, st>>>(hist, count, tsums);
+        scan_totals<<<1, SCAN_THREADS, 0, st>>>(tsums, sb);
+        scan_add<<<sb, SCAN_THREADS, 0, st>>>(hist, count, tsums);
+        downsweep<<<grid, THREADS, downsweep_smem(radix), st>>>(ka, va, kb, vb, n, shift, radix, ntiles, hist);
+        PRC_CHECK_LAUNCH();
+        uint32_t* t;
+        t = ka; ka = kb; kb = t;
+        t = va; va = vb; vb = t;
+    }
+    *kres = ka;
+    *vres = va;
+    return PRC_OK;
+}
+
+}  // namespace rsort
+
+// ---------------------------------------------------------------------------------------------
+// Particle helpers
+// ---------------------------------------------------------------------------------------------
+
+template <typename T> __device__ __forceinline__ bool finite3(T a, T b, T c) {
+    return isfinite(a) && isfinite(b) && isfinite(c);
+}
+
+// Box check of pyrecon/mesh.py:549-551 (inclusive on both faces), compared in the promoted type.
+template <typename P, typename F> __device__ __forceinline__ bool in_box(P p, const BoxGeom& g, int d) {
+    typedef typename promote<P, F>::type T;
+    F bs = (F)g.boxsize[d], bc = (F)g.boxcenter[d];
+    F half = rn_div(bs, (F)2);
+    F low = rn_sub(bc, half), high = rn_add(bc, half);
+    return (T)p >= (T)low && (T)p <= (T)high;
+}
+
+// Index-space coordinates (mesh dtype F) of particle i, after the optional wrap; flags
+// out-of-box / non-finite.  Returns false when the particle is invalid.
+template <typename P, typename F>
+__device__ __forceinline__ bool particle_index(const P* __restrict__ pos, int64_t i, const BoxGeom& g, int wrap,
+                                               F q[3], int* bad) {
+    typedef typename promote<P, F>::type T;
+    P p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    if (wrap) {
+        T w[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) w[d] = wrap_position<P, F>(p[d], g, d);
+        if (!finite3(w[0], w[1], w[2])) {
+            *bad |= PRC_FLAG_NONFINITE;
+            return false;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++) q[d] = index_coord<T, F>(w[d], g, d);
+    } else {
+        bool inside = in_box<P, F>(p[0], g, 0) && in_box<P, F>(p[1], g, 1) && in_box<P, F>(p[2], g, 2);
+        if (!inside) {
+            *bad |= PRC_FLAG_OUT_OF_BOX;   // NaN compares false: reported as out of box, as numpy does
+            return false;
+        }
+        if (!finite3(p[0], p[1], p[2])) {
+            *bad |= PRC_FLAG_NONFINITE;
+            return false;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++) q[d] = index_coord<P, F>(p[d], g, d);
+    }
+    return true;
+}
+
+// Base cell: C (int) truncation, then modulo n (src/mesh.c:35-37); kept in [0, n) for any input.
+template <typename F> __device__ __forceinline__ int base_cell(F q, int n) {
+    int b = (int)q;
+    b %= n;
+    return b < 0 ? b + n : b;
+}
+
+__device__ __forceinline__ void raise_flags(int32_t* flags, int bad) {
+    // one atomic per warp that saw a problem
+    unsigned m = __ballot_sync(0xffffffffu, bad != 0);
+    int all = bad;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) all |= __shfl_xor_sync(0xffffffffu, all, o);
+    if (m && (threadIdx.x & 31) == __ffs(m) - 1) atomicOr(flags, all);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Paint kernels
+// ---------------------------------------------------------------------------------------------
+
+template <typename P, typename F, typename W>
+__global__ void __launch_bounds__(256) paint_keys(const P* __restrict__ pos, const W* __restrict__ weights, int64_t n,
+                                                  BoxGeom g, int wrap, uint32_t* __restrict__ keys,
+                                                  uint32_t* __restrict__ ids, int32_t* __restrict__ flags) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t start = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // iterate a warp-uniform number of times so raise_flags' warp collectives see every lane
+    int64_t nround = (n + stride - 1) / stride;
+    for (int64_t r = 0; r < nround; r++) {
+        int64_t i = start + r * stride;
+        int bad = 0;
+        if (i < n) {
+            F q[3];
+            uint32_t key = 0;
+            if (particle_index<P, F>(pos, i, g, wrap, q, &bad)) {
+                if (weights != nullptr && !isfinite((double)weights[i])) bad |= PRC_FLAG_NONFINITE;
+                int ix = base_cell(q[0], g.n[0]), iy = base_cell(q[1], g.n[1]), iz = base_cell(q[2], g.n[2]);
+                key = ((uint32_t)ix * (uint32_t)g.n[1] + (uint32_t)iy) * (uint32_t)g.n[2] + (uint32_t)iz;
+            }
+            keys[i] = key;
+            ids[i] = (uint32_t)i;
+        }
+        raise_flags(flags, bad);
+    }
+}
+
+// (dx, dy, dz, w) of every particle in sorted order, in the mesh dtype F; the fractional
+// offsets are taken after the modulo as src/mesh.c:45-47 does.
+template <typename F> struct alignas(4 * sizeof(F)) Payload { F t[3]; F w; };
+
+template <typename P, typename F, typename W>
+__global__ void __launch_bounds__(256) paint_payload(const P* __restrict__ pos, const W* __restrict__ weights, int64_t n,
+                                                     BoxGeom g, int wrap, const uint32_t* __restrict__ order,
+                                                     Payload<F>* __restrict__ out, const int32_t* __restrict__ flags) {
+    if (*flags) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t id = order[i];
+        F q[3];
+        int bad = 0;
+        Payload<F> pl;
+        particle_index<P, F>(pos, id, g, wrap, q, &bad);
+#pragma unroll
+        for (int d = 0; d < 3; d++) pl.t[d] = rn_sub(q[d], (F)base_cell(q[d], g.n[d]));
+        pl.w = weights != nullptr ? (F)weights[id] : (F)1;
+        out[i] = pl;
+    }
+}
+
+// col_start[c] = first sorted index whose column (key / n2) is >= c, for c in [0, ncol].
+__global__ void column_starts(const uint32_t* __restrict__ keys, int64_t n, int n2, int64_t ncol,
+                              uint32_t* __restrict__ col_start, const int32_t* __restrict__ flags) {
+    if (*flags) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t col = i < n ? (int64_t)(keys[i] / (uint32_t)n2) : ncol;
+        int64_t prev = i > 0 ? (int64_t)(keys[i - 1] / (uint32_t)n2) : -1;
+        for (int64_t c = prev + 1; c <= col; c++) col_start[c] = (uint32_t)i;
+    }
+}
+
+constexpr int PULL_WARPS = 4;
+
+template <typename F>
+__global__ void __launch_bounds__(PULL_WARPS * 32) paint_pull(const uint32_t* __restrict__ keys,
+                                                              const Payload<F>* __restrict__ payload,
+                                                              const uint32_t* __restrict__ col_start, Dims dims,
+                                                              int accumulate, double* __restrict__ mesh,
+                                                              double* __restrict__ column_sums,
+                                                              const int32_t* __restrict__ flags) {
+    if (*flags) return;
+    extern __shared__ double s_col[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n0 = dims.n[0], n1 = dims.n[1], n2 = dims.n[2];
+    double* col = s_col + (size_t)warp * n2;
+    const int64_t ncol = (int64_t)n0 * n1;
+    for (int64_t c = (int64_t)blockIdx.x * PULL_WARPS + warp; c < ncol; c += (int64_t)gridDim.x * PULL_WARPS) {
+        const int X = (int)(c / n1), Y = (int)(c % n1);
+        for (int z = lane; z < n2; z += 32) col[z] = 0.;
+        __syncwarp();
+        // base columns contributing corner (cx, cy) to this column, in a fixed order
+#pragma unroll 1
+        for (int s = 0; s < 4; s++) {
+            const int cx = s >> 1, cy = s & 1;
+            const int Xs = cx ? wrap_dn(X, n0) : X, Ys = cy ? wrap_dn(Y, n1) : Y;
+            const int64_t src = (int64_t)Xs * n1 + Ys;
+            const int64_t beg = col_start[src], end = col_start[src + 1];
+            for (int64_t b0 = beg; b0 < end; b0 += 32) {
+                const int64_t i = b0 + lane;
+                const bool ok = i < end;
+                int iz = INT_MAX;
+                double a = 0., b = 0.;
+                if (ok) {
+                    iz = (int)(keys[i] % (uint32_t)n2);
+                    const Payload<F> pl = payload[i];
+                    const F wx = cx ? pl.t[0] : rn_sub((F)1, pl.t[0]);
+                    const F wy = cy ? pl.t[1] : rn_sub((F)1, pl.t[1]);
+                    const F wxy = rn_mul(wx, wy);
+                    // ((wx * wy) * wz) * weight, the reference's evaluation order (mesh.c:55-62)
+                    a = (double)rn_mul(rn_mul(wxy, rn_sub((F)1, pl.t[2])), pl.w);
+                    b = (double)rn_mul(rn_mul(wxy, pl.t[2]), pl.w);
+                }
+                // segmented inclusive scan over runs of equal iz (keys are sorted within a column)
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const double ua = __shfl_up_sync(0xffffffffu, a, o);
+                    const double ub = __shfl_up_sync(0xffffffffu, b, o);
+                    const int uz = __shfl_up_sync(0xffffffffu, iz, o);
+                    if (lane >= o && uz == iz) {
+                        a += ua;
+                        b += ub;
+                    }
+                }
+                const int nz = __shfl_down_sync(0xffffffffu, iz, 1);
+                const bool tail = ok && (lane == 31 || nz != iz);
+                if (tail) col[iz] += a;
+                __syncwarp();
+                if (tail) col[iz + 1 == n2 ? 0 : iz + 1] += b;
+                __syncwarp();
+            }
+        }
+        double* dst = mesh + c * (int64_t)n2;
+        double part = 0.;
+        for (int z = lane; z < n2; z += 32) {
+            double v = col[z];
+            if (accumulate) v += dst[z];
+            dst[z] = v;
+            part += v;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (column_sums != nullptr && lane == 0) column_sums[c] = part;
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Deterministic sum
+// ---------------------------------------------------------------------------------------------
+constexpr int SUM_THREADS = 256;
+constexpr int SUM_BLOCKS = 512;
+
+__global__ void __launch_bounds__(SUM_THREADS) sum_partials(const double* __restrict__ x, int64_t n,
+                                                            double* __restrict__ partial) {
+    __shared__ double s[SUM_THREADS];
+    double acc = 0.;
+    for (int64_t i = (int64_t)blockIdx.x * SUM_THREADS + threadIdx.x; i < n; i += (int64_t)SUM_BLOCKS * SUM_THREADS)
+        acc += x[i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = SUM_THREADS / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
+}
+
+__global__ void __launch_bounds__(SUM_THREADS) sum_final(const double* __restrict__ partial, double* __restrict__ out) {
+    __shared__ double s[SUM_THREADS];
+    double acc = 0.;
+    for (int i = threadIdx.x; i < SUM_BLOCKS; i += SUM_THREADS) acc += partial[i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = SUM_THREADS / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gathers
+// ---------------------------------------------------------------------------------------------
+
+// Fractional offset before the modulo (src/mesh.c:278-283) and base cells.
+template <typename F> struct Cic {
+    int lo[3], hi[3];
+    F w[3][2];
+};
+
+template <typename F> __device__ __forceinline__ Cic<F> cic_setup(const F q[3], const int n[3]) {
+    Cic<F> c;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        F t = rn_sub(q[d], (F)(int)q[d]);
+        c.lo[d] = base_cell(q[d], n[d]);
+        c.hi[d] = wrap_up(c.lo[d], n[d]);
+        c.w[d][0] = rn_sub((F)1, t);
+        c.w[d][1] = t;
+    }
+    return c;
+}
+
+__device__ __forceinline__ int64_t at3(const int n[3], int x, int y, int z) {
+    return ((int64_t)x * n[1] + y) * n[2] + z;
+}
+
+// CIC read of one mesh: corners in (x, y, z) order with z fastest, each term
+// ((m * w_x) * w_y) * w_z accumulated in order (src/mesh.c:294-301).
+template <typename F> __device__ __forceinline__ F cic_read(const F* __restrict__ m, const Cic<F>& c, const int n[3]) {
+    F acc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+        const F v = __ldg(m + at3(n, cx ? c.hi[0] : c.lo[0], cy ? c.hi[1] : c.lo[1], cz ? c.hi[2] : c.lo[2]));
+        const F term = rn_mul(rn_mul(rn_mul(v, c.w[0][cx]), c.w[1][cy]), c.w[2][cz]);
+        acc = k == 0 ? term : rn_add(acc, term);
+    }
+    return acc;
+}
+
+// Finite-difference gradient CIC read (src/mesh.c:187-266): corners in the order
+// 000, 100, 010, 001, 110, 101, 011, 111; divided by 2 * boxsize / n in F.
+template <typename F>
+__device__ __forceinline__ void fd_read(const F* __restrict__ m, const Cic<F>& c, const int n[3], const F twocell[3],
+                                        F out[3]) {
+    const int order[8] = {0, 4, 2, 1, 6, 5, 3, 7};   // (cx<<2 | cy<<1 | cz)
+    F g[3] = {0, 0, 0};
+#pragma unroll
+    for (int kk = 0; kk < 8; kk++) {
+        const int k = order[kk];
+        const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+        const int x = cx ? c.hi[0] : c.lo[0], y = cy ? c.hi[1] : c.lo[1], z = cz ? c.hi[2] : c.lo[2];
+        const F wt = rn_mul(rn_mul(c.w[0][cx], c.w[1][cy]), c.w[2][cz]);
+        const F gx = rn_mul(rn_sub(__ldg(m + at3(n, wrap_up(x, n[0]), y, z)), __ldg(m + at3(n, wrap_dn(x, n[0]), y, z))), wt);
+        const F gy = rn_mul(rn_sub(__ldg(m + at3(n, x, wrap_up(y, n[1]), z)), __ldg(m + at3(n, x, wrap_dn(y, n[1]), z))), wt);
+        const F gz = rn_mul(rn_sub(__ldg(m + at3(n, x, y, wrap_up(z, n[2]))), __ldg(m + at3(n, x, y, wrap_dn(z, n[2])))), wt);
+        if (kk == 0) {
+            g[0] = gx; g[1] = gy; g[2] = gz;
+        } else {
+            g[0] = rn_add(g[0], gx); g[1] = rn_add(g[1], gy); g[2] = rn_add(g[2], gz);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) out[a] = rn_div(g[a], twocell[a]);
+}
+
+template <typename P, typename F>
+__global__ void __launch_bounds__(256) read_cic_kernel(const F* __restrict__ mesh, BoxGeom g, const P* __restrict__ pos,
+                                                       int64_t n, int wrap, P* __restrict__ out, int32_t* flags) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t nround = (n + stride - 1) / stride;
+    for (int64_t r = 0; r < nround; r++) {
+        int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + r * stride;
+        int bad = 0;
+        if (i < n) {
+            F q[3] = {0, 0, 0};
+            P v = (P)NAN;
+            if (particle_index<P, F>(pos, i, g, wrap, q, &bad)) v = (P)cic_read(mesh, cic_setup(q, g.n), g.n);
+            out[i] = v;
+        }
+        raise_flags(flags, bad & PRC_FLAG_OUT_OF_BOX);   // non-finite only warns in the reference
+    }
+}
+
+template <typename F> __host__ __forceinline__ void twocell_of(const BoxGeom& g, F out[3]) {
+    for (int d = 0; d < 3; d++) out[d] = (F)(2.0 * (double)(F)g.boxsize[d] / (double)g.n[d]);
+}
+
+template <typename P, typename F>
+__global__ void __launch_bounds__(256) read_fd_kernel(const F* __restrict__ mesh, BoxGeom g, F tc0, F tc1, F tc2,
+                                                      const P* __restrict__ pos, int64_t n, int wrap,
+                                                      P* __restrict__ out, int32_t* flags) {
+    const F twocell[3] = {tc0, tc1, tc2};
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t nround = (n + stride - 1) / stride;
+    for (int64_t r = 0; r < nround; r++) {
+        int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + r * stride;
+        int bad = 0;
+        if (i < n) {
+            F q[3] = {0, 0, 0}, s[3] = {(F)NAN, (F)NAN, (F)NAN};
+            if (particle_index<P, F>(pos, i, g, wrap, q, &bad)) fd_read(mesh, cic_setup(q, g.n), g.n, twocell, s);
+#pragma unroll
+            for (int a = 0; a < 3; a++) out[3 * i + a] = (P)s[a];
+        }
+        raise_flags(flags, bad & PRC_FLAG_OUT_OF_BOX);
+    }
+}
+
+// Fused shifts.  Type flow of the reference (pyrecon/recon.py:255-325, multigrid.py:137-158):
+// displacement read in F then cast to P (the shifts array has the positions' dtype); RSD in
+// R = promoted type of (shifts, los); result cast back to P; positions - shifts in P, then
+// wrapped in T = promote(P, F) when `wrap`; the output type O is chosen by the caller.
+template <typename P, typename F, typename O, bool PHI>
+__global__ void __launch_bounds__(256) read_shifts_kernel(const F* __restrict__ m0, const F* __restrict__ m1,
+                                                          const F* __restrict__ m2, BoxGeom g, F tc0, F tc1, F tc2,
+                                                          const P* __restrict__ pos, int64_t n, double f,
+                                                          int global_los, double l0, double l1, double l2, int field,
+                                                          int shifted, int wrap, O* __restrict__ out, int32_t* flags) {
+    typedef typename promote<P, F>::type T;
+    const F twocell[3] = {tc0, tc1, tc2};
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t nround = (n + stride - 1) / stride;
+    for (int64_t r = 0; r < nround; r++) {
+        int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + r * stride;
+        int bad = 0;
+        if (i < n) {
+            F q[3] = {0, 0, 0};
+            P s[3];
+            const P p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+            const bool ok = particle_index<P, F>(pos, i, g, wrap, q, &bad);
+            const Cic<F> c = cic_setup(q, g.n);
+            if (PHI) {
+                F d[3] = {(F)NAN, (F)NAN, (F)NAN};
+                if (ok) fd_read(m0, c, g.n, twocell, d);
+#pragma unroll
+                for (int a = 0; a < 3; a++) s[a] = (P)d[a];
+            } else {
+                s[0] = ok ? (P)cic_read(m0, c, g.n) : (P)NAN;
+                s[1] = ok ? (P)cic_read(m1, c, g.n) : (P)NAN;
+                s[2] = ok ? (P)cic_read(m2, c, g.n) : (P)NAN;
+            }
+            if (field != PRC_FIELD_DISP) {
+                // line of sight: global (mesh dtype) or p / |p| of the positions the reference uses
+                // (wrapped ones for psi, unwrapped ones for phi); all in double here, then the sum
+                // s.l is accumulated in order ((s0 l0 + s1 l1) + s2 l2) as numpy's reduction does.
+                double l[3];
+                if (global_los) {
+                    l[0] = (double)(F)l0; l[1] = (double)(F)l1; l[2] = (double)(F)l2;
+                } else {
+                    double x[3];
+#pragma unroll
+                    for (int a = 0; a < 3; a++) x[a] = (!PHI && wrap) ? (double)wrap_position<P, F>(p[a], g, a) : (double)p[a];
+                    double dist = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+#pragma unroll
+                    for (int a = 0; a < 3; a++) l[a] = x[a] / dist;
+                }
+                double proj = (double)s[0] * l[0];
+                proj = rn_add(proj, rn_mul((double)s[1], l[1]));
+                proj = rn_add(proj, rn_mul((double)s[2], l[2]));
+                proj *= f;
+                P rsd[3];
+#pragma unroll
+                for (int a = 0; a < 3; a++) rsd[a] = (P)(proj * l[a]);
+                if (field == PRC_FIELD_RSD) {
+#pragma unroll
+                    for (int a = 0; a < 3; a++) s[a] = rsd[a];
+                } else {
+#pragma unroll
+                    for (int a = 0; a < 3; a++) s[a] = (P)rn_add(s[a], rsd[a]);
+                }
+            }
+            if (shifted) {
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    P v = rn_sub(p[a], s[a]);
+                    out[3 * i + a] = wrap ? (O)wrap_position<P, F>(v, g, a) : (O)v;
+                }
+            } else {
+#pragma unroll
+                for (int a = 0; a < 3; a++) out[3 * i + a] = (O)s[a];
+            }
+        }
+        raise_flags(flags, bad & PRC_FLAG_OUT_OF_BOX);
+    }
+}
+
+int device_sm_count() {
+    static int cached = -1;
+    if (cached < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cached = sms > 0 ? sms : 148;
+    }
+    return cached;
+}
+
+inline BoxGeom make_geom(const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3]) {
+    BoxGeom g;
+    for (int d = 0; d < 3; d++) {
+        g.n[d] = nmesh[d];
+        g.boxsize[d] = boxsize[d];
+        g.boxcenter[d] = boxcenter[d];
+    }
+    return g;
+}
+
+inline bool valid_nmesh(const int32_t* nmesh) {
+    if (!nmesh) return false;
+    for (int d = 0; d < 3; d++)
+        if (nmesh[d] < 1 || nmesh[d] > 65536) return false;
+    return (int64_t)nmesh[0] * nmesh[1] * nmesh[2] < ((int64_t)1 << 32);
+}
+
+inline int key_bits(const int32_t* nmesh) {
+    uint64_t N = (uint64_t)nmesh[0] * nmesh[1] * nmesh[2];
+    int b = 0;
+    while (((uint64_t)1 << b) < N) b++;
+    return b;
+}
+
+inline int particle_grid(int64_t n) {
+    int64_t blocks = (n + 255) / 256;
+    int64_t cap = (int64_t)device_sm_count() * 16;
+    return (int)std::max<int64_t>(1, std::min(blocks, cap));
+}
+
+// Workspace layout of the paint.
+struct PaintWs {
+    uint32_t *k0, *v0, *k1, *v1, *col_start, *scratch;
+    void* payload;
+};
+
+inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+inline size_t paint_layout(const int32_t nmesh[3], int64_t npos, int mesh_bytes, char* base, PaintWs* ws) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char* p = base ? base + off : nullptr;
+        off += align_up(bytes);
+        return p;
+    };
+    int64_t ncol = (int64_t)nmesh[0] * nmesh[1];
+    size_t kb = (size_t)std::max<int64_t>(npos, 1) * sizeof(uint32_t);
+    PaintWs w;
+    w.k0 = (uint32_t*)take(kb);
+    w.v0 = (uint32_t*)take(kb);
+    w.k1 = (uint32_t*)take(kb);
+    w.v1 = (uint32_t*)take(kb);
+    w.col_start = (uint32_t*)take((size_t)(ncol + 1) * sizeof(uint32_t));
+    w.scratch = (uint32_t*)take(rsort::scratch_bytes(std::max<int64_t>(npos, 1)));
+    w.payload = take((size_t)std::max<int64_t>(npos, 1) * 4 * (mesh_bytes == 4 ? 4 : 8));
+    if (ws) *ws = w;
+    return off;
+}
+
+template <typename P, typename F, typename W>
+int paint_sort(const P* pos, const W* w, int64_t n, const BoxGeom& g, int wrap, const PaintWs& ws, int32_t* flags,
+               uint32_t** keys, uint32_t** order, cudaStream_t st) {
+    paint_keys<P, F, W><<<particle_grid(n), 256, 0, st>>>(pos, w, n, g, wrap, ws.k0, ws.v0, flags);
+    PRC_CHECK_LAUNCH();
+    int32_t nm[3] = {g.n[0], g.n[1], g.n[2]};
+    return rsort::sort_pairs(ws.k0, ws.v0, ws.k1, ws.v1, n, key_bits(nm), ws.scratch, keys, order, st);
+}
+
+template <typename P, typename F, typename W>
+int paint_run(double* mesh, double* colsums, const BoxGeom& g, const P* pos, const W* w, int64_t n, int wrap,
+              int accumulate, int32_t* flags, const PaintWs& ws, cudaStream_t st) {
+    uint32_t *keys = nullptr, *order = nullptr;
+    if (n > 0) PRC_TRY((paint_sort<P, F, W>(pos, w, n, g, wrap, ws, flags, &keys, &order, st)));
+    Payload<F>* pl = (Payload<F>*)ws.payload;
+    if (n > 0) {
+        paint_payload<P, F, W><<<particle_grid(n), 256, 0, st>>>(pos, w, n, g, wrap, order, pl, flags);
+        PRC_CHECK_LAUNCH();
+    } else {
+        keys = ws.k0;
+    }
+    int64_t ncol = (int64_t)g.n[0] * g.n[1];
+    column_starts<<<particle_grid(n + 1), 256, 0, st>>>(keys, n, g.n[2], ncol, ws.col_start, flags);
+    PRC_CHECK_LAUNCH();
+    size_t smem = (size_t)PULL_WARPS * g.n[2] * sizeof(double);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(paint_pull<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int64_t blocks = (ncol + PULL_WARPS - 1) / PULL_WARPS;
+    int grid = (int)std::min<int64_t>(blocks, (int64_t)device_sm_count() * 16);
+    Dims dims = {{g.n[0], g.n[1], g.n[2]}};
+    paint_pull<F><<<grid, PULL_WARPS * 32, smem, st>>>(keys, pl, ws.col_start, dims, accumulate, mesh, colsums, flags);
+    PRC_CHECK_LAUNCH();
+    return PRC_OK;
+}
+
+template <typename P, typename F>
+int paint_dispatch_w(double* mesh, double* colsums, const BoxGeom& g, const void* pos, const void* w, int wb, int64_t n,
+                     int wrap, int acc, int32_t* flags, const PaintWs& ws, cudaStream_t st) {
+    if (w == nullptr) return paint_run<P, F, F>(mesh, colsums, g, (const P*)pos, (const F*)nullptr, n, wrap, acc, flags, ws, st);
+    if (wb == 4) return paint_run<P, F, float>(mesh, colsums, g, (const P*)pos, (const float*)w, n, wrap, acc, flags, ws, st);
+    return paint_run<P, F, double>(mesh, colsums, g, (const P*)pos, (const double*)w, n, wrap, acc, flags, ws, st);
+}
+
+template <typename P, typename F>
+int read_shifts_launch(const F* m0, const F* m1, const F* m2, bool phi, const BoxGeom& g, const void* pos, int64_t n,
+                       double f, const double* los, int field, int shifted, int wrap, void* out, int ob, int32_t* flags,
+                       cudaStream_t st) {
+    F tc[3];
+    twocell_of(g, tc);
+    double l[3] = {0, 0, 0};
+    if (los)
+        for (int a = 0; a < 3; a++) l[a] = los[a];
+    int grid = particle_grid(n);
+#define LAUNCH(O, PH)                                                                                            \
+    read_shifts_kernel<P, F, O, PH><<<grid, 256, 0, st>>>(m0, m1, m2, g, tc[0], tc[1], tc[2], (const P*)pos, n, f, \
+                                                          los != nullptr, l[0], l[1], l[2], field, shifted, wrap,  \
+                                                          (O*)out, flags)
+    if (phi) {
+        if (ob == 4) LAUNCH(float, true); else LAUNCH(double, true);
+    } else {
+        if (ob == 4) LAUNCH(float, false); else LAUNCH(double, false);
+    }
+#undef LAUNCH
+    PRC_CHECK_LAUNCH();
+    return PRC_OK;
+}
+
+}  // namespace prc
+
+using namespace prc;
+
+extern "C" {
+
+size_t prc_assign_cic_workspace_bytes(const int32_t nmesh[3], int64_t npos, int mesh_bytes) {
+    if (!valid_nmesh(nmesh) || npos < 0) return 0;
+    return paint_layout(nmesh, npos, mesh_bytes, nullptr, nullptr);
+}
+
+prc_status_t prc_assign_cic(double* mesh, double* column_sums, const int32_t nmesh[3], const double boxsize[3],
+                            const double boxcenter[3], int mesh_bytes, const void* positions, int pos_bytes,
+                            const void* weights, int weight_bytes, int64_t npos, int wrap, int accumulate,
+                            int32_t* flags, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!mesh || !valid_nmesh(nmesh) || !boxsize || !boxcenter || !flags || npos < 0) return PRC_ERR_ARG;
+    if (npos >= ((int64_t)1 << 32) || (npos > 0 && !positions)) return PRC_ERR_ARG;
+    if ((mesh_bytes != 4 && mesh_bytes != 8) || (pos_bytes != 4 && pos_bytes != 8)) return PRC_ERR_ARG;
+    if (weights && weight_bytes != 4 && weight_bytes != 8) return PRC_ERR_ARG;
+    if (nmesh[2] > 4096) return PRC_ERR_UNSUPPORTED;   // one FP64 column per warp in shared memory
+    if (workspace_bytes < prc_assign_cic_workspace_bytes(nmesh, npos, mesh_bytes) || !workspace) return PRC_ERR_WORKSPACE;
+    cudaStream_t st = (cudaStream_t)stream;
+    PaintWs ws;
+    paint_layout(nmesh, npos, mesh_bytes, (char*)workspace, &ws);
+    BoxGeom g = make_geom(nmesh, boxsize, boxcenter);
+    if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return PRC_ERR_CUDA;
+    if (pos_bytes == 4 && mesh_bytes == 4)
+        return paint_dispatch_w<float, float>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st);
+    if (pos_bytes == 4 && mesh_bytes == 8)
+        return paint_dispatch_w<float, double>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st);
+    if (pos_bytes == 8 && mesh_bytes == 4)
+        return paint_dispatch_w<double, float>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st);
+    return paint_dispatch_w<double, double>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st);
+}
+
+prc_status_t prc_cic_cell_order(uint32_t* keys_sorted, uint32_t* order, const int32_t nmesh[3], const double boxsize[3],
+                                const double boxcenter[3], int mesh_bytes, const void* positions, int pos_bytes,
+                                int64_t npos, int wrap, int32_t* flags, void* workspace, size_t workspace_bytes,
+                                void* stream) {
+    if (!keys_sorted || !order || !valid_nmesh(nmesh) || !boxsize || !boxcenter || !flags || npos < 0) return PRC_ERR_ARG;
+    if (npos >= ((int64_t)1 << 32) || (npos > 0 && !positions)) return PRC_ERR_ARG;
+    if ((mesh_bytes != 4 && mesh_bytes != 8) || (pos_bytes != 4 && pos_bytes != 8)) return PRC_ERR_ARG;
+    if (workspace_bytes < prc_assign_cic_workspace_bytes(nmesh, npos, mesh_bytes) || !workspace) return PRC_ERR_WORKSPACE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return PRC_ERR_CUDA;
+    if (npos == 0) return PRC_OK;
+    PaintWs ws;
+    paint_layout(nmesh, npos, mesh_bytes, (char*)workspace, &ws);
+    BoxGeom g = make_geom(nmesh, boxsize, boxcenter);
+    uint32_t *k = nullptr, *v = nullptr;
+    int s;
+    if (pos_bytes == 4 && mesh_bytes == 4) s = paint_sort<float, float, float>((const float*)positions, nullptr, npos, g, wrap, ws, flags, &k, &v, st);
+    else if (pos_bytes == 4) s = paint_sort<float, double, double>((const float*)positions, nullptr, npos, g, wrap, ws, flags, &k, &v, st);
+    else if (mesh_bytes == 4) s = paint_sort<double, float, float>((const double*)positions, nullptr, npos, g, wrap, ws, flags, &k, &v, st);
+    else s = paint_sort<double, double, double>((const double*)positions, nullptr, npos, g, wrap, ws, flags, &k, &v, st);
+    if (s != PRC_OK) return s;
+    if (cudaMemcpyAsync(keys_sorted, k, (size_t)npos * 4, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return PRC_ERR_CUDA;
+    if (cudaMemcpyAsync(order, v, (size_t)npos * 4, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return PRC_ERR_CUDA;
+    return PRC_OK;
+}
+
+size_t prc_sum_workspace_bytes(int64_t n) {
+    (void)n;
+    return SUM_BLOCKS * sizeof(double);
+}
+
+prc_status_t prc_sum_f64(const double* x, int64_t n, double* out, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!out || n < 0 || (n > 0 && !x)) return PRC_ERR_ARG;
+    if (!workspace || workspace_bytes < prc_sum_workspace_bytes(n)) return PRC_ERR_WORKSPACE;
+    cudaStream_t st = (cudaStream_t)stream;
+    sum_partials<<<SUM_BLOCKS, SUM_THREADS, 0, st>>>(x, n, (double*)workspace);
+    sum_final<<<1, SUM_THREADS, 0, st>>>((const double*)workspace, out);
+    PRC_CHECK_LAUNCH();
+    return PRC_OK;
+}
+
+#define READ_CIC_IMPL(NAME, F)                                                                                     \
+    prc_status_t NAME(const F* mesh, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],   \
+                      const void* positions, int pos_bytes, int64_t npos, int wrap, void* out, int32_t* flags,      \
+                      void* stream) {                                                                              \
+        if (!mesh || !valid_nmesh(nmesh) || !boxsize || !boxcenter || !flags || npos < 0) return PRC_ERR_ARG;    \
+        if (npos > 0 && (!positions || !out)) return PRC_ERR_ARG;                                                  \
+        if (pos_bytes != 4 && pos_bytes != 8) return PRC_ERR_ARG;                                                  \
+        cudaStream_t st = (cudaStream_t)stream;                                                                    \
+        if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return PRC_ERR_CUDA;                   \
+        if (npos == 0) return PRC_OK;                                                                              \
+        BoxGeom g = make_geom(nmesh, boxsize, boxcenter);                                                          \
+        if (pos_bytes == 4)                                                                                        \
+            read_cic_kernel<float, F><<<particle_grid(npos), 256, 0, st>>>(mesh, g, (const float*)positions, npos, \
+                                                                           wrap, (float*)out, flags);             \
+        else                                                                                                       \
+            read_cic_kernel<double, F><<<particle_grid(npos), 256, 0, st>>>(mesh, g, (const double*)positions,     \
+                                                                            npos, wrap, (double*)out, flags);     \
+        PRC_CHECK_LAUNCH();                                                                                        \
+        return PRC_OK;                                                                                             \
+    }
+
+READ_CIC_IMPL(prc_read_cic_f32, float)
+READ_CIC_IMPL(prc_read_cic_f64, double)
+
+#define READ_FD_IMPL(NAME, F)                                                                                      \
+    prc_status_t NAME(const F* mesh, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],   \
+                      const void* positions, int pos_bytes, int64_t npos, int wrap, void* out, int32_t* flags,      \
+                      void* stream) {                                                                              \
+        if (!mesh || !valid_nmesh(nmesh) || !boxsize || !boxcenter || !flags || npos < 0) return PRC_ERR_ARG;    \
+        if (npos > 0 && (!positions || !out)) return PRC_ERR_ARG;                                                  \
+        if (pos_bytes != 4 && pos_bytes != 8) return PRC_ERR_ARG;                                                  \
+        cudaStream_t st = (cudaStream_t)stream;                                                                    \
+        if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return PRC_ERR_CUDA;                   \
+        if (npos == 0) return PRC_OK;                                                                              \
+        BoxGeom g = make_geom(nmesh, boxsize, boxcenter);                                                          \
+        F tc[3];                                                                                                   \
+        twocell_of(g, tc);                                                                                         \
+        if (pos_bytes == 4)                                                                                        \
+            read_fd_kernel<float, F><<<particle_grid(npos), 256, 0, st>>>(mesh, g, tc[0], tc[1], tc[2],            \
+                                                                          (const float*)positions, npos, wrap,    \
+                                                                          (float*)out, flags);                    \
+        else                                                                                                       \
+            read_fd_kernel<double, F><<<particle_grid(npos), 256, 0, st>>>(mesh, g, tc[0], tc[1], tc[2],           \
+                                                                           (const double*)positions, npos, wrap,  \
+                                                                           (double*)out, flags);                  \
+        PRC_CHECK_LAUNCH();                                                                                        \
+        return PRC_OK;                                                                                             \
+    }
+
+READ_FD_IMPL(prc_read_finite_difference_cic_f32, float)
+READ_FD_IMPL(prc_read_finite_difference_cic_f64, double)
+
+#define READ_SHIFTS_IMPL(NAME, F, PHI, ARGS, M0, M1, M2)                                                           \
+    prc_status_t NAME ARGS {                                                                                       \
+        if (!M0 || !M1 || !M2 || !valid_nmesh(nmesh) || !boxsize || !boxcenter || !flags || npos < 0)             \
+            return PRC_ERR_ARG;                                                                                    \
+        if (npos > 0 && (!positions || !out)) return PRC_ERR_ARG;                                                  \
+        if ((pos_bytes != 4 && pos_bytes != 8) || (out_bytes != 4 && out_bytes != 8)) return PRC_ERR_ARG;        \
+        if (field < PRC_FIELD_DISP || field > PRC_FIELD_DISP_RSD) return PRC_ERR_ARG;                             \
+        cudaStream_t st = (cudaStream_t)stream;                                                                    \
+        if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return PRC_ERR_CUDA;                   \
+        if (npos == 0) return PRC_OK;                                                                              \
+        BoxGeom g = make_geom(nmesh, boxsize, boxcenter);                                                          \
+        if (pos_bytes == 4)                                                                                        \
+            return read_shifts_launch<float, F>(M0, M1, M2, PHI, g, positions, npos, f, los, field, shifted, wrap, \
+                                                out, out_bytes, flags, st);                                       \
+        return read_shifts_launch<double, F>(M0, M1, M2, PHI, g, positions, npos, f, los, field, shifted, wrap,   \
+                                             out, out_bytes, flags, st);                                          \
+    }
+
+READ_SHIFTS_IMPL(prc_read_shifts_psi_f32, float, false,
+                 (const float* psi_x, const float* psi_y, const float* psi_z, const int32_t nmesh[3],
+                  const double boxsize[3], const double boxcenter[3], const void* positions, int pos_bytes,
+                  int64_t npos, double f, const double* los, int field, int shifted, int wrap, void* out,
+                  int out_bytes, int32_t* flags, void* stream),
+                 psi_x, psi_y, psi_z)
+READ_SHIFTS_IMPL(prc_read_shifts_psi_f64, double, false,
+                 (const double* psi_x, const double* psi_y, const double* psi_z, const int32_t nmesh[3],
+                  const double boxsize[3], const double boxcenter[3], const void* positions, int pos_bytes,
+                  int64_t npos, double f, const double* los, int field, int shifted, int wrap, void* out,
+                  int out_bytes, int32_t* flags, void* stream),
+                 psi_x, psi_y, psi_z)
+READ_SHIFTS_IMPL(prc_read_shifts_phi_f32, float, true,
+                 (const float* phi, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
+                  const void* positions, int pos_bytes, int64_t npos, double f, const double* los, int field,
+                  int shifted, int wrap, void* out, int out_bytes, int32_t* flags, void* stream),
+                 phi, phi, phi)
+READ_SHIFTS_IMPL(prc_read_shifts_phi_f64, double, true,
+                 (const double* phi, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
+                  const void* positions, int pos_bytes, int64_t npos, double f, const double* los, int field,
+                  int shifted, int wrap, void* out, int out_bytes, int32_t* flags, void* stream),
+                 phi, phi, phi)
+
+}  // extern "C"

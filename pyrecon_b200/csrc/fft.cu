@@ -1,0 +1,1027 @@
+// Batched 3D real FFTs with fused k-space multipliers and real-space epilogues.
+//
+// A forward 3D r2c transform of an (n0, n1, n2) real mesh is three passes over the
+// (n0, n1, nh = n2/2 + 1) half spectrum:
+//   z: each row of n2 reals is read as n2/2 complex pairs, transformed (n2/2-point FFT) and
+//      unpacked to nh complex (the standard real-FFT packing);
+//   y, x: strided lines, a tile of B adjacent z-columns loaded per CTA so global accesses are
+//      coalesced, transformed in shared memory.
+// The k-space step of every algorithm sits between the forward and the inverse x transform,
+// so one kernel does forward x, multiply (one or several outputs), inverse x.  The inverse z
+// pass (c2r) ends with the real-space epilogue of the step (store, density contrast, or the
+// Burden et al. RSD-removal update), so no intermediate real mesh is written.
+//
+// FFT core: Stockham autosort with mixed radices 8/4/2/3/5/7 (Govindaraju et al., SC08:
+// pass with radix R and sub-transform size Ns reads x[j + r n/R], twiddles by w_{Ns R}^{r (j mod Ns)},
+// does an R-point DFT and writes y[(j - j mod Ns) R + (j mod Ns) + r Ns]), ping-ponging between two
+// shared-memory buffers laid out (k, line) with the line index fastest.
+//
+// Multipliers are applied Hermitian-symmetrised, M_h(k) = (M(k) + conj M(k~)) / 2 with
+// k~ the wavevector of the reflected index (-k except on a Nyquist plane, where k~ = k), which
+// is exactly what the reference's full complex transform followed by .real computes
+// (pyrecon/mesh.py:842, recon.py:117).
+#include "common.cuh"
+
+#include <algorithm>
+#include <math.h>
+#include <string.h>
+
+namespace prc {
+
+constexpr int FFT_THREADS = 256;
+constexpr int MAX_RADICES = 16;
+constexpr int MAX_FFT_N = 1024;
+constexpr int MAX_BATCH = 6;
+
+struct Radices {
+    int n;
+    int count;
+    int r[MAX_RADICES];
+};
+
+static bool factorize(int n, Radices* out) {
+    Radices rd;
+    rd.n = n;
+    rd.count = 0;
+    int m = n;
+    while (m % 8 == 0 && m > 0) { rd.r[rd.count++] = 8; m /= 8; }
+    if (m % 4 == 0) { rd.r[rd.count++] = 4; m /= 4; }
+    if (m % 2 == 0) { rd.r[rd.count++] = 2; m /= 2; }
+    const int odd[3] = {3, 5, 7};
+    for (int i = 0; i < 3; i++)
+        while (m % odd[i] == 0) {
+            if (rd.count >= MAX_RADICES) return false;
+            rd.r[rd.count++] = odd[i];
+            m /= odd[i];
+        }
+    if (m != 1) return false;
+    *out = rd;
+    return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Small DFTs (DIR = -1 forward, +1 inverse)
+// ---------------------------------------------------------------------------------------------
+template <typename C, int DIR> __device__ __forceinline__ void dft2(C* v) {
+    C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+}
+
+template <typename C, int DIR> __device__ __forceinline__ void dft4(C* v) {
+    C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    C t2 = cadd(v[1], v[3]), t3 = cmul_i(csub(v[1], v[3]), DIR);
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+}
+
+template <typename C, int DIR> __device__ __forceinline__ void dft8(C* v) {
+    typedef decltype(C().x) T;
+    const T h = (T)0.70710678118654752440;   // 1/sqrt(2)
+    C e[4] = {v[0], v[2], v[4], v[6]};
+    C o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<C, DIR>(e);
+    dft4<C, DIR>(o);
+    // o_k *= w8^k, w8 = exp(DIR i pi / 4)
+    C o1 = o[1];
+    o[1] = cmake<C>(h * (o1.x - DIR * o1.y), h * (o1.y + DIR * o1.x));
+    o[2] = cmul_i(o[2], DIR);
+    C o3 = o[3];
+    o[3] = cmake<C>(h * (-o3.x - DIR * o3.y), h * (-o3.y + DIR * o3.x));
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        v[k] = cadd(e[k], o[k]);
+        v[k + 4] = csub(e[k], o[k]);
+    }
+}
+
+template <typename C, int DIR> __device__ __forceinline__ void dft3(C* v) {
+    typedef decltype(C().x) T;
+    const T s = (T)0.86602540378443864676;   // sin(2 pi / 3)
+    C a = v[0], b = v[1], c = v[2];
+    C sum = cadd(b, c), dif = csub(b, c);
+    C t = cmake<C>(a.x - (T)0.5 * sum.x, a.y - (T)0.5 * sum.y);
+    C u = cmul_i(cscale(dif, s), DIR);   // DIR i s (b - c)
+    v[0] = cadd(a, sum);
+    v[1] = cadd(t, u);
+    v[2] = csub(t, u);
+}
+
+template <typename C, int DIR> __device__ __forceinline__ void dft5(C* v) {
+    typedef decltype(C().x) T;
+    const T c1 = (T)0.30901699437494742410;   // cos(2 pi / 5)
+    const T c2 = (T)-0.80901699437494742410;  // cos(4 pi / 5)
+    const T s1 = (T)0.95105651629515357212;   // sin(2 pi / 5)
+    const T s2 = (T)0.58778525229247312917;   // sin(4 pi / 5)
+    C a = v[0];
+    C b1 = cadd(v[1], v[4]), d1 = csub(v[1], v[4]);
+    C b2 = cadd(v[2], v[3]), d2 = csub(v[2], v[3]);
+    C t1 = cmake<C>(a.x + c1 * b1.x + c2 * b2.x, a.y + c1 * b1.y + c2 * b2.y);
+    C t2 = cmake<C>(a.x + c2 * b1.x + c1 * b2.x, a.y + c2 * b1.y + c1 * b2.y);
+    C u1 = cmul_i(cmake<C>(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y), DIR);
+    C u2 = cmul_i(cmake<C>(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y), DIR);
+    v[0] = cadd(a, cadd(b1, b2));
+    v[1] = cadd(t1, u1);
+    v[4] = csub(t1, u1);
+    v[2] = cadd(t2, u2);
+    v[3] = csub(t2, u2);
+}
+
+// Generic R-point DFT from the twiddle table (w_n^m, n a multiple of R): used for R = 7.
+template <typename C, int DIR, int R>
+__device__ __forceinline__ void dft_generic(C* v, const C* __restrict__ tw, int n, int tws) {
+    C out[R];
+    const int step = n / R;
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+        C acc = v[0];
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+            C w = tw[(((r * m) % R) * step) * tws];
+            if (DIR > 0) w = cconj(w);
+            acc = cadd(acc, cmul(v[r], w));
+        }
+        out[m] = acc;
+    }
+#pragma unroll
+    for (int m = 0; m < R; m++) v[m] = out[m];
+}
+
+// One Stockham pass of radix R over B lines of length n stored (k, line) at k * bp + line.
+template <typename C, int DIR, int R>
+__device__ __forceinline__ void stockham_pass(const C* __restrict__ src, C* __restrict__ dst, int n, int B, int bp,
+                                              int Ns, const C* __restrict__ tw, int tws) {
+    const int nb = n / R;
+    const int twstep = n / (Ns * R);
+    for (int q = threadIdx.x; q < nb * B; q += blockDim.x) {
+        const int line = q % B, j = q / B;
+        const int k = j % Ns;
+        C v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = src[(j + r * nb) * bp + line];
+        if (k > 0) {
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                C w = tw[((r * k * twstep) % n) * tws];
+                if (DIR > 0) w = cconj(w);
+                v[r] = cmul(v[r], w);
+            }
+        }
+        if (R == 2) dft2<C, DIR>(v);
+        else if (R == 4) dft4<C, DIR>(v);
+        else if (R == 8) dft8<C, DIR>(v);
+        else if (R == 3) dft3<C, DIR>(v);
+        else if (R == 5) dft5<C, DIR>(v);
+        else dft_generic<C, DIR, R>(v, tw, n, tws);
+        const int d = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) dst[(d + r * Ns) * bp + line] = v[r];
+    }
+}
+
+// Transforms B lines in place-ish: data in `a`, scratch `b`; returns the buffer with the result.
+// tw holds w_{n*tws}^m (so entry m*tws is w_n^m).
+template <typename C, int DIR>
+__device__ C* fft_lines(C* a, C* b, int n, int B, int bp, const Radices& rd, const C* __restrict__ tw, int tws) {
+    int Ns = 1;
+    for (int p = 0; p < rd.count; p++) {
+        const int R = rd.r[p];
+        switch (R) {
+            case 8: stockham_pass<C, DIR, 8>(a, b, n, B, bp, Ns, tw, tws); break;
+            case 4: stockham_pass<C, DIR, 4>(a, b, n, B, bp, Ns, tw, tws); break;
+            case 2: stockham_pass<C, DIR, 2>(a, b, n, B, bp, Ns, tw, tws); break;
+            case 3: stockham_pass<C, DIR, 3>(a, b, n, B, bp, Ns, tw, tws); break;
+            case 5: stockham_pass<C, DIR, 5>(a, b, n, B, bp, Ns, tw, tws); break;
+            default: stockham_pass<C, DIR, 7>(a, b, n, B, bp, Ns, tw, tws); break;
+        }
+        __syncthreads();
+        C* t = a;
+        a = b;
+        b = t;
+        Ns *= R;
+    }
+    return a;
+}
+
+// Twiddle table w_n^m = exp(-2 pi i m / n), m in [0, n), computed in double then rounded.
+template <typename C> __device__ void fill_twiddles(C* tw, int n) {
+    for (int m = threadIdx.x; m < n; m += blockDim.x) {
+        double s, c;
+        sincospi(-2.0 * (double)m / (double)n, &s, &c);
+        tw[m] = cmake<C>((decltype(C().x))c, (decltype(C().x))s);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Pointer packs
+// ---------------------------------------------------------------------------------------------
+template <typename C> struct Specs { C* p[MAX_BATCH]; };
+struct RealsIn { const void* p[MAX_BATCH]; };
+
+// ---------------------------------------------------------------------------------------------
+// z pass, forward r2c.  Tile = B rows (lines along z) of one mesh of the batch.
+// ---------------------------------------------------------------------------------------------
+template <typename T, typename TIN>
+__global__ void __launch_bounds__(FFT_THREADS) fft_z_r2c(RealsIn in, Specs<cplx_t<T>> out, int nbatch, Dims dims,
+                                                          Radices rd, int B) {
+    typedef cplx_t<T> C;
+    extern __shared__ unsigned char smem_raw[];
+    const int n2 = dims.n[2], M = n2 / 2, nh = M + 1;
+    const int bp = B + 1;
+    C* tw = (C*)smem_raw;                          // n2 entries
+    C* bufa = tw + n2;                             // (M + 1) * bp
+    C* bufb = bufa + (M + 1) * bp;
+    fill_twiddles(tw, n2);
+    __syncthreads();
+    const int64_t rows = (int64_t)dims.n[0] * dims.n[1];
+    const int64_t tiles_per = (rows + B - 1) / B;
+    const int64_t ntiles = tiles_per * nbatch;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int bi = (int)(t / tiles_per);
+        const int64_t row0 = (t % tiles_per) * B;
+        const int nrow = (int)min((int64_t)B, rows - row0);
+        const TIN* src = (const TIN*)in.p[bi] + row0 * n2;
+        // load rows as complex pairs (x[2m], x[2m+1])
+        for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
+            const int line = q / M, m = q % M;
+            C v = cmake<C>((T)0, (T)0);
+            if (line < nrow) {
+                const TIN* r = src + (int64_t)line * n2 + 2 * m;
+                v = cmake<C>((T)r[0], (T)r[1]);
+            }
+            bufa[m * bp + line] = v;
+        }
+        __syncthreads();
+        C* z = fft_lines<C, -1>(bufa, bufb, M, B, bp, rd, tw, 2);
+        C* x = z == bufa ? bufb : bufa;
+        // unpack: X[k] = (Z[k] + conj Z[M-k]) / 2 - i w^k (Z[k] - conj Z[M-k]) / 2
+        for (int q = threadIdx.x; q < B * nh; q += blockDim.x) {
+            const int line = q % B, k = q / B;
+            const C zk = z[(k == M ? 0 : k) * bp + line];
+            const C zc = cconj(z[(k == 0 ? 0 : M - k) * bp + line]);
+            const C e = cscale(cadd(zk, zc), (T)0.5);
+            const C o = cmul_i(cscale(csub(zk, zc), (T)0.5), -1);   // -i (Zk - Zc*) / 2
+            x[k * bp + line] = cadd(e, cmul(tw[k == M ? M : k], o));
+        }
+        __syncthreads();
+        C* dst = out.p[bi] + row0 * nh;
+        for (int q = threadIdx.x; q < B * nh; q += blockDim.x) {
+            const int line = q / nh, k = q % nh;
+            if (line < nrow) dst[(int64_t)line * nh + k] = x[k * bp + line];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Strided pass (y or x axis), in place.  Element (k, col) of a tile at
+// base + k * ls + col, base = outer * os + c0.
+// ---------------------------------------------------------------------------------------------
+struct Strided {
+    int n;          // line length
+    int64_t ls;     // stride between line elements
+    int outer;      // number of outer positions
+    int64_t os;     // outer stride
+    int ncols;      // columns (z extent nh)
+};
+
+template <typename C>
+__device__ __forceinline__ void load_tile(C* buf, const C* __restrict__ g, const Strided& s, int B, int cols) {
+    for (int q = threadIdx.x; q < s.n * B; q += blockDim.x) {
+        const int k = q / B, col = q % B;
+        buf[k * B + col] = col < cols ? g[(int64_t)k * s.ls + col] : cmake<C>(0, 0);
+    }
+}
+
+template <typename C>
+__device__ __forceinline__ void store_tile(C* __restrict__ g, const C* buf, const Strided& s, int B, int cols) {
+    for (int q = threadIdx.x; q < s.n * B; q += blockDim.x) {
+        const int k = q / B, col = q % B;
+        if (col < cols) g[(int64_t)k * s.ls + col] = buf[k * B + col];
+    }
+}
+
+template <typename T, int DIR>
+__global__ void __launch_bounds__(FFT_THREADS) fft_strided(Specs<cplx_t<T>> data, int nbatch, Strided s, Radices rd,
+                                                            int B) {
+    typedef cplx_t<T> C;
+    extern __shared__ unsigned char smem_raw[];
+    C* tw = (C*)smem_raw;
+    C* bufa = tw + s.n;
+    C* bufb = bufa + s.n * B;
+    fill_twiddles(tw, s.n);
+    __syncthreads();
+    const int ctiles = (s.ncols + B - 1) / B;
+    const int64_t tiles_per = (int64_t)s.outer * ctiles;
+    const int64_t ntiles = tiles_per * nbatch;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int bi = (int)(t / tiles_per);
+        const int64_t r = t % tiles_per;
+        const int o = (int)(r / ctiles), c0 = (int)(r % ctiles) * B;
+        const int cols = min(B, s.ncols - c0);
+        C* g = data.p[bi] + (int64_t)o * s.os + c0;
+        load_tile(bufa, g, s, B, cols);
+        __syncthreads();
+        C* res = fft_lines<C, DIR>(bufa, bufb, s.n, B, B, rd, tw, 1);
+        store_tile(g, res, s, B, cols);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k-space operators (applied between forward and inverse x transforms)
+// ---------------------------------------------------------------------------------------------
+enum KOpType { KOP_IDENTITY = 0, KOP_GAUSS = 1, KOP_PP = 2, KOP_ITER_GLOBAL = 3, KOP_ITER_LOCAL = 4, KOP_PSI = 5 };
+
+struct KOp {
+    int type;
+    int nper;            // outputs per input
+    int n[3];
+    double fscale[3];    // numpy fftfreq spacing 1 / (n d), d = boxsize / n
+    double radius[3];
+    double los[3];
+    double beta;
+    double norm;         // overall scale (1 / (n0 n1 n2) when the inverse follows)
+};
+
+__device__ __forceinline__ double kvalue(int i, int n, double fscale) {
+    const int s = i < (n + 1) / 2 ? i : i - n;
+    return 6.283185307179586 * ((double)s * fscale);   // 2 * np.pi * fftfreq(n, d)
+}
+
+__device__ __forceinline__ bool nyquist(int i, int n) { return (n % 2 == 0) && i == n / 2; }
+
+// Complex multiplier (re, im) of output `o` at grid point (ix, iy, iz), symmetrised.
+__device__ __forceinline__ double2 kmultiplier(const KOp& op, int o, int ix, int iy, int iz) {
+    const int idx[3] = {ix, iy, iz};
+    double k[3], kt[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        k[a] = kvalue(idx[a], op.n[a], op.fscale[a]);
+        kt[a] = nyquist(idx[a], op.n[a]) ? k[a] : -k[a];
+    }
+    const double k2 = (k[1] * k[1] + k[0] * k[0]) + k[2] * k[2];   // prod_sum order (mesh.c:335-337)
+    const bool zero = (ix == 0 && iy == 0 && iz == 0);
+    double re = 0., im = 0.;
+    switch (op.type) {
+        case KOP_GAUSS: {
+            double e = 0.;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const double rk = op.radius[a] * k[a];
+                e += -0.5 * (rk * rk);
+            }
+            re = exp(e);
+            break;
+        }
+        case KOP_PP: {
+            if (zero) break;
+            const double kl = k[0] * op.los[0] + k[1] * op.los[1] + k[2] * op.los[2];
+            const double klt = kt[0] * op.los[0] + kt[1] * op.los[1] + kt[2] * op.los[2];
+            const double m = k[o] / (k2 * (1. + op.beta * (kl * kl / k2)));
+            const double mt = kt[o] / (k2 * (1. + op.beta * (klt * klt / k2)));
+            im = 0.5 * (m - mt);   // (i m + conj(i mt)) / 2
+            break;
+        }
+        case KOP_ITER_GLOBAL: {
+            if (zero) break;
+            const double kl = k[0] * op.los[0] + k[1] * op.los[1] + k[2] * op.los[2];
+            const double klt = kt[0] * op.los[0] + kt[1] * op.los[1] + kt[2] * op.los[2];
+            re = 0.5 * (kl * kl + klt * klt) / k2;
+            break;
+        }
+        case KOP_ITER_LOCAL: {
+            if (zero) break;
+            const int pi[6] = {0, 0, 0, 1, 1, 2}, pj[6] = {0, 1, 2, 1, 2, 2};
+            const int i = pi[o], j = pj[o];
+            re = 0.5 * (k[i] * k[j] + kt[i] * kt[j]) / k2;
+            break;
+        }
+        case KOP_PSI: {
+            if (zero) break;
+            im = 0.5 * (k[o] - kt[o]) / k2;
+            break;
+        }
+        default:
+            re = 1.;
+    }
+    return make_double2(re * op.norm, im * op.norm);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS) fft_x_fused(Specs<cplx_t<T>> in, int nin, Specs<cplx_t<T>> out,
+                                                            Dims dims, Radices rd, int B, KOp op) {
+    typedef cplx_t<T> C;
+    extern __shared__ unsigned char smem_raw[];
+    const int n0 = dims.n[0], n1 = dims.n[1], nh = dims.n[2] / 2 + 1;
+    C* tw = (C*)smem_raw;
+    C* spec = tw + n0;
+    C* bufa = spec + n0 * B;
+    C* bufb = bufa + n0 * B;
+    fill_twiddles(tw, n0);
+    __syncthreads();
+    Strided s;
+    s.n = n0;
+    s.ls = (int64_t)n1 * nh;
+    s.outer = n1;
+    s.os = nh;
+    s.ncols = nh;
+    const int ctiles = (nh + B - 1) / B;
+    const int64_t tiles_per = (int64_t)n1 * ctiles;
+    const int64_t ntiles = tiles_per * nin;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int bi = (int)(t / tiles_per);
+        const int64_t r = t % tiles_per;
+        const int iy = (int)(r / ctiles), c0 = (int)(r % ctiles) * B;
+        const int cols = min(B, nh - c0);
+        const int64_t off = (int64_t)iy * nh + c0;
+        load_tile(bufa, in.p[bi] + off, s, B, cols);
+        __syncthreads();
+        C* fwd = fft_lines<C, -1>(bufa, bufb, n0, B, B, rd, tw, 1);
+        // keep the spectrum: copy to `spec` (the other buffer becomes free)
+        for (int q = threadIdx.x; q < n0 * B; q += blockDim.x) spec[q] = fwd[q];
+        __syncthreads();
+        for (int o = 0; o < op.nper; o++) {
+            for (int q = threadIdx.x; q < n0 * B; q += blockDim.x) {
+                const int ix = q / B, col = q % B;
+                const double2 m = kmultiplier(op, o, ix, iy, c0 + col);
+                const C v = spec[q];
+                bufa[q] = cmake<C>((T)(m.x * (double)v.x - m.y * (double)v.y), (T)(m.x * (double)v.y + m.y * (double)v.x));
+            }
+            __syncthreads();
+            C* res = fft_lines<C, +1>(bufa, bufb, n0, B, B, rd, tw, 1);
+            store_tile(out.p[bi * op.nper + o] + off, res, s, B, cols);
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// z pass, inverse c2r, with real-space epilogues
+// ---------------------------------------------------------------------------------------------
+enum EpiType { EPI_STORE = 0, EPI_DENSITY = 1, EPI_DENSITY_NORANDOMS = 2, EPI_ITER_GLOBAL = 3, EPI_ITER_LOCAL = 4 };
+
+template <typename T> struct Epi {
+    int type;
+    T* out[3];             // EPI_STORE: one output per input
+    const T* delta;        // original density contrast (EPI_ITER_*)
+    const double* sums;    // device {sum data, sum randoms} (EPI_DENSITY*)
+    double scale;          // applied to every inverse-transformed value
+    double bias, ran_min, size_randoms, ncells;
+    double factor[6];      // RSD-removal factors (EPI_ITER_*)
+    double offset[3], cell[3];   // node coordinates x_a = offset_a + cell_a * i (EPI_ITER_LOCAL)
+};
+
+template <typename T>
+__device__ __forceinline__ void epilogue_pair(const Epi<T>& e, int nin, const T* vals /* [nin][2] */, int64_t row,
+                                              int m, const Dims& dims, T out2[2]) {
+    const int n2 = dims.n[2];
+    for (int h = 0; h < 2; h++) {
+        const int64_t cell = row * n2 + 2 * m + h;
+        double res = 0.;
+        switch (e.type) {
+            case EPI_DENSITY: {
+                const double d = (double)vals[0 * 2 + h], r = (double)vals[1 * 2 + h];
+                const double sd = e.sums[0], sr = e.sums[1];
+                const double alpha = sd * 1. / sr;
+                const double threshold = e.ran_min * sr / e.size_randoms;
+                res = r > threshold ? (d - alpha * r) / (e.bias * alpha * r) : 0.;
+                break;
+            }
+            case EPI_DENSITY_NORANDOMS: {
+                const double mean = e.sums[0] / e.ncells;
+                res = ((double)vals[h] / mean - 1.) / e.bias;
+                break;
+            }
+            case EPI_ITER_GLOBAL: {
+                res = (double)e.delta[cell] - e.factor[0] * (double)vals[h];
+                break;
+            }
+            case EPI_ITER_LOCAL: {
+                const int iz = 2 * m + h;
+                const int ix = (int)(row / dims.n[1]), iy = (int)(row % dims.n[1]);
+                const double x[3] = {e.offset[0] + e.cell[0] * ix, e.offset[1] + e.cell[1] * iy,
+                                     e.offset[2] + e.cell[2] * iz};
+                const double x2 = (x[0] * x[0] + x[1] * x[1]) + x[2] * x[2];
+                const int pi[6] = {0, 0, 0, 1, 1, 2}, pj[6] = {0, 1, 2, 1, 2, 2};
+                double v = (double)e.delta[cell];
+                for (int c = 0; c < 6; c++)
+                    v -= e.factor[c] * ((x[pi[c]] * x[pj[c]] * (double)vals[c * 2 + h]) / x2);
+                res = v;
+                break;
+            }
+            default:
+                res = (double)vals[h];
+        }
+        out2[h] = (T)res;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, int nin, Dims dims, Radices rd, int B,
+                                                          Epi<T> e) {
+    typedef cplx_t<T> C;
+    extern __shared__ unsigned char smem_raw[];
+    const int n2 = dims.n[2], M = n2 / 2, nh = M + 1;
+    const int bp = B + 1;
+    C* tw = (C*)smem_raw;                    // n2
+    C* bufa = tw + n2;                       // nh * bp
+    C* bufb = bufa + nh * bp;                // nh * bp
+    C* acc = bufb + nh * bp;                 // nin * M * B (results kept for the epilogue)
+    fill_twiddles(tw, n2);
+    __syncthreads();
+    const int64_t rows = (int64_t)dims.n[0] * dims.n[1];
+    const int64_t ntiles = (rows + B - 1) / B;
+    const bool multi_store = (e.type == EPI_STORE);
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t row0 = t * B;
+        const int nrow = (int)min((int64_t)B, rows - row0);
+        for (int i = 0; i < nin; i++) {
+            const C* src = in.p[i] + row0 * nh;
+            for (int q = threadIdx.x; q < B * nh; q += blockDim.x) {
+                const int line = q / nh, k = q % nh;
+                bufa[k * bp + line] = line < nrow ? src[(int64_t)line * nh + k] : cmake<C>(0, 0);
+            }
+            __syncthreads();
+            // pack: Z[k] = (X[k] + conj X[M-k]) + i w^-k (X[k] - conj X[M-k]), k < M
+            for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
+                const int line = q % B, k = q / B;
+                const C xk = bufa[k * bp + line];
+                const C xc = cconj(bufa[(M - k) * bp + line]);
+                const C ev = cadd(xk, xc);
+                const C od = cmul(cconj(tw[k]), csub(xk, xc));
+                bufb[k * bp + line] = cadd(ev, cmul_i(od, +1));
+            }
+            __syncthreads();
+            C* z = fft_lines<C, +1>(bufb, bufa, M, B, bp, rd, tw, 2);
+            // keep (x[2m], x[2m+1]) * scale for the epilogue, row-major per input
+            for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
+                const int line = q / M, m = q % M;
+                const C v = z[m * bp + line];
+                acc[((int64_t)i * B + line) * M + m] = cmake<C>((T)(v.x * e.scale), (T)(v.y * e.scale));
+            }
+            __syncthreads();
+        }
+        for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
+            const int line = q / M, m = q % M;
+            if (line >= nrow) continue;
+            const int64_t row = row0 + line;
+            if (multi_store) {
+                for (int i = 0; i < nin; i++) {
+                    const C v = acc[((int64_t)i * B + line) * M + m];
+                    T* o = e.out[i] + row * n2 + 2 * m;
+                    o[0] = v.x;
+                    o[1] = v.y;
+                }
+            } else {
+                T vals[2 * MAX_BATCH];
+                for (int i = 0; i < nin; i++) {
+                    const C v = acc[((int64_t)i * B + line) * M + m];
+                    vals[2 * i] = v.x;
+                    vals[2 * i + 1] = v.y;
+                }
+                T r2[2];
+                epilogue_pair(e, nin, vals, row, m, dims, r2);
+                T* o = e.out[0] + row * n2 + 2 * m;
+                o[0] = r2[0];
+                o[1] = r2[1];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host-side planning and launches
+// ---------------------------------------------------------------------------------------------
+struct Plan3 {
+    Dims dims;
+    int nh;
+    Radices rz, ry, rx;   // rz is for the n2/2-point complex transform
+};
+
+static int make_plan(const int32_t nmesh[3], Plan3* p) {
+    for (int d = 0; d < 3; d++)
+        if (nmesh[d] < 2 || nmesh[d] > MAX_FFT_N) return PRC_ERR_UNSUPPORTED;
+    if (nmesh[2] % 2 != 0) return PRC_ERR_UNSUPPORTED;
+    for (int d = 0; d < 3; d++) p->dims.n[d] = nmesh[d];
+    p->nh = nmesh[2] / 2 + 1;
+    if (!factorize(nmesh[2] / 2, &p->rz) || !factorize(nmesh[1], &p->ry) || !factorize(nmesh[0], &p->rx))
+        return PRC_ERR_UNSUPPORTED;
+    return PRC_OK;
+}
+
+static size_t spectrum_elems(const Plan3& p) { return (size_t)p.dims.n[0] * p.dims.n[1] * p.nh; }
+
+// Lines per tile B (power of two) so that `nbuf` buffers of n * B complex fit the budget.
+static int choose_B(int n, int nbuf, size_t csize, size_t budget, int bmax) {
+    int B = bmax;
+    while (B > 1 && (size_t)nbuf * n * B * csize > budget) B >>= 1;
+    return B;
+}
+
+static int fft_grid(int64_t ntiles, int ctas_per_sm) {
+    int64_t cap = (int64_t)device_sm_count() * ctas_per_sm;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, cap));
+}
+
+template <typename T> struct FFTLaunch {
+    typedef cplx_t<T> C;
+    static constexpr size_t CS = sizeof(C);
+    static constexpr size_t BUDGET = 100 * 1024;
+
+    template <typename TIN>
+    static int z_r2c(const Plan3& p, const void* const* in, C* const* out, int nb, cudaStream_t st) {
+        const int M = p.dims.n[2] / 2;
+        int B = 16;
+        while (B > 1 && (size_t)(2 * (M + 1) * (B + 1) + p.dims.n[2]) * CS > BUDGET) B >>= 1;
+        size_t smem = (size_t)(2 * (M + 1) * (B + 1) + p.dims.n[2]) * CS;
+        RealsIn ri;
+        Specs<C> so;
+        for (int i = 0; i < nb; i++) {
+            ri.p[i] = in[i];
+            so.p[i] = out[i];
+        }
+        cudaFuncSetAttribute(fft_z_r2c<T, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
+        int64_t ntiles = ((rows + B - 1) / B) * nb;
+        fft_z_r2c<T, TIN><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(ri, so, nb, p.dims, p.rz, B);
+        PRC_CHECK_LAUNCH();
+        return PRC_OK;
+    }
+
+    template <int DIR> static int strided(const Plan3& p, int axis, C* const* data, int nb, cudaStream_t st) {
+        Strided s;
+        const int nh = p.nh;
+        if (axis == 1) {
+            s.n = p.dims.n[1];
+            s.ls = nh;
+            s.outer = p.dims.n[0];
+            s.os = (int64_t)p.dims.n[1] * nh;
+        } else {
+            s.n = p.dims.n[0];
+            s.ls = (int64_t)p.dims.n[1] * nh;
+            s.outer = p.dims.n[1];
+            s.os = nh;
+        }
+        s.ncols = nh;
+        int B = choose_B(s.n, 2, CS, BUDGET - s.n * CS, 16);
+        size_t smem = (size_t)(2 * s.n * B + s.n) * CS;
+        Specs<C> sp;
+        for (int i = 0; i < nb; i++) sp.p[i] = data[i];
+        cudaFuncSetAttribute(fft_strided<T, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int64_t ntiles = (int64_t)s.outer * ((nh + B - 1) / B) * nb;
+        fft_strided<T, DIR><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(sp, nb, s, axis == 1 ? p.ry : p.rx, B);
+        PRC_CHECK_LAUNCH();
+        return PRC_OK;
+    }
+
+    static int x_fused(const Plan3& p, C* const* in, int nin, C* const* out, const KOp& op, cudaStream_t st) {
+        const int n0 = p.dims.n[0];
+        int B = choose_B(n0, 3, CS, BUDGET - n0 * CS, 16);
+        size_t smem = (size_t)(3 * n0 * B + n0) * CS;
+        Specs<C> si, so;
+        for (int i = 0; i < nin; i++) si.p[i] = in[i];
+        for (int i = 0; i < nin * op.nper; i++) so.p[i] = out[i];
+        cudaFuncSetAttribute(fft_x_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int64_t ntiles = (int64_t)p.dims.n[1] * ((p.nh + B - 1) / B) * nin;
+        fft_x_fused<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, so, p.dims, p.rx, B, op);
+        PRC_CHECK_LAUNCH();
+        return PRC_OK;
+    }
+
+    static int z_c2r(const Plan3& p, C* const* in, int nin, const Epi<T>& e, cudaStream_t st) {
+        const int M = p.dims.n[2] / 2, nh = M + 1;
+        int B = 16;
+        auto need = [&](int b) { return (size_t)(2 * nh * (b + 1) + nin * M * b + p.dims.n[2]) * CS; };
+        while (B > 1 && need(B) > BUDGET) B >>= 1;
+        size_t smem = need(B);
+        Specs<C> si;
+        for (int i = 0; i < nin; i++) si.p[i] = in[i];
+        cudaFuncSetAttribute(fft_z_c2r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
+        int64_t ntiles = (rows + B - 1) / B;
+        fft_z_c2r<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, p.dims, p.rz, B, e);
+        PRC_CHECK_LAUNCH();
+        return PRC_OK;
+    }
+};
+
+static void fill_kop_geometry(KOp* op, const Plan3& p, const double boxsize[3], int mesh_bytes) {
+    for (int a = 0; a < 3; a++) {
+        op->n[a] = p.dims.n[a];
+        // numpy: d = boxsize / nmesh (boxsize stored in the mesh dtype), val = 1.0 / (n * d)
+        double bs = mesh_bytes == 4 ? (double)(float)boxsize[a] : boxsize[a];
+        double d = bs / (double)p.dims.n[a];
+        op->fscale[a] = 1.0 / ((double)p.dims.n[a] * d);
+        op->radius[a] = 0.;
+        op->los[a] = 0.;
+    }
+    op->beta = 0.;
+    op->nper = 1;
+    op->norm = 1.0 / ((double)p.dims.n[0] * p.dims.n[1] * p.dims.n[2]);
+}
+
+template <typename T> static Epi<T> epi_default() {
+    Epi<T> e;
+    memset(&e, 0, sizeof(e));
+    e.type = EPI_STORE;
+    e.scale = 1.;
+    return e;
+}
+
+// Forward z, y then x (x only when `do_x`).
+template <typename T, typename TIN>
+static int forward_zy(const Plan3& p, const void* const* in, cplx_t<T>* const* spec, int nb, cudaStream_t st) {
+    PRC_TRY((FFTLaunch<T>::template z_r2c<TIN>(p, in, spec, nb, st)));
+    PRC_TRY(FFTLaunch<T>::template strided<-1>(p, 1, spec, nb, st));
+    return PRC_OK;
+}
+
+template <typename T> static size_t spec_bytes(const Plan3& p) {
+    return (spectrum_elems(p) * sizeof(cplx_t<T>) + 255) & ~(size_t)255;
+}
+
+// ---- composites ----
+
+template <typename T>
+static int smooth_impl(const void* in, int in_bytes, T* out, const int32_t nmesh[3], const double boxsize[3],
+                       const double radius[3], void* ws, size_t wsb, cudaStream_t st) {
+    Plan3 p;
+    PRC_TRY(make_plan(nmesh, &p));
+    if (!ws || wsb < spec_bytes<T>(p)) return PRC_ERR_WORKSPACE;
+    cplx_t<T>* S = (cplx_t<T>*)ws;
+    const void* ins[1] = {in};
+    if (in_bytes == 8) PRC_TRY((forward_zy<T, double>(p, ins, &S, 1, st)));
+    else PRC_TRY((forward_zy<T, float>(p, ins, &S, 1, st)));
+    KOp op;
+    fill_kop_geometry(&op, p, boxsize, sizeof(T));
+    op.type = KOP_GAUSS;
+    for (int a = 0; a < 3; a++) op.radius[a] = sizeof(T) == 4 ? (double)(float)radius[a] : radius[a];
+    PRC_TRY(FFTLaunch<T>::x_fused(p, &S, 1, &S, op, st));
+    PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, &S, 1, st));
+    Epi<T> e = epi_default<T>();
+    e.out[0] = out;
+    return FFTLaunch<T>::z_c2r(p, &S, 1, e, st);
+}
+
+template <typename T>
+static int density_impl(const double* md, const double* mr, const double* sums, const int32_t nmesh[3],
+                        const double boxsize[3], const double radius[3], double bias, double ran_min,
+                        double size_randoms, T* delta, void* ws, size_t wsb, cudaStream_t st) {
+    Plan3 p;
+    PRC_TRY(make_plan(nmesh, &p));
+    const int nb = mr ? 2 : 1;
+    if (!ws || wsb < nb * spec_bytes<T>(p)) return PRC_ERR_WORKSPACE;
+    cplx_t<T>* S[2] = {(cplx_t<T>*)ws, (cplx_t<T>*)((char*)ws + spec_bytes<T>(p))};
+    const void* ins[2] = {md, mr};
+    PRC_TRY((forward_zy<T, double>(p, ins, S, nb, st)));
+    KOp op;
+    fill_kop_geometry(&op, p, boxsize, sizeof(T));
+    op.type = KOP_GAUSS;
+    for (int a = 0; a < 3; a++) op.radius[a] = sizeof(T) == 4 ? (double)(float)radius[a] : radius[a];
+    PRC_TRY(FFTLaunch<T>::x_fused(p, S, nb, S, op, st));
+    PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S, nb, st));
+    Epi<T> e = epi_default<T>();
+    e.type = mr ? EPI_DENSITY : EPI_DENSITY_NORANDOMS;
+    e.out[0] = delta;
+    e.sums = sums;
+    e.bias = bias;
+    e.ran_min = ran_min;
+    e.size_randoms = size_randoms;
+    e.ncells = (double)p.dims.n[0] * p.dims.n[1] * p.dims.n[2];
+    return FFTLaunch<T>::z_c2r(p, S, nb, e, st);
+}
+
+template <typename T>
+static int pp_impl(const T* delta, const int32_t nmesh[3], const double boxsize[3], double beta, const double los[3],
+                   T* px, T* py, T* pz, void* ws, size_t wsb, cudaStream_t st) {
+    Plan3 p;
+    PRC_TRY(make_plan(nmesh, &p));
+    if (!ws || wsb < 4 * spec_bytes<T>(p)) return PRC_ERR_WORKSPACE;
+    cplx_t<T>* S[4];
+    for (int i = 0; i < 4; i++) S[i] = (cplx_t<T>*)((char*)ws + i * spec_bytes<T>(p));
+    const void* ins[1] = {delta};
+    PRC_TRY((forward_zy<T, T>(p, ins, S, 1, st)));
+    KOp op;
+    fill_kop_geometry(&op, p, boxsize, sizeof(T));
+    op.type = KOP_PP;
+    op.nper = 3;
+    op.beta = beta;
+    for (int a = 0; a < 3; a++) op.los[a] = sizeof(T) == 4 ? (double)(float)los[a] : los[a];
+    PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));
+    PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, 3, st));
+    Epi<T> e = epi_default<T>();
+    e.out[0] = px;
+    e.out[1] = py;
+    e.out[2] = pz;
+    return FFTLaunch<T>::z_c2r(p, S + 1, 3, e, st);
+}
+
+template <typename T>
+static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
+                     double beta, const double* los, int niter, T* px, T* py, T* pz, void* ws, size_t wsb,
+                     cudaStream_t st) {
+    Plan3 p;
+    PRC_TRY(make_plan(nmesh, &p));
+    const int nout = los ? 1 : 6;
+    const size_t sb = spec_bytes<T>(p);
+    const size_t mesh_b = ((size_t)p.dims.size() * sizeof(T) + 255) & ~(size_t)255;
+    if (!ws || wsb < (1 + nout) * sb + mesh_b) return PRC_ERR_WORKSPACE;
+    cplx_t<T>* S[7];
+    for (int i = 0; i < 1 + nout; i++) S[i] = (cplx_t<T>*)((char*)ws + i * sb);
+    T* dreal = (T*)((char*)ws + (1 + nout) * sb);
+    KOp op;
+    fill_kop_geometry(&op, p, boxsize, sizeof(T));
+    if (los)
+        for (int a = 0; a < 3; a++) op.los[a] = sizeof(T) == 4 ? (double)(float)los[a] : los[a];
+    Epi<T> e = epi_default<T>();
+    e.delta = delta;
+    e.out[0] = dreal;
+    for (int a = 0; a < 3; a++) {
+        // node coordinates of RealMesh.coords (mesh.py:522-527): offset (mesh dtype) + d * i, d in f64
+        double bs = sizeof(T) == 4 ? (double)(float)boxsize[a] : boxsize[a];
+        double bc = sizeof(T) == 4 ? (double)(float)boxcenter[a] : boxcenter[a];
+        e.offset[a] = sizeof(T) == 4 ? (double)(float)((float)bc - (float)bs / 2.f) : bc - bs / 2.;
+        e.cell[a] = bs / (double)p.dims.n[a];
+    }
+    for (int it = 0; it < niter; it++) {
+        const void* ins[1] = {it == 0 ? (const void*)delta : (const void*)dreal};
+        PRC_TRY((forward_zy<T, T>(p, ins, S, 1, st)));
+        op.type = los ? KOP_ITER_GLOBAL : KOP_ITER_LOCAL;
+        op.nper = nout;
+        PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));
+        PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, nout, st));
+        double base = beta;
+        if (it == 0) base /= (1. + beta);
+        if (los) {
+            e.type = EPI_ITER_GLOBAL;
+            e.factor[0] = base;
+        } else {
+            e.type = EPI_ITER_LOCAL;
+            const int pi[6] = {0, 0, 0, 1, 1, 2}, pj[6] = {0, 1, 2, 1, 2, 2};
+            for (int c = 0; c < 6; c++) e.factor[c] = (1. + (pi[c] != pj[c])) * beta / (it == 0 ? (1. + beta) : 1.);
+        }
+        PRC_TRY(FFTLaunch<T>::z_c2r(p, S + 1, nout, e, st));
+    }
+    const void* ins[1] = {niter > 0 ? (const void*)dreal : (const void*)delta};
+    PRC_TRY((forward_zy<T, T>(p, ins, S, 1, st)));
+    op.type = KOP_PSI;
+    op.nper = 3;
+    PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));
+    PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, 3, st));
+    Epi<T> es = epi_default<T>();
+    es.out[0] = px;
+    es.out[1] = py;
+    es.out[2] = pz;
+    return FFTLaunch<T>::z_c2r(p, S + 1, 3, es, st);
+}
+
+template <typename T>
+static int rfft_impl(const void* in, int in_bytes, void* out, const int32_t nmesh[3], cudaStream_t st) {
+    Plan3 p;
+    PRC_TRY(make_plan(nmesh, &p));
+    cplx_t<T>* S = (cplx_t<T>*)out;
+    const void* ins[1] = {in};
+    if (in_bytes == 8) PRC_TRY((forward_zy<T, double>(p, ins, &S, 1, st)));
+    else PRC_TRY((forward_zy<T, float>(p, ins, &S, 1, st)));
+    return FFTLaunch<T>::template strided<-1>(p, 0, &S, 1, st);
+}
+
+template <typename T>
+static int irfft_impl(void* in, T* out, const int32_t nmesh[3], cudaStream_t st) {
+    Plan3 p;
+    PRC_TRY(make_plan(nmesh, &p));
+    cplx_t<T>* S = (cplx_t<T>*)in;
+    PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 0, &S, 1, st));
+    PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, &S, 1, st));
+    Epi<T> e = epi_default<T>();
+    e.out[0] = out;
+    e.scale = 1.0 / ((double)p.dims.n[0] * p.dims.n[1] * p.dims.n[2]);
+    return FFTLaunch<T>::z_c2r(p, &S, 1, e, st);
+}
+
+}  // namespace prc
+
+using namespace prc;
+
+static bool geom_ok(const int32_t* nmesh, const double* boxsize) {
+    if (!nmesh || !boxsize) return false;
+    for (int a = 0; a < 3; a++)
+        if (!(boxsize[a] > 0)) return false;
+    return true;
+}
+
+extern "C" {
+
+int prc_fft_supported(const int32_t nmesh[3]) {
+    if (!nmesh) return 0;
+    Plan3 p;
+    return make_plan(nmesh, &p) == PRC_OK ? 1 : 0;
+}
+
+size_t prc_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int nspectra) {
+    Plan3 p;
+    if (!nmesh || make_plan(nmesh, &p) != PRC_OK) return 0;
+    return (size_t)nspectra * (mesh_bytes == 4 ? spec_bytes<float>(p) : spec_bytes<double>(p));
+}
+
+prc_status_t prc_rfft3d_f32(const void* in, int in_bytes, void* out, const int32_t nmesh[3], void* stream) {
+    if (!in || !out || !nmesh || (in_bytes != 4 && in_bytes != 8)) return PRC_ERR_ARG;
+    return rfft_impl<float>(in, in_bytes, out, nmesh, (cudaStream_t)stream);
+}
+prc_status_t prc_rfft3d_f64(const void* in, int in_bytes, void* out, const int32_t nmesh[3], void* stream) {
+    if (!in || !out || !nmesh || (in_bytes != 4 && in_bytes != 8)) return PRC_ERR_ARG;
+    return rfft_impl<double>(in, in_bytes, out, nmesh, (cudaStream_t)stream);
+}
+prc_status_t prc_irfft3d_f32(void* in, float* out, const int32_t nmesh[3], void* stream) {
+    if (!in || !out || !nmesh) return PRC_ERR_ARG;
+    return irfft_impl<float>(in, out, nmesh, (cudaStream_t)stream);
+}
+prc_status_t prc_irfft3d_f64(void* in, double* out, const int32_t nmesh[3], void* stream) {
+    if (!in || !out || !nmesh) return PRC_ERR_ARG;
+    return irfft_impl<double>(in, out, nmesh, (cudaStream_t)stream);
+}
+
+prc_status_t prc_smooth_gaussian_f32(const void* in, int in_bytes, float* out, const int32_t nmesh[3],
+                                     const double boxsize[3], const double radius[3], void* workspace,
+                                     size_t workspace_bytes, void* stream) {
+    if (!in || !out || !geom_ok(nmesh, boxsize) || !radius || (in_bytes != 4 && in_bytes != 8)) return PRC_ERR_ARG;
+    return smooth_impl<float>(in, in_bytes, out, nmesh, boxsize, radius, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+prc_status_t prc_smooth_gaussian_f64(const void* in, int in_bytes, double* out, const int32_t nmesh[3],
+                                     const double boxsize[3], const double radius[3], void* workspace,
+                                     size_t workspace_bytes, void* stream) {
+    if (!in || !out || !geom_ok(nmesh, boxsize) || !radius || (in_bytes != 4 && in_bytes != 8)) return PRC_ERR_ARG;
+    return smooth_impl<double>(in, in_bytes, out, nmesh, boxsize, radius, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+size_t prc_density_contrast_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int with_randoms) {
+    return prc_fft_workspace_bytes(nmesh, mesh_bytes, with_randoms ? 2 : 1);
+}
+
+prc_status_t prc_density_contrast_f32(const double* mesh_data, const double* mesh_randoms, const double* sums,
+                                      const int32_t nmesh[3], const double boxsize[3], const double radius[3],
+                                      double bias, double ran_min, double size_randoms, float* delta, void* workspace,
+                                      size_t workspace_bytes, void* stream) {
+    if (!mesh_data || !sums || !delta || !geom_ok(nmesh, boxsize) || !radius) return PRC_ERR_ARG;
+    return density_impl<float>(mesh_data, mesh_randoms, sums, nmesh, boxsize, radius, bias, ran_min, size_randoms,
+                               delta, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+prc_status_t prc_density_contrast_f64(const double* mesh_data, const double* mesh_randoms, const double* sums,
+                                      const int32_t nmesh[3], const double boxsize[3], const double radius[3],
+                                      double bias, double ran_min, double size_randoms, double* delta, void* workspace,
+                                      size_t workspace_bytes, void* stream) {
+    if (!mesh_data || !sums || !delta || !geom_ok(nmesh, boxsize) || !radius) return PRC_ERR_ARG;
+    return density_impl<double>(mesh_data, mesh_randoms, sums, nmesh, boxsize, radius, bias, ran_min, size_randoms,
+                                delta, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+size_t prc_plane_parallel_workspace_bytes(const int32_t nmesh[3], int mesh_bytes) {
+    return prc_fft_workspace_bytes(nmesh, mesh_bytes, 4);
+}
+
+prc_status_t prc_plane_parallel_fft_f32(const float* delta, const int32_t nmesh[3], const double boxsize[3], double beta,
+                                        const double los[3], float* psi_x, float* psi_y, float* psi_z, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+    if (!delta || !geom_ok(nmesh, boxsize) || !los || !psi_x || !psi_y || !psi_z) return PRC_ERR_ARG;
+    return pp_impl<float>(delta, nmesh, boxsize, beta, los, psi_x, psi_y, psi_z, workspace, workspace_bytes,
+                          (cudaStream_t)stream);
+}
+prc_status_t prc_plane_parallel_fft_f64(const double* delta, const int32_t nmesh[3], const double boxsize[3],
+                                        double beta, const double los[3], double* psi_x, double* psi_y, double* psi_z,
+                                        void* workspace, size_t workspace_bytes, void* stream) {
+    if (!delta || !geom_ok(nmesh, boxsize) || !los || !psi_x || !psi_y || !psi_z) return PRC_ERR_ARG;
+    return pp_impl<double>(delta, nmesh, boxsize, beta, los, psi_x, psi_y, psi_z, workspace, workspace_bytes,
+                           (cudaStream_t)stream);
+}
+
+size_t prc_iterative_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int local_los) {
+    Plan3 p;
+    if (!nmesh || make_plan(nmesh, &p) != PRC_OK) return 0;
+    size_t mesh_b = ((size_t)p.dims.size() * mesh_bytes + 255) & ~(size_t)255;
+    return prc_fft_workspace_bytes(nmesh, mesh_bytes, local_los ? 7 : 4) + mesh_b;
+}
+
+prc_status_t prc_iterative_fft_f32(const float* delta, const int32_t nmesh[3], const double boxsize[3],
+                                   const double boxcenter[3], double beta, const double* los, int niterations,
+                                   float* psi_x, float* psi_y, float* psi_z, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+    if (!delta || !geom_ok(nmesh, boxsize) || !boxcenter || niterations < 0 || !psi_x || !psi_y || !psi_z)
+        return PRC_ERR_ARG;
+    return iter_impl<float>(delta, nmesh, boxsize, boxcenter, beta, los, niterations, psi_x, psi_y, psi_z, workspace,
+                            workspace_bytes, (cudaStream_t)stream);
+}
+prc_status_t prc_iterative_fft_f64(const double* delta, const int32_t nmesh[3], const double boxsize[3],
+                                   const double boxcenter[3], double beta, const double* los, int niterations,
+                                   double* psi_x, double* psi_y, double* psi_z, void* workspace,
+                                   size_t workspace_bytes, void* stream) {
+    if (!delta || !geom_ok(nmesh, boxsize) || !boxcenter || niterations < 0 || !psi_x || !psi_y || !psi_z)
+        return PRC_ERR_ARG;
+    return iter_impl<double>(delta, nmesh, boxsize, boxcenter, beta, los, niterations, psi_x, psi_y, psi_z, workspace,
+                             workspace_bytes, (cudaStream_t)stream);
+}
+
+}  // extern "C"

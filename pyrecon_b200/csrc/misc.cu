@@ -1,0 +1,63 @@
+// Library metadata and the element-wise mesh kernels of the reference's C ABI.
+#include "common.cuh"
+
+#include <algorithm>
+#include <math.h>
+
+namespace prc {
+
+// mesh[ix, iy, iz] *= (ax[ix] + ay[iy] + az[iz])^exp, coords = az | ay | ax (src/mesh.c:327-365).
+template <typename T>
+__global__ void prod_sum_kernel(T* __restrict__ mesh, Dims d, const T* __restrict__ coords, int exp) {
+    const int64_t N = d.size();
+    const T* az = coords;
+    const T* ay = coords + d.n[2];
+    const T* ax = coords + d.n[2] + d.n[1];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int iz = (int)(i % d.n[2]);
+        const int64_t r = i / d.n[2];
+        const int iy = (int)(r % d.n[1]), ix = (int)(r / d.n[1]);
+        const T s = (ay[iy] + ax[ix]) + az[iz];
+        if (exp == -1) mesh[i] = mesh[i] / s;
+        else if (exp == 1) mesh[i] = mesh[i] * s;
+        else mesh[i] = mesh[i] * (T)pow((double)s, (double)exp);
+    }
+}
+
+template <typename T> static int prod_sum(T* mesh, const int32_t shape[3], const T* coords, int exp, cudaStream_t st) {
+    if (!mesh || !shape || !coords) return PRC_ERR_ARG;
+    Dims d = {{shape[0], shape[1], shape[2]}};
+    if (d.size() <= 0) return PRC_ERR_ARG;
+    int64_t blocks = std::min<int64_t>((d.size() + 255) / 256, (int64_t)device_sm_count() * 16);
+    prod_sum_kernel<T><<<(int)blocks, 256, 0, st>>>(mesh, d, coords, exp);
+    PRC_CHECK_LAUNCH();
+    return PRC_OK;
+}
+
+}  // namespace prc
+
+extern "C" {
+
+const char* prc_version(void) { return "pyrecon_b200 0.1.0 (sm_100a)"; }
+
+const char* prc_status_string(prc_status_t status) {
+    switch (status) {
+        case PRC_OK: return "ok";
+        case PRC_ERR_ARG: return "invalid argument";
+        case PRC_ERR_WORKSPACE: return "workspace too small";
+        case PRC_ERR_CUDA: return "CUDA launch or runtime error";
+        case PRC_ERR_UNSUPPORTED: return "unsupported mesh size";
+        case PRC_ERR_TIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+prc_status_t prc_prod_sum_f32(float* mesh, const int32_t shape[3], const float* coords, int exp, void* stream) {
+    return prc::prod_sum<float>(mesh, shape, coords, exp, (cudaStream_t)stream);
+}
+
+prc_status_t prc_prod_sum_f64(double* mesh, const int32_t shape[3], const double* coords, int exp, void* stream) {
+    return prc::prod_sum<double>(mesh, shape, coords, exp, (cudaStream_t)stream);
+}
+
+}  // extern "C"

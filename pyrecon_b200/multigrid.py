@@ -1,0 +1,65 @@
+"""Full-multigrid reconstruction after M. J. White's recon_code (pyrecon/multigrid.py) on CUDA."""
+import numpy as np
+
+from . import _lib
+from .mesh import RealMesh, MeshError, torch_dtype
+from .recon import BaseReconstruction
+
+
+class OriginalMultiGridReconstruction(BaseReconstruction):
+    """
+    Solves the RSD-modified Poisson equation for the displacement potential :attr:`mesh_phi` with the
+    reference's fixed full-multigrid schedule of damped-Jacobi V-cycles (pyrecon/multigrid.py:13-158,
+    src/multigrid.c), and reads shifts as its finite-difference gradient.
+    """
+
+    @staticmethod
+    def _select_nmesh(nmesh):
+        """Smallest size >= n of the form 2^k, 3 2^k, 5 2^k or 7 2^k (multigrid.py:24-36)."""
+        out = []
+        for n in nmesh:
+            nbits = int(n).bit_length() - 1
+            ntries = [2 ** nbits, 3 * 2 ** (nbits - 1), 5 * 2 ** (nbits - 2), 7 * 2 ** (nbits - 2), 2 ** (nbits + 1)]
+            mindiff, iclosest = n, None
+            for itry, ntry in enumerate(ntries):
+                diff = ntry - n
+                if 0 <= diff < mindiff:
+                    mindiff, iclosest = diff, itry
+            out.append(ntries[iclosest])
+        return np.array(out, dtype='i8')
+
+    def run(self, jacobi_damping_factor=0.4, jacobi_niterations=5, vcycle_niterations=6):
+        """Compute the displacement potential :attr:`mesh_phi` (multigrid.py:99-135)."""
+        import torch
+        with self._stream_ctx():
+            nm, bs, bc = self.info.c_geometry()
+            lib = _lib.load()
+            phi = RealMesh(info=self.info, device=self.device)
+            phi.__dict__['value'] = torch.empty(self.info.shape, dtype=torch_dtype(self.info.dtype), device=self.device)
+            self.log_info('Computing displacement potential.')
+            f32 = self.info.dtype.itemsize == 4
+            ws = self._ws.get(lib.prc_multigrid_workspace_bytes(nm, self.info.dtype.itemsize, int(self.mixed_precision)))
+            args = [_lib.ptr(self.mesh_delta.value), _lib.ptr(phi.value), nm, bs, bc, float(self.beta),
+                    float(jacobi_damping_factor), int(jacobi_niterations), int(vcycle_niterations), self._los_arg()]
+            if f32:
+                args.append(int(self.mixed_precision))
+            _lib.call('prc_multigrid_' + _lib.suffix(self.info.dtype), *args, _lib.ptr(ws), ws.numel(),
+                      _lib.stream_of(self.device), error=MeshError)
+            del self.mesh_delta
+            self.mesh_phi = phi
+
+    def _shift_call(self, p, field, shifted, out, obytes):
+        if not hasattr(self, 'mesh_phi'):
+            from .recon import ReconstructionError
+            raise ReconstructionError('run() must be called before reading shifts')
+        nm, bs, bc = self._geometry_args()
+        _lib.call('prc_read_shifts_phi_' + _lib.suffix(self.info.dtype), _lib.ptr(self.mesh_phi.value), nm, bs, bc,
+                  _lib.ptr(p.pos), p.pos_bytes, p.size, float(self.f), self._los_arg(), field, shifted, int(self.wrap),
+                  _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device), error=MeshError)
+
+
+class MultiGridReconstruction(OriginalMultiGridReconstruction):
+    """Multigrid reconstruction with the base class's density contrast (multigrid.py:161-167)."""
+
+    def set_density_contrast(self, *args, **kwargs):
+        BaseReconstruction.set_density_contrast(self, *args, **kwargs)

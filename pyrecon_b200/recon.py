@@ -1,0 +1,238 @@
+"""
+BaseReconstruction: the reference's pipeline (pyrecon/recon.py) on one CUDA device.
+
+    recon = MultiGridReconstruction(f=0.8, bias=2.0, los=None, nmesh=512, boxsize=1000., boxcenter=2000.)
+    recon.assign_data(positions_data, weights_data)
+    recon.assign_randoms(positions_randoms, weights_randoms)
+    recon.set_density_contrast()
+    recon.run()
+    positions_rec_data = recon.read_shifted_positions(positions_data)
+
+Positions and weights may be numpy arrays, CPU torch tensors (pinned memory makes the
+host-to-device copies asynchronous) or CUDA tensors; results come back in the same kind of
+container.  ``dtype='f4'`` runs the FP32 pipeline with FP64 cloud-in-cell sums, FP64
+normalisation and (multigrid) FP64 defect correction; ``dtype='f8'`` runs everything in FP64.
+"""
+import numpy as np
+
+from . import _lib
+from .mesh import (MeshInfo, RealMesh, MeshError, Particles, _Workspace, _Flags, _device_of, torch_dtype, paint,
+                   _array3)
+from .utils import BaseClass, distance
+
+
+class ReconstructionError(Exception):
+    """Error raised when issue with reconstruction."""
+
+
+ALLOWED_FIELDS = ['disp', 'rsd', 'disp+rsd']
+
+
+class BaseReconstruction(BaseClass):
+    """Base template reconstruction class (pyrecon/recon.py:15-325).  Algorithms implement :meth:`run`."""
+
+    _needs_fft_mesh = True
+
+    @staticmethod
+    def _select_nmesh(nmesh):
+        return nmesh.copy()
+
+    def __init__(self, f=0., bias=1., los=None, fft_engine='numpy', fft_wisdom=None, save_fft_wisdom=None,
+                 fft_plan='measure', wrap=False, device=None, mixed_precision=True, stream=None, **kwargs):
+        """
+        Parameters are the reference's (recon.py:66-120): growth rate ``f``, ``bias``, line of sight
+        ``los`` (None / 'local' for a varying one, 'x' / 'y' / 'z' or a 3-vector), ``wrap`` and the
+        mesh keywords nmesh, boxsize, boxcenter, cellsize, positions, boxpad, dtype.  ``fft_engine``,
+        ``fft_wisdom``, ``save_fft_wisdom``, ``fft_plan`` and ``nthreads`` are accepted for
+        compatibility and ignored (the FFTs are this library's CUDA kernels).
+
+        Extra: ``device`` (CUDA device, default current), ``mixed_precision`` (dtype 'f4' multigrid
+        with FP64 defect correction, default True), ``stream`` (torch.cuda.Stream to enqueue on).
+        """
+        import torch
+        self.set_cosmo(f=f, bias=bias)
+        self.wrap = bool(wrap)
+        kwargs.pop('nthreads', None)
+        self.info = MeshInfo(select_nmesh=self._select_nmesh, **kwargs)
+        self.device = _device_of(device)
+        self.stream = stream
+        self.mixed_precision = bool(mixed_precision)
+        self.set_los(los)
+        _lib.load()
+        if not _lib.load().prc_fft_supported(_lib.i3(self.info.nmesh)):
+            raise MeshError('nmesh {} is not supported by the CUDA FFT (each axis must be 2^a 3^b 5^c 7^d <= 1024, '
+                            'the last one even)'.format(self.info.nmesh))
+        self.fft_engine = 'cuda'
+        self.fft_wisdom = None
+        self._ws = _Workspace(self.device)
+        self._flags = _Flags(self.device)
+        self._size_randoms = 0
+        with self._stream_ctx():
+            self.mesh_data = self._new_paint_mesh()
+            self.mesh_randoms = self._new_paint_mesh()
+        self.log_info('Using mesh {}.'.format(self.mesh_data))
+        del torch
+
+    def _stream_ctx(self):
+        import torch
+        if self.stream is None:
+            return torch.cuda.device(self.device)
+        return torch.cuda.stream(self.stream)
+
+    def _new_paint_mesh(self):
+        mesh = RealMesh(info=self.info, device=self.device)
+        mesh._ws = self._ws
+        mesh._fl = self._flags
+        return mesh
+
+    @property
+    def beta(self):
+        r""":math:`\beta = f / b`."""
+        return self.f / self.bias
+
+    def set_cosmo(self, f=None, bias=None, beta=None):
+        """recon.py:127-147."""
+        if bias is None:
+            bias = self.bias
+        if beta is not None:
+            f = beta * bias
+        if f is None:
+            f = self.f
+        self.f = f
+        self.bias = bias
+
+    def set_los(self, los=None):
+        """recon.py:149-170: None / 'local' -> local; 'x', 'y', 'z' or a 3-vector -> unit vector."""
+        if los is None or (isinstance(los, str) and los == 'local'):
+            self.los = None
+        else:
+            if isinstance(los, str):
+                los = 'xyz'.index(los)
+            if np.ndim(los) == 0:
+                ilos = los
+                los = np.zeros(3, dtype=self.info._type_float)
+                los[ilos] = 1.
+            los = np.array(los, dtype=self.info._type_float)
+            self.los = los / distance(los)
+
+    # -- geometry shortcuts (recon.py:328-338) --
+    boxsize = property(lambda self: self.info.boxsize)
+    boxcenter = property(lambda self: self.info.boxcenter)
+    nmesh = property(lambda self: self.info.nmesh)
+    offset = property(lambda self: self.info.offset)
+    cellsize = property(lambda self: self.info.cellsize)
+
+    # -- painting (recon.py:172-196) --
+
+    def assign_data(self, positions, weights=None, check=True):
+        """Paint data (accumulates over calls, e.g. slab by slab).  ``check=False`` defers the
+        box / NaN check (no host synchronisation)."""
+        with self._stream_ctx():
+            self.mesh_data.assign_cic(positions, weights=weights, wrap=self.wrap, check=check)
+
+    def assign_randoms(self, positions, weights=None, check=True):
+        """Same as :meth:`assign_data`, for randoms."""
+        if self.mesh_randoms.value is None:
+            self._size_randoms = 0
+        with self._stream_ctx():
+            self.mesh_randoms.assign_cic(positions, weights=weights, wrap=self.wrap, check=check)
+        self._size_randoms += len(positions)
+
+    @property
+    def has_randoms(self):
+        return self.mesh_randoms.value is not None
+
+    # -- density contrast (recon.py:198-249) --
+
+    def set_density_contrast(self, ran_min=0.01, smoothing_radius=15., check=False, **kwargs):
+        r"""Smooth data and randoms, then :math:`\delta = (d - \alpha r) / (b \alpha r)` where the smoothed
+        randoms exceed ``ran_min`` times their mean weight, else 0 (no randoms: :math:`d / \bar{d} - 1`, / b)."""
+        import torch
+        method = kwargs.pop('method', 'fft')
+        if method != 'fft':
+            raise MeshError("set_density_contrast(method='{}') is not provided by pyrecon_b200; use 'fft'".format(method))
+        with self._stream_ctx():
+            nm, bs, _ = self.info.c_geometry()
+            radius = _array3(smoothing_radius, self.info._type_float)
+            lib = _lib.load()
+            st = _lib.stream_of(self.device)
+            if self.mesh_data.value is None:
+                raise ReconstructionError('assign_data must be called before set_density_contrast')
+            sums = torch.zeros(2, dtype=torch.float64, device=self.device)
+            sws = torch.empty(lib.prc_sum_workspace_bytes(0), dtype=torch.uint8, device=self.device)
+            ncol = int(self.info.nmesh[0]) * int(self.info.nmesh[1])
+            _lib.call('prc_sum_f64', _lib.ptr(self.mesh_data._colsums), ncol, _lib.ptr(sums), _lib.ptr(sws),
+                      sws.numel(), st)
+            has_randoms = self.has_randoms
+            if has_randoms:
+                _lib.call('prc_sum_f64', _lib.ptr(self.mesh_randoms._colsums), ncol, _lib.c_void_p(sums.data_ptr() + 8),
+                          _lib.ptr(sws), sws.numel(), st)
+                if check:
+                    nnonzero = int((self.mesh_randoms._accum > 0.).sum())
+                    if nnonzero < 2:
+                        raise ValueError('Very few randoms!')
+            delta = RealMesh(info=self.info, device=self.device)
+            delta.__dict__['value'] = torch.empty(self.info.shape, dtype=torch_dtype(self.info.dtype), device=self.device)
+            ws = self._ws.get(lib.prc_density_contrast_workspace_bytes(nm, self.info.dtype.itemsize, int(has_randoms)))
+            _lib.call('prc_density_contrast_' + _lib.suffix(self.info.dtype), _lib.ptr(self.mesh_data._accum),
+                      _lib.ptr(self.mesh_randoms._accum) if has_randoms else None, _lib.ptr(sums), nm, bs,
+                      _lib.d3(radius), float(self.bias), float(ran_min), float(self._size_randoms),
+                      _lib.ptr(delta.value), _lib.ptr(ws), ws.numel(), st, error=MeshError)
+            if check and has_randoms:
+                s = sums.cpu().numpy()
+                threshold = ran_min * s[1] / self._size_randoms
+                self.log_info('Smoothed random threshold is (ran_min * mean weight) = {:.4f}.'.format(threshold))
+            self._sums = sums
+            self.mesh_delta = delta
+            del self.mesh_data
+            del self.mesh_randoms
+
+    def run(self, *args, **kwargs):
+        raise NotImplementedError('Implement method "run" in your "{}"-inherited algorithm'.format(self.__class__.__name__))
+
+    # -- shifts (recon.py:255-325) --
+
+    def _shift_call(self, particles, field, shifted, out, out_bytes):
+        raise NotImplementedError
+
+    def _read(self, positions, field, shifted):
+        import torch
+        field = field.lower()
+        if field not in ALLOWED_FIELDS:
+            raise ReconstructionError('Unknown field {}. Choices are {}'.format(field, ALLOWED_FIELDS))
+        with self._stream_ctx():
+            p = Particles(positions, self.device)
+            pbytes = p.pos_bytes
+            obytes = max(pbytes, self.info.dtype.itemsize) if (shifted and self.wrap) else pbytes
+            out = torch.empty((p.size, 3), dtype=torch_dtype('f4' if obytes == 4 else 'f8'), device=self.device)
+            self._shift_call(p, _lib.FIELDS[field], int(shifted), out, obytes)
+            low, high = self.info.boxcenter - self.info.boxsize / 2., self.info.boxcenter + self.info.boxsize / 2.
+            self._flags.raise_if_set(low, high)
+            return p.output(out)
+
+    def read_shifts(self, positions, field='disp+rsd'):
+        """Displacements at ``positions``: 'disp' (Zeldovich), 'rsd' or 'disp+rsd'."""
+        return self._read(positions, field, False)
+
+    def read_shifted_positions(self, positions, field='disp+rsd'):
+        """``positions - read_shifts(positions, field)``, wrapped into the box if :attr:`wrap`."""
+        return self._read(positions, field, True)
+
+    def _geometry_args(self):
+        return self.info.c_geometry()
+
+    def _los_arg(self):
+        return _lib.opt_d3(None if self.los is None else [float(x) for x in self.los])
+
+
+class FFTShiftsMixin(object):
+    """Shift read-out from the three displacement meshes ``mesh_psi`` (recon.py:255-302)."""
+
+    def _shift_call(self, p, field, shifted, out, obytes):
+        if not hasattr(self, 'mesh_psi'):
+            raise ReconstructionError('run() must be called before reading shifts')
+        nm, bs, bc = self._geometry_args()
+        px, py, pz = (m.value for m in self.mesh_psi)
+        _lib.call('prc_read_shifts_psi_' + _lib.suffix(self.info.dtype), _lib.ptr(px), _lib.ptr(py), _lib.ptr(pz), nm, bs,
+                  bc, _lib.ptr(p.pos), p.pos_bytes, p.size, float(self.f), self._los_arg(), field, shifted,
+                  int(self.wrap), _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device), error=MeshError)

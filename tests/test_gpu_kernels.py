@@ -1,0 +1,277 @@
+"""
+Kernel-level parity of libpyrecon_cuda.so against the CPU oracle, called through the C ABI.
+
+Bit-exact: cell keys and their stable sort order, CIC gathers (same arithmetic, same order,
+no FMA contraction).  FP64 sums: painted meshes to 1e-13 relative (order of summation only).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from oracle import pipeline  # noqa: E402
+from _util import maxrel  # noqa: E402
+
+
+def torch():
+    import torch as t
+    return t
+
+
+def dev(x):
+    return torch().from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def lib():
+    from pyrecon_b200 import _lib
+    return _lib
+
+
+def stream():
+    return lib().stream_of(torch().device('cuda'))
+
+
+def flags():
+    return torch().zeros(1, dtype=torch().int32, device='cuda')
+
+
+def ws(nbytes):
+    return torch().empty(max(int(nbytes), 256), dtype=torch().uint8, device='cuda')
+
+
+def catalog(n, boxsize, boxcenter, seed=0, dtype='f8'):
+    rng = np.random.default_rng(seed)
+    return (np.asarray(boxcenter) + rng.uniform(-0.5, 0.5, (n, 3)) * np.asarray(boxsize)).astype(dtype)
+
+
+@pytest.mark.parametrize('nmesh,npos,pos_dtype,mesh_dtype,wrap', [
+    ((8, 8, 8), 200000, 'f8', 'f8', False),         # ~390 particles per cell: long runs of equal keys
+    ((64, 48, 40), 300000, 'f4', 'f4', False),
+    ((16, 12, 20), 50000, 'f4', 'f8', True),
+    ((512, 512, 512), 100000, 'f8', 'f4', False),    # 27-bit keys: three 9-bit digit passes
+])
+def test_cell_order_bit_exact(nmesh, npos, pos_dtype, mesh_dtype, wrap):
+    L = lib()
+    boxsize, boxcenter = np.array([1000., 900., 800.]), np.array([100., -200., 3000.])
+    pos = catalog(npos, boxsize * (1.3 if wrap else 1.), boxcenter, seed=1, dtype=pos_dtype)
+    geom = pipeline.Geometry(nmesh, boxsize, boxcenter, dtype=mesh_dtype)
+    key, order = pipeline.sorted_cell_order(pos, geom, wrap=wrap)
+    t = torch()
+    k = t.empty(npos, dtype=t.int32, device='cuda')
+    o = t.empty(npos, dtype=t.int32, device='cuda')
+    fl = flags()
+    nm, bs, bc = L.i3(geom.nmesh), L.d3(geom.boxsize), L.d3(geom.boxcenter)
+    w = ws(L.load().prc_assign_cic_workspace_bytes(nm, npos, np.dtype(mesh_dtype).itemsize))
+    L.call('prc_cic_cell_order', L.ptr(k), L.ptr(o), nm, bs, bc, np.dtype(mesh_dtype).itemsize, L.ptr(dev(pos)),
+           np.dtype(pos_dtype).itemsize, npos, int(wrap), L.ptr(fl), L.ptr(w), w.numel(), stream())
+    assert int(fl.item()) == 0
+    np.testing.assert_array_equal(k.cpu().numpy().view(np.uint32).astype('i8'), key[order])
+    np.testing.assert_array_equal(o.cpu().numpy().view(np.uint32).astype('i8'), order)
+
+
+def gpu_paint(pos, weights, geom, wrap=False, accumulate_into=None):
+    L = lib()
+    t = torch()
+    n = geom.shape
+    mesh = accumulate_into if accumulate_into is not None else t.zeros(n, dtype=t.float64, device='cuda')
+    colsums = t.zeros(n[0] * n[1], dtype=t.float64, device='cuda')
+    fl = flags()
+    nm, bs, bc = L.i3(geom.nmesh), L.d3(geom.boxsize), L.d3(geom.boxcenter)
+    w = ws(L.load().prc_assign_cic_workspace_bytes(nm, len(pos), geom.dtype.itemsize))
+    wt = dev(weights) if weights is not None else None
+    L.call('prc_assign_cic', L.ptr(mesh), L.ptr(colsums), nm, bs, bc, geom.dtype.itemsize, L.ptr(dev(pos)) if len(pos) else None,
+           pos.dtype.itemsize, L.ptr(wt), 0 if weights is None else weights.dtype.itemsize, len(pos), int(wrap),
+           int(accumulate_into is not None), L.ptr(fl), L.ptr(w), w.numel(), stream())
+    return mesh, colsums, int(fl.item())
+
+
+@pytest.mark.parametrize('mesh_dtype', ['f4', 'f8'])
+def test_paint_matches_oracle(mesh_dtype):
+    boxsize, boxcenter = 1000., 0.
+    geom = pipeline.Geometry((16, 12, 20), boxsize, boxcenter, dtype=mesh_dtype)
+    pos = catalog(100000, [boxsize] * 3, [boxcenter] * 3, seed=2, dtype=mesh_dtype)
+    pos[0] = [500., -500., 500.]          # exactly on the upper / lower faces: index == n and 0
+    weights = np.random.default_rng(3).uniform(0.5, 1.5, len(pos)).astype(mesh_dtype)
+    ref = np.zeros(geom.shape, dtype='f8')
+    k = pipeline._Kernels('f8')
+    k.assign_cic(ref, geom.nmesh, geom.to_index(pos).astype('f8'), weights.astype('f8'))
+    mesh, colsums, fl = gpu_paint(pos, weights, geom)
+    assert fl == 0
+    m = mesh.cpu().numpy()
+    tol = 1e-13 if mesh_dtype == 'f8' else 1e-6   # f4: CIC fractions computed in float, as the reference does
+    assert maxrel(m, ref) < tol
+    np.testing.assert_allclose(colsums.cpu().numpy(), m.sum(axis=2), rtol=1e-12, atol=1e-9)
+    # deterministic: a second run gives the same bits
+    mesh2, _, _ = gpu_paint(pos, weights, geom)
+    assert torch().equal(mesh, mesh2)
+    # accumulation over two calls equals one call over both halves (up to FP64 rounding)
+    half = len(pos) // 2
+    acc, _, _ = gpu_paint(pos[:half], weights[:half], geom)
+    acc, _, _ = gpu_paint(pos[half:], weights[half:], geom, accumulate_into=acc)
+    assert maxrel(acc.cpu().numpy(), m) < 1e-13
+
+
+def test_paint_empty_and_unit_weights():
+    geom = pipeline.Geometry(8, 100., 0.)
+    mesh, colsums, fl = gpu_paint(np.zeros((0, 3)), None, geom)
+    assert fl == 0 and float(mesh.abs().sum()) == 0.
+    pos = catalog(1000, [100.] * 3, [0.] * 3, seed=4)
+    mesh, _, _ = gpu_paint(pos, None, geom)
+    assert abs(float(mesh.sum()) - 1000.) < 1e-9
+
+
+def test_paint_flags_leave_mesh_untouched():
+    geom = pipeline.Geometry(8, 100., 0.)
+    pos = catalog(1000, [100.] * 3, [0.] * 3, seed=5)
+    t = torch()
+    base = t.full(geom.shape, 7., dtype=t.float64, device='cuda')
+    bad = pos.copy()
+    bad[10, 1] = 60.                     # outside [-50, 50]
+    mesh, _, fl = gpu_paint(bad, None, geom, accumulate_into=base.clone())
+    assert fl & lib().PRC_FLAG_OUT_OF_BOX
+    assert torch().equal(mesh, base)
+    bad = pos.copy()
+    bad[3, 0] = np.nan
+    mesh, _, fl = gpu_paint(bad, None, geom, wrap=True, accumulate_into=base.clone())
+    assert fl & lib().PRC_FLAG_NONFINITE
+    assert torch().equal(mesh, base)
+
+
+@pytest.mark.parametrize('mesh_dtype,pos_dtype', [('f8', 'f8'), ('f4', 'f4'), ('f4', 'f8')])
+def test_gathers_bit_exact(mesh_dtype, pos_dtype):
+    L = lib()
+    geom = pipeline.Geometry((16, 12, 20), 1000., 0., dtype=mesh_dtype)
+    rng = np.random.default_rng(6)
+    mesh = rng.standard_normal(geom.shape).astype(mesh_dtype)
+    pos = catalog(20000, [1000.] * 3, [0.] * 3, seed=7, dtype=pos_dtype)
+    k = pipeline._Kernels(mesh_dtype)
+    idx = geom.to_index(pos)
+    ref_read = k.read_cic(mesh, geom.nmesh, idx).astype(pos_dtype)
+    ref_fd = k.read_finite_difference_cic(mesh, geom.nmesh, geom.boxsize, idx).astype(pos_dtype)
+    t = torch()
+    out = t.empty(len(pos), dtype=t.float32 if pos_dtype == 'f4' else t.float64, device='cuda')
+    out3 = t.empty((len(pos), 3), dtype=out.dtype, device='cuda')
+    fl = flags()
+    nm, bs, bc = L.i3(geom.nmesh), L.d3(geom.boxsize), L.d3(geom.boxcenter)
+    sfx = L.suffix(mesh_dtype)
+    dm, dp = dev(mesh), dev(pos)
+    L.call('prc_read_cic_' + sfx, L.ptr(dm), nm, bs, bc, L.ptr(dp), pos.dtype.itemsize, len(pos), 0, L.ptr(out), L.ptr(fl), stream())
+    L.call('prc_read_finite_difference_cic_' + sfx, L.ptr(dm), nm, bs, bc, L.ptr(dp), pos.dtype.itemsize, len(pos), 0,
+           L.ptr(out3), L.ptr(fl), stream())
+    np.testing.assert_array_equal(out.cpu().numpy(), ref_read)
+    np.testing.assert_array_equal(out3.cpu().numpy(), ref_fd)
+
+
+@pytest.mark.parametrize('nmesh', [(8, 8, 8), (16, 12, 20), (18, 14, 10), (64, 64, 64), (96, 48, 24), (7, 5, 6)])
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+def test_fft_against_numpy(nmesh, dtype):
+    L = lib()
+    t = torch()
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal(nmesh).astype(dtype)
+    ref = np.fft.rfftn(x.astype('f8'))
+    cdt = t.complex64 if dtype == 'f4' else t.complex128
+    spec = t.empty((nmesh[0], nmesh[1], nmesh[2] // 2 + 1), dtype=cdt, device='cuda')
+    nm = L.i3(nmesh)
+    sfx = L.suffix(dtype)
+    L.call('prc_rfft3d_' + sfx, L.ptr(dev(x)), np.dtype(dtype).itemsize, L.ptr(spec), nm, stream())
+    tol = 1e-5 if dtype == 'f4' else 1e-13
+    assert maxrel(spec.cpu().numpy(), ref) < tol
+    back = t.empty(nmesh, dtype=t.float32 if dtype == 'f4' else t.float64, device='cuda')
+    L.call('prc_irfft3d_' + sfx, L.ptr(spec), L.ptr(back), nm, stream())
+    assert maxrel(back.cpu().numpy(), x) < tol
+
+
+def test_fft_unsupported_sizes():
+    L = lib()
+    assert L.load().prc_fft_supported(L.i3((16, 16, 16))) == 1
+    assert L.load().prc_fft_supported(L.i3((11, 16, 16))) == 0     # prime factor 11
+    assert L.load().prc_fft_supported(L.i3((16, 16, 15))) == 0     # odd last axis
+    assert L.load().prc_fft_supported(L.i3((2048, 16, 16))) == 0   # above 1024
+
+
+@pytest.mark.parametrize('los', [None, [0., 0., 1.], [0.3, -0.5, 0.8]])
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+def test_multigrid_components(los, dtype):
+    L = lib()
+    t = torch()
+    n = (16, 12, 20)
+    boxsize, boxcenter, beta = np.array([800., 600., 1000.]), np.array([1600., 0., 300.]), 0.4
+    if los is not None:
+        los = np.asarray(los) / np.linalg.norm(los)
+    rng = np.random.default_rng(9)
+    v = rng.standard_normal(n).astype(dtype)
+    f = rng.standard_normal(n).astype(dtype)
+    lib_o = pipeline._Kernels(dtype)._mesh
+    import ctypes
+    from numpy import ctypeslib
+    ct = ctypeslib.as_ctypes_type(np.dtype(dtype))
+    arr = lambda a: np.ascontiguousarray(a, dtype=dtype)
+    nn = np.array(n, dtype='i8')
+    losp = None if los is None else arr(los).ctypes.data_as(ctypes.POINTER(ct))
+    # residual
+    r_ref = np.empty(n, dtype=dtype)
+    fn = lib_o.oracle_mg_residual
+    fn.argtypes = None
+    fn(arr(v).ctypes.data_as(ctypes.c_void_p), arr(f).ctypes.data_as(ctypes.c_void_p), r_ref.ctypes.data_as(ctypes.c_void_p),
+       nn.ctypes.data_as(ctypes.c_void_p), arr(boxsize).ctypes.data_as(ctypes.c_void_p),
+       arr(boxcenter).ctypes.data_as(ctypes.c_void_p), ct(beta), losp)
+    sfx = L.suffix(dtype)
+    r = t.empty(n, dtype=t.float32 if dtype == 'f4' else t.float64, device='cuda')
+    los_arg = L.opt_d3(None if los is None else list(arr(los)))
+    L.call('prc_mg_residual_' + sfx, L.ptr(dev(v)), L.ptr(dev(f)), L.ptr(r), L.i3(n), L.d3(boxsize), L.d3(boxcenter),
+           beta, los_arg, stream())
+    tol = 1e-12 if dtype == 'f8' else 2e-5
+    assert maxrel(r.cpu().numpy(), r_ref) < tol
+    # jacobi, 3 sweeps
+    vj = arr(v).copy()
+    fn = lib_o.oracle_mg_jacobi
+    fn(vj.ctypes.data_as(ctypes.c_void_p), arr(f).ctypes.data_as(ctypes.c_void_p), nn.ctypes.data_as(ctypes.c_void_p),
+       arr(boxsize).ctypes.data_as(ctypes.c_void_p), arr(boxcenter).ctypes.data_as(ctypes.c_void_p), ct(beta), ct(0.4),
+       ctypes.c_int(3), losp)
+    dv = dev(v)
+    scratch = t.empty_like(dv)
+    L.call('prc_mg_jacobi_' + sfx, L.ptr(dv), L.ptr(dev(f)), L.ptr(scratch), L.i3(n), L.d3(boxsize), L.d3(boxcenter),
+           beta, 0.4, 3, los_arg, stream())
+    assert maxrel(dv.cpu().numpy(), vj) < tol
+    # reduce / prolong
+    c_ref = np.empty((8, 6, 10), dtype=dtype)
+    lib_o.oracle_mg_reduce(arr(v).ctypes.data_as(ctypes.c_void_p), c_ref.ctypes.data_as(ctypes.c_void_p),
+                           nn.ctypes.data_as(ctypes.c_void_p))
+    c = t.empty((8, 6, 10), dtype=r.dtype, device='cuda')
+    L.call('prc_mg_reduce_' + sfx, L.ptr(dev(v)), L.ptr(c), L.i3(n), stream())
+    assert maxrel(c.cpu().numpy(), c_ref) < tol
+    p_ref = np.empty(n, dtype=dtype)
+    nc = np.array([8, 6, 10], dtype='i8')
+    lib_o.oracle_mg_prolong(c_ref.ctypes.data_as(ctypes.c_void_p), p_ref.ctypes.data_as(ctypes.c_void_p),
+                            nc.ctypes.data_as(ctypes.c_void_p))
+    pr = t.empty(n, dtype=r.dtype, device='cuda')
+    L.call('prc_mg_prolong_' + sfx, L.ptr(dev(c_ref)), L.ptr(pr), L.i3((8, 6, 10)), stream())
+    assert maxrel(pr.cpu().numpy(), p_ref) < tol
+
+
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+def test_prod_sum(dtype):
+    L = lib()
+    rng = np.random.default_rng(10)
+    shape = (4, 3, 10)
+    mesh = rng.uniform(0.5, 1.5, shape).astype(dtype)
+    coords = rng.uniform(1., 2., sum(shape)).astype(dtype)
+    ref = mesh.copy()
+    pipeline._Kernels(dtype).prod_sum(ref.reshape(-1), shape, coords, -1)
+    d = dev(mesh)
+    L.call('prc_prod_sum_' + L.suffix(dtype), L.ptr(d), L.i3(shape), L.ptr(dev(coords)), -1, stream())
+    assert maxrel(d.cpu().numpy(), ref) < (1e-15 if dtype == 'f8' else 1e-6)
+
+
+def test_sum_deterministic():
+    L = lib()
+    t = torch()
+    x = t.randn(1000003, dtype=t.float64, device='cuda')
+    out = t.empty(2, dtype=t.float64, device='cuda')
+    w = ws(L.load().prc_sum_workspace_bytes(x.numel()))
+    L.call('prc_sum_f64', L.ptr(x), x.numel(), L.ptr(out), L.ptr(w), w.numel(), stream())
+    L.call('prc_sum_f64', L.ptr(x), x.numel(), L.c_void_p(out.data_ptr() + 8), L.ptr(w), w.numel(), stream())
+    o = out.cpu().numpy()
+    assert o[0] == o[1]
+    assert abs(o[0] - x.double().sum().item()) < 1e-9

@@ -1,0 +1,70 @@
+"""
+End-to-end parity of the CUDA reconstruction against the reference's own outputs
+(golden fixtures) and the FP64 oracle, through the public Python API.
+
+Tolerances (stated by the north-star contract): shifted positions within 1e-6 Mpc/h of the
+FP64 oracle in the all-FP64 mode ('f8'), within 1e-3 Mpc/h in the FP32 mode ('f4').
+Intermediate meshes are compared relative to their maximum.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_cases
+from _util import load_golden, run_oracle, run_gpu, maxrel, maxabs
+
+pytestmark = pytest.mark.gpu
+
+F8_CASES = [c for c in golden_cases() if load_golden(c)['meta']['dtype'] == 'f8']
+
+
+@pytest.mark.parametrize('name', F8_CASES)
+def test_f8_matches_reference(name):
+    g = load_golden(name)
+    out, rec = run_gpu(g)
+    assert maxrel(out['mesh_data'], g['mesh_data']) < 1e-13
+    if 'mesh_randoms' in g:
+        assert maxrel(out['mesh_randoms'], g['mesh_randoms']) < 1e-13
+    assert maxrel(out['mesh_delta'], g['mesh_delta']) < 1e-10, name
+    key = 'mesh_phi' if 'mesh_phi' in g else 'mesh_psi'
+    assert maxrel(out[key], g[key]) < 1e-9, name
+    for k in ['shifts_disp', 'shifts_rsd', 'shifted_data', 'shifted_randoms']:
+        if k in g:
+            assert out[k].dtype == g[k].dtype, k
+            assert maxabs(out[k], g[k]) < 1e-6, (name, k, maxabs(out[k], g[k]))
+
+
+@pytest.mark.parametrize('name', golden_cases())
+def test_f4_within_1e3_of_f8_oracle(name):
+    """FP32 mode (FP64 paint sums / normalisation / multigrid defects) against the FP64 oracle."""
+    g = load_golden(name)
+    for k in ['data', 'randoms']:
+        if k in g:
+            g[k] = g[k].astype('f4')
+    ref = run_oracle(g, dtype='f8')
+    out, rec = run_gpu(g, dtype='f4')
+    assert maxrel(out['mesh_data'], ref['mesh_data']) < 1e-6
+    for k in ['shifted_data', 'shifted_randoms']:
+        if k in ref:
+            assert out[k].dtype == np.float32
+            assert maxabs(out[k], ref[k]) < 1e-3, (name, k, maxabs(out[k], ref[k]))
+
+
+def test_f4_multigrid_mixed_and_plain():
+    """Both FP32 multigrid variants stay within tolerance; the FP64-defect one is the closer."""
+    g = load_golden('mg_f8_local')
+    ref = run_oracle(g, dtype='f8')
+    errs = {}
+    for mixed in [True, False]:
+        out, _ = run_gpu(g, dtype='f4', mixed_precision=mixed)
+        errs[mixed] = maxabs(out['shifted_data'], ref['shifted_data'])
+        assert errs[mixed] < 1e-3
+    assert errs[True] <= errs[False] * 1.5 + 1e-6
+
+
+def test_repeatable_bitwise():
+    """Same inputs, same bits: the deterministic paint makes the whole pipeline reproducible."""
+    g = load_golden('ifft_f8_local')
+    a, _ = run_gpu(g)
+    b, _ = run_gpu(g)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k

@@ -1,0 +1,100 @@
+"""
+CPU-only tests: the C ABI library loads and exports every entry point of
+include/pyrecon_cuda.h (no compute call without a GPU), and the host-side logic of the
+drop-in (geometry, nmesh selection, line of sight, argument checks) matches the reference.
+"""
+import os
+import re
+import ctypes
+import warnings
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, 'include', 'pyrecon_cuda.h')).read()
+    return sorted(set(re.findall(r'^PRC_API [^(]*?\b(prc_\w+)\(', text, flags=re.M)))
+
+
+def test_library_exports_every_header_symbol():
+    from pyrecon_b200 import _lib
+    lib = _lib.load()
+    names = header_functions()
+    assert len(names) >= 40
+    for name in names:
+        assert hasattr(lib, name), name
+    # the Python binding declares a signature for every entry point, and nothing else
+    assert sorted(_lib.exported_symbols()) == names
+    # exported with default visibility from the .so itself
+    out = os.popen('nm -D --defined-only {}'.format(_lib.library_path())).read()
+    for name in names:
+        assert re.search(r'\bT {}\b'.format(name), out), name
+
+
+def test_host_only_entry_points():
+    from pyrecon_b200 import _lib
+    lib = _lib.load()
+    assert lib.prc_version().startswith(b'pyrecon_b200')
+    assert _lib.status_string(2) == 'workspace too small'
+    assert lib.prc_fft_supported(_lib.i3((512, 512, 512))) == 1
+    assert lib.prc_fft_supported(_lib.i3((384, 192, 320))) == 1
+    assert lib.prc_fft_supported(_lib.i3((13, 16, 16))) == 0
+    assert lib.prc_assign_cic_workspace_bytes(_lib.i3((512, 512, 512)), 25_000_000, 4) > 25_000_000 * 16
+    assert lib.prc_iterative_fft_workspace_bytes(_lib.i3((512, 512, 512)), 4, 1) > 7 * 512 * 512 * 257 * 8
+    assert lib.prc_multigrid_workspace_bytes(_lib.i3((64, 64, 64)), 4, 1) > 64 ** 3 * 8 * 2
+    # argument checks run before anything touches a device
+    assert lib.prc_assign_cic(None, None, _lib.i3((8, 8, 8)), _lib.d3([1.] * 3), _lib.d3([0.] * 3), 8, None, 8, None, 0,
+                              0, 0, 0, None, None, 0, None) == 1
+
+
+def test_meshinfo_semantics():
+    from pyrecon_b200 import MeshInfo, MeshError
+    info = MeshInfo(boxsize=1000., boxcenter=0., nmesh=64)
+    assert np.all(info.boxsize == 1000)
+    info.boxsize = 2000.
+    assert np.all(info.boxsize == 2000)
+    assert info.nmesh.dtype == np.int32
+    info = MeshInfo(boxsize=1000., boxcenter=0., nmesh=64, dtype='f4')
+    assert info.boxsize.dtype == np.float32
+    pos = np.random.default_rng(0).uniform(-100, 100, (1000, 3))
+    info = MeshInfo(positions=pos, nmesh=32, boxpad=2.)
+    np.testing.assert_allclose(info.boxsize, 2. * (pos.max(axis=0) - pos.min(axis=0)))
+    with pytest.raises(MeshError):
+        MeshInfo(nmesh=32)
+    with pytest.raises(MeshError):
+        MeshInfo(positions=pos, boxsize=10., nmesh=32)
+    info = MeshInfo(positions=pos, cellsize=10., boxsize=300.)
+    assert np.all(info.nmesh == 30)
+    w = ((pos + 1000.) - info.offset) % info.boxsize + info.offset
+    np.testing.assert_allclose(info.wrap(pos + 1000.), w)
+
+
+def test_select_nmesh_matches_reference_rule():
+    from pyrecon_b200.multigrid import OriginalMultiGridReconstruction as MG
+    sel = MG._select_nmesh
+    assert list(sel(np.array([12, 13, 17]))) == [12, 14, 20]
+    assert list(sel(np.array([512, 500, 384]))) == [512, 512, 384]
+    assert list(sel(np.array([64, 65, 100]))) == [64, 80, 112]
+
+
+def test_reconstruction_needs_gpu_or_raises():
+    """No silent CPU path: without a CUDA device the constructor raises."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip('a GPU is present')
+    from pyrecon_b200 import MultiGridReconstruction
+    from pyrecon_b200._lib import LibraryError
+    with pytest.raises(LibraryError):
+        MultiGridReconstruction(f=0.8, bias=2., nmesh=16, boxsize=100., boxcenter=0.)
+
+
+def test_fft_engine_kwargs_accepted():
+    """The reference's FFTW / threading keywords are accepted (and ignored) by the constructor signature."""
+    import inspect
+    from pyrecon_b200 import BaseReconstruction
+    params = inspect.signature(BaseReconstruction.__init__).parameters
+    for name in ['f', 'bias', 'los', 'fft_engine', 'fft_wisdom', 'save_fft_wisdom', 'fft_plan', 'wrap']:
+        assert name in params
