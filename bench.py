@@ -1,0 +1,361 @@
+"""
+Reconstructions per second of the pyrecon hot path on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--workload iterative_fft_512] [--impl ours|reference]
+
+One step = one complete reconstruction of the workload (constructor, assign_data, assign_randoms,
+set_density_contrast, run, read_shifted_positions of data and of randoms), as the reference's
+own timing of a reconstruction goes from the constructor to both read_shifted_positions calls.
+
+* value: steps/s with the catalogues resident in HBM (device-side CUDA-event timing, max over
+  ranks, N ranks run independent replicas: "replicas only", weak scaling).
+* e2e: the same reconstruction through the public API from pinned HOST tensors: every step copies
+  the catalogues host->device and the shifted positions device->host.
+* roofline: the kernel with the largest device time in the timed region, its compulsory bytes
+  (reported by the library per launch) / its event-timed duration, against MEASURED_PEAKS.json.
+* cpu_baseline / --impl reference: the reference's CPU path (its C kernels compiled from source
+  into oracle/_ref with OpenMP on all host cores, numpy glue, pocketfft with all cores) on a
+  1/8-scale sample of the workload (nmesh/2 per axis, 1/8 of the particles), scaled x8.
+"""
+import os
+import sys
+import json
+import time
+import argparse
+import subprocess
+import statistics
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'recons/s + p50/p99 latency vs plain GPU path, nmesh 512, shift err<1e-3 Mpc/h'
+
+WORKLOADS = {
+    # BASELINE config: IterativeFFTReconstruction nmesh=512, boxsize=2000, niterations=3, f=0.8, bias=2, local los,
+    # smoothing_radius=15, 5M lognormal data, 20M uniform randoms, float32 positions
+    'iterative_fft_512': dict(algorithm='IterativeFFTReconstruction', nmesh=512, boxsize=2000., boxcenter=2000.,
+                              los=None, ndata=5_000_000, nrandoms=20_000_000, pos_dtype='f4', dtype='f4',
+                              weights=None, run_kwargs=dict(niterations=3)),
+    # BASELINE config: MultiGridReconstruction nmesh=256, boxsize=2000, local los, 2M data, 10M randoms,
+    # weights uniform in [0.5, 1.5]; FP32 stencils with FP64 residual refinement
+    'multigrid_256': dict(algorithm='MultiGridReconstruction', nmesh=256, boxsize=2000., boxcenter=2000., los=None,
+                          ndata=2_000_000, nrandoms=10_000_000, pos_dtype='f8', dtype='f4', weights=(0.5, 1.5),
+                          run_kwargs={}),
+    # small case of the same pipeline for ncu captures (spectra of 134 MB, above L2)
+    'iterative_fft_256': dict(algorithm='IterativeFFTReconstruction', nmesh=256, boxsize=2000., boxcenter=2000.,
+                              los=None, ndata=1_000_000, nrandoms=4_000_000, pos_dtype='f4', dtype='f4',
+                              weights=None, run_kwargs=dict(niterations=3)),
+    'multigrid_512': dict(algorithm='MultiGridReconstruction', nmesh=512, boxsize=2000., boxcenter=2000., los=None,
+                          ndata=5_000_000, nrandoms=20_000_000, pos_dtype='f4', dtype='f4', weights=None, run_kwargs={}),
+    'plane_parallel_512': dict(algorithm='PlaneParallelFFTReconstruction', nmesh=512, boxsize=2000., boxcenter=2000.,
+                               los='z', ndata=5_000_000, nrandoms=20_000_000, pos_dtype='f4', dtype='f4', weights=None,
+                               run_kwargs={}),
+}
+DEFAULT_WORKLOAD = 'iterative_fft_512'
+
+
+def workload_name(w):
+    return '{algorithm} nmesh={nmesh} boxsize={boxsize:g} boxcenter={boxcenter:g} los={los} f=0.8 bias=2.0 ' \
+           'smoothing_radius=15 data={ndata} lognormal randoms={nrandoms} uniform positions={pos_dtype}'.format(**w)
+
+
+def dist_env():
+    return int(os.environ.get('RANK', 0)), int(os.environ.get('LOCAL_RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU reference arm
+# ---------------------------------------------------------------------------------------------
+
+def reference_sample(w, seed=0):
+    """Time the reference's CPU path on a 1/8-scale sample of workload `w`; returns (seconds, info)."""
+    import numpy as np
+    from oracle import pipeline
+    from pyrecon_b200 import mocks
+    cores = os.cpu_count() or 1
+    kernels = 'reference' if pipeline.reference_kernels_available() else 'oracle'
+    n = w['nmesh'] // 2
+    nd, nr = w['ndata'] // 8, w['nrandoms'] // 8
+    algo = {'IterativeFFTReconstruction': 'iterative_fft', 'MultiGridReconstruction': 'multigrid',
+            'PlaneParallelFFTReconstruction': 'plane_parallel_fft'}[w['algorithm']]
+    data = mocks.lognormal_positions_numpy(nd, n, w['boxsize'], w['boxcenter'], seed=2002 + seed,
+                                           field_seed=1002 + seed, dtype=w['pos_dtype'])
+    randoms = mocks.uniform_positions_numpy(nr, w['boxsize'], w['boxcenter'], seed=3002 + seed, dtype=w['pos_dtype'])
+    wd = wr = None
+    if w['weights'] is not None:
+        wd = mocks.weights_numpy(nd, *w['weights'], seed=4002 + seed)
+        wr = mocks.weights_numpy(nr, *w['weights'], seed=4003 + seed)
+    t0 = time.perf_counter()
+    rec = pipeline.OracleReconstruction(algo, f=0.8, bias=2., los=w['los'], nmesh=n, boxsize=w['boxsize'],
+                                        boxcenter=w['boxcenter'], dtype=w['dtype'], kernels=kernels,
+                                        fft_engine='scipy', nthreads=cores)
+    rec.assign_data(data, wd)
+    rec.assign_randoms(randoms, wr)
+    rec.set_density_contrast(smoothing_radius=15.)
+    rec.run(**w['run_kwargs'])
+    rec.read_shifted_positions(data)
+    rec.read_shifted_positions(randoms)
+    dt = time.perf_counter() - t0
+    info = dict(cores=cores, kind='reference' if kernels == 'reference' else 'port',
+                sample='reference CPU path ({} C kernels with OpenMP x{}, numpy glue, scipy pocketfft x{}) on a 1/8 '
+                       'sample: nmesh {} and {} + {} particles, time x8'.format(
+                           'reference' if kernels == 'reference' else 'restated', cores, cores, n, nd, nr))
+    return dt, info
+
+
+def run_reference_arm(args, w):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    times, info = [], None
+    budget = float(os.environ.get('PRC_REFERENCE_BUDGET_S', 150.))
+    t_start = time.perf_counter()
+    for i in range(args.warmup + args.steps):
+        dt, info = reference_sample(w, seed=i)
+        if i >= args.warmup:
+            times.append(dt * 8.)
+        if time.perf_counter() - t_start > budget and len(times) >= 1:
+            break
+    sec = statistics.median(times)
+    value = 1. / sec
+    line = dict(metric=METRIC, value=value, unit='recons/s', n_gpus=args.gpus, steps=len(times), warmup=args.warmup,
+                ms_per_step=sec * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype=w['dtype'],
+                data='synthetic seeded lognormal data + uniform randoms',
+                config=dict(workload=workload_name(w)), impl='reference',
+                cpu_baseline=dict(value=value, unit='recons/s', cores=info['cores'], kind=info['kind'],
+                                  sample=info['sample']),
+                e2e=dict(value=value, unit='recons/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------------
+
+class ClockSampler(object):
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, 'gpurun_out', 'clocks_rank{}.csv'.format(index))
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, 'w')
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.FIELDS,
+                                          '--format=csv,noheader,nounits', '-lms', '200'], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.isfile(self.path):
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=['nvidia-smi unavailable'])
+        sms, maxs, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxs.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == 'active':
+                    reasons.add(name)
+        if not sms:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=['no samples'])
+        return dict(sm_mhz=statistics.median(sms), sm_max_mhz=max(maxs), reasons=sorted(reasons), samples=len(sms))
+
+
+def make_catalogs(w, device, rank):
+    import torch
+    from pyrecon_b200 import mocks
+    g = dict(device=device)
+    data = mocks.lognormal_positions_torch(w['ndata'], w['nmesh'], w['boxsize'], w['boxcenter'], seed=2003 + rank,
+                                           field_seed=1003 + rank, dtype=w['pos_dtype'], **g)
+    randoms = mocks.uniform_positions_torch(w['nrandoms'], w['boxsize'], w['boxcenter'], seed=3003 + rank,
+                                            dtype=w['pos_dtype'], **g)
+    wd = wr = None
+    if w['weights'] is not None:
+        wd = mocks.weights_torch(w['ndata'], *w['weights'], seed=4003 + rank, dtype=w['pos_dtype'], **g)
+        wr = mocks.weights_torch(w['nrandoms'], *w['weights'], seed=4004 + rank, dtype=w['pos_dtype'], **g)
+    torch.cuda.synchronize(device)
+    return data, wd, randoms, wr
+
+
+def reconstruct(w, device, data, wd, randoms, wr, check):
+    import pyrecon_b200
+    Cls = getattr(pyrecon_b200, w['algorithm'])
+    rec = Cls(f=0.8, bias=2., los=w['los'], nmesh=w['nmesh'], boxsize=w['boxsize'], boxcenter=w['boxcenter'],
+              dtype=w['dtype'], device=device)
+    rec.assign_data(data, wd, check=check)
+    rec.assign_randoms(randoms, wr, check=check)
+    rec.set_density_contrast(smoothing_radius=15.)
+    rec.run(**w['run_kwargs'])
+    out_d = rec.read_shifted_positions(data)
+    out_r = rec.read_shifted_positions(randoms)
+    return out_d, out_r
+
+
+def load_peaks():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.isfile(path):
+        with open(path) as fh:
+            p = json.load(fh)
+        return float(p['hbm_gbs']), 'measured'
+    return 6650., 'fallback'
+
+
+def timed_loop(fn, steps, device):
+    """Per-step CUDA events on the current stream; returns (total ms, per-step ms list)."""
+    import torch
+    st = torch.cuda.current_stream(device)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    evs[0].record(st)
+    for i in range(steps):
+        fn()
+        evs[i + 1].record(st)
+    torch.cuda.synchronize(device)
+    per = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+    return evs[0].elapsed_time(evs[-1]), per
+
+
+def percentile(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = (len(xs) - 1) * q / 100.
+    f, c = int(k), min(int(k) + 1, len(xs) - 1)
+    return xs[f] + (xs[c] - xs[f]) * (k - f)
+
+
+def run_gpu_arm(args, w):
+    import torch
+    import torch.distributed as dist
+    from pyrecon_b200 import _lib
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    device = torch.device('cuda', local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300), device_id=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    data, wd, randoms, wr = make_catalogs(w, device, rank)
+    step = lambda: reconstruct(w, device, data, wd, randoms, wr, check=False)
+    # correctness of the measured configuration: a checked run first (raises on bad inputs)
+    reconstruct(w, device, data, wd, randoms, wr, check=True)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(device)
+
+    # --- device-resident timed region ---
+    barrier()
+    torch.cuda.synchronize(device)
+    launches0 = _lib.launch_count()
+    _lib.profile_enable(True)
+    with ClockSampler(local_rank) as clocks:
+        total_ms, per_step = timed_loop(step, args.steps, device)
+    prof = _lib.profile_collect()
+    _lib.profile_enable(False)
+    launches = _lib.launch_count() - launches0
+    barrier()
+    total_ms = max_over_ranks(total_ms)
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1e3)
+
+    # --- end to end through the public API from pinned host memory ---
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda t: None if t is None else t.cpu().pin_memory()
+        hd, hwd, hr, hwr = pin(data), pin(wd), pin(randoms), pin(wr)
+        h2d = sum(t.numel() * t.element_size() for t in [hd, hwd, hr, hwr] if t is not None)
+        d2h = (hd.numel() + hr.numel()) * hd.element_size()
+        e2e_step = lambda: reconstruct(w, device, hd, hwd, hr, hwr, check=False)
+        e2e_step()
+        barrier()
+        e_ms, _ = timed_loop(e2e_step, max(1, args.steps), device)
+        barrier()
+        e_ms = max_over_ranks(e_ms)
+        e2e = dict(value=world * max(1, args.steps) / (e_ms / 1e3), unit='recons/s', h2d_bytes_per_step=int(h2d),
+                   d2h_bytes_per_step=int(d2h), ms_per_step=e_ms / max(1, args.steps))
+
+    # --- roofline of the dominant kernel ---
+    peak, peak_kind = load_peaks()
+    name, (nl, kms, kbytes) = max(prof.items(), key=lambda kv: kv[1][1])
+    achieved = (kbytes / 1e9) / (kms / 1e3) if kms > 0 else 0.
+    kernels = {k: dict(launches=v[0], ms=round(v[1], 3), share=round(v[1] / max(sum(x[1] for x in prof.values()), 1e-9), 4),
+                       gbs=round((v[2] / 1e9) / (v[1] / 1e3), 1) if v[1] > 0 else None) for k, v in prof.items()}
+    roofline = dict(bound='hbm', kernel=name, achieved=round(achieved, 1), peak=peak, unit='GB/s',
+                    frac=round(achieved / peak, 4), traffic=None,
+                    bytes_per_launch=kbytes / nl, launch_ms=kms / nl, peak_source=peak_kind + ' (MEASURED_PEAKS.json hbm_gbs)')
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sec, info = reference_sample(w)
+        cpu = dict(value=1. / (8. * sec), unit='recons/s', cores=info['cores'], kind=info['kind'], sample=info['sample'])
+
+    if rank == 0:
+        line = dict(metric=METRIC, value=value, unit='recons/s', n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=ms_per_step, higher_is_better=True, scaling='weak', vs_baseline=None, dtype=w['dtype'],
+                    data='synthetic: seeded lognormal data (sigma_G=0.8, P(k)~k^-1.5 exp(-(8k)^2)) + uniform randoms',
+                    config=dict(workload=workload_name(w), parallelism='replicas (one independent reconstruction per GPU)',
+                                precision='f4 mesh pipeline, FP64 CIC sums and normalisation',
+                                l2='inputs larger than L2 (positions {:.0f} MB)'.format(
+                                    (data.numel() + randoms.numel()) * data.element_size() / 1e6)),
+                    latency_ms=dict(p50=percentile(per_step, 50), p99=percentile(per_step, 99)),
+                    e2e=e2e, roofline=roofline, cpu_baseline=cpu, gpu_launches=int(launches),
+                    clocks=clocks.summary(), kernels=kernels)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args(argv)
+    w = WORKLOADS[args.workload]
+    if args.impl == 'reference':
+        return run_reference_arm(args, w)
+    return run_gpu_arm(args, w)
+
+
+if __name__ == '__main__':
+    sys.exit(main())

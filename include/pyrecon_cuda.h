@@ -57,6 +57,18 @@ PRC_API const char *prc_version(void);
 /* Human-readable name of a status code. */
 PRC_API const char *prc_status_string(prc_status_t status);
 
+/* Number of kernels this library has launched since it was loaded (all devices, all streams). */
+PRC_API unsigned long long prc_launch_count(void);
+
+/* Per-kernel device timing: enable(1) clears previous records and brackets every later launch
+ * with CUDA events on its stream; enable(0) stops recording.  collect() waits for the recorded
+ * events, writes {"kernel name": [launches, total ms, compulsory bytes], ...} (JSON,
+ * NUL-terminated, truncated to cap) into buf, clears the records and returns the size the full
+ * text needs.  Compulsory bytes = what each launch must read and write at least (its algorithmic
+ * DRAM traffic), so bytes / ms is the achieved bandwidth against the HBM roofline. */
+PRC_API void prc_profile_enable(int on);
+PRC_API int prc_profile_collect(char *buf, size_t cap);
+
 /* 1 if every axis of nmesh is handled by the FFT kernels (n = 2^a 3^b 5^c 7^d, n2 even,
  * n <= 1024), else 0. */
 PRC_API int prc_fft_supported(const int32_t nmesh[3]);

@@ -29,6 +29,9 @@ _p = c_void_p
 _SIGNATURES = {
     'prc_version': (ctypes.c_char_p, []),
     'prc_status_string': (ctypes.c_char_p, [c_int]),
+    'prc_launch_count': (ctypes.c_ulonglong, []),
+    'prc_profile_enable': (None, [c_int]),
+    'prc_profile_collect': (c_int, [ctypes.c_char_p, c_size]),
     'prc_fft_supported': (c_int, [I3]),
     'prc_assign_cic_workspace_bytes': (c_size, [I3, c_i64, c_int]),
     'prc_assign_cic': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size, _p]),
@@ -129,6 +132,23 @@ def call(name, *args, error=None):
         exc = error or LibraryError
         raise exc('{} failed: {} (status {})'.format(name, status_string(status), status))
     return status
+
+
+def launch_count():
+    """Kernels launched by the library so far."""
+    return int(load().prc_launch_count())
+
+
+def profile_enable(on=True):
+    load().prc_profile_enable(int(bool(on)))
+
+
+def profile_collect():
+    """{kernel name: (launches, total device ms)} of the launches since profile_enable(True)."""
+    import json
+    buf = ctypes.create_string_buffer(1 << 16)
+    load().prc_profile_collect(buf, len(buf))
+    return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
 
 
 def suffix(dtype):

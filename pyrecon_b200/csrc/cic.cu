@@ -224,12 +224,12 @@ int sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, int64_t n
     uint32_t *ka = k0, *va = v0, *kb = k1, *vb = v1;
     for (int p = 0; p < npass; p++) {
         int shift = p * dbits;
-        upsweep<<<grid, THREADS, 0, st>>>(ka, n, shift, radix, ntiles, hist);
+        PRC_LAUNCH_B("sort_upsweep", st, 4.0 * n + 4.0 * count, upsweep<<<grid, THREADS, 0, st>>>(ka, n, shift, radix, ntiles, hist));
         int sb = scan_blocks(count);
-        scan_tiles<<<sb, SCAN_THREADS, 0, st>>>(hist, count, tsums);
-        scan_totals<<<1, SCAN_THREADS, 0, st>>>(tsums, sb);
-        scan_add<<<sb, SCAN_THREADS, 0, st>>>(hist, count, tsums);
-        downsweep<<<grid, THREADS, downsweep_smem(radix), st>>>(ka, va, kb, vb, n, shift, radix, ntiles, hist);
+        PRC_LAUNCH_B("sort_scan", st, 8.0 * count, scan_tiles<<<sb, SCAN_THREADS, 0, st>>>(hist, count, tsums));
+        PRC_LAUNCH("sort_scan", st, scan_totals<<<1, SCAN_THREADS, 0, st>>>(tsums, sb));
+        PRC_LAUNCH_B("sort_scan", st, 8.0 * count, scan_add<<<sb, SCAN_THREADS, 0, st>>>(hist, count, tsums));
+        PRC_LAUNCH_B("sort_downsweep", st, 16.0 * n + 4.0 * count, downsweep<<<grid, THREADS, downsweep_smem(radix), st>>>(ka, va, kb, vb, n, shift, radix, ntiles, hist));
         PRC_CHECK_LAUNCH();
         uint32_t* t;
         t = ka; ka = kb; kb = t;
@@ -741,7 +741,7 @@ inline size_t paint_layout(const int32_t nmesh[3], int64_t npos, int mesh_bytes,
 template <typename P, typename F, typename W>
 int paint_sort(const P* pos, const W* w, int64_t n, const BoxGeom& g, int wrap, const PaintWs& ws, int32_t* flags,
                uint32_t** keys, uint32_t** order, cudaStream_t st) {
-    paint_keys<P, F, W><<<particle_grid(n), 256, 0, st>>>(pos, w, n, g, wrap, ws.k0, ws.v0, flags);
+    PRC_LAUNCH_B("paint_keys", st, (double)n * (3 * sizeof(P) + (w ? sizeof(W) : 0) + 8), paint_keys<P, F, W><<<particle_grid(n), 256, 0, st>>>(pos, w, n, g, wrap, ws.k0, ws.v0, flags));
     PRC_CHECK_LAUNCH();
     int32_t nm[3] = {g.n[0], g.n[1], g.n[2]};
     return rsort::sort_pairs(ws.k0, ws.v0, ws.k1, ws.v1, n, key_bits(nm), ws.scratch, keys, order, st);
@@ -754,20 +754,20 @@ int paint_run(double* mesh, double* colsums, const BoxGeom& g, const P* pos, con
     if (n > 0) PRC_TRY((paint_sort<P, F, W>(pos, w, n, g, wrap, ws, flags, &keys, &order, st)));
     Payload<F>* pl = (Payload<F>*)ws.payload;
     if (n > 0) {
-        paint_payload<P, F, W><<<particle_grid(n), 256, 0, st>>>(pos, w, n, g, wrap, order, pl, flags);
+        PRC_LAUNCH_B("paint_payload", st, (double)n * (4 + 3 * sizeof(P) + (w ? sizeof(W) : 0) + sizeof(Payload<F>)), paint_payload<P, F, W><<<particle_grid(n), 256, 0, st>>>(pos, w, n, g, wrap, order, pl, flags));
         PRC_CHECK_LAUNCH();
     } else {
         keys = ws.k0;
     }
     int64_t ncol = (int64_t)g.n[0] * g.n[1];
-    column_starts<<<particle_grid(n + 1), 256, 0, st>>>(keys, n, g.n[2], ncol, ws.col_start, flags);
+    PRC_LAUNCH_B("paint_columns", st, 8.0 * n + 4.0 * ncol, column_starts<<<particle_grid(n + 1), 256, 0, st>>>(keys, n, g.n[2], ncol, ws.col_start, flags));
     PRC_CHECK_LAUNCH();
     size_t smem = (size_t)PULL_WARPS * g.n[2] * sizeof(double);
     if (smem > 48 * 1024) cudaFuncSetAttribute(paint_pull<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int64_t blocks = (ncol + PULL_WARPS - 1) / PULL_WARPS;
     int grid = (int)std::min<int64_t>(blocks, (int64_t)device_sm_count() * 16);
     Dims dims = {{g.n[0], g.n[1], g.n[2]}};
-    paint_pull<F><<<grid, PULL_WARPS * 32, smem, st>>>(keys, pl, ws.col_start, dims, accumulate, mesh, colsums, flags);
+    PRC_LAUNCH_B("paint_pull", st, (double)n * (4 + sizeof(Payload<F>)) + 4.0 * ncol + 8.0 * (accumulate ? 2 : 1) * ncol * g.n[2] + 8.0 * ncol, paint_pull<F><<<grid, PULL_WARPS * 32, smem, st>>>(keys, pl, ws.col_start, dims, accumulate, mesh, colsums, flags));
     PRC_CHECK_LAUNCH();
     return PRC_OK;
 }
@@ -790,10 +790,15 @@ int read_shifts_launch(const F* m0, const F* m1, const F* m2, bool phi, const Bo
     if (los)
         for (int a = 0; a < 3; a++) l[a] = los[a];
     int grid = particle_grid(n);
-#define LAUNCH(O, PH)                                                                                            \
-    read_shifts_kernel<P, F, O, PH><<<grid, 256, 0, st>>>(m0, m1, m2, g, tc[0], tc[1], tc[2], (const P*)pos, n, f, \
-                                                          los != nullptr, l[0], l[1], l[2], field, shifted, wrap,  \
-                                                          (O*)out, flags)
+    // particles in and out, plus every mesh cell the gathers touch (at most 8 or 32 per particle)
+    const double ncell = (double)g.n[0] * g.n[1] * g.n[2];
+    const double gather_bytes = (double)n * 3 * (sizeof(P) + ob) +
+                                (phi ? std::min(ncell, 32.0 * n) : 3 * std::min(ncell, 8.0 * n)) * sizeof(F);
+#define LAUNCH(O, PH)                                                                                              \
+    PRC_LAUNCH_B(PH ? "read_shifts_phi" : "read_shifts_psi", st, gather_bytes,                                                     \
+               read_shifts_kernel<P, F, O, PH><<<grid, 256, 0, st>>>(m0, m1, m2, g, tc[0], tc[1], tc[2], (const P*)pos, \
+                                                                     n, f, los != nullptr, l[0], l[1], l[2], field,   \
+                                                                     shifted, wrap, (O*)out, flags))
     if (phi) {
         if (ob == 4) LAUNCH(float, true); else LAUNCH(double, true);
     } else {
@@ -874,8 +879,8 @@ prc_status_t prc_sum_f64(const double* x, int64_t n, double* out, void* workspac
     if (!out || n < 0 || (n > 0 && !x)) return PRC_ERR_ARG;
     if (!workspace || workspace_bytes < prc_sum_workspace_bytes(n)) return PRC_ERR_WORKSPACE;
     cudaStream_t st = (cudaStream_t)stream;
-    sum_partials<<<SUM_BLOCKS, SUM_THREADS, 0, st>>>(x, n, (double*)workspace);
-    sum_final<<<1, SUM_THREADS, 0, st>>>((const double*)workspace, out);
+    PRC_LAUNCH("sum", st, sum_partials<<<SUM_BLOCKS, SUM_THREADS, 0, st>>>(x, n, (double*)workspace));
+    PRC_LAUNCH("sum", st, sum_final<<<1, SUM_THREADS, 0, st>>>((const double*)workspace, out));
     PRC_CHECK_LAUNCH();
     return PRC_OK;
 }
@@ -892,11 +897,11 @@ prc_status_t prc_sum_f64(const double* x, int64_t n, double* out, void* workspac
         if (npos == 0) return PRC_OK;                                                                              \
         BoxGeom g = make_geom(nmesh, boxsize, boxcenter);                                                          \
         if (pos_bytes == 4)                                                                                        \
-            read_cic_kernel<float, F><<<particle_grid(npos), 256, 0, st>>>(mesh, g, (const float*)positions, npos, \
-                                                                           wrap, (float*)out, flags);             \
+            PRC_LAUNCH("read_cic", st, read_cic_kernel<float, F><<<particle_grid(npos), 256, 0, st>>>(             \
+                                           mesh, g, (const float*)positions, npos, wrap, (float*)out, flags));      \
         else                                                                                                       \
-            read_cic_kernel<double, F><<<particle_grid(npos), 256, 0, st>>>(mesh, g, (const double*)positions,     \
-                                                                            npos, wrap, (double*)out, flags);     \
+            PRC_LAUNCH("read_cic", st, read_cic_kernel<double, F><<<particle_grid(npos), 256, 0, st>>>(            \
+                                           mesh, g, (const double*)positions, npos, wrap, (double*)out, flags));    \
         PRC_CHECK_LAUNCH();                                                                                        \
         return PRC_OK;                                                                                             \
     }
@@ -918,13 +923,13 @@ READ_CIC_IMPL(prc_read_cic_f64, double)
         F tc[3];                                                                                                   \
         twocell_of(g, tc);                                                                                         \
         if (pos_bytes == 4)                                                                                        \
-            read_fd_kernel<float, F><<<particle_grid(npos), 256, 0, st>>>(mesh, g, tc[0], tc[1], tc[2],            \
-                                                                          (const float*)positions, npos, wrap,    \
-                                                                          (float*)out, flags);                    \
+            PRC_LAUNCH("read_fd_cic", st, read_fd_kernel<float, F><<<particle_grid(npos), 256, 0, st>>>(           \
+                                              mesh, g, tc[0], tc[1], tc[2], (const float*)positions, npos, wrap,   \
+                                              (float*)out, flags));                                                \
         else                                                                                                       \
-            read_fd_kernel<double, F><<<particle_grid(npos), 256, 0, st>>>(mesh, g, tc[0], tc[1], tc[2],           \
-                                                                           (const double*)positions, npos, wrap,  \
-                                                                           (double*)out, flags);                  \
+            PRC_LAUNCH("read_fd_cic", st, read_fd_kernel<double, F><<<particle_grid(npos), 256, 0, st>>>(          \
+                                              mesh, g, tc[0], tc[1], tc[2], (const double*)positions, npos, wrap,  \
+                                              (double*)out, flags));                                               \
         PRC_CHECK_LAUNCH();                                                                                        \
         return PRC_OK;                                                                                             \
     }

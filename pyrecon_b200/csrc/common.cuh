@@ -129,4 +129,30 @@ __host__ __forceinline__ int ceil_div(int64_t a, int64_t b) { return (int)((a + 
 
 int device_sm_count();
 
+// Every kernel launch goes through PRC_LAUNCH: it counts launches (prc_launch_count) and, when
+// prc_profile_enable(1) is on, brackets the launch with CUDA events on its stream so the
+// per-kernel device time can be read back with prc_profile_collect.
+// `bytes` is the launch's compulsory DRAM traffic (what it must read and write at least), so
+// the profile reports achieved bandwidth against the HBM roofline.
+struct KernelScope {
+    KernelScope(const char* name, cudaStream_t st, double bytes = 0.);
+    ~KernelScope();
+    const char* name;
+    cudaStream_t st;
+    cudaEvent_t start;
+    double bytes;
+};
+
 }  // namespace prc
+
+#define PRC_LAUNCH(NAME, STREAM, ...)                 \
+    do {                                              \
+        ::prc::KernelScope _prc_scope(NAME, STREAM);  \
+        __VA_ARGS__;                                  \
+    } while (0)
+
+#define PRC_LAUNCH_B(NAME, STREAM, BYTES, ...)                 \
+    do {                                                       \
+        ::prc::KernelScope _prc_scope(NAME, STREAM, BYTES);    \
+        __VA_ARGS__;                                           \
+    } while (0)

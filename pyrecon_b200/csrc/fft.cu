@@ -647,7 +647,7 @@ template <typename T> struct FFTLaunch {
         cudaFuncSetAttribute(fft_z_r2c<T, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
         int64_t ntiles = ((rows + B - 1) / B) * nb;
-        fft_z_r2c<T, TIN><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(ri, so, nb, p.dims, p.rz, B);
+        PRC_LAUNCH_B("fft_z_r2c", st, (double)nb * rows * (p.dims.n[2] * sizeof(TIN) + p.nh * CS), fft_z_r2c<T, TIN><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(ri, so, nb, p.dims, p.rz, B));
         PRC_CHECK_LAUNCH();
         return PRC_OK;
     }
@@ -673,7 +673,7 @@ template <typename T> struct FFTLaunch {
         for (int i = 0; i < nb; i++) sp.p[i] = data[i];
         cudaFuncSetAttribute(fft_strided<T, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int64_t ntiles = (int64_t)s.outer * ((nh + B - 1) / B) * nb;
-        fft_strided<T, DIR><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(sp, nb, s, axis == 1 ? p.ry : p.rx, B);
+        PRC_LAUNCH_B((DIR < 0 ? (axis == 1 ? "fft_y_fwd" : "fft_x_fwd") : (axis == 1 ? "fft_y_inv" : "fft_x_inv")), st, 2.0 * nb * spectrum_elems(p) * CS, fft_strided<T, DIR><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(sp, nb, s, axis == 1 ? p.ry : p.rx, B));
         PRC_CHECK_LAUNCH();
         return PRC_OK;
     }
@@ -687,7 +687,7 @@ template <typename T> struct FFTLaunch {
         for (int i = 0; i < nin * op.nper; i++) so.p[i] = out[i];
         cudaFuncSetAttribute(fft_x_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int64_t ntiles = (int64_t)p.dims.n[1] * ((p.nh + B - 1) / B) * nin;
-        fft_x_fused<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, so, p.dims, p.rx, B, op);
+        PRC_LAUNCH_B("fft_x_kspace", st, (double)nin * (1 + op.nper) * spectrum_elems(p) * CS, fft_x_fused<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, so, p.dims, p.rx, B, op));
         PRC_CHECK_LAUNCH();
         return PRC_OK;
     }
@@ -703,7 +703,7 @@ template <typename T> struct FFTLaunch {
         cudaFuncSetAttribute(fft_z_c2r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
         int64_t ntiles = (rows + B - 1) / B;
-        fft_z_c2r<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, p.dims, p.rz, B, e);
+        PRC_LAUNCH_B("fft_z_c2r", st, (double)nin * rows * nh * CS + (double)rows * p.dims.n[2] * sizeof(T) * (e.type == EPI_STORE ? nin : (e.delta ? 2 : 1)), fft_z_c2r<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, p.dims, p.rz, B, e));
         PRC_CHECK_LAUNCH();
         return PRC_OK;
     }
@@ -827,12 +827,14 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
     Plan3 p;
     PRC_TRY(make_plan(nmesh, &p));
     const int nout = los ? 1 : 6;
+    // spectra: the forward transform + max(nout, 3) outputs (3 for the final displacements)
+    const int nspec = 1 + std::max(nout, 3);
     const size_t sb = spec_bytes<T>(p);
     const size_t mesh_b = ((size_t)p.dims.size() * sizeof(T) + 255) & ~(size_t)255;
-    if (!ws || wsb < (1 + nout) * sb + mesh_b) return PRC_ERR_WORKSPACE;
+    if (!ws || wsb < (size_t)nspec * sb + mesh_b) return PRC_ERR_WORKSPACE;
     cplx_t<T>* S[7];
-    for (int i = 0; i < 1 + nout; i++) S[i] = (cplx_t<T>*)((char*)ws + i * sb);
-    T* dreal = (T*)((char*)ws + (1 + nout) * sb);
+    for (int i = 0; i < nspec; i++) S[i] = (cplx_t<T>*)((char*)ws + i * sb);
+    T* dreal = (T*)((char*)ws + nspec * sb);
     KOp op;
     fill_kop_geometry(&op, p, boxsize, sizeof(T));
     if (los)

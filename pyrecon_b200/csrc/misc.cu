@@ -2,9 +2,51 @@
 #include "common.cuh"
 
 #include <algorithm>
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
 #include <math.h>
+#include <stdio.h>
+#include <string.h>
 
 namespace prc {
+
+// ---------------------------------------------------------------------------------------------
+// Launch counter and optional per-kernel event timing
+// ---------------------------------------------------------------------------------------------
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+std::atomic<int> g_profiling{0};
+struct TimedLaunch {
+    const char* name;
+    cudaEvent_t start, stop;
+    double bytes;
+};
+std::mutex g_mutex;
+std::vector<TimedLaunch> g_timed;
+}  // namespace
+
+KernelScope::KernelScope(const char* n, cudaStream_t s, double b) : name(n), st(s), start(nullptr), bytes(b) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (g_profiling.load(std::memory_order_relaxed)) {
+        if (cudaEventCreate(&start) == cudaSuccess) cudaEventRecord(start, st);
+        else start = nullptr;
+    }
+}
+
+KernelScope::~KernelScope() {
+    if (start == nullptr) return;
+    cudaEvent_t stop;
+    if (cudaEventCreate(&stop) != cudaSuccess) {
+        cudaEventDestroy(start);
+        return;
+    }
+    cudaEventRecord(stop, st);
+    std::lock_guard<std::mutex> lock(g_mutex);
+    g_timed.push_back({name, start, stop, bytes});
+}
 
 // mesh[ix, iy, iz] *= (ax[ix] + ay[iy] + az[iz])^exp, coords = az | ay | ax (src/mesh.c:327-365).
 template <typename T>
@@ -29,7 +71,7 @@ template <typename T> static int prod_sum(T* mesh, const int32_t shape[3], const
     Dims d = {{shape[0], shape[1], shape[2]}};
     if (d.size() <= 0) return PRC_ERR_ARG;
     int64_t blocks = std::min<int64_t>((d.size() + 255) / 256, (int64_t)device_sm_count() * 16);
-    prod_sum_kernel<T><<<(int)blocks, 256, 0, st>>>(mesh, d, coords, exp);
+    PRC_LAUNCH("prod_sum", st, prod_sum_kernel<T><<<(int)blocks, 256, 0, st>>>(mesh, d, coords, exp));
     PRC_CHECK_LAUNCH();
     return PRC_OK;
 }
@@ -50,6 +92,54 @@ const char* prc_status_string(prc_status_t status) {
         case PRC_ERR_TIMEOUT: return "device wait timed out";
         default: return "unknown status";
     }
+}
+
+unsigned long long prc_launch_count(void) { return prc::g_launches.load(); }
+
+void prc_profile_enable(int on) {
+    std::lock_guard<std::mutex> lock(prc::g_mutex);
+    for (auto& t : prc::g_timed) {
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.stop);
+    }
+    prc::g_timed.clear();
+    prc::g_profiling.store(on ? 1 : 0);
+}
+
+int prc_profile_collect(char* buf, size_t cap) {
+    struct Agg { long long n = 0; double ms = 0., bytes = 0.; };
+    std::map<std::string, Agg> agg;
+    {
+        std::lock_guard<std::mutex> lock(prc::g_mutex);
+        for (auto& t : prc::g_timed) {
+            float ms = 0.f;
+            if (cudaEventSynchronize(t.stop) == cudaSuccess && cudaEventElapsedTime(&ms, t.start, t.stop) == cudaSuccess) {
+                auto& a = agg[t.name];
+                a.n += 1;
+                a.ms += ms;
+                a.bytes += t.bytes;
+            }
+            cudaEventDestroy(t.start);
+            cudaEventDestroy(t.stop);
+        }
+        prc::g_timed.clear();
+    }
+    std::string out = "{";
+    bool first = true;
+    for (auto& kv : agg) {
+        char item[256];
+        snprintf(item, sizeof(item), "%s\"%s\": [%lld, %.6f, %.1f]", first ? "" : ", ", kv.first.c_str(), kv.second.n,
+                 kv.second.ms, kv.second.bytes);
+        out += item;
+        first = false;
+    }
+    out += "}";
+    if (buf && cap > 0) {
+        size_t n = std::min(cap - 1, out.size());
+        memcpy(buf, out.data(), n);
+        buf[n] = 0;
+    }
+    return (int)out.size() + 1;
 }
 
 prc_status_t prc_prod_sum_f32(float* mesh, const int32_t shape[3], const float* coords, int exp, void* stream) {

@@ -272,7 +272,7 @@ template <typename T> struct MGRunner {
         T* dst = tmp;
         if (niter == 0 && zero_first && cudaMemsetAsync(v, 0, N * sizeof(T), st) != cudaSuccess) return PRC_ERR_CUDA;
         for (int it = 0; it < niter; it++) {
-            jacobi_sweep<T, T><<<grid_for(N), 256, 0, st>>>(src, f, dst, s, (T)P.damping, zero_first && it == 0);
+            PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * ((zero_first && it == 0) ? 2 : 3), jacobi_sweep<T, T><<<grid_for(N), 256, 0, st>>>(src, f, dst, s, (T)P.damping, zero_first && it == 0));
             std::swap(src, dst);
         }
         if (src != v) cudaMemcpyAsync(v, src, N * sizeof(T), cudaMemcpyDeviceToDevice, st);
@@ -286,13 +286,13 @@ template <typename T> struct MGRunner {
         if (l + 1 < (int)L.size()) {
             Stencil<T> s = stencil(l);
             const int64_t N = L[l].size();
-            residual_kernel<T, T, T, T, T><<<grid_for(N), 256, 0, st>>>(v, f, B[l].r, s);
+            PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T), residual_kernel<T, T, T, T, T><<<grid_for(N), 256, 0, st>>>(v, f, B[l].r, s));
             Dims nf = {{L[l].n[0], L[l].n[1], L[l].n[2]}};
-            reduce_kernel<T, T, T><<<grid_for(L[l + 1].size()), 256, 0, st>>>(B[l].r, B[l + 1].f, nf);
+            PRC_LAUNCH_B("mg_reduce", st, (double)(N + L[l + 1].size()) * sizeof(T), reduce_kernel<T, T, T><<<grid_for(L[l + 1].size()), 256, 0, st>>>(B[l].r, B[l + 1].f, nf));
             PRC_CHECK_LAUNCH();
             PRC_TRY(vcycle(l + 1, B[l + 1].v, B[l + 1].f, true));
             Dims nc = {{L[l + 1].n[0], L[l + 1].n[1], L[l + 1].n[2]}};
-            prolong_kernel<T, T, T, true><<<grid_for(L[l + 1].size()), 256, 0, st>>>(B[l + 1].v, v, nc);
+            PRC_LAUNCH_B("mg_prolong_add", st, (double)(2 * N + L[l + 1].size()) * sizeof(T), prolong_kernel<T, T, T, true><<<grid_for(L[l + 1].size()), 256, 0, st>>>(B[l + 1].v, v, nc));
             PRC_CHECK_LAUNCH();
         }
         return jacobi(l, v, f, B[l].tmp, P.jn, false);
@@ -307,7 +307,7 @@ template <typename T> static int fmg_plain(MGRunner<T>& R, const T* f0, T* v0) {
     R.B[0].f = const_cast<T*>(f0);
     for (int l = 0; l + 1 < nl; l++) {
         Dims nf = {{R.L[l].n[0], R.L[l].n[1], R.L[l].n[2]}};
-        reduce_kernel<T, T, T><<<grid_for(R.L[l + 1].size()), 256, 0, st>>>(R.B[l].f, R.B[l + 1].f, nf);
+        PRC_LAUNCH_B("mg_reduce", st, (double)(R.L[l].size() + R.L[l + 1].size()) * sizeof(T), reduce_kernel<T, T, T><<<grid_for(R.L[l + 1].size()), 256, 0, st>>>(R.B[l].f, R.B[l + 1].f, nf));
     }
     PRC_CHECK_LAUNCH();
     // the FMG solution of level l lives in fmg_v[l]; level 0 writes straight into v0
@@ -317,7 +317,7 @@ template <typename T> static int fmg_plain(MGRunner<T>& R, const T* f0, T* v0) {
             if (cudaMemsetAsync(v, 0, R.L[l].size() * sizeof(T), st) != cudaSuccess) return PRC_ERR_CUDA;
         } else {
             Dims nc = {{R.L[l + 1].n[0], R.L[l + 1].n[1], R.L[l + 1].n[2]}};
-            prolong_kernel<T, T, T, false><<<grid_for(R.L[l + 1].size()), 256, 0, st>>>(R.B[l + 1].v, v, nc);
+            PRC_LAUNCH_B("mg_prolong", st, (double)(R.L[l].size() + R.L[l + 1].size()) * sizeof(T), prolong_kernel<T, T, T, false><<<grid_for(R.L[l + 1].size()), 256, 0, st>>>(R.B[l + 1].v, v, nc));
             PRC_CHECK_LAUNCH();
         }
         // V-cycles at level l use the coarser levels' v as scratch: keep this level's FMG
@@ -437,10 +437,10 @@ int run_mixed(const float* delta, float* phi, const int32_t nmesh[3], const Para
     R.P = P;
     R.st = st;
     const int64_t N0 = m.L[0].size();
-    convert_kernel<float, double><<<grid_for(N0), 256, 0, st>>>(delta, m.f64[0], N0);
+    PRC_LAUNCH_B("mg_convert", st, 12.0 * N0, convert_kernel<float, double><<<grid_for(N0), 256, 0, st>>>(delta, m.f64[0], N0));
     for (int l = 0; l + 1 < nl; l++) {
         Dims nf = {{m.L[l].n[0], m.L[l].n[1], m.L[l].n[2]}};
-        reduce_kernel<double, double, double><<<grid_for(m.L[l + 1].size()), 256, 0, st>>>(m.f64[l], m.f64[l + 1], nf);
+        PRC_LAUNCH_B("mg_reduce", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()), reduce_kernel<double, double, double><<<grid_for(m.L[l + 1].size()), 256, 0, st>>>(m.f64[l], m.f64[l + 1], nf));
     }
     PRC_CHECK_LAUNCH();
     for (int l = nl - 1; l >= 0; l--) {
@@ -449,22 +449,22 @@ int run_mixed(const float* delta, float* phi, const int32_t nmesh[3], const Para
             if (cudaMemsetAsync(m.v64[l], 0, N * 8, st) != cudaSuccess) return PRC_ERR_CUDA;
         } else {
             Dims nc = {{m.L[l + 1].n[0], m.L[l + 1].n[1], m.L[l + 1].n[2]}};
-            prolong_kernel<double, double, double, false><<<grid_for(m.L[l + 1].size()), 256, 0, st>>>(m.v64[l + 1],
-                                                                                                    m.v64[l], nc);
+            PRC_LAUNCH_B("mg_prolong", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()), prolong_kernel<double, double, double, false><<<grid_for(m.L[l + 1].size()), 256, 0, st>>>(m.v64[l + 1],
+                                                                                                    m.v64[l], nc));
         }
         Stencil<double> s64 = make_stencil<double>(m.L[l].n, P.boxsize, P.boxcenter, P.beta,
                                                    P.has_los ? P.los : nullptr);
         for (int it = 0; it < P.vn; it++) {
             // defect in FP64 (stored FP32 as the inner V-cycle's right-hand side)
-            residual_kernel<double, double, double, float, double><<<grid_for(N), 256, 0, st>>>(m.v64[l], m.f64[l],
-                                                                                            m.b32[l].f, s64);
+            PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N, residual_kernel<double, double, double, float, double><<<grid_for(N), 256, 0, st>>>(m.v64[l], m.f64[l],
+                                                                                            m.b32[l].f, s64));
             PRC_CHECK_LAUNCH();
             PRC_TRY(R.vcycle(l, m.b32[l].v, m.b32[l].f, true));
-            add_kernel<double, float><<<grid_for(N), 256, 0, st>>>(m.v64[l], m.b32[l].v, N);
+            PRC_LAUNCH_B("mg_correct_fp64", st, 20.0 * N, add_kernel<double, float><<<grid_for(N), 256, 0, st>>>(m.v64[l], m.b32[l].v, N));
             PRC_CHECK_LAUNCH();
         }
     }
-    convert_kernel<double, float><<<grid_for(N0), 256, 0, st>>>(m.v64[0], phi, N0);
+    PRC_LAUNCH_B("mg_convert", st, 12.0 * N0, convert_kernel<double, float><<<grid_for(N0), 256, 0, st>>>(m.v64[0], phi, N0));
     PRC_CHECK_LAUNCH();
     return PRC_OK;
 }
@@ -519,7 +519,8 @@ prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t n
         int n[3] = {nmesh[0], nmesh[1], nmesh[2]};                                                                   \
         Stencil<T> s = make_stencil<T>(n, boxsize, boxcenter, beta, los);                                            \
         int64_t N = (int64_t)n[0] * n[1] * n[2];                                                                     \
-        residual_kernel<T, T, T, T, T><<<grid_for(N), 256, 0, (cudaStream_t)stream>>>(v, f, r, s);                  \
+        PRC_LAUNCH("mg_residual", (cudaStream_t)stream,                                                              \
+                   residual_kernel<T, T, T, T, T><<<grid_for(N), 256, 0, (cudaStream_t)stream>>>(v, f, r, s));     \
         PRC_CHECK_LAUNCH();                                                                                          \
         return PRC_OK;                                                                                               \
     }                                                                                                                \
@@ -527,7 +528,8 @@ prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t n
         if (!fine || !coarse || !nf) return PRC_ERR_ARG;                                                             \
         Dims d = {{nf[0], nf[1], nf[2]}};                                                                            \
         int64_t N = (int64_t)(nf[0] / 2) * (nf[1] / 2) * (nf[2] / 2);                                                \
-        reduce_kernel<T, T, T><<<grid_for(N), 256, 0, (cudaStream_t)stream>>>(fine, coarse, d);                    \
+        PRC_LAUNCH("mg_reduce", (cudaStream_t)stream,                                                                \
+                   reduce_kernel<T, T, T><<<grid_for(N), 256, 0, (cudaStream_t)stream>>>(fine, coarse, d));       \
         PRC_CHECK_LAUNCH();                                                                                          \
         return PRC_OK;                                                                                               \
     }                                                                                                                \
@@ -535,7 +537,8 @@ prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t n
         if (!fine || !coarse || !nc) return PRC_ERR_ARG;                                                             \
         Dims d = {{nc[0], nc[1], nc[2]}};                                                                            \
         int64_t N = (int64_t)nc[0] * nc[1] * nc[2];                                                                  \
-        prolong_kernel<T, T, T, false><<<grid_for(N), 256, 0, (cudaStream_t)stream>>>(coarse, fine, d);             \
+        PRC_LAUNCH("mg_prolong", (cudaStream_t)stream,                                                               \
+                   prolong_kernel<T, T, T, false><<<grid_for(N), 256, 0, (cudaStream_t)stream>>>(coarse, fine, d)); \
         PRC_CHECK_LAUNCH();                                                                                          \
         return PRC_OK;                                                                                               \
     }

@@ -62,7 +62,8 @@ def test_cell_order_bit_exact(nmesh, npos, pos_dtype, mesh_dtype, wrap):
     fl = flags()
     nm, bs, bc = L.i3(geom.nmesh), L.d3(geom.boxsize), L.d3(geom.boxcenter)
     w = ws(L.load().prc_assign_cic_workspace_bytes(nm, npos, np.dtype(mesh_dtype).itemsize))
-    L.call('prc_cic_cell_order', L.ptr(k), L.ptr(o), nm, bs, bc, np.dtype(mesh_dtype).itemsize, L.ptr(dev(pos)),
+    dpos = dev(pos)
+    L.call('prc_cic_cell_order', L.ptr(k), L.ptr(o), nm, bs, bc, np.dtype(mesh_dtype).itemsize, L.ptr(dpos),
            np.dtype(pos_dtype).itemsize, npos, int(wrap), L.ptr(fl), L.ptr(w), w.numel(), stream())
     assert int(fl.item()) == 0
     np.testing.assert_array_equal(k.cpu().numpy().view(np.uint32).astype('i8'), key[order])
@@ -79,7 +80,8 @@ def gpu_paint(pos, weights, geom, wrap=False, accumulate_into=None):
     nm, bs, bc = L.i3(geom.nmesh), L.d3(geom.boxsize), L.d3(geom.boxcenter)
     w = ws(L.load().prc_assign_cic_workspace_bytes(nm, len(pos), geom.dtype.itemsize))
     wt = dev(weights) if weights is not None else None
-    L.call('prc_assign_cic', L.ptr(mesh), L.ptr(colsums), nm, bs, bc, geom.dtype.itemsize, L.ptr(dev(pos)) if len(pos) else None,
+    dpos = dev(pos) if len(pos) else None
+    L.call('prc_assign_cic', L.ptr(mesh), L.ptr(colsums), nm, bs, bc, geom.dtype.itemsize, L.ptr(dpos),
            pos.dtype.itemsize, L.ptr(wt), 0 if weights is None else weights.dtype.itemsize, len(pos), int(wrap),
            int(accumulate_into is not None), L.ptr(fl), L.ptr(w), w.numel(), stream())
     return mesh, colsums, int(fl.item())
@@ -100,7 +102,7 @@ def test_paint_matches_oracle(mesh_dtype):
     m = mesh.cpu().numpy()
     tol = 1e-13 if mesh_dtype == 'f8' else 1e-6   # f4: CIC fractions computed in float, as the reference does
     assert maxrel(m, ref) < tol
-    np.testing.assert_allclose(colsums.cpu().numpy(), m.sum(axis=2), rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(colsums.cpu().numpy().reshape(m.shape[:2]), m.sum(axis=2), rtol=1e-12, atol=1e-9)
     # deterministic: a second run gives the same bits
     mesh2, _, _ = gpu_paint(pos, weights, geom)
     assert torch().equal(mesh, mesh2)
@@ -174,7 +176,8 @@ def test_fft_against_numpy(nmesh, dtype):
     spec = t.empty((nmesh[0], nmesh[1], nmesh[2] // 2 + 1), dtype=cdt, device='cuda')
     nm = L.i3(nmesh)
     sfx = L.suffix(dtype)
-    L.call('prc_rfft3d_' + sfx, L.ptr(dev(x)), np.dtype(dtype).itemsize, L.ptr(spec), nm, stream())
+    dx = dev(x)
+    L.call('prc_rfft3d_' + sfx, L.ptr(dx), np.dtype(dtype).itemsize, L.ptr(spec), nm, stream())
     tol = 1e-5 if dtype == 'f4' else 1e-13
     assert maxrel(spec.cpu().numpy(), ref) < tol
     back = t.empty(nmesh, dtype=t.float32 if dtype == 'f4' else t.float64, device='cuda')
@@ -219,7 +222,8 @@ def test_multigrid_components(los, dtype):
     sfx = L.suffix(dtype)
     r = t.empty(n, dtype=t.float32 if dtype == 'f4' else t.float64, device='cuda')
     los_arg = L.opt_d3(None if los is None else list(arr(los)))
-    L.call('prc_mg_residual_' + sfx, L.ptr(dev(v)), L.ptr(dev(f)), L.ptr(r), L.i3(n), L.d3(boxsize), L.d3(boxcenter),
+    dv0, df = dev(v), dev(f)     # keep the device copies alive until the kernels have run
+    L.call('prc_mg_residual_' + sfx, L.ptr(dv0), L.ptr(df), L.ptr(r), L.i3(n), L.d3(boxsize), L.d3(boxcenter),
            beta, los_arg, stream())
     tol = 1e-12 if dtype == 'f8' else 2e-5
     assert maxrel(r.cpu().numpy(), r_ref) < tol
@@ -231,7 +235,7 @@ def test_multigrid_components(los, dtype):
        ctypes.c_int(3), losp)
     dv = dev(v)
     scratch = t.empty_like(dv)
-    L.call('prc_mg_jacobi_' + sfx, L.ptr(dv), L.ptr(dev(f)), L.ptr(scratch), L.i3(n), L.d3(boxsize), L.d3(boxcenter),
+    L.call('prc_mg_jacobi_' + sfx, L.ptr(dv), L.ptr(df), L.ptr(scratch), L.i3(n), L.d3(boxsize), L.d3(boxcenter),
            beta, 0.4, 3, los_arg, stream())
     assert maxrel(dv.cpu().numpy(), vj) < tol
     # reduce / prolong
@@ -239,14 +243,15 @@ def test_multigrid_components(los, dtype):
     lib_o.oracle_mg_reduce(arr(v).ctypes.data_as(ctypes.c_void_p), c_ref.ctypes.data_as(ctypes.c_void_p),
                            nn.ctypes.data_as(ctypes.c_void_p))
     c = t.empty((8, 6, 10), dtype=r.dtype, device='cuda')
-    L.call('prc_mg_reduce_' + sfx, L.ptr(dev(v)), L.ptr(c), L.i3(n), stream())
+    L.call('prc_mg_reduce_' + sfx, L.ptr(dv0), L.ptr(c), L.i3(n), stream())
     assert maxrel(c.cpu().numpy(), c_ref) < tol
     p_ref = np.empty(n, dtype=dtype)
     nc = np.array([8, 6, 10], dtype='i8')
     lib_o.oracle_mg_prolong(c_ref.ctypes.data_as(ctypes.c_void_p), p_ref.ctypes.data_as(ctypes.c_void_p),
                             nc.ctypes.data_as(ctypes.c_void_p))
     pr = t.empty(n, dtype=r.dtype, device='cuda')
-    L.call('prc_mg_prolong_' + sfx, L.ptr(dev(c_ref)), L.ptr(pr), L.i3((8, 6, 10)), stream())
+    dc = dev(c_ref)
+    L.call('prc_mg_prolong_' + sfx, L.ptr(dc), L.ptr(pr), L.i3((8, 6, 10)), stream())
     assert maxrel(pr.cpu().numpy(), p_ref) < tol
 
 
@@ -259,8 +264,8 @@ def test_prod_sum(dtype):
     coords = rng.uniform(1., 2., sum(shape)).astype(dtype)
     ref = mesh.copy()
     pipeline._Kernels(dtype).prod_sum(ref.reshape(-1), shape, coords, -1)
-    d = dev(mesh)
-    L.call('prc_prod_sum_' + L.suffix(dtype), L.ptr(d), L.i3(shape), L.ptr(dev(coords)), -1, stream())
+    d, dc = dev(mesh), dev(coords)
+    L.call('prc_prod_sum_' + L.suffix(dtype), L.ptr(d), L.i3(shape), L.ptr(dc), -1, stream())
     assert maxrel(d.cpu().numpy(), ref) < (1e-15 if dtype == 'f8' else 1e-6)
 
 

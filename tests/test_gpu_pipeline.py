@@ -42,7 +42,7 @@ def test_f4_within_1e3_of_f8_oracle(name):
             g[k] = g[k].astype('f4')
     ref = run_oracle(g, dtype='f8')
     out, rec = run_gpu(g, dtype='f4')
-    assert maxrel(out['mesh_data'], ref['mesh_data']) < 1e-6
+    assert maxrel(out['mesh_data'], ref['mesh_data']) < 1e-5   # float index coordinates, as the reference's f4
     for k in ['shifted_data', 'shifted_randoms']:
         if k in ref:
             assert out[k].dtype == np.float32
