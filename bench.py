@@ -281,9 +281,12 @@ def run_gpu_arm(args, w):
     # --- device-resident timed region ---
     barrier()
     torch.cuda.synchronize(device)
-    launches0 = _lib.launch_count()
-    _lib.profile_enable(True)
     with ClockSampler(local_rank) as clocks:
+        time.sleep(1.0)                     # let nvidia-smi start sampling before the timed region
+        barrier()
+        torch.cuda.synchronize(device)
+        launches0 = _lib.launch_count()
+        _lib.profile_enable(True)
         total_ms, per_step = timed_loop(step, args.steps, device)
     prof = _lib.profile_collect()
     _lib.profile_enable(False)

@@ -19,7 +19,8 @@ BUILD = os.path.join(HERE, '_build')
 LIBDIR = os.path.join(HERE, 'lib')
 LIBNAME = 'libpyrecon_cuda.so'
 SOURCES = ['cic.cu', 'fft.cu', 'multigrid.cu', 'misc.cu']
-HEADERS = [os.path.join(CSRC, 'common.cuh'), os.path.join(ROOT, 'include', 'pyrecon_cuda.h')]
+HEADERS = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith('.cuh')) + \
+    [os.path.join(ROOT, 'include', 'pyrecon_cuda.h')]
 
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
@@ -62,7 +63,7 @@ def build(force=False, verbose=False, extra=()):
                 pass
     lib = library_path()
     if force or todo or _stale(lib, objs):
-        cmd = [NVCC] + ARCH + ['-shared', '-o', lib] + objs + ['-lcudart_static' if False else '-cudart', 'static']
+        cmd = [NVCC] + ARCH + ['-shared', '-o', lib] + objs + ['-cudart', 'static']
         subprocess.run(cmd, check=True)
         if verbose:
             print('built', lib)

@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <math.h>
 #include <string.h>
+#include <stdlib.h>
 
 namespace prc {
 
@@ -593,6 +594,8 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, in
     }
 }
 
+#include "fft_fast.cuh"
+
 // ---------------------------------------------------------------------------------------------
 // Host-side planning and launches
 // ---------------------------------------------------------------------------------------------
@@ -627,6 +630,140 @@ static int fft_grid(int64_t ntiles, int ctas_per_sm) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, cap));
 }
 
+static bool fast_len(int n) { return n >= 8 && n <= MAX_FFT_N && (n & (n - 1)) == 0; }
+
+// PRC_FFT_GENERIC=1 in the environment routes every size through the mixed-radix kernels
+// (the tests use it to keep that path checked on power-of-two sizes too).
+static bool getenv_generic() {
+    static int cached = -1;
+    if (cached < 0) {
+        const char* v = getenv("PRC_FFT_GENERIC");
+        cached = (v != nullptr && v[0] == '1') ? 1 : 0;
+    }
+    return cached == 1;
+}
+
+// Compile-time dispatch of a runtime power-of-two length onto F<N>::run(args...).
+template <template <int> class F, typename... A> static int dispatch_pow2(int n, A... a) {
+    switch (n) {
+        case 8: return F<8>::run(a...);
+        case 16: return F<16>::run(a...);
+        case 32: return F<32>::run(a...);
+        case 64: return F<64>::run(a...);
+        case 128: return F<128>::run(a...);
+        case 256: return F<256>::run(a...);
+        case 512: return F<512>::run(a...);
+        case 1024: return F<1024>::run(a...);
+        default: return PRC_ERR_UNSUPPORTED;
+    }
+}
+
+// Lines per strided tile: 64-byte rows (8 FP32 / 4 FP64 complex), at most 1024 threads.
+template <typename T, int N> struct StridedCfg {
+    static constexpr int B0 = sizeof(T) == 4 ? 8 : 4;
+    static constexpr int B = (N / 8) * B0 <= 1024 ? B0 : 1024 / (N / 8);
+    static constexpr int THREADS = (N / 8) * B;
+    static constexpr size_t SMEM = (size_t)(N + N * B) * sizeof(cplx_t<T>);
+};
+
+// Rows per z tile: about 256 threads.
+template <typename T, int M> struct RowCfg {
+    static constexpr int TL = M / 8;
+    static constexpr int ROWS = TL >= 256 ? 1 : 256 / TL;
+    static constexpr int THREADS = TL * ROWS;
+    static constexpr size_t SMEM = (size_t)(2 * M + ROWS * fast::row_stride(M)) * sizeof(cplx_t<T>);
+};
+
+static int fast_grid(int64_t ntiles, int threads) {
+    int per_sm = std::max(1, 2048 / threads);
+    int64_t cap = (int64_t)device_sm_count() * per_sm;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, cap));
+}
+
+template <typename T, int DIR> struct FastStrided {
+    template <int N> struct K {
+        static int run(Specs<cplx_t<T>> sp, int nb, Strided s, const char* name, double bytes, cudaStream_t st) {
+            typedef StridedCfg<T, N> cfg;
+            auto kern = fast::strided<T, N, cfg::B, DIR>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
+            int64_t ntiles = (int64_t)s.outer * ((s.ncols + cfg::B - 1) / cfg::B) * nb;
+            PRC_LAUNCH_B(name, st, bytes, kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(sp, nb, s));
+            PRC_CHECK_LAUNCH();
+            return PRC_OK;
+        }
+    };
+};
+
+template <typename T> struct FastX {
+    template <int N> struct K {
+        template <int KT>
+        static int go(Specs<cplx_t<T>> si, int nin, Specs<cplx_t<T>> so, Dims dims, KOp op, double bytes,
+                      cudaStream_t st) {
+            typedef StridedCfg<T, N> cfg;
+            auto kern = fast::x_kspace<T, N, cfg::B, KT>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
+            const int nh = dims.n[2] / 2 + 1;
+            int64_t ntiles = (int64_t)dims.n[1] * ((nh + cfg::B - 1) / cfg::B) * nin;
+            PRC_LAUNCH_B("fft_x_kspace", st, bytes,
+                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(si, nin, so, dims, op));
+            PRC_CHECK_LAUNCH();
+            return PRC_OK;
+        }
+        static int run(Specs<cplx_t<T>> si, int nin, Specs<cplx_t<T>> so, Dims dims, KOp op, double bytes,
+                       cudaStream_t st) {
+            switch (op.type) {
+                case KOP_GAUSS: return go<KOP_GAUSS>(si, nin, so, dims, op, bytes, st);
+                case KOP_PP: return go<KOP_PP>(si, nin, so, dims, op, bytes, st);
+                case KOP_ITER_GLOBAL: return go<KOP_ITER_GLOBAL>(si, nin, so, dims, op, bytes, st);
+                case KOP_ITER_LOCAL: return go<KOP_ITER_LOCAL>(si, nin, so, dims, op, bytes, st);
+                case KOP_PSI: return go<KOP_PSI>(si, nin, so, dims, op, bytes, st);
+                default: return go<KOP_IDENTITY>(si, nin, so, dims, op, bytes, st);
+            }
+        }
+    };
+};
+
+template <typename T, typename TIN> struct FastZR2C {
+    template <int M> struct K {
+        static int run(RealsIn ri, Specs<cplx_t<T>> so, int nb, int64_t rows, double bytes, cudaStream_t st) {
+            typedef RowCfg<T, M> cfg;
+            auto kern = fast::z_r2c<T, TIN, M, cfg::ROWS>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
+            int64_t ntiles = ((rows + cfg::ROWS - 1) / cfg::ROWS) * nb;
+            PRC_LAUNCH_B("fft_z_r2c", st, bytes,
+                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(ri, so, nb, rows));
+            PRC_CHECK_LAUNCH();
+            return PRC_OK;
+        }
+    };
+};
+
+template <typename T> struct FastZC2R {
+    template <int M> struct K {
+        static int run(Specs<cplx_t<T>> si, int nin, Dims dims, Epi<T> e, double bytes, cudaStream_t st) {
+            switch (e.type) {
+                case EPI_DENSITY: return go<EPI_DENSITY>(si, nin, dims, e, bytes, st);
+                case EPI_DENSITY_NORANDOMS: return go<EPI_DENSITY_NORANDOMS>(si, nin, dims, e, bytes, st);
+                case EPI_ITER_GLOBAL: return go<EPI_ITER_GLOBAL>(si, nin, dims, e, bytes, st);
+                case EPI_ITER_LOCAL: return go<EPI_ITER_LOCAL>(si, nin, dims, e, bytes, st);
+                default: return go<EPI_STORE>(si, nin, dims, e, bytes, st);
+            }
+        }
+        template <int ET>
+        static int go(Specs<cplx_t<T>> si, int nin, Dims dims, Epi<T> e, double bytes, cudaStream_t st) {
+            typedef RowCfg<T, M> cfg;
+            auto kern = fast::z_c2r<T, M, cfg::ROWS, ET>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
+            int64_t rows = (int64_t)dims.n[0] * dims.n[1];
+            int64_t ntiles = (rows + cfg::ROWS - 1) / cfg::ROWS;
+            PRC_LAUNCH_B("fft_z_c2r", st, bytes,
+                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(si, nin, dims, e));
+            PRC_CHECK_LAUNCH();
+            return PRC_OK;
+        }
+    };
+};
+
 template <typename T> struct FFTLaunch {
     typedef cplx_t<T> C;
     static constexpr size_t CS = sizeof(C);
@@ -634,6 +771,17 @@ template <typename T> struct FFTLaunch {
 
     template <typename TIN>
     static int z_r2c(const Plan3& p, const void* const* in, C* const* out, int nb, cudaStream_t st) {
+        if (fast_len(p.dims.n[2] / 2) && !getenv_generic()) {
+            RealsIn ri;
+            Specs<C> so;
+            for (int i = 0; i < nb; i++) {
+                ri.p[i] = in[i];
+                so.p[i] = out[i];
+            }
+            int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
+            double bytes = (double)nb * rows * (p.dims.n[2] * sizeof(TIN) + p.nh * CS);
+            return dispatch_pow2<FastZR2C<T, TIN>::template K>(p.dims.n[2] / 2, ri, so, nb, rows, bytes, st);
+        }
         const int M = p.dims.n[2] / 2;
         int B = 16;
         while (B > 1 && (size_t)(2 * (M + 1) * (B + 1) + p.dims.n[2]) * CS > BUDGET) B >>= 1;
@@ -653,6 +801,28 @@ template <typename T> struct FFTLaunch {
     }
 
     template <int DIR> static int strided(const Plan3& p, int axis, C* const* data, int nb, cudaStream_t st) {
+        const int nline = axis == 1 ? p.dims.n[1] : p.dims.n[0];
+        if (fast_len(nline) && !getenv_generic()) {
+            Strided s;
+            const int nh = p.nh;
+            if (axis == 1) {
+                s.n = p.dims.n[1];
+                s.ls = nh;
+                s.outer = p.dims.n[0];
+                s.os = (int64_t)p.dims.n[1] * nh;
+            } else {
+                s.n = p.dims.n[0];
+                s.ls = (int64_t)p.dims.n[1] * nh;
+                s.outer = p.dims.n[1];
+                s.os = nh;
+            }
+            s.ncols = nh;
+            Specs<C> sp;
+            for (int i = 0; i < nb; i++) sp.p[i] = data[i];
+            const char* name = DIR < 0 ? (axis == 1 ? "fft_y_fwd" : "fft_x_fwd") : (axis == 1 ? "fft_y_inv" : "fft_x_inv");
+            double bytes = 2.0 * nb * spectrum_elems(p) * CS;
+            return dispatch_pow2<FastStrided<T, DIR>::template K>(nline, sp, nb, s, name, bytes, st);
+        }
         Strided s;
         const int nh = p.nh;
         if (axis == 1) {
@@ -680,6 +850,13 @@ template <typename T> struct FFTLaunch {
 
     static int x_fused(const Plan3& p, C* const* in, int nin, C* const* out, const KOp& op, cudaStream_t st) {
         const int n0 = p.dims.n[0];
+        if (fast_len(n0) && !getenv_generic()) {
+            Specs<C> si, so;
+            for (int i = 0; i < nin; i++) si.p[i] = in[i];
+            for (int i = 0; i < nin * op.nper; i++) so.p[i] = out[i];
+            double bytes = (double)nin * (1 + op.nper) * spectrum_elems(p) * CS;
+            return dispatch_pow2<FastX<T>::template K>(n0, si, nin, so, p.dims, op, bytes, st);
+        }
         int B = choose_B(n0, 3, CS, BUDGET - n0 * CS, 16);
         size_t smem = (size_t)(3 * n0 * B + n0) * CS;
         Specs<C> si, so;
@@ -694,6 +871,14 @@ template <typename T> struct FFTLaunch {
 
     static int z_c2r(const Plan3& p, C* const* in, int nin, const Epi<T>& e, cudaStream_t st) {
         const int M = p.dims.n[2] / 2, nh = M + 1;
+        if (fast_len(M) && !getenv_generic()) {
+            Specs<C> si;
+            for (int i = 0; i < nin; i++) si.p[i] = in[i];
+            int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
+            double bytes = (double)nin * rows * nh * CS +
+                           (double)rows * p.dims.n[2] * sizeof(T) * (e.type == EPI_STORE ? nin : (e.delta ? 2 : 1));
+            return dispatch_pow2<FastZC2R<T>::template K>(M, si, nin, p.dims, e, bytes, st);
+        }
         int B = 16;
         auto need = [&](int b) { return (size_t)(2 * nh * (b + 1) + nin * M * b + p.dims.n[2]) * CS; };
         while (B > 1 && need(B) > BUDGET) B >>= 1;

@@ -205,11 +205,15 @@ class Particles(object):
         return self.np_dtype.itemsize
 
     def output(self, t):
-        """Return a device result in the caller's container type."""
+        """Return a device result in the caller's container type (host tensors: pinned memory)."""
         if self.kind == 'numpy':
             return t.cpu().numpy()
         if self.host_device is not None and self.host_device.type != 'cuda':
-            return t.to(self.host_device)
+            torch = _torch()
+            out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            out.copy_(t, non_blocking=True)
+            torch.cuda.current_stream(t.device).synchronize()
+            return out
         return t
 
 

@@ -280,3 +280,66 @@ def test_sum_deterministic():
     o = out.cpu().numpy()
     assert o[0] == o[1]
     assert abs(o[0] - x.double().sum().item()) < 1e-9
+
+
+def _smooth(dtype, mesh, nmesh, boxsize, radius):
+    L = lib()
+    t = torch()
+    nm = L.i3(nmesh)
+    w = ws(L.load().prc_fft_workspace_bytes(nm, np.dtype(dtype).itemsize, 1))
+    out = t.empty(nmesh, dtype=t.float32 if dtype == 'f4' else t.float64, device='cuda')
+    L.call('prc_smooth_gaussian_' + L.suffix(dtype), L.ptr(mesh), mesh.element_size(), L.ptr(out), nm,
+           L.d3(boxsize), L.d3(radius), L.ptr(w), w.numel(), stream())
+    return out.double().cpu().numpy()
+
+
+@pytest.mark.parametrize('nmesh', [(16, 16, 16), (32, 32, 32), (64, 32, 16), (24, 20, 18)])
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+@pytest.mark.parametrize('randoms', [True, False])
+def test_density_contrast_batched(nmesh, dtype, randoms):
+    """Data and randoms smoothed in one batched pass equal two separate smoothings + the formula
+    of set_density_contrast (pyrecon/recon.py:227-247)."""
+    L = lib()
+    t = torch()
+    rng = np.random.default_rng(11)
+    md = dev(rng.uniform(0.5, 1.5, nmesh))
+    mr = dev(rng.uniform(0.2, 1.8, nmesh))
+    sums = t.tensor([float(md.sum()), float(mr.sum())], dtype=t.float64, device='cuda')
+    boxsize, radius, bias, ran_min = [800., 700., 600.], [30.] * 3, 2., 0.01
+    ncell = int(np.prod(nmesh))
+    size_randoms = ran_min * float(mr.sum()) / 1.0   # threshold = 1.0: about half the cells masked
+    nm = L.i3(nmesh)
+    w = ws(L.load().prc_density_contrast_workspace_bytes(nm, np.dtype(dtype).itemsize, int(randoms)))
+    delta = t.empty(nmesh, dtype=t.float32 if dtype == 'f4' else t.float64, device='cuda')
+    L.call('prc_density_contrast_' + L.suffix(dtype), L.ptr(md), L.ptr(mr) if randoms else None, L.ptr(sums), nm,
+           L.d3(boxsize), L.d3(radius), bias, ran_min, size_randoms, L.ptr(delta), L.ptr(w), w.numel(), stream())
+    got = delta.double().cpu().numpy()
+    d = _smooth(dtype, md, nmesh, boxsize, radius)
+    s = sums.cpu().numpy()
+    if randoms:
+        r = _smooth(dtype, mr, nmesh, boxsize, radius)
+        alpha = s[0] / s[1]
+        threshold = ran_min * s[1] / size_randoms
+        mask = r > threshold
+        assert 0.1 < mask.mean() < 0.9
+        ref = np.where(mask, (d - alpha * r) / (bias * alpha * np.where(mask, r, 1.)), 0.)
+        ok = np.abs(r - threshold) > 1e-4      # cells on the threshold may flip between precisions
+    else:
+        ref = (d / (s[0] / ncell) - 1.) / bias
+        ok = np.ones(nmesh, dtype=bool)
+    tol = 2e-5 if dtype == 'f4' else 1e-12
+    assert np.abs(got - ref)[ok].max() < tol * max(np.abs(ref).max(), 1.)
+
+
+def test_generic_fft_path_on_power_of_two_sizes():
+    """The mixed-radix kernels also serve power-of-two sizes when forced (PRC_FFT_GENERIC=1)."""
+    import subprocess
+    import sys
+    import os
+    code = ("import sys; sys.path.insert(0, '.'); sys.path.insert(0, 'tests');"
+            "import test_gpu_kernels as T; T.test_fft_against_numpy((64, 32, 16), 'f4'); "
+            "T.test_fft_against_numpy((16, 16, 16), 'f8'); T.test_density_contrast_batched((32, 32, 32), 'f4', True)")
+    env = dict(os.environ, PRC_FFT_GENERIC='1')
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = subprocess.run([sys.executable, '-c', code], cwd=root, env=env, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
