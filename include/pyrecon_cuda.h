@@ -90,6 +90,22 @@ PRC_API prc_status_t prc_assign_cic(double *mesh, double *column_sums, const int
                             int weight_bytes, int64_t npos, int wrap, int accumulate,
                             int32_t *flags, void *workspace, size_t workspace_bytes, void *stream);
 
+/* Allocation-free variant of prc_assign_cic, with no counterpart in the reference.  For callers
+ * that cannot allocate device memory (no allocator of their own, or code running where a
+ * cudaMalloc is not allowed): it takes no workspace and calls no cudaMalloc / cudaFree; its
+ * scratch is a 17 MiB array in the library's own device memory (held on every GPU that loads
+ * the library until the process exits).  Same arguments, results and flags as prc_assign_cic
+ * (equal to it to FP64 rounding), but particles are painted in chunks of 2^18, each accumulated
+ * into the mesh.  Meshes with more than 2^20 (x, y) columns, or n2 > 4096, are rejected with
+ * PRC_ERR_UNSUPPORTED.  The first call on a device looks up the array's address (make it before
+ * any stream capture).  Every call shares the array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller. */
+PRC_API prc_status_t prc_assign_cic_noalloc(double *mesh, double *column_sums, const int32_t nmesh[3],
+                                            const double boxsize[3], const double boxcenter[3], int mesh_bytes,
+                                            const void *positions, int pos_bytes, const void *weights,
+                                            int weight_bytes, int64_t npos, int wrap, int accumulate,
+                                            int32_t *flags, void *stream);
+
 /* Base-cell keys and the stable order that sorts them (the permutation the paint uses):
  * keys_sorted[i] = key[order[i]], key = (ix * n1 + iy) * n2 + iz.  Exposed so the sort can be
  * checked bit for bit against a stable argsort. Uses the paint workspace. */

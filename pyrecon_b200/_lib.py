@@ -36,6 +36,7 @@ _SIGNATURES = {
     'prc_assign_cic_workspace_bytes': (c_size, [I3, c_i64, c_int]),
     'prc_assign_cic': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size, _p]),
     'prc_cic_cell_order': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, c_i64, c_int, _p, _p, c_size, _p]),
+    'prc_assign_cic_noalloc': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p]),
     'prc_sum_workspace_bytes': (c_size, [c_i64]),
     'prc_sum_f64': (c_int, [_p, c_i64, _p, _p, c_size, _p]),
     'prc_fft_workspace_bytes': (c_size, [I3, c_int, c_int]),

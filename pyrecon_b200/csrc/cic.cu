@@ -16,6 +16,8 @@
 #include <limits.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 namespace prc {
 
@@ -809,11 +811,94 @@ int read_shifts_launch(const F* m0, const F* m1, const F* m2, bool phi, const Bo
     return PRC_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Allocation-free paint: scratch in a file-scope device array
+// ---------------------------------------------------------------------------------------------
+// Particles are painted in chunks of at most NOALLOC_CHUNK (each chunk accumulates into the mesh,
+// so the scratch does not grow with the catalogue); meshes up to NOALLOC_MAX_COLUMNS (x, y)
+// columns.  The array lives in every GPU that loads this library until the process exits.
+constexpr int64_t NOALLOC_CHUNK = (int64_t)1 << 18;
+constexpr int64_t NOALLOC_MAX_COLUMNS = (int64_t)1 << 20;
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)17 << 20;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device.
+static void* noalloc_scratch_address() {
+    static std::mutex mu;
+    static std::map<int, void*> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return it->second;
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return nullptr;
+    cache[dev] = p;
+    return p;
+}
+
+template <typename P, typename F, typename W>
+int paint_noalloc(double* mesh, double* colsums, const BoxGeom& g, const P* pos, const W* w, int64_t n, int wrap,
+                  int accumulate, int32_t* flags, const PaintWs& ws, cudaStream_t st) {
+    // validate every particle first (raises flags; the painting kernels of all chunks then skip,
+    // leaving the mesh untouched as the single-call paint does)
+    for (int64_t off = 0; off < n; off += NOALLOC_CHUNK) {
+        const int64_t cnt = std::min(NOALLOC_CHUNK, n - off);
+        PRC_LAUNCH_B("paint_keys", st, (double)cnt * (3 * sizeof(P) + (w ? sizeof(W) : 0) + 8),
+                     paint_keys<P, F, W><<<particle_grid(cnt), 256, 0, st>>>(pos + 3 * off, w ? w + off : nullptr, cnt,
+                                                                            g, wrap, ws.k0, ws.v0, flags));
+        PRC_CHECK_LAUNCH();
+    }
+    if (n == 0) return paint_run<P, F, W>(mesh, colsums, g, pos, w, 0, wrap, accumulate, flags, ws, st);
+    for (int64_t off = 0; off < n; off += NOALLOC_CHUNK) {
+        const int64_t cnt = std::min(NOALLOC_CHUNK, n - off);
+        PRC_TRY((paint_run<P, F, W>(mesh, colsums, g, pos + 3 * off, w ? w + off : nullptr, cnt, wrap,
+                                    off == 0 ? accumulate : 1, flags, ws, st)));
+    }
+    return PRC_OK;
+}
+
+template <typename P, typename F>
+int paint_noalloc_w(double* mesh, double* colsums, const BoxGeom& g, const void* pos, const void* w, int wb, int64_t n,
+                    int wrap, int acc, int32_t* flags, const PaintWs& ws, cudaStream_t st) {
+    if (w == nullptr) return paint_noalloc<P, F, F>(mesh, colsums, g, (const P*)pos, (const F*)nullptr, n, wrap, acc, flags, ws, st);
+    if (wb == 4) return paint_noalloc<P, F, float>(mesh, colsums, g, (const P*)pos, (const float*)w, n, wrap, acc, flags, ws, st);
+    return paint_noalloc<P, F, double>(mesh, colsums, g, (const P*)pos, (const double*)w, n, wrap, acc, flags, ws, st);
+}
+
 }  // namespace prc
 
 using namespace prc;
 
 extern "C" {
+
+prc_status_t prc_assign_cic_noalloc(double* mesh, double* column_sums, const int32_t nmesh[3], const double boxsize[3],
+                                    const double boxcenter[3], int mesh_bytes, const void* positions, int pos_bytes,
+                                    const void* weights, int weight_bytes, int64_t npos, int wrap, int accumulate,
+                                    int32_t* flags, void* stream) {
+    if (!mesh || !valid_nmesh(nmesh) || !boxsize || !boxcenter || !flags || npos < 0) return PRC_ERR_ARG;
+    if (npos >= ((int64_t)1 << 32) || (npos > 0 && !positions)) return PRC_ERR_ARG;
+    if ((mesh_bytes != 4 && mesh_bytes != 8) || (pos_bytes != 4 && pos_bytes != 8)) return PRC_ERR_ARG;
+    if (weights && weight_bytes != 4 && weight_bytes != 8) return PRC_ERR_ARG;
+    if (nmesh[2] > 4096 || (int64_t)nmesh[0] * nmesh[1] > NOALLOC_MAX_COLUMNS) return PRC_ERR_UNSUPPORTED;
+    if (paint_layout(nmesh, std::min(npos, NOALLOC_CHUNK), mesh_bytes, nullptr, nullptr) > NOALLOC_SCRATCH_BYTES)
+        return PRC_ERR_UNSUPPORTED;
+    void* scratch = noalloc_scratch_address();
+    if (scratch == nullptr) return PRC_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    PaintWs ws;
+    paint_layout(nmesh, std::min(npos, NOALLOC_CHUNK), mesh_bytes, (char*)scratch, &ws);
+    BoxGeom g = make_geom(nmesh, boxsize, boxcenter);
+    if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return PRC_ERR_CUDA;
+    if (pos_bytes == 4 && mesh_bytes == 4)
+        return paint_noalloc_w<float, float>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st);
+    if (pos_bytes == 4 && mesh_bytes == 8)
+        return paint_noalloc_w<float, double>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st);
+    if (pos_bytes == 8 && mesh_bytes == 4)
+        return paint_noalloc_w<double, float>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st);
+    return paint_noalloc_w<double, double>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st);
+}
 
 size_t prc_assign_cic_workspace_bytes(const int32_t nmesh[3], int64_t npos, int mesh_bytes) {
     if (!valid_nmesh(nmesh) || npos < 0) return 0;
