@@ -146,14 +146,16 @@ PRC_API prc_status_t prc_read_finite_difference_cic_f64(const double *mesh, cons
  * term f (s.l) l with l = los (global, unit 3-vector) or p/|p| of the wrapped positions (los =
  * NULL), field selection and, if `shifted`, positions - shifts wrapped when `wrap`.
  * Replaces BaseReconstruction.read_shifts / read_shifted_positions (pyrecon/recon.py:255-325).
+ * psi_stride: 1 for three separate meshes, 4 for one interleaved (x, y, z, 0) mesh with
+ * psi_y = psi_x + 1, psi_z = psi_x + 2 (one vector load per CIC corner).
  * out is (npos, 3) in `out_bytes` precision. */
-PRC_API prc_status_t prc_read_shifts_psi_f32(const float *psi_x, const float *psi_y, const float *psi_z,
+PRC_API prc_status_t prc_read_shifts_psi_f32(const float *psi_x, const float *psi_y, const float *psi_z, int psi_stride,
                                      const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
                                      int64_t npos, double f, const double *los, int field, int shifted,
                                      int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
 PRC_API prc_status_t prc_read_shifts_psi_f64(const double *psi_x, const double *psi_y, const double *psi_z,
-                                     const int32_t nmesh[3], const double boxsize[3],
+                                     int psi_stride, const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
                                      int64_t npos, double f, const double *los, int field, int shifted,
                                      int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
@@ -212,14 +214,18 @@ PRC_API prc_status_t prc_density_contrast_f64(const double *mesh_data, const dou
                                       size_t workspace_bytes, void *stream);
 
 /* PlaneParallelFFTReconstruction.run (pyrecon/plane_parallel_fft.py:41-55):
- * psi_a = IFFT(i k_a delta_k / (k^2 (1 + beta mu^2))), los a unit 3-vector. */
+ * psi_a = IFFT(i k_a delta_k / (k^2 (1 + beta mu^2))), los a unit 3-vector.
+ * psi_stride (here and in prc_iterative_fft_*): 1 writes three separate meshes, 4 writes one
+ * interleaved (x, y, z, 0) mesh at psi_x (psi_y = psi_x + 1, psi_z = psi_x + 2, 16/32-byte aligned). */
 PRC_API size_t prc_plane_parallel_workspace_bytes(const int32_t nmesh[3], int mesh_bytes);
 PRC_API prc_status_t prc_plane_parallel_fft_f32(const float *delta, const int32_t nmesh[3], const double boxsize[3],
                                         double beta, const double los[3], float *psi_x, float *psi_y,
-                                        float *psi_z, void *workspace, size_t workspace_bytes, void *stream);
+                                        float *psi_z, int psi_stride, void *workspace, size_t workspace_bytes,
+                                        void *stream);
 PRC_API prc_status_t prc_plane_parallel_fft_f64(const double *delta, const int32_t nmesh[3], const double boxsize[3],
                                         double beta, const double los[3], double *psi_x, double *psi_y,
-                                        double *psi_z, void *workspace, size_t workspace_bytes, void *stream);
+                                        double *psi_z, int psi_stride, void *workspace, size_t workspace_bytes,
+                                        void *stream);
 
 /* IterativeFFTReconstruction.run (pyrecon/iterative_fft.py:12-82), niterations of the
  * Burden et al. 2015 field-level iteration then psi_a = IFFT(i k_a delta_k / k^2).
@@ -227,11 +233,11 @@ PRC_API prc_status_t prc_plane_parallel_fft_f64(const double *delta, const int32
 PRC_API size_t prc_iterative_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int local_los);
 PRC_API prc_status_t prc_iterative_fft_f32(const float *delta, const int32_t nmesh[3], const double boxsize[3],
                                    const double boxcenter[3], double beta, const double *los,
-                                   int niterations, float *psi_x, float *psi_y, float *psi_z,
+                                   int niterations, float *psi_x, float *psi_y, float *psi_z, int psi_stride,
                                    void *workspace, size_t workspace_bytes, void *stream);
 PRC_API prc_status_t prc_iterative_fft_f64(const double *delta, const int32_t nmesh[3], const double boxsize[3],
                                    const double boxcenter[3], double beta, const double *los,
-                                   int niterations, double *psi_x, double *psi_y, double *psi_z,
+                                   int niterations, double *psi_x, double *psi_y, double *psi_z, int psi_stride,
                                    void *workspace, size_t workspace_bytes, void *stream);
 
 /* Mirror of prod_sum (reference src/mesh.c:327-365): mesh *= (ax[i] + ay[j] + az[k])^exp on a

@@ -49,16 +49,16 @@ for _s in ['f32', 'f64']:
     _SIGNATURES.update({
         'prc_read_cic_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, c_int, _p, _p, _p]),
         'prc_read_finite_difference_cic_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, c_int, _p, _p, _p]),
-        'prc_read_shifts_psi_' + _s: (c_int, [_p, _p, _p, I3, D3, D3, _p, c_int, c_i64, c_double, DP, c_int, c_int,
-                                              c_int, _p, c_int, _p, _p]),
+        'prc_read_shifts_psi_' + _s: (c_int, [_p, _p, _p, c_int, I3, D3, D3, _p, c_int, c_i64, c_double, DP, c_int,
+                                              c_int, c_int, _p, c_int, _p, _p]),
         'prc_read_shifts_phi_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, c_double, DP, c_int, c_int, c_int, _p,
                                               c_int, _p, _p]),
         'prc_rfft3d_' + _s: (c_int, [_p, c_int, _p, I3, _p]),
         'prc_irfft3d_' + _s: (c_int, [_p, _p, I3, _p]),
         'prc_smooth_gaussian_' + _s: (c_int, [_p, c_int, _p, I3, D3, D3, _p, c_size, _p]),
         'prc_density_contrast_' + _s: (c_int, [_p, _p, _p, I3, D3, D3, c_double, c_double, c_double, _p, _p, c_size, _p]),
-        'prc_plane_parallel_fft_' + _s: (c_int, [_p, I3, D3, c_double, D3, _p, _p, _p, _p, c_size, _p]),
-        'prc_iterative_fft_' + _s: (c_int, [_p, I3, D3, D3, c_double, DP, c_int, _p, _p, _p, _p, c_size, _p]),
+        'prc_plane_parallel_fft_' + _s: (c_int, [_p, I3, D3, c_double, D3, _p, _p, _p, c_int, _p, c_size, _p]),
+        'prc_iterative_fft_' + _s: (c_int, [_p, I3, D3, D3, c_double, DP, c_int, _p, _p, _p, c_int, _p, c_size, _p]),
         'prc_prod_sum_' + _s: (c_int, [_p, I3, _p, c_int, _p]),
         'prc_mg_jacobi_' + _s: (c_int, [_p, _p, _p, I3, D3, D3, c_double, c_double, c_int, DP, _p]),
         'prc_mg_residual_' + _s: (c_int, [_p, _p, _p, I3, D3, D3, c_double, DP, _p]),

@@ -523,6 +523,33 @@ template <typename F> __device__ __forceinline__ F cic_read(const F* __restrict_
     return acc;
 }
 
+template <typename F> __device__ __forceinline__ typename vec4_of<F>::type load4(const typename vec4_of<F>::type* p);
+template <> __device__ __forceinline__ float4 load4<float>(const float4* p) { return __ldg(p); }
+template <> __device__ __forceinline__ double4 load4<double>(const double4* p) {
+    const double2* q = (const double2*)p;
+    const double2 a = __ldg(q), b = __ldg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// Same as cic_read for the three components of an interleaved (x, y, z, 0) mesh at once: one
+// vector load per corner, each component accumulated in the same order as cic_read.
+template <typename F>
+__device__ __forceinline__ void cic_read3(const typename vec4_of<F>::type* __restrict__ m, const Cic<F>& c,
+                                          const int n[3], F out[3]) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+        const typename vec4_of<F>::type v =
+            load4<F>(m + at3(n, cx ? c.hi[0] : c.lo[0], cy ? c.hi[1] : c.lo[1], cz ? c.hi[2] : c.lo[2]));
+        const F comp[3] = {v.x, v.y, v.z};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const F term = rn_mul(rn_mul(rn_mul(comp[a], c.w[0][cx]), c.w[1][cy]), c.w[2][cz]);
+            out[a] = k == 0 ? term : rn_add(out[a], term);
+        }
+    }
+}
+
 // Finite-difference gradient CIC read (src/mesh.c:187-266): corners in the order
 // 000, 100, 010, 001, 110, 101, 011, 111; divided by 2 * boxsize / n in F.
 template <typename F>
@@ -595,7 +622,7 @@ __global__ void __launch_bounds__(256) read_fd_kernel(const F* __restrict__ mesh
 // displacement read in F then cast to P (the shifts array has the positions' dtype); RSD in
 // R = promoted type of (shifts, los); result cast back to P; positions - shifts in P, then
 // wrapped in T = promote(P, F) when `wrap`; the output type O is chosen by the caller.
-template <typename P, typename F, typename O, bool PHI>
+template <typename P, typename F, typename O, bool PHI, bool IL>
 __global__ void __launch_bounds__(256) read_shifts_kernel(const F* __restrict__ m0, const F* __restrict__ m1,
                                                           const F* __restrict__ m2, BoxGeom g, F tc0, F tc1, F tc2,
                                                           const P* __restrict__ pos, int64_t n, double f,
@@ -617,6 +644,11 @@ __global__ void __launch_bounds__(256) read_shifts_kernel(const F* __restrict__ 
             if (PHI) {
                 F d[3] = {(F)NAN, (F)NAN, (F)NAN};
                 if (ok) fd_read(m0, c, g.n, twocell, d);
+#pragma unroll
+                for (int a = 0; a < 3; a++) s[a] = (P)d[a];
+            } else if (IL) {
+                F d[3] = {(F)NAN, (F)NAN, (F)NAN};
+                if (ok) cic_read3<F>((const typename vec4_of<F>::type*)m0, c, g.n, d);
 #pragma unroll
                 for (int a = 0; a < 3; a++) s[a] = (P)d[a];
             } else {
@@ -783,9 +815,12 @@ int paint_dispatch_w(double* mesh, double* colsums, const BoxGeom& g, const void
 }
 
 template <typename P, typename F>
-int read_shifts_launch(const F* m0, const F* m1, const F* m2, bool phi, const BoxGeom& g, const void* pos, int64_t n,
-                       double f, const double* los, int field, int shifted, int wrap, void* out, int ob, int32_t* flags,
-                       cudaStream_t st) {
+int read_shifts_launch(const F* m0, const F* m1, const F* m2, int stride, bool phi, const BoxGeom& g, const void* pos,
+                       int64_t n, double f, const double* los, int field, int shifted, int wrap, void* out, int ob,
+                       int32_t* flags, cudaStream_t st) {
+    const bool il = !phi && stride == 4;
+    if (il && (m1 != m0 + 1 || m2 != m0 + 2 || ((uintptr_t)m0 % (4 * sizeof(F))) != 0)) return PRC_ERR_ARG;
+    if (!phi && !il && stride != 1) return PRC_ERR_ARG;
     F tc[3];
     twocell_of(g, tc);
     double l[3] = {0, 0, 0};
@@ -796,15 +831,18 @@ int read_shifts_launch(const F* m0, const F* m1, const F* m2, bool phi, const Bo
     const double ncell = (double)g.n[0] * g.n[1] * g.n[2];
     const double gather_bytes = (double)n * 3 * (sizeof(P) + ob) +
                                 (phi ? std::min(ncell, 32.0 * n) : 3 * std::min(ncell, 8.0 * n)) * sizeof(F);
-#define LAUNCH(O, PH)                                                                                              \
-    PRC_LAUNCH_B(PH ? "read_shifts_phi" : "read_shifts_psi", st, gather_bytes,                                                     \
-               read_shifts_kernel<P, F, O, PH><<<grid, 256, 0, st>>>(m0, m1, m2, g, tc[0], tc[1], tc[2], (const P*)pos, \
-                                                                     n, f, los != nullptr, l[0], l[1], l[2], field,   \
-                                                                     shifted, wrap, (O*)out, flags))
+#define LAUNCH(O, PH, IL)                                                                                          \
+    PRC_LAUNCH_B(PH ? "read_shifts_phi" : "read_shifts_psi", st, gather_bytes,                                     \
+                 read_shifts_kernel<P, F, O, PH, IL><<<grid, 256, 0, st>>>(m0, m1, m2, g, tc[0], tc[1], tc[2],     \
+                                                                         (const P*)pos, n, f, los != nullptr, l[0], \
+                                                                         l[1], l[2], field, shifted, wrap,          \
+                                                                         (O*)out, flags))
     if (phi) {
-        if (ob == 4) LAUNCH(float, true); else LAUNCH(double, true);
+        if (ob == 4) LAUNCH(float, true, false); else LAUNCH(double, true, false);
+    } else if (il) {
+        if (ob == 4) LAUNCH(float, false, true); else LAUNCH(double, false, true);
     } else {
-        if (ob == 4) LAUNCH(float, false); else LAUNCH(double, false);
+        if (ob == 4) LAUNCH(float, false, false); else LAUNCH(double, false, false);
     }
 #undef LAUNCH
     PRC_CHECK_LAUNCH();
@@ -1022,7 +1060,7 @@ READ_CIC_IMPL(prc_read_cic_f64, double)
 READ_FD_IMPL(prc_read_finite_difference_cic_f32, float)
 READ_FD_IMPL(prc_read_finite_difference_cic_f64, double)
 
-#define READ_SHIFTS_IMPL(NAME, F, PHI, ARGS, M0, M1, M2)                                                           \
+#define READ_SHIFTS_IMPL(NAME, F, PHI, ARGS, M0, M1, M2, STRIDE)                                                           \
     prc_status_t NAME ARGS {                                                                                       \
         if (!M0 || !M1 || !M2 || !valid_nmesh(nmesh) || !boxsize || !boxcenter || !flags || npos < 0)             \
             return PRC_ERR_ARG;                                                                                    \
@@ -1034,33 +1072,33 @@ READ_FD_IMPL(prc_read_finite_difference_cic_f64, double)
         if (npos == 0) return PRC_OK;                                                                              \
         BoxGeom g = make_geom(nmesh, boxsize, boxcenter);                                                          \
         if (pos_bytes == 4)                                                                                        \
-            return read_shifts_launch<float, F>(M0, M1, M2, PHI, g, positions, npos, f, los, field, shifted, wrap, \
-                                                out, out_bytes, flags, st);                                       \
-        return read_shifts_launch<double, F>(M0, M1, M2, PHI, g, positions, npos, f, los, field, shifted, wrap,   \
-                                             out, out_bytes, flags, st);                                          \
+            return read_shifts_launch<float, F>(M0, M1, M2, STRIDE, PHI, g, positions, npos, f, los, field, shifted, \
+                                                wrap, out, out_bytes, flags, st);                                 \
+        return read_shifts_launch<double, F>(M0, M1, M2, STRIDE, PHI, g, positions, npos, f, los, field, shifted,  \
+                                             wrap, out, out_bytes, flags, st);                                    \
     }
 
 READ_SHIFTS_IMPL(prc_read_shifts_psi_f32, float, false,
-                 (const float* psi_x, const float* psi_y, const float* psi_z, const int32_t nmesh[3],
+                 (const float* psi_x, const float* psi_y, const float* psi_z, int psi_stride, const int32_t nmesh[3],
                   const double boxsize[3], const double boxcenter[3], const void* positions, int pos_bytes,
                   int64_t npos, double f, const double* los, int field, int shifted, int wrap, void* out,
                   int out_bytes, int32_t* flags, void* stream),
-                 psi_x, psi_y, psi_z)
+                 psi_x, psi_y, psi_z, psi_stride)
 READ_SHIFTS_IMPL(prc_read_shifts_psi_f64, double, false,
-                 (const double* psi_x, const double* psi_y, const double* psi_z, const int32_t nmesh[3],
+                 (const double* psi_x, const double* psi_y, const double* psi_z, int psi_stride, const int32_t nmesh[3],
                   const double boxsize[3], const double boxcenter[3], const void* positions, int pos_bytes,
                   int64_t npos, double f, const double* los, int field, int shifted, int wrap, void* out,
                   int out_bytes, int32_t* flags, void* stream),
-                 psi_x, psi_y, psi_z)
+                 psi_x, psi_y, psi_z, psi_stride)
 READ_SHIFTS_IMPL(prc_read_shifts_phi_f32, float, true,
                  (const float* phi, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
                   const void* positions, int pos_bytes, int64_t npos, double f, const double* los, int field,
                   int shifted, int wrap, void* out, int out_bytes, int32_t* flags, void* stream),
-                 phi, phi, phi)
+                 phi, phi, phi, 1)
 READ_SHIFTS_IMPL(prc_read_shifts_phi_f64, double, true,
                  (const double* phi, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
                   const void* positions, int pos_bytes, int64_t npos, double f, const double* los, int field,
                   int shifted, int wrap, void* out, int out_bytes, int32_t* flags, void* stream),
-                 phi, phi, phi)
+                 phi, phi, phi, 1)
 
 }  // extern "C"

@@ -55,6 +55,19 @@ template <typename C> __device__ __forceinline__ C cmul_i(C a, int dir) {
     return dir < 0 ? cmake<C>(a.y, -a.x) : cmake<C>(-a.y, a.x);
 }
 
+// Four-component vectors for interleaved (x, y, z, 0) meshes
+template <typename T> struct vec4_of;
+template <> struct vec4_of<float> { typedef float4 type; };
+template <> struct vec4_of<double> { typedef double4 type; };
+template <typename T> __host__ __device__ __forceinline__ typename vec4_of<T>::type make_vec4(T x, T y, T z) {
+    typename vec4_of<T>::type v;
+    v.x = x;
+    v.y = y;
+    v.z = z;
+    v.w = 0;
+    return v;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Mesh geometry passed by value to kernels
 // ---------------------------------------------------------------------------------------------

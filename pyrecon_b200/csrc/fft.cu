@@ -462,11 +462,12 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_x_fused(Specs<cplx_t<T>> in, 
 // ---------------------------------------------------------------------------------------------
 // z pass, inverse c2r, with real-space epilogues
 // ---------------------------------------------------------------------------------------------
-enum EpiType { EPI_STORE = 0, EPI_DENSITY = 1, EPI_DENSITY_NORANDOMS = 2, EPI_ITER_GLOBAL = 3, EPI_ITER_LOCAL = 4 };
+enum EpiType { EPI_STORE = 0, EPI_DENSITY = 1, EPI_DENSITY_NORANDOMS = 2, EPI_ITER_GLOBAL = 3, EPI_ITER_LOCAL = 4,
+               EPI_STORE4 = 5 };
 
 template <typename T> struct Epi {
     int type;
-    T* out[3];             // EPI_STORE: one output per input
+    T* out[3];             // EPI_STORE: one output per input; EPI_STORE4: out[0] = (N, 4) interleaved
     const T* delta;        // original density contrast (EPI_ITER_*)
     const double* sums;    // device {sum data, sum randoms} (EPI_DENSITY*)
     double scale;          // applied to every inverse-transformed value
@@ -576,6 +577,15 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, in
                     o[0] = v.x;
                     o[1] = v.y;
                 }
+            } else if (e.type == EPI_STORE4) {
+                T* o = e.out[0] + (row * n2 + 2 * m) * 4;
+                for (int i = 0; i < 3; i++) {
+                    const C v = acc[((int64_t)i * B + line) * M + m];
+                    o[i] = v.x;
+                    o[4 + i] = v.y;
+                }
+                o[3] = 0;
+                o[7] = 0;
             } else {
                 T vals[2 * MAX_BATCH];
                 for (int i = 0; i < nin; i++) {
@@ -658,9 +668,23 @@ template <template <int> class F, typename... A> static int dispatch_pow2(int n,
     }
 }
 
+// Tile shapes (tuning knobs, overridable at build time):
+//   PRC_STRIDED_B  columns per strided-pass tile in FP32 (FP64 uses half as many bytes' worth)
+//   PRC_KSPACE_B   columns per k-space tile in FP32
+//   PRC_ROW_THREADS target threads per z-pass CTA
+#ifndef PRC_STRIDED_B
+#define PRC_STRIDED_B 8
+#endif
+#ifndef PRC_KSPACE_B
+#define PRC_KSPACE_B 8
+#endif
+#ifndef PRC_ROW_THREADS
+#define PRC_ROW_THREADS 256
+#endif
+
 // Lines per strided tile: 64-byte rows (8 FP32 / 4 FP64 complex), at most 1024 threads.
 template <typename T, int N> struct StridedCfg {
-    static constexpr int B0 = sizeof(T) == 4 ? 8 : 4;
+    static constexpr int B0 = sizeof(T) == 4 ? PRC_STRIDED_B : PRC_STRIDED_B / 2;
     static constexpr int B = (N / 8) * B0 <= 1024 ? B0 : 1024 / (N / 8);
     static constexpr int THREADS = (N / 8) * B;
     static constexpr size_t SMEM = (size_t)(N + N * B) * sizeof(cplx_t<T>);
@@ -669,9 +693,9 @@ template <typename T, int N> struct StridedCfg {
 // Rows per z tile: about 256 threads.
 template <typename T, int M> struct RowCfg {
     static constexpr int TL = M / 8;
-    static constexpr int ROWS = TL >= 256 ? 1 : 256 / TL;
+    static constexpr int ROWS = TL >= PRC_ROW_THREADS ? 1 : PRC_ROW_THREADS / TL;
     static constexpr int THREADS = TL * ROWS;
-    static constexpr size_t SMEM = (size_t)(2 * M + ROWS * fast::row_stride(M)) * sizeof(cplx_t<T>);
+    static constexpr size_t SMEM = (size_t)(2 * M + 1 + ROWS * fast::row_stride(M)) * sizeof(cplx_t<T>);
 };
 
 static int fast_grid(int64_t ntiles, int threads) {
@@ -694,12 +718,20 @@ template <typename T, int DIR> struct FastStrided {
     };
 };
 
+// The k-space kernel keeps two 8-point sets per thread (the spectrum and one output).
+template <typename T, int N> struct KSpaceCfg {
+    static constexpr int B0 = sizeof(T) == 4 ? PRC_KSPACE_B : 4;
+    static constexpr int B = (N / 8) * B0 <= 1024 ? B0 : 1024 / (N / 8);
+    static constexpr int THREADS = (N / 8) * B;
+    static constexpr size_t SMEM = (size_t)(N + N * B) * sizeof(cplx_t<T>);
+};
+
 template <typename T> struct FastX {
     template <int N> struct K {
         template <int KT>
         static int go(Specs<cplx_t<T>> si, int nin, Specs<cplx_t<T>> so, Dims dims, KOp op, double bytes,
                       cudaStream_t st) {
-            typedef StridedCfg<T, N> cfg;
+            typedef KSpaceCfg<T, N> cfg;
             auto kern = fast::x_kspace<T, N, cfg::B, KT>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
             const int nh = dims.n[2] / 2 + 1;
@@ -746,6 +778,7 @@ template <typename T> struct FastZC2R {
                 case EPI_DENSITY_NORANDOMS: return go<EPI_DENSITY_NORANDOMS>(si, nin, dims, e, bytes, st);
                 case EPI_ITER_GLOBAL: return go<EPI_ITER_GLOBAL>(si, nin, dims, e, bytes, st);
                 case EPI_ITER_LOCAL: return go<EPI_ITER_LOCAL>(si, nin, dims, e, bytes, st);
+                case EPI_STORE4: return go<EPI_STORE4>(si, nin, dims, e, bytes, st);
                 default: return go<EPI_STORE>(si, nin, dims, e, bytes, st);
             }
         }
@@ -876,7 +909,8 @@ template <typename T> struct FFTLaunch {
             for (int i = 0; i < nin; i++) si.p[i] = in[i];
             int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
             double bytes = (double)nin * rows * nh * CS +
-                           (double)rows * p.dims.n[2] * sizeof(T) * (e.type == EPI_STORE ? nin : (e.delta ? 2 : 1));
+                           (double)rows * p.dims.n[2] * sizeof(T) *
+                               (e.type == EPI_STORE ? nin : (e.type == EPI_STORE4 ? 4 : (e.delta ? 2 : 1)));
             return dispatch_pow2<FastZC2R<T>::template K>(M, si, nin, p.dims, e, bytes, st);
         }
         int B = 16;
@@ -980,9 +1014,30 @@ static int density_impl(const double* md, const double* mr, const double* sums, 
     return FFTLaunch<T>::z_c2r(p, S, nb, e, st);
 }
 
+// Epilogue writing the three displacement meshes: separate (stride 1) or interleaved as
+// (x, y, z, 0) per cell (stride 4, psi_y = psi_x + 1, psi_z = psi_x + 2).
+template <typename T> static int psi_epilogue(T* px, T* py, T* pz, int stride, Epi<T>* e) {
+    *e = epi_default<T>();
+    if (stride == 1) {
+        e->type = EPI_STORE;
+        e->out[0] = px;
+        e->out[1] = py;
+        e->out[2] = pz;
+        return PRC_OK;
+    }
+    if (stride == 4 && py == px + 1 && pz == px + 2 && ((uintptr_t)px % (4 * sizeof(T))) == 0) {
+        e->type = EPI_STORE4;
+        e->out[0] = px;
+        return PRC_OK;
+    }
+    return PRC_ERR_ARG;
+}
+
 template <typename T>
 static int pp_impl(const T* delta, const int32_t nmesh[3], const double boxsize[3], double beta, const double los[3],
-                   T* px, T* py, T* pz, void* ws, size_t wsb, cudaStream_t st) {
+                   T* px, T* py, T* pz, int psi_stride, void* ws, size_t wsb, cudaStream_t st) {
+    Epi<T> e;
+    PRC_TRY(psi_epilogue(px, py, pz, psi_stride, &e));
     Plan3 p;
     PRC_TRY(make_plan(nmesh, &p));
     if (!ws || wsb < 4 * spec_bytes<T>(p)) return PRC_ERR_WORKSPACE;
@@ -998,17 +1053,15 @@ static int pp_impl(const T* delta, const int32_t nmesh[3], const double boxsize[
     for (int a = 0; a < 3; a++) op.los[a] = sizeof(T) == 4 ? (double)(float)los[a] : los[a];
     PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));
     PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, 3, st));
-    Epi<T> e = epi_default<T>();
-    e.out[0] = px;
-    e.out[1] = py;
-    e.out[2] = pz;
     return FFTLaunch<T>::z_c2r(p, S + 1, 3, e, st);
 }
 
 template <typename T>
 static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
-                     double beta, const double* los, int niter, T* px, T* py, T* pz, void* ws, size_t wsb,
-                     cudaStream_t st) {
+                     double beta, const double* los, int niter, T* px, T* py, T* pz, int psi_stride, void* ws,
+                     size_t wsb, cudaStream_t st) {
+    Epi<T> es;
+    PRC_TRY(psi_epilogue(px, py, pz, psi_stride, &es));
     Plan3 p;
     PRC_TRY(make_plan(nmesh, &p));
     const int nout = los ? 1 : 6;
@@ -1059,10 +1112,6 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
     op.nper = 3;
     PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));
     PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, 3, st));
-    Epi<T> es = epi_default<T>();
-    es.out[0] = px;
-    es.out[1] = py;
-    es.out[2] = pz;
     return FFTLaunch<T>::z_c2r(p, S + 1, 3, es, st);
 }
 
@@ -1171,17 +1220,17 @@ size_t prc_plane_parallel_workspace_bytes(const int32_t nmesh[3], int mesh_bytes
 }
 
 prc_status_t prc_plane_parallel_fft_f32(const float* delta, const int32_t nmesh[3], const double boxsize[3], double beta,
-                                        const double los[3], float* psi_x, float* psi_y, float* psi_z, void* workspace,
-                                        size_t workspace_bytes, void* stream) {
+                                        const double los[3], float* psi_x, float* psi_y, float* psi_z, int psi_stride,
+                                        void* workspace, size_t workspace_bytes, void* stream) {
     if (!delta || !geom_ok(nmesh, boxsize) || !los || !psi_x || !psi_y || !psi_z) return PRC_ERR_ARG;
-    return pp_impl<float>(delta, nmesh, boxsize, beta, los, psi_x, psi_y, psi_z, workspace, workspace_bytes,
+    return pp_impl<float>(delta, nmesh, boxsize, beta, los, psi_x, psi_y, psi_z, psi_stride, workspace, workspace_bytes,
                           (cudaStream_t)stream);
 }
 prc_status_t prc_plane_parallel_fft_f64(const double* delta, const int32_t nmesh[3], const double boxsize[3],
                                         double beta, const double los[3], double* psi_x, double* psi_y, double* psi_z,
-                                        void* workspace, size_t workspace_bytes, void* stream) {
+                                        int psi_stride, void* workspace, size_t workspace_bytes, void* stream) {
     if (!delta || !geom_ok(nmesh, boxsize) || !los || !psi_x || !psi_y || !psi_z) return PRC_ERR_ARG;
-    return pp_impl<double>(delta, nmesh, boxsize, beta, los, psi_x, psi_y, psi_z, workspace, workspace_bytes,
+    return pp_impl<double>(delta, nmesh, boxsize, beta, los, psi_x, psi_y, psi_z, psi_stride, workspace, workspace_bytes,
                            (cudaStream_t)stream);
 }
 
@@ -1194,21 +1243,21 @@ size_t prc_iterative_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes,
 
 prc_status_t prc_iterative_fft_f32(const float* delta, const int32_t nmesh[3], const double boxsize[3],
                                    const double boxcenter[3], double beta, const double* los, int niterations,
-                                   float* psi_x, float* psi_y, float* psi_z, void* workspace, size_t workspace_bytes,
-                                   void* stream) {
-    if (!delta || !geom_ok(nmesh, boxsize) || !boxcenter || niterations < 0 || !psi_x || !psi_y || !psi_z)
-        return PRC_ERR_ARG;
-    return iter_impl<float>(delta, nmesh, boxsize, boxcenter, beta, los, niterations, psi_x, psi_y, psi_z, workspace,
-                            workspace_bytes, (cudaStream_t)stream);
-}
-prc_status_t prc_iterative_fft_f64(const double* delta, const int32_t nmesh[3], const double boxsize[3],
-                                   const double boxcenter[3], double beta, const double* los, int niterations,
-                                   double* psi_x, double* psi_y, double* psi_z, void* workspace,
+                                   float* psi_x, float* psi_y, float* psi_z, int psi_stride, void* workspace,
                                    size_t workspace_bytes, void* stream) {
     if (!delta || !geom_ok(nmesh, boxsize) || !boxcenter || niterations < 0 || !psi_x || !psi_y || !psi_z)
         return PRC_ERR_ARG;
-    return iter_impl<double>(delta, nmesh, boxsize, boxcenter, beta, los, niterations, psi_x, psi_y, psi_z, workspace,
-                             workspace_bytes, (cudaStream_t)stream);
+    return iter_impl<float>(delta, nmesh, boxsize, boxcenter, beta, los, niterations, psi_x, psi_y, psi_z, psi_stride,
+                            workspace, workspace_bytes, (cudaStream_t)stream);
+}
+prc_status_t prc_iterative_fft_f64(const double* delta, const int32_t nmesh[3], const double boxsize[3],
+                                   const double boxcenter[3], double beta, const double* los, int niterations,
+                                   double* psi_x, double* psi_y, double* psi_z, int psi_stride, void* workspace,
+                                   size_t workspace_bytes, void* stream) {
+    if (!delta || !geom_ok(nmesh, boxsize) || !boxcenter || niterations < 0 || !psi_x || !psi_y || !psi_z)
+        return PRC_ERR_ARG;
+    return iter_impl<double>(delta, nmesh, boxsize, boxcenter, beta, los, niterations, psi_x, psi_y, psi_z, psi_stride,
+                             workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 }  // extern "C"

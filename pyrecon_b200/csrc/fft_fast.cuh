@@ -15,6 +15,12 @@
 //   row tiles (z passes): R rows, point k of row r at r * RS + k + k / 8 (one pad per 8 points).
 #pragma once
 
+// PRC_PREFETCH=1: strided and k-space kernels issue the next tile's loads before computing the
+// current one (register double buffering).
+#ifndef PRC_PREFETCH
+#define PRC_PREFETCH 1
+#endif
+
 namespace fast {
 
 constexpr int ilog8(int n) { return n >= 8 ? 1 + ilog8(n / 8) : 0; }
@@ -28,16 +34,61 @@ template <int N> struct Plan {
     static constexpr int NPASS = P8 + (REM > 1 ? 1 : 0);
 };
 
+// Twiddles of every pass in one table: pass P (radix R_P, sub-transform size NS_P = 8^P) owns
+// NS_P (R_P - 1) entries laid out [k][r - 1] = w_{NS_P R_P}^{r k}, so the lanes of a warp, which
+// differ in k, read addresses R_P - 1 complex apart (an odd pitch: no bank conflicts).  The sizes
+// telescope: the table has exactly N - 1 entries.
+template <int N> struct TwLayout {
+    static constexpr int radix(int P) { return P < Plan<N>::P8 ? 8 : Plan<N>::REM; }
+    static constexpr int offset(int P) {
+        int o = 0, ns = 1;
+        for (int q = 0; q < P; q++) {
+            o += ns * (radix(q) - 1);
+            ns *= radix(q);
+        }
+        return o;
+    }
+    static constexpr int SIZE = N - 1;
+};
+
+template <typename C, int N> __device__ void fill_pass_twiddles(C* tw) {
+    typedef decltype(C().x) T;
+    for (int idx = threadIdx.x; idx < TwLayout<N>::SIZE; idx += blockDim.x) {
+        int off = 0, ns = 1, R = 8;
+        for (int q = 0; q < Plan<N>::NPASS; q++) {
+            R = TwLayout<N>::radix(q);
+            if (idx < off + ns * (R - 1)) break;
+            off += ns * (R - 1);
+            ns *= R;
+        }
+        const int local = idx - off, k = local / (R - 1), r = local % (R - 1) + 1;
+        const int m = (r * k * (N / (ns * R))) & (N - 1);
+        double sn, cs;
+        sincospi(-2.0 * (double)m / (double)N, &sn, &cs);
+        tw[idx] = cmake<C>((T)cs, (T)sn);
+    }
+}
+
+// tw[m] = w_n^m = exp(-2 pi i m / n) for m < count.
+template <typename C> __device__ void fill_roots(C* tw, int count, int n) {
+    typedef decltype(C().x) T;
+    for (int m = threadIdx.x; m < count; m += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * (double)m / (double)n, &sn, &cs);
+        tw[m] = cmake<C>((T)cs, (T)sn);
+    }
+}
+
 template <typename C, int DIR, int R> __device__ __forceinline__ void dftR(C* u) {
     if constexpr (R == 8) dft8<C, DIR>(u);
     else if constexpr (R == 4) dft4<C, DIR>(u);
     else dft2<C, DIR>(u);
 }
 
-// One radix-R pass on the thread's 8 points (8 / R butterflies).  tw[m * TWS] = w_N^m.
-template <typename C, int N, int R, int NS, int DIR, int TWS>
+// One radix-R pass on the thread's 8 points (8 / R butterflies); tw = this pass's table.
+template <typename C, int N, int R, int NS, int DIR>
 __device__ __forceinline__ void pass_regs(C (&v)[8], int t, const C* __restrict__ tw) {
-    constexpr int T = N / 8, NB = 8 / R, TWSTEP = N / (NS * R);
+    constexpr int T = N / 8, NB = 8 / R;
 #pragma unroll
     for (int b = 0; b < NB; b++) {
         C u[R];
@@ -45,9 +96,10 @@ __device__ __forceinline__ void pass_regs(C (&v)[8], int t, const C* __restrict_
         for (int r = 0; r < R; r++) u[r] = v[b + r * NB];
         if constexpr (NS > 1) {
             const int k = (t + b * T) & (NS - 1);
+            const C* row = tw + k * (R - 1);
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                C w = tw[((r * k * TWSTEP) & (N - 1)) * TWS];
+                C w = row[r - 1];
                 if (DIR > 0) w = cconj(w);
                 u[r] = cmul(u[r], w);
             }
@@ -76,23 +128,24 @@ __device__ __forceinline__ void exchange(C (&v)[8], int t, C* s, const Addr& add
     __syncthreads();
 }
 
-template <typename C, int N, int DIR, int TWS, int P> struct Passes {
+template <typename C, int N, int DIR, int P> struct Passes {
     template <class Addr>
     static __device__ __forceinline__ void run(C (&v)[8], int t, C* s, const Addr& addr, const C* tw) {
-        constexpr int R = (P < Plan<N>::P8) ? 8 : Plan<N>::REM;
+        constexpr int R = TwLayout<N>::radix(P);
         constexpr int NS = ipow8(P);
-        pass_regs<C, N, R, NS, DIR, TWS>(v, t, tw);
+        pass_regs<C, N, R, NS, DIR>(v, t, tw + TwLayout<N>::offset(P));
         if constexpr (P + 1 < Plan<N>::NPASS) {
             exchange<C, N, R, NS>(v, t, s, addr);
-            Passes<C, N, DIR, TWS, P + 1>::run(v, t, s, addr, tw);
+            Passes<C, N, DIR, P + 1>::run(v, t, s, addr, tw);
         }
     }
 };
 
-// In: v[i] = x[t + i T].  Out: v[i] = X[t + i T] (unnormalised DFT, sign DIR).
-template <typename C, int N, int DIR, int TWS = 1, class Addr>
+// In: v[i] = x[t + i T].  Out: v[i] = X[t + i T] (unnormalised DFT, sign DIR).  tw: the pass
+// table filled by fill_pass_twiddles<C, N>.
+template <typename C, int N, int DIR, class Addr>
 __device__ __forceinline__ void fft_regs(C (&v)[8], int t, C* s, const Addr& addr, const C* tw) {
-    Passes<C, N, DIR, TWS, 0>::run(v, t, s, addr, tw);
+    Passes<C, N, DIR, 0>::run(v, t, s, addr, tw);
 }
 
 struct ColAddr {
@@ -117,26 +170,54 @@ __global__ void __launch_bounds__(N / 8 * B) strided(Specs<cplx_t<T>> data, int 
     extern __shared__ unsigned char smem_raw[];
     C* tw = (C*)smem_raw;
     C* buf = tw + N;
-    fill_twiddles(tw, N);
+    fill_pass_twiddles<C, N>(tw);
     __syncthreads();
     const int col = threadIdx.x % B, t = threadIdx.x / B;
     const ColAddr addr{B, col};
     const int ctiles = (s.ncols + B - 1) / B;
     const int64_t tiles_per = (int64_t)s.outer * ctiles;
     const int64_t ntiles = tiles_per * nbatch;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    auto locate = [&](int64_t tile, bool& ok) {
         const int bi = (int)(tile / tiles_per);
         const int64_t r = tile % tiles_per;
         const int o = (int)(r / ctiles), c0 = (int)(r % ctiles) * B;
-        const bool ok = c0 + col < s.ncols;
-        C* g = data.p[bi] + (int64_t)o * s.os + c0 + col;
-        C v[8];
+        ok = c0 + col < s.ncols;
+        return data.p[bi] + (int64_t)o * s.os + c0 + col;
+    };
+    C v[8];
+    bool ok = false;
+    C* g = nullptr;
+    if (blockIdx.x < ntiles) {
+        g = locate(blockIdx.x, ok);
 #pragma unroll
         for (int i = 0; i < 8; i++) v[i] = ok ? g[(int64_t)(t + i * TL) * s.ls] : cmake<C>(0, 0);
+    }
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t next = tile + gridDim.x;
+        bool nok = false;
+        C* ng = nullptr;
+        C nv[8];
+        if (PRC_PREFETCH && next < ntiles) {
+            ng = locate(next, nok);
+#pragma unroll
+            for (int i = 0; i < 8; i++) nv[i] = nok ? ng[(int64_t)(t + i * TL) * s.ls] : cmake<C>(0, 0);
+        }
         fft_regs<C, N, DIR>(v, t, buf, addr, tw);
         if (ok) {
 #pragma unroll
             for (int i = 0; i < 8; i++) g[(int64_t)(t + i * TL) * s.ls] = v[i];
+        }
+        if (next < ntiles) {
+            if (PRC_PREFETCH) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) v[i] = nv[i];
+                g = ng;
+                ok = nok;
+            } else {
+                g = locate(next, ok);
+#pragma unroll
+                for (int i = 0; i < 8; i++) v[i] = ok ? g[(int64_t)(t + i * TL) * s.ls] : cmake<C>(0, 0);
+            }
         }
     }
 }
@@ -207,15 +288,35 @@ __device__ __forceinline__ void kmult(const KOp& op, int o, int ix, int iy, int 
     }
 }
 
+// Per-point quantities of the multiplier that do not depend on the output: computed once after the
+// forward x transform and reused by every output (one division per point instead of one per
+// point and output).
+template <typename T, int KT> struct KPoint {
+    T a, b;        // GAUSS: a = exp(...) * norm; PP: a = 1/(k^2 + beta (k.l)^2), b = same at k~;
+                   // ITER_*, PSI: a = norm / k^2 (0 at k = 0)
+};
+
+// Blocks per SM requested from the register allocator for the FP32 k-space and c2r kernels
+// (tuning knobs PRC_KSPACE_MINB / PRC_C2R_MINB; 1 leaves the allocator free).
+#ifndef PRC_KSPACE_MINB
+#define PRC_KSPACE_MINB 1
+#endif
+#ifndef PRC_C2R_MINB
+#define PRC_C2R_MINB 2
+#endif
+template <typename T, int THREADS, int MINB> struct MinBlocks {
+    static constexpr int value = (sizeof(T) == 4 && THREADS * MINB <= 2048) ? MINB : 1;
+};
+
 template <typename T, int N, int B, int KT>
-__global__ void __launch_bounds__(N / 8 * B) x_kspace(Specs<cplx_t<T>> in, int nin, Specs<cplx_t<T>> out, Dims dims,
+__global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE_MINB>::value)) x_kspace(Specs<cplx_t<T>> in, int nin, Specs<cplx_t<T>> out, Dims dims,
                                                       KOp op) {
     typedef cplx_t<T> C;
     constexpr int TL = N / 8;
     extern __shared__ unsigned char smem_raw[];
     C* tw = (C*)smem_raw;
     C* buf = tw + N;
-    fill_twiddles(tw, N);
+    fill_pass_twiddles<C, N>(tw);
     __syncthreads();
     const int n1 = dims.n[1], nh = dims.n[2] / 2 + 1;
     const int64_t ls = (int64_t)n1 * nh;
@@ -224,6 +325,8 @@ __global__ void __launch_bounds__(N / 8 * B) x_kspace(Specs<cplx_t<T>> in, int n
     const int ctiles = (nh + B - 1) / B;
     const int64_t tiles_per = (int64_t)n1 * ctiles;
     const int64_t ntiles = tiles_per * nin;
+    const T norm = (T)op.norm, beta = (T)op.beta;
+    const T l0 = (T)op.los[0], l1 = (T)op.los[1], l2 = (T)op.los[2];
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int bi = (int)(tile / tiles_per);
         const int64_t r = tile % tiles_per;
@@ -236,12 +339,57 @@ __global__ void __launch_bounds__(N / 8 * B) x_kspace(Specs<cplx_t<T>> in, int n
 #pragma unroll
         for (int i = 0; i < 8; i++) v[i] = ok ? g[(int64_t)(t + i * TL) * ls] : cmake<C>(0, 0);
         fft_regs<C, N, -1>(v, t, buf, addr, tw);
+        // wavenumbers: ky, kz fixed for this thread, kx per point
+        const T ky = kval<T>(iy, dims.n[1], (T)op.fscale[1]), kz = kval<T>(iz, dims.n[2], (T)op.fscale[2]);
+        const T ty = nyquist(iy, dims.n[1]) ? ky : -ky, tz = nyquist(iz, dims.n[2]) ? kz : -kz;
+        KPoint<T, KT> kp[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int ix = t + i * TL;
+            const T kx = kval<T>(ix, dims.n[0], (T)op.fscale[0]);
+            const T tx = nyquist(ix, dims.n[0]) ? kx : -kx;
+            const T k2 = (ky * ky + kx * kx) + kz * kz;
+            const bool zero = (ix == 0 && iy == 0 && iz == 0);
+            if constexpr (KT == KOP_GAUSS) {
+                const T rx = (T)op.radius[0] * kx, ry = (T)op.radius[1] * ky, rz = (T)op.radius[2] * kz;
+                kp[i].a = exp((T)-0.5 * (rx * rx) + (T)-0.5 * (ry * ry) + (T)-0.5 * (rz * rz)) * norm;
+            } else if constexpr (KT == KOP_PP) {
+                const T kl = kx * l0 + ky * l1 + kz * l2, klt = tx * l0 + ty * l1 + tz * l2;
+                kp[i].a = zero ? (T)0 : (T)1 / (k2 + beta * (kl * kl));
+                kp[i].b = zero ? (T)0 : (T)1 / (k2 + beta * (klt * klt));
+            } else {
+                kp[i].a = zero ? (T)0 : norm / k2;
+            }
+        }
         for (int o = 0; o < op.nper; o++) {
             C u[8];
 #pragma unroll
             for (int i = 0; i < 8; i++) {
-                T re, im;
-                kmult<T, KT>(op, o, t + i * TL, iy, iz, re, im);
+                T re = 0, im = 0;
+                const int ix = t + i * TL;
+                const T kx = kval<T>(ix, dims.n[0], (T)op.fscale[0]);
+                const T tx = nyquist(ix, dims.n[0]) ? kx : -kx;
+                if constexpr (KT == KOP_GAUSS) {
+                    re = kp[i].a;
+                } else if constexpr (KT == KOP_PP) {
+                    // (i m(k) + conj(i m(k~))) / 2 with m = k_o / (k^2 (1 + beta mu^2))
+                    const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
+                    im = (T)0.5 * (ko * kp[i].a - to * kp[i].b) * norm;
+                } else if constexpr (KT == KOP_ITER_GLOBAL) {
+                    const T kl = kx * l0 + ky * l1 + kz * l2, klt = tx * l0 + ty * l1 + tz * l2;
+                    re = (T)0.5 * (kl * kl + klt * klt) * kp[i].a;
+                } else if constexpr (KT == KOP_ITER_LOCAL) {
+                    const int ci = o < 3 ? 0 : (o < 5 ? 1 : 2);
+                    const int cj = o < 3 ? o : (o < 5 ? o - 2 : 2);
+                    const T ki = ci == 0 ? kx : (ci == 1 ? ky : kz), ti = ci == 0 ? tx : (ci == 1 ? ty : tz);
+                    const T kj = cj == 0 ? kx : (cj == 1 ? ky : kz), tj = cj == 0 ? tx : (cj == 1 ? ty : tz);
+                    re = (T)0.5 * (ki * kj + ti * tj) * kp[i].a;
+                } else if constexpr (KT == KOP_PSI) {
+                    const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
+                    im = (T)0.5 * (ko - to) * kp[i].a;
+                } else {
+                    re = norm;
+                }
                 u[i] = cmake<C>(re * v[i].x - im * v[i].y, re * v[i].y + im * v[i].x);
             }
             fft_regs<C, N, +1>(u, t, buf, addr, tw);
@@ -263,9 +411,11 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
     typedef cplx_t<T> C;
     constexpr int TL = M / 8, N2 = 2 * M, NH = M + 1, RS = row_stride(M);
     extern __shared__ unsigned char smem_raw[];
-    C* tw = (C*)smem_raw;                 // N2 entries: w_{n2}^m
-    C* buf = tw + N2;                     // ROWS * RS
-    fill_twiddles(tw, N2);
+    C* tw = (C*)smem_raw;                 // pass table of the M-point transform (M entries)
+    C* wk = tw + M;                       // w_{n2}^k, k < M + 1, for the real-FFT unpack
+    C* buf = wk + M + 1;                  // ROWS * RS
+    fill_pass_twiddles<C, M>(tw);
+    fill_roots(wk, M + 1, N2);
     __syncthreads();
     const int line = threadIdx.x / TL, t = threadIdx.x % TL;
     const RowAddr addr{line * RS};
@@ -289,7 +439,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
                 v[i] = cmake<C>((T)x.x, (T)x.y);
             }
         }
-        fft_regs<C, M, -1, 2>(v, t, buf, addr, tw);
+        fft_regs<C, M, -1>(v, t, buf, addr, tw);
         // unpack needs Z[M - k]: publish Z, then combine
 #pragma unroll
         for (int i = 0; i < 8; i++) buf[addr(t + i * TL)] = v[i];
@@ -302,7 +452,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
             const C zc = cconj(buf[addr(k == 0 ? 0 : M - k)]);
             const C e = cscale(cadd(zk, zc), (T)0.5);
             const C o = cmul_i(cscale(csub(zk, zc), (T)0.5), -1);
-            const C x = cadd(e, cmul(tw[k], o));
+            const C x = cadd(e, cmul(wk[k], o));
             if (ok) dst[k] = x;
         }
         if (t == 0 && ok) {
@@ -318,14 +468,24 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
 // The input loop is unrolled at compile time (at most NMAX inputs for epilogue ET), so every
 // input pointer and every per-input register array is indexed statically.
 // ---------------------------------------------------------------------------------------------
+// p[c] for a rolled loop index c, written as selects so no parameter array is indexed at run time.
+template <typename C> __device__ __forceinline__ const C* select6(const Specs<C>& s, int c) {
+    return c == 0 ? s.p[0] : c == 1 ? s.p[1] : c == 2 ? s.p[2] : c == 3 ? s.p[3] : c == 4 ? s.p[4] : s.p[5];
+}
+__device__ __forceinline__ double select6(const double (&f)[6], int c) {
+    return c == 0 ? f[0] : c == 1 ? f[1] : c == 2 ? f[2] : c == 3 ? f[3] : c == 4 ? f[4] : f[5];
+}
+
 template <int ET> struct EpiInputs {
-    static constexpr int NMAX = ET == EPI_ITER_LOCAL ? 6 : (ET == EPI_DENSITY ? 2 : (ET == EPI_STORE ? 3 : 1));
+    static constexpr int NMAX =
+        ET == EPI_ITER_LOCAL ? 6 : (ET == EPI_DENSITY ? 2 : ((ET == EPI_STORE || ET == EPI_STORE4) ? 3 : 1));
 };
 
 // Inverse z transform of one row: returns v[i] = (x[2k], x[2k+1]), k = t + i TL, unscaled.
 template <typename T, int M, class Addr>
 __device__ __forceinline__ void row_c2r(const cplx_t<T>* __restrict__ src, bool ok, int t, cplx_t<T>* buf,
-                                        const Addr& addr, const cplx_t<T>* tw, cplx_t<T> (&v)[8]) {
+                                        const Addr& addr, const cplx_t<T>* tw, const cplx_t<T>* wk,
+                                        cplx_t<T> (&v)[8]) {
     typedef cplx_t<T> C;
     constexpr int TL = M / 8;
     // stage X (M + 1 points) in shared memory for the X[M - k] partner reads
@@ -339,22 +499,24 @@ __device__ __forceinline__ void row_c2r(const cplx_t<T>* __restrict__ src, bool 
         const C xk = buf[addr(k)];
         const C xc = cconj(buf[addr(M - k)]);
         const C ev = cadd(xk, xc);
-        const C od = cmul(cconj(tw[k]), csub(xk, xc));
+        const C od = cmul(cconj(wk[k]), csub(xk, xc));
         v[i] = cadd(ev, cmul_i(od, +1));
     }
     __syncthreads();
-    fft_regs<C, M, +1, 2>(v, t, buf, addr, tw);
+    fft_regs<C, M, +1>(v, t, buf, addr, tw);
 }
 
 template <typename T, int M, int ROWS, int ET>
-__global__ void __launch_bounds__(M / 8 * ROWS) z_c2r(Specs<cplx_t<T>> in, int nin, Dims dims, Epi<T> e) {
+__global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_C2R_MINB>::value)) z_c2r(Specs<cplx_t<T>> in, int nin, Dims dims, Epi<T> e) {
     typedef cplx_t<T> C;
     constexpr int TL = M / 8, N2 = 2 * M, NH = M + 1, RS = row_stride(M);
     constexpr int NMAX = EpiInputs<ET>::NMAX;
     extern __shared__ unsigned char smem_raw[];
     C* tw = (C*)smem_raw;
-    C* buf = tw + N2;
-    fill_twiddles(tw, N2);
+    C* wk = tw + M;
+    C* buf = wk + M + 1;
+    fill_pass_twiddles<C, M>(tw);
+    fill_roots(wk, M + 1, N2);
     __syncthreads();
     const int line = threadIdx.x / TL, t = threadIdx.x % TL;
     const RowAddr addr{line * RS};
@@ -371,7 +533,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_c2r(Specs<cplx_t<T>> in, int n
             for (int c = 0; c < NMAX; c++) {
                 if (c < nin) {
                     C v[8];
-                    row_c2r<T, M>(in.p[c] + row * NH, ok, t, buf, addr, tw, v);
+                    row_c2r<T, M>(in.p[c] + row * NH, ok, t, buf, addr, tw, wk, v);
                     C* o = (C*)(e.out[c] + (ok ? row : 0) * N2);
                     if (ok) {
 #pragma unroll
@@ -379,10 +541,26 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_c2r(Specs<cplx_t<T>> in, int n
                     }
                 }
             }
+        } else if constexpr (ET == EPI_STORE4) {
+            // three inputs -> one interleaved (x, y, z, 0) quadruple per cell
+            C v0[8], v1[8], v2[8];
+            row_c2r<T, M>(in.p[0] + row * NH, ok, t, buf, addr, tw, wk, v0);
+            row_c2r<T, M>(in.p[1] + row * NH, ok, t, buf, addr, tw, wk, v1);
+            row_c2r<T, M>(in.p[2] + row * NH, ok, t, buf, addr, tw, wk, v2);
+            if (ok) {
+                typedef typename vec4_of<T>::type V4;
+                V4* o = (V4*)(e.out[0] + row * N2 * 4);
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int k = t + i * TL;
+                    o[2 * k] = make_vec4<T>(v0[i].x * sc, v1[i].x * sc, v2[i].x * sc);
+                    o[2 * k + 1] = make_vec4<T>(v0[i].y * sc, v1[i].y * sc, v2[i].y * sc);
+                }
+            }
         } else if constexpr (ET == EPI_DENSITY) {
             C d[8], r[8];
-            row_c2r<T, M>(in.p[0] + row * NH, ok, t, buf, addr, tw, d);
-            row_c2r<T, M>(in.p[1] + row * NH, ok, t, buf, addr, tw, r);
+            row_c2r<T, M>(in.p[0] + row * NH, ok, t, buf, addr, tw, wk, d);
+            row_c2r<T, M>(in.p[1] + row * NH, ok, t, buf, addr, tw, wk, r);
             const double sd = e.sums[0], sr = e.sums[1];
             const double alpha = sd * 1. / sr;
             const double threshold = e.ran_min * sr / e.size_randoms;
@@ -398,7 +576,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_c2r(Specs<cplx_t<T>> in, int n
             }
         } else if constexpr (ET == EPI_DENSITY_NORANDOMS) {
             C d[8];
-            row_c2r<T, M>(in.p[0] + row * NH, ok, t, buf, addr, tw, d);
+            row_c2r<T, M>(in.p[0] + row * NH, ok, t, buf, addr, tw, wk, d);
             const double mean = e.sums[0] / e.ncells;
             if (ok) {
 #pragma unroll
@@ -409,36 +587,45 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_c2r(Specs<cplx_t<T>> in, int n
                 }
             }
         } else {
-            // RSD removal: delta_real = delta - sum_c factor_c w_c(x) IFFT_c, accumulated in registers
+            // RSD removal: delta_real = delta - sum_c factor_c w_c(x) IFFT_c, accumulated in registers;
+            // w_c = x_i x_j / |x|^2 with 1/|x|^2 computed once per point, all in the mesh precision.
             const C* dl = (const C*)(e.delta + (ok ? row : 0) * N2);
-            T acc[8][2];
+            const T x0 = (T)(e.offset[0] + e.cell[0] * ix), x1 = (T)(e.offset[1] + e.cell[1] * iy);
+            const T oz = (T)e.offset[2], cz = (T)e.cell[2];
+            T acc[8][2], ix2[8][2];
 #pragma unroll
             for (int i = 0; i < 8; i++) {
                 const C d0 = ok ? dl[t + i * TL] : cmake<C>(0, 0);
                 acc[i][0] = d0.x;
                 acc[i][1] = d0.y;
-            }
-#pragma unroll
-            for (int c = 0; c < NMAX; c++) {
-                C v[8];
-                row_c2r<T, M>(in.p[c] + row * NH, ok, t, buf, addr, tw, v);
-#pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const int k = t + i * TL;
+                if constexpr (ET == EPI_ITER_LOCAL) {
 #pragma unroll
                     for (int h = 0; h < 2; h++) {
-                        const double val = (double)((h ? v[i].y : v[i].x) * sc);
+                        const T xz = oz + cz * (T)(2 * (t + i * TL) + h);
+                        ix2[i][h] = (T)1 / ((x0 * x0 + x1 * x1) + xz * xz);
+                    }
+                }
+            }
+#pragma unroll 1
+            for (int c = 0; c < NMAX; c++) {
+                C v[8];
+                row_c2r<T, M>(select6(in, c) + row * NH, ok, t, buf, addr, tw, wk, v);
+                const T fc = (T)select6(e.factor, c) * sc;
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const T val = h ? v[i].y : v[i].x;
                         if constexpr (ET == EPI_ITER_GLOBAL) {
-                            acc[i][h] = (T)((double)acc[i][h] - e.factor[0] * val);
+                            acc[i][h] -= fc * val;
                         } else {
-                            // component c = (pi, pj) in the order (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
-                            const int pi = c < 3 ? 0 : (c < 5 ? 1 : 2);
-                            const int pj = c < 3 ? c : (c < 5 ? c - 2 : 2);
-                            const int iz = 2 * k + h;
-                            const double x[3] = {e.offset[0] + e.cell[0] * ix, e.offset[1] + e.cell[1] * iy,
-                                                 e.offset[2] + e.cell[2] * iz};
-                            const double x2 = (x[0] * x[0] + x[1] * x[1]) + x[2] * x[2];
-                            acc[i][h] = (T)((double)acc[i][h] - e.factor[c] * ((x[pi] * x[pj] * val) / x2));
+                            // component c = (ci, cj) in the order (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+                            const int ci = c < 3 ? 0 : (c < 5 ? 1 : 2);
+                            const int cj = c < 3 ? c : (c < 5 ? c - 2 : 2);
+                            const T xz = oz + cz * (T)(2 * (t + i * TL) + h);
+                            const T xi = ci == 0 ? x0 : (ci == 1 ? x1 : xz);
+                            const T xj = cj == 0 ? x0 : (cj == 1 ? x1 : xz);
+                            acc[i][h] -= fc * (xi * xj * val) * ix2[i][h];
                         }
                     }
                 }

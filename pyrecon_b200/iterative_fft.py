@@ -17,16 +17,13 @@ class IterativeFFTReconstruction(FFTShiftsMixin, BaseReconstruction):
         with self._stream_ctx():
             nm, bs, bc = self.info.c_geometry()
             lib = _lib.load()
-            psis = []
-            for _ in range(3):
-                m = RealMesh(info=self.info, device=self.device)
-                m.__dict__['value'] = torch.empty(self.info.shape, dtype=torch_dtype(self.info.dtype), device=self.device)
-                psis.append(m)
+            psi4, psis = self._new_psi()
             self.log_info('Running {:d} iterations.'.format(niterations))
             ws = self._ws.get(lib.prc_iterative_fft_workspace_bytes(nm, self.info.dtype.itemsize, int(self.los is None)))
             _lib.call('prc_iterative_fft_' + _lib.suffix(self.info.dtype), _lib.ptr(self.mesh_delta.value), nm, bs, bc,
-                      float(self.beta), self._los_arg(), int(niterations), *[_lib.ptr(m.value) for m in psis],
+                      float(self.beta), self._los_arg(), int(niterations), *self._psi_pointers(psi4), 4,
                       _lib.ptr(ws), ws.numel(), _lib.stream_of(self.device), error=MeshError)
             self._iter = int(niterations)
             del self.mesh_delta
+            self._psi4 = psi4
             self.mesh_psi = psis

@@ -24,14 +24,11 @@ class PlaneParallelFFTReconstruction(FFTShiftsMixin, BaseReconstruction):
         with self._stream_ctx():
             nm, bs, _ = self.info.c_geometry()
             lib = _lib.load()
-            psis = []
-            for _ in range(3):
-                m = RealMesh(info=self.info, device=self.device)
-                m.__dict__['value'] = torch.empty(self.info.shape, dtype=torch_dtype(self.info.dtype), device=self.device)
-                psis.append(m)
+            psi4, psis = self._new_psi()
             ws = self._ws.get(lib.prc_plane_parallel_workspace_bytes(nm, self.info.dtype.itemsize))
             _lib.call('prc_plane_parallel_fft_' + _lib.suffix(self.info.dtype), _lib.ptr(self.mesh_delta.value), nm, bs,
-                      float(self.beta), _lib.d3([float(x) for x in self.los]), *[_lib.ptr(m.value) for m in psis],
+                      float(self.beta), _lib.d3([float(x) for x in self.los]), *self._psi_pointers(psi4), 4,
                       _lib.ptr(ws), ws.numel(), _lib.stream_of(self.device), error=MeshError)
             del self.mesh_delta
+            self._psi4 = psi4
             self.mesh_psi = psis

@@ -226,13 +226,29 @@ class BaseReconstruction(BaseClass):
 
 
 class FFTShiftsMixin(object):
-    """Shift read-out from the three displacement meshes ``mesh_psi`` (recon.py:255-302)."""
+    """Displacements stored interleaved, (psi_x, psi_y, psi_z, 0) per cell, so the CIC read-out does
+    one vector load per corner; ``mesh_psi`` are the three component views (recon.py:255-302)."""
+
+    def _new_psi(self):
+        import torch
+        psi4 = torch.empty(self.info.shape + (4,), dtype=torch_dtype(self.info.dtype), device=self.device)
+        meshes = []
+        for a in range(3):
+            m = RealMesh(info=self.info, device=self.device)
+            m.__dict__['value'] = psi4[..., a]
+            meshes.append(m)
+        return psi4, meshes
+
+    @staticmethod
+    def _psi_pointers(psi4):
+        base = psi4.data_ptr()
+        item = psi4.element_size()
+        return [_lib.c_void_p(base), _lib.c_void_p(base + item), _lib.c_void_p(base + 2 * item)]
 
     def _shift_call(self, p, field, shifted, out, obytes):
         if not hasattr(self, 'mesh_psi'):
             raise ReconstructionError('run() must be called before reading shifts')
         nm, bs, bc = self._geometry_args()
-        px, py, pz = (m.value for m in self.mesh_psi)
-        _lib.call('prc_read_shifts_psi_' + _lib.suffix(self.info.dtype), _lib.ptr(px), _lib.ptr(py), _lib.ptr(pz), nm, bs,
+        _lib.call('prc_read_shifts_psi_' + _lib.suffix(self.info.dtype), *self._psi_pointers(self._psi4), 4, nm, bs,
                   bc, _lib.ptr(p.pos), p.pos_bytes, p.size, float(self.f), self._los_arg(), field, shifted,
                   int(self.wrap), _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device), error=MeshError)
