@@ -171,12 +171,22 @@ PRC_API prc_status_t prc_read_shifts_phi_f64(const double *phi, const int32_t nm
                                      int64_t npos, double f, const double *los, int field, int shifted,
                                      int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
 
+/* Device fault word of the FFT kernels on the current device (no counterpart in the reference,
+ * whose FFTs run on the host): PRC_FAULT_WAIT_TIMEOUT when a kernel gave up a bounded wait for its
+ * own tile copies (its outputs are then incomplete), PRC_FAULT_SMEM_ALIGN when shared memory was
+ * misaligned for the copy unit.  Synchronises with the device; reset != 0 clears the word. */
+#define PRC_FAULT_WAIT_TIMEOUT 1u
+#define PRC_FAULT_SMEM_ALIGN 2u
+PRC_API unsigned int prc_device_fault_flags(int reset);
+
 /* ------------------------------------------------------------------------------------------
  * FFTs and the k-space steps (the numpy / pyfftw sites of pyrecon/mesh.py:974-1118 and the
  * algorithm modules).  Forward transforms are unnormalised; inverse ones divide by n0*n1*n2,
  * as numpy's fftn / ifftn.  Spectra are the r2c half; multipliers are applied in their
  * Hermitian-symmetrised form so results equal the reference's c2c transform followed by .real.
  * ------------------------------------------------------------------------------------------ */
+/* Workspace of `nspectra` half spectra as the composite entry points below lay them out inside
+ * their workspace (rows padded to a multiple of 32 bytes). */
 PRC_API size_t prc_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int nspectra);
 
 /* Forward r2c: in is a real mesh of `in_bytes` (4 or 8) precision, out the half spectrum. */

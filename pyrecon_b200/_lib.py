@@ -20,6 +20,7 @@ DP = ctypes.POINTER(ctypes.c_double)   # optional 3-vector (NULL = local line of
 PRC_OK = 0
 PRC_FLAG_OUT_OF_BOX = 1
 PRC_FLAG_NONFINITE = 2
+PRC_ERR_TIMEOUT = 5
 FIELDS = {'disp': 0, 'rsd': 1, 'disp+rsd': 2}
 
 _lock = threading.Lock()
@@ -33,6 +34,7 @@ _SIGNATURES = {
     'prc_profile_enable': (None, [c_int]),
     'prc_profile_collect': (c_int, [ctypes.c_char_p, c_size]),
     'prc_fft_supported': (c_int, [I3]),
+    'prc_device_fault_flags': (ctypes.c_uint, [c_int]),
     'prc_assign_cic_workspace_bytes': (c_size, [I3, c_i64, c_int]),
     'prc_assign_cic': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size, _p]),
     'prc_cic_cell_order': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, c_i64, c_int, _p, _p, c_size, _p]),
@@ -150,6 +152,14 @@ def profile_collect():
     buf = ctypes.create_string_buffer(1 << 16)
     load().prc_profile_collect(buf, len(buf))
     return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
+
+
+def check_device_faults(error=RuntimeError):
+    """Raise ``error`` if a kernel on the current device gave up a bounded wait (the device fault
+    word, cleared here); synchronises with the device."""
+    flags = load().prc_device_fault_flags(1)
+    if flags:
+        raise error('{} (device fault flags {:#x})'.format(status_string(PRC_ERR_TIMEOUT), flags))
 
 
 def suffix(dtype):

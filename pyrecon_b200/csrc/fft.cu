@@ -21,6 +21,7 @@
 // is exactly what the reference's full complex transform followed by .real computes
 // (pyrecon/mesh.py:842, recon.py:117).
 #include "common.cuh"
+#include "tma.cuh"
 
 #include <algorithm>
 #include <math.h>
@@ -226,7 +227,7 @@ struct RealsIn { const void* p[MAX_BATCH]; };
 // ---------------------------------------------------------------------------------------------
 template <typename T, typename TIN>
 __global__ void __launch_bounds__(FFT_THREADS) fft_z_r2c(RealsIn in, Specs<cplx_t<T>> out, int nbatch, Dims dims,
-                                                          Radices rd, int B) {
+                                                          int pitch, Radices rd, int B) {
     typedef cplx_t<T> C;
     extern __shared__ unsigned char smem_raw[];
     const int n2 = dims.n[2], M = n2 / 2, nh = M + 1;
@@ -267,10 +268,10 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_z_r2c(RealsIn in, Specs<cplx_
             x[k * bp + line] = cadd(e, cmul(tw[k == M ? M : k], o));
         }
         __syncthreads();
-        C* dst = out.p[bi] + row0 * nh;
+        C* dst = out.p[bi] + row0 * pitch;
         for (int q = threadIdx.x; q < B * nh; q += blockDim.x) {
             const int line = q / nh, k = q % nh;
-            if (line < nrow) dst[(int64_t)line * nh + k] = x[k * bp + line];
+            if (line < nrow) dst[(int64_t)line * pitch + k] = x[k * bp + line];
         }
         __syncthreads();
     }
@@ -413,7 +414,7 @@ __device__ __forceinline__ double2 kmultiplier(const KOp& op, int o, int ix, int
 
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS) fft_x_fused(Specs<cplx_t<T>> in, int nin, Specs<cplx_t<T>> out,
-                                                            Dims dims, Radices rd, int B, KOp op) {
+                                                            Dims dims, int pitch, Radices rd, int B, KOp op) {
     typedef cplx_t<T> C;
     extern __shared__ unsigned char smem_raw[];
     const int n0 = dims.n[0], n1 = dims.n[1], nh = dims.n[2] / 2 + 1;
@@ -425,9 +426,9 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_x_fused(Specs<cplx_t<T>> in, 
     __syncthreads();
     Strided s;
     s.n = n0;
-    s.ls = (int64_t)n1 * nh;
+    s.ls = (int64_t)n1 * pitch;
     s.outer = n1;
-    s.os = nh;
+    s.os = pitch;
     s.ncols = nh;
     const int ctiles = (nh + B - 1) / B;
     const int64_t tiles_per = (int64_t)n1 * ctiles;
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_x_fused(Specs<cplx_t<T>> in, 
         const int64_t r = t % tiles_per;
         const int iy = (int)(r / ctiles), c0 = (int)(r % ctiles) * B;
         const int cols = min(B, nh - c0);
-        const int64_t off = (int64_t)iy * nh + c0;
+        const int64_t off = (int64_t)iy * pitch + c0;
         load_tile(bufa, in.p[bi] + off, s, B, cols);
         __syncthreads();
         C* fwd = fft_lines<C, -1>(bufa, bufb, n0, B, B, rd, tw, 1);
@@ -522,8 +523,8 @@ __device__ __forceinline__ void epilogue_pair(const Epi<T>& e, int nin, const T*
 }
 
 template <typename T>
-__global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, int nin, Dims dims, Radices rd, int B,
-                                                          Epi<T> e) {
+__global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, int nin, Dims dims, int pitch,
+                                                          Radices rd, int B, Epi<T> e) {
     typedef cplx_t<T> C;
     extern __shared__ unsigned char smem_raw[];
     const int n2 = dims.n[2], M = n2 / 2, nh = M + 1;
@@ -541,10 +542,10 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, in
         const int64_t row0 = t * B;
         const int nrow = (int)min((int64_t)B, rows - row0);
         for (int i = 0; i < nin; i++) {
-            const C* src = in.p[i] + row0 * nh;
+            const C* src = in.p[i] + row0 * pitch;
             for (int q = threadIdx.x; q < B * nh; q += blockDim.x) {
                 const int line = q / nh, k = q % nh;
-                bufa[k * bp + line] = line < nrow ? src[(int64_t)line * nh + k] : cmake<C>(0, 0);
+                bufa[k * bp + line] = line < nrow ? src[(int64_t)line * pitch + k] : cmake<C>(0, 0);
             }
             __syncthreads();
             // pack: Z[k] = (X[k] + conj X[M-k]) + i w^-k (X[k] - conj X[M-k]), k < M
@@ -604,7 +605,11 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, in
     }
 }
 
+// Device fault word of the FFT kernels (bits prc::tma::FAULT_*), read by prc_device_fault_flags.
+__device__ unsigned int g_fault;
+
 #include "fft_fast.cuh"
+#include "fft_tma.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // Host-side planning and launches
@@ -612,6 +617,7 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, in
 struct Plan3 {
     Dims dims;
     int nh;
+    int pitch;            // row stride of the half spectra in complex elements (>= nh)
     Radices rz, ry, rx;   // rz is for the n2/2-point complex transform
 };
 
@@ -621,12 +627,23 @@ static int make_plan(const int32_t nmesh[3], Plan3* p) {
     if (nmesh[2] % 2 != 0) return PRC_ERR_UNSUPPORTED;
     for (int d = 0; d < 3; d++) p->dims.n[d] = nmesh[d];
     p->nh = nmesh[2] / 2 + 1;
+    p->pitch = p->nh;
     if (!factorize(nmesh[2] / 2, &p->rz) || !factorize(nmesh[1], &p->ry) || !factorize(nmesh[0], &p->rx))
         return PRC_ERR_UNSUPPORTED;
     return PRC_OK;
 }
 
-static size_t spectrum_elems(const Plan3& p) { return (size_t)p.dims.n[0] * p.dims.n[1] * p.nh; }
+static size_t spectrum_elems(const Plan3& p) { return (size_t)p.dims.n[0] * p.dims.n[1] * p.pitch; }
+// Complex values of one half spectrum, without the row padding (the compulsory bytes of a pass).
+static double spectrum_values(const Plan3& p) { return (double)p.dims.n[0] * p.dims.n[1] * p.nh; }
+
+// Spectra inside the library's own workspaces get rows padded to a multiple of 32 bytes, so every
+// row and every tile of adjacent z-columns starts on a sector boundary (and the row stride meets the
+// 16-byte rule of the tensor-memory-access copies).
+template <typename T> static void pad_pitch(Plan3* p) {
+    const int q = (int)(32 / sizeof(cplx_t<T>));
+    p->pitch = (p->nh + q - 1) / q * q;
+}
 
 // Lines per tile B (power of two) so that `nbuf` buffers of n * B complex fit the budget.
 static int choose_B(int n, int nbuf, size_t csize, size_t budget, int bmax) {
@@ -729,7 +746,7 @@ template <typename T, int N> struct KSpaceCfg {
 template <typename T> struct FastX {
     template <int N> struct K {
         template <int KT>
-        static int go(Specs<cplx_t<T>> si, int nin, Specs<cplx_t<T>> so, Dims dims, KOp op, double bytes,
+        static int go(Specs<cplx_t<T>> si, int nin, Specs<cplx_t<T>> so, Dims dims, int pitch, KOp op, double bytes,
                       cudaStream_t st) {
             typedef KSpaceCfg<T, N> cfg;
             auto kern = fast::x_kspace<T, N, cfg::B, KT>;
@@ -737,19 +754,19 @@ template <typename T> struct FastX {
             const int nh = dims.n[2] / 2 + 1;
             int64_t ntiles = (int64_t)dims.n[1] * ((nh + cfg::B - 1) / cfg::B) * nin;
             PRC_LAUNCH_B("fft_x_kspace", st, bytes,
-                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(si, nin, so, dims, op));
+                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(si, nin, so, dims, pitch, op));
             PRC_CHECK_LAUNCH();
             return PRC_OK;
         }
-        static int run(Specs<cplx_t<T>> si, int nin, Specs<cplx_t<T>> so, Dims dims, KOp op, double bytes,
+        static int run(Specs<cplx_t<T>> si, int nin, Specs<cplx_t<T>> so, Dims dims, int pitch, KOp op, double bytes,
                        cudaStream_t st) {
             switch (op.type) {
-                case KOP_GAUSS: return go<KOP_GAUSS>(si, nin, so, dims, op, bytes, st);
-                case KOP_PP: return go<KOP_PP>(si, nin, so, dims, op, bytes, st);
-                case KOP_ITER_GLOBAL: return go<KOP_ITER_GLOBAL>(si, nin, so, dims, op, bytes, st);
-                case KOP_ITER_LOCAL: return go<KOP_ITER_LOCAL>(si, nin, so, dims, op, bytes, st);
-                case KOP_PSI: return go<KOP_PSI>(si, nin, so, dims, op, bytes, st);
-                default: return go<KOP_IDENTITY>(si, nin, so, dims, op, bytes, st);
+                case KOP_GAUSS: return go<KOP_GAUSS>(si, nin, so, dims, pitch, op, bytes, st);
+                case KOP_PP: return go<KOP_PP>(si, nin, so, dims, pitch, op, bytes, st);
+                case KOP_ITER_GLOBAL: return go<KOP_ITER_GLOBAL>(si, nin, so, dims, pitch, op, bytes, st);
+                case KOP_ITER_LOCAL: return go<KOP_ITER_LOCAL>(si, nin, so, dims, pitch, op, bytes, st);
+                case KOP_PSI: return go<KOP_PSI>(si, nin, so, dims, pitch, op, bytes, st);
+                default: return go<KOP_IDENTITY>(si, nin, so, dims, pitch, op, bytes, st);
             }
         }
     };
@@ -757,13 +774,13 @@ template <typename T> struct FastX {
 
 template <typename T, typename TIN> struct FastZR2C {
     template <int M> struct K {
-        static int run(RealsIn ri, Specs<cplx_t<T>> so, int nb, int64_t rows, double bytes, cudaStream_t st) {
+        static int run(RealsIn ri, Specs<cplx_t<T>> so, int nb, int64_t rows, int pitch, double bytes, cudaStream_t st) {
             typedef RowCfg<T, M> cfg;
             auto kern = fast::z_r2c<T, TIN, M, cfg::ROWS>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
             int64_t ntiles = ((rows + cfg::ROWS - 1) / cfg::ROWS) * nb;
             PRC_LAUNCH_B("fft_z_r2c", st, bytes,
-                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(ri, so, nb, rows));
+                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(ri, so, nb, rows, pitch));
             PRC_CHECK_LAUNCH();
             return PRC_OK;
         }
@@ -772,25 +789,213 @@ template <typename T, typename TIN> struct FastZR2C {
 
 template <typename T> struct FastZC2R {
     template <int M> struct K {
-        static int run(Specs<cplx_t<T>> si, int nin, Dims dims, Epi<T> e, double bytes, cudaStream_t st) {
+        static int run(Specs<cplx_t<T>> si, int nin, Dims dims, int pitch, Epi<T> e, double bytes, cudaStream_t st) {
             switch (e.type) {
-                case EPI_DENSITY: return go<EPI_DENSITY>(si, nin, dims, e, bytes, st);
-                case EPI_DENSITY_NORANDOMS: return go<EPI_DENSITY_NORANDOMS>(si, nin, dims, e, bytes, st);
-                case EPI_ITER_GLOBAL: return go<EPI_ITER_GLOBAL>(si, nin, dims, e, bytes, st);
-                case EPI_ITER_LOCAL: return go<EPI_ITER_LOCAL>(si, nin, dims, e, bytes, st);
-                case EPI_STORE4: return go<EPI_STORE4>(si, nin, dims, e, bytes, st);
-                default: return go<EPI_STORE>(si, nin, dims, e, bytes, st);
+                case EPI_DENSITY: return go<EPI_DENSITY>(si, nin, dims, pitch, e, bytes, st);
+                case EPI_DENSITY_NORANDOMS: return go<EPI_DENSITY_NORANDOMS>(si, nin, dims, pitch, e, bytes, st);
+                case EPI_ITER_GLOBAL: return go<EPI_ITER_GLOBAL>(si, nin, dims, pitch, e, bytes, st);
+                case EPI_ITER_LOCAL: return go<EPI_ITER_LOCAL>(si, nin, dims, pitch, e, bytes, st);
+                case EPI_STORE4: return go<EPI_STORE4>(si, nin, dims, pitch, e, bytes, st);
+                default: return go<EPI_STORE>(si, nin, dims, pitch, e, bytes, st);
             }
         }
         template <int ET>
-        static int go(Specs<cplx_t<T>> si, int nin, Dims dims, Epi<T> e, double bytes, cudaStream_t st) {
+        static int go(Specs<cplx_t<T>> si, int nin, Dims dims, int pitch, Epi<T> e, double bytes, cudaStream_t st) {
             typedef RowCfg<T, M> cfg;
             auto kern = fast::z_c2r<T, M, cfg::ROWS, ET>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
             int64_t rows = (int64_t)dims.n[0] * dims.n[1];
             int64_t ntiles = (rows + cfg::ROWS - 1) / cfg::ROWS;
             PRC_LAUNCH_B("fft_z_c2r", st, bytes,
-                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(si, nin, dims, e));
+                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(si, nin, dims, pitch, e));
+            PRC_CHECK_LAUNCH();
+            return PRC_OK;
+        }
+    };
+};
+
+// ---- TMA-fed passes ----
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The driver's tensor-map encoder, looked up once through the runtime (no libcuda link).
+static EncodeTiledFn tensor_map_encoder() {
+    static EncodeTiledFn fn = []() -> EncodeTiledFn {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return (EncodeTiledFn)f;
+    }();
+    return fn;
+}
+
+// PRC_FFT_TMA=0 in the environment keeps the register-prefetch kernels (tests compare both).
+static bool tma_enabled() {
+    static int cached = -1;
+    if (cached < 0) {
+        const char* v = getenv("PRC_FFT_TMA");
+        cached = (v != nullptr && v[0] == '0') ? 0 : 1;
+    }
+    return cached == 1 && tensor_map_encoder() != nullptr;
+}
+
+// Tensor map over the half spectrum at `base` (rows of p.pitch complex values) in 8-byte elements:
+// dims (nh U, n1, n0), box (bcols U, b1, b2).  False when the layout breaks a copy rule (base not
+// 16-byte aligned, row stride not a multiple of 16 bytes), so the caller uses the register kernels.
+static bool spectrum_map(CUtensorMap* m, const void* base, const Plan3& p, size_t csize, int bcols, int b1, int b2) {
+    EncodeTiledFn enc = tensor_map_encoder();
+    const cuuint64_t U = csize / 8, row = (cuuint64_t)p.pitch * csize;
+    if (!enc || ((uintptr_t)base & 15) != 0 || row % 16 != 0 || (bcols * U * 8) % 16 != 0) return false;
+    cuuint64_t dim[3] = {(cuuint64_t)p.nh * U, (cuuint64_t)p.dims.n[1], (cuuint64_t)p.dims.n[0]};
+    cuuint64_t stride[2] = {row, row * (cuuint64_t)p.dims.n[1]};
+    cuuint32_t box[3] = {(cuuint32_t)(bcols * U), (cuuint32_t)b1, (cuuint32_t)b2};
+    cuuint32_t es[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<void*>(base), dim, stride, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Persistent grid: as many CTAs as fit on the device at once (occupancy of this kernel), at most
+// one per tile.
+template <typename K> static int resident_grid(K kern, int threads, size_t smem, int64_t ntiles) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int64_t cap = (int64_t)device_sm_count() * per_sm;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, cap));
+}
+
+constexpr int TMA_UNAVAILABLE = -1;
+
+// Tuning knobs of the TMA-fed passes:
+//   PRC_TMA_STAGE_KB   shared memory of tile stages per strided-pass CTA (2 to 4 stages)
+//   PRC_TMA_STRIDED_B  columns per strided tile in FP32 (FP64 half as many; 128-byte row segments);
+//                      0 = as the register kernel
+//   PRC_TMA_C2R_S      row stages of the inverse z pass
+#ifndef PRC_TMA_STAGE_KB
+#define PRC_TMA_STAGE_KB 96
+#endif
+#ifndef PRC_TMA_STRIDED_B
+#define PRC_TMA_STRIDED_B 16
+#endif
+#ifndef PRC_TMA_C2R_S
+#define PRC_TMA_C2R_S 3
+#endif
+
+template <int S0> struct StageCount {
+    static constexpr int value = S0 < 2 ? 2 : (S0 > 4 ? 4 : S0);
+};
+
+template <typename T, int N> struct StridedTmaB {
+    static constexpr int B0 = PRC_TMA_STRIDED_B == 0 ? StridedCfg<T, N>::B
+                                                     : (sizeof(T) == 4 ? PRC_TMA_STRIDED_B : PRC_TMA_STRIDED_B / 2);
+    static constexpr int value = (N / 8) * B0 <= 1024 ? B0 : 1024 / (N / 8);
+};
+
+template <typename T, int N> struct StridedTmaCfg {
+    static constexpr int B = StridedTmaB<T, N>::value;
+    static constexpr int THREADS = (N / 8) * B;
+    static constexpr int S = StageCount<(int)(PRC_TMA_STAGE_KB * 1024 / fast::TileShape<T, N, B>::BYTES)>::value;
+    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, 0>::BYTES;
+};
+
+template <typename T, int DIR> struct FastStridedTma {
+    template <int N> struct K {
+        static int run(const Plan3& p, Specs<cplx_t<T>> sp, int nb, Strided s, int axis, const char* name,
+                       double bytes, cudaStream_t st) {
+            typedef StridedTmaCfg<T, N> cfg;
+            typedef fast::TileShape<T, N, cfg::B> TS;
+            tma::Maps maps;
+            for (int i = 0; i < nb; i++)
+                if (!spectrum_map(&maps.m[i], sp.p[i], p, sizeof(cplx_t<T>), cfg::B, axis == 1 ? TS::BOXL : 1,
+                                  axis == 1 ? 1 : TS::BOXL))
+                    return TMA_UNAVAILABLE;
+            auto kern = fast::strided_tma<T, N, cfg::B, cfg::S, DIR>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
+            const int64_t ntiles = (int64_t)s.outer * ((s.ncols + cfg::B - 1) / cfg::B) * nb;
+            PRC_LAUNCH_B(name, st, bytes,
+                         kern<<<resident_grid(kern, cfg::THREADS, cfg::SMEM, ntiles), cfg::THREADS, cfg::SMEM, st>>>(
+                             maps, sp, nb, s, axis));
+            PRC_CHECK_LAUNCH();
+            return PRC_OK;
+        }
+    };
+};
+
+template <typename T, int N> struct KSpaceTmaCfg {
+    static constexpr int B = KSpaceCfg<T, N>::B;
+    static constexpr int THREADS = KSpaceCfg<T, N>::THREADS;
+    static constexpr int S = 2;
+    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, 1>::BYTES;
+};
+
+template <typename T> struct FastXTma {
+    template <int N> struct K {
+        template <int KT>
+        static int go(const tma::Maps& maps, int nin, Specs<cplx_t<T>> so, const Plan3& p, KOp op, double bytes,
+                      cudaStream_t st) {
+            typedef KSpaceTmaCfg<T, N> cfg;
+            auto kern = fast::x_kspace_tma<T, N, cfg::B, cfg::S, KT>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
+            const int64_t ntiles = (int64_t)p.dims.n[1] * ((p.nh + cfg::B - 1) / cfg::B) * nin;
+            PRC_LAUNCH_B("fft_x_kspace", st, bytes,
+                         kern<<<resident_grid(kern, cfg::THREADS, cfg::SMEM, ntiles), cfg::THREADS, cfg::SMEM, st>>>(
+                             maps, nin, so, p.dims, p.pitch, op));
+            PRC_CHECK_LAUNCH();
+            return PRC_OK;
+        }
+        static int run(const Plan3& p, Specs<cplx_t<T>> si, int nin, Specs<cplx_t<T>> so, KOp op, double bytes,
+                       cudaStream_t st) {
+            typedef KSpaceTmaCfg<T, N> cfg;
+            typedef fast::TileShape<T, N, cfg::B> TS;
+            tma::Maps maps;
+            for (int i = 0; i < nin; i++)
+                if (!spectrum_map(&maps.m[i], si.p[i], p, sizeof(cplx_t<T>), cfg::B, 1, TS::BOXL))
+                    return TMA_UNAVAILABLE;
+            switch (op.type) {
+                case KOP_GAUSS: return go<KOP_GAUSS>(maps, nin, so, p, op, bytes, st);
+                case KOP_PP: return go<KOP_PP>(maps, nin, so, p, op, bytes, st);
+                case KOP_ITER_GLOBAL: return go<KOP_ITER_GLOBAL>(maps, nin, so, p, op, bytes, st);
+                case KOP_ITER_LOCAL: return go<KOP_ITER_LOCAL>(maps, nin, so, p, op, bytes, st);
+                case KOP_PSI: return go<KOP_PSI>(maps, nin, so, p, op, bytes, st);
+                default: return go<KOP_IDENTITY>(maps, nin, so, p, op, bytes, st);
+            }
+        }
+    };
+};
+
+template <typename T> struct FastZC2RTma {
+    template <int M> struct K {
+        typedef RowCfg<T, M> cfg;
+        static constexpr int S = PRC_TMA_C2R_S;
+        typedef fast::TmaRows<T, M, cfg::ROWS, S> Rows;
+        static int run(const Plan3& p, Specs<cplx_t<T>> si, int nin, Epi<T> e, double bytes, cudaStream_t st) {
+            if (p.pitch != Rows::PS) return TMA_UNAVAILABLE;
+            for (int i = 0; i < nin; i++)
+                if (((uintptr_t)si.p[i] & 15) != 0) return TMA_UNAVAILABLE;
+            switch (e.type) {
+                case EPI_DENSITY: return go<EPI_DENSITY>(p, si, nin, e, bytes, st);
+                case EPI_DENSITY_NORANDOMS: return go<EPI_DENSITY_NORANDOMS>(p, si, nin, e, bytes, st);
+                case EPI_ITER_GLOBAL: return go<EPI_ITER_GLOBAL>(p, si, nin, e, bytes, st);
+                case EPI_ITER_LOCAL: return go<EPI_ITER_LOCAL>(p, si, nin, e, bytes, st);
+                case EPI_STORE4: return go<EPI_STORE4>(p, si, nin, e, bytes, st);
+                default: return go<EPI_STORE>(p, si, nin, e, bytes, st);
+            }
+        }
+        template <int ET>
+        static int go(const Plan3& p, Specs<cplx_t<T>> si, int nin, Epi<T> e, double bytes, cudaStream_t st) {
+            auto kern = fast::z_c2r_tma<T, M, cfg::ROWS, ET, S>;
+            const size_t smem = fast::C2RTmaSmem<T, M, cfg::ROWS, S>::BYTES;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            const int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
+            const int64_t ntiles = (rows + cfg::ROWS - 1) / cfg::ROWS;
+            PRC_LAUNCH_B("fft_z_c2r", st, bytes,
+                         kern<<<resident_grid(kern, cfg::THREADS, smem, ntiles), cfg::THREADS, smem, st>>>(si, nin,
+                                                                                                       p.dims, e));
             PRC_CHECK_LAUNCH();
             return PRC_OK;
         }
@@ -813,7 +1018,7 @@ template <typename T> struct FFTLaunch {
             }
             int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
             double bytes = (double)nb * rows * (p.dims.n[2] * sizeof(TIN) + p.nh * CS);
-            return dispatch_pow2<FastZR2C<T, TIN>::template K>(p.dims.n[2] / 2, ri, so, nb, rows, bytes, st);
+            return dispatch_pow2<FastZR2C<T, TIN>::template K>(p.dims.n[2] / 2, ri, so, nb, rows, p.pitch, bytes, st);
         }
         const int M = p.dims.n[2] / 2;
         int B = 16;
@@ -828,7 +1033,7 @@ template <typename T> struct FFTLaunch {
         cudaFuncSetAttribute(fft_z_r2c<T, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
         int64_t ntiles = ((rows + B - 1) / B) * nb;
-        PRC_LAUNCH_B("fft_z_r2c", st, (double)nb * rows * (p.dims.n[2] * sizeof(TIN) + p.nh * CS), fft_z_r2c<T, TIN><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(ri, so, nb, p.dims, p.rz, B));
+        PRC_LAUNCH_B("fft_z_r2c", st, (double)nb * rows * (p.dims.n[2] * sizeof(TIN) + p.nh * CS), fft_z_r2c<T, TIN><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(ri, so, nb, p.dims, p.pitch, p.rz, B));
         PRC_CHECK_LAUNCH();
         return PRC_OK;
     }
@@ -840,34 +1045,38 @@ template <typename T> struct FFTLaunch {
             const int nh = p.nh;
             if (axis == 1) {
                 s.n = p.dims.n[1];
-                s.ls = nh;
+                s.ls = p.pitch;
                 s.outer = p.dims.n[0];
-                s.os = (int64_t)p.dims.n[1] * nh;
+                s.os = (int64_t)p.dims.n[1] * p.pitch;
             } else {
                 s.n = p.dims.n[0];
-                s.ls = (int64_t)p.dims.n[1] * nh;
+                s.ls = (int64_t)p.dims.n[1] * p.pitch;
                 s.outer = p.dims.n[1];
-                s.os = nh;
+                s.os = p.pitch;
             }
             s.ncols = nh;
             Specs<C> sp;
             for (int i = 0; i < nb; i++) sp.p[i] = data[i];
             const char* name = DIR < 0 ? (axis == 1 ? "fft_y_fwd" : "fft_x_fwd") : (axis == 1 ? "fft_y_inv" : "fft_x_inv");
-            double bytes = 2.0 * nb * spectrum_elems(p) * CS;
+            double bytes = 2.0 * nb * spectrum_values(p) * CS;
+            if (tma_enabled()) {
+                const int r = dispatch_pow2<FastStridedTma<T, DIR>::template K>(nline, p, sp, nb, s, axis, name, bytes, st);
+                if (r != TMA_UNAVAILABLE) return r;
+            }
             return dispatch_pow2<FastStrided<T, DIR>::template K>(nline, sp, nb, s, name, bytes, st);
         }
         Strided s;
         const int nh = p.nh;
         if (axis == 1) {
             s.n = p.dims.n[1];
-            s.ls = nh;
+            s.ls = p.pitch;
             s.outer = p.dims.n[0];
-            s.os = (int64_t)p.dims.n[1] * nh;
+            s.os = (int64_t)p.dims.n[1] * p.pitch;
         } else {
             s.n = p.dims.n[0];
-            s.ls = (int64_t)p.dims.n[1] * nh;
+            s.ls = (int64_t)p.dims.n[1] * p.pitch;
             s.outer = p.dims.n[1];
-            s.os = nh;
+            s.os = p.pitch;
         }
         s.ncols = nh;
         int B = choose_B(s.n, 2, CS, BUDGET - s.n * CS, 16);
@@ -876,7 +1085,7 @@ template <typename T> struct FFTLaunch {
         for (int i = 0; i < nb; i++) sp.p[i] = data[i];
         cudaFuncSetAttribute(fft_strided<T, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int64_t ntiles = (int64_t)s.outer * ((nh + B - 1) / B) * nb;
-        PRC_LAUNCH_B((DIR < 0 ? (axis == 1 ? "fft_y_fwd" : "fft_x_fwd") : (axis == 1 ? "fft_y_inv" : "fft_x_inv")), st, 2.0 * nb * spectrum_elems(p) * CS, fft_strided<T, DIR><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(sp, nb, s, axis == 1 ? p.ry : p.rx, B));
+        PRC_LAUNCH_B((DIR < 0 ? (axis == 1 ? "fft_y_fwd" : "fft_x_fwd") : (axis == 1 ? "fft_y_inv" : "fft_x_inv")), st, 2.0 * nb * spectrum_values(p) * CS, fft_strided<T, DIR><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(sp, nb, s, axis == 1 ? p.ry : p.rx, B));
         PRC_CHECK_LAUNCH();
         return PRC_OK;
     }
@@ -887,8 +1096,12 @@ template <typename T> struct FFTLaunch {
             Specs<C> si, so;
             for (int i = 0; i < nin; i++) si.p[i] = in[i];
             for (int i = 0; i < nin * op.nper; i++) so.p[i] = out[i];
-            double bytes = (double)nin * (1 + op.nper) * spectrum_elems(p) * CS;
-            return dispatch_pow2<FastX<T>::template K>(n0, si, nin, so, p.dims, op, bytes, st);
+            double bytes = (double)nin * (1 + op.nper) * spectrum_values(p) * CS;
+            if (tma_enabled()) {
+                const int r = dispatch_pow2<FastXTma<T>::template K>(n0, p, si, nin, so, op, bytes, st);
+                if (r != TMA_UNAVAILABLE) return r;
+            }
+            return dispatch_pow2<FastX<T>::template K>(n0, si, nin, so, p.dims, p.pitch, op, bytes, st);
         }
         int B = choose_B(n0, 3, CS, BUDGET - n0 * CS, 16);
         size_t smem = (size_t)(3 * n0 * B + n0) * CS;
@@ -897,7 +1110,7 @@ template <typename T> struct FFTLaunch {
         for (int i = 0; i < nin * op.nper; i++) so.p[i] = out[i];
         cudaFuncSetAttribute(fft_x_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int64_t ntiles = (int64_t)p.dims.n[1] * ((p.nh + B - 1) / B) * nin;
-        PRC_LAUNCH_B("fft_x_kspace", st, (double)nin * (1 + op.nper) * spectrum_elems(p) * CS, fft_x_fused<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, so, p.dims, p.rx, B, op));
+        PRC_LAUNCH_B("fft_x_kspace", st, (double)nin * (1 + op.nper) * spectrum_values(p) * CS, fft_x_fused<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, so, p.dims, p.pitch, p.rx, B, op));
         PRC_CHECK_LAUNCH();
         return PRC_OK;
     }
@@ -911,7 +1124,11 @@ template <typename T> struct FFTLaunch {
             double bytes = (double)nin * rows * nh * CS +
                            (double)rows * p.dims.n[2] * sizeof(T) *
                                (e.type == EPI_STORE ? nin : (e.type == EPI_STORE4 ? 4 : (e.delta ? 2 : 1)));
-            return dispatch_pow2<FastZC2R<T>::template K>(M, si, nin, p.dims, e, bytes, st);
+            if (tma_enabled()) {
+                const int r = dispatch_pow2<FastZC2RTma<T>::template K>(M, p, si, nin, e, bytes, st);
+                if (r != TMA_UNAVAILABLE) return r;
+            }
+            return dispatch_pow2<FastZC2R<T>::template K>(M, si, nin, p.dims, p.pitch, e, bytes, st);
         }
         int B = 16;
         auto need = [&](int b) { return (size_t)(2 * nh * (b + 1) + nin * M * b + p.dims.n[2]) * CS; };
@@ -922,7 +1139,7 @@ template <typename T> struct FFTLaunch {
         cudaFuncSetAttribute(fft_z_c2r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
         int64_t ntiles = (rows + B - 1) / B;
-        PRC_LAUNCH_B("fft_z_c2r", st, (double)nin * rows * nh * CS + (double)rows * p.dims.n[2] * sizeof(T) * (e.type == EPI_STORE ? nin : (e.delta ? 2 : 1)), fft_z_c2r<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, p.dims, p.rz, B, e));
+        PRC_LAUNCH_B("fft_z_c2r", st, (double)nin * rows * nh * CS + (double)rows * p.dims.n[2] * sizeof(T) * (e.type == EPI_STORE ? nin : (e.delta ? 2 : 1)), fft_z_c2r<T><<<fft_grid(ntiles, 2), FFT_THREADS, smem, st>>>(si, nin, p.dims, p.pitch, p.rz, B, e));
         PRC_CHECK_LAUNCH();
         return PRC_OK;
     }
@@ -970,6 +1187,7 @@ static int smooth_impl(const void* in, int in_bytes, T* out, const int32_t nmesh
                        const double radius[3], void* ws, size_t wsb, cudaStream_t st) {
     Plan3 p;
     PRC_TRY(make_plan(nmesh, &p));
+    pad_pitch<T>(&p);
     if (!ws || wsb < spec_bytes<T>(p)) return PRC_ERR_WORKSPACE;
     cplx_t<T>* S = (cplx_t<T>*)ws;
     const void* ins[1] = {in};
@@ -992,6 +1210,7 @@ static int density_impl(const double* md, const double* mr, const double* sums, 
                         double size_randoms, T* delta, void* ws, size_t wsb, cudaStream_t st) {
     Plan3 p;
     PRC_TRY(make_plan(nmesh, &p));
+    pad_pitch<T>(&p);
     const int nb = mr ? 2 : 1;
     if (!ws || wsb < nb * spec_bytes<T>(p)) return PRC_ERR_WORKSPACE;
     cplx_t<T>* S[2] = {(cplx_t<T>*)ws, (cplx_t<T>*)((char*)ws + spec_bytes<T>(p))};
@@ -1040,6 +1259,7 @@ static int pp_impl(const T* delta, const int32_t nmesh[3], const double boxsize[
     PRC_TRY(psi_epilogue(px, py, pz, psi_stride, &e));
     Plan3 p;
     PRC_TRY(make_plan(nmesh, &p));
+    pad_pitch<T>(&p);
     if (!ws || wsb < 4 * spec_bytes<T>(p)) return PRC_ERR_WORKSPACE;
     cplx_t<T>* S[4];
     for (int i = 0; i < 4; i++) S[i] = (cplx_t<T>*)((char*)ws + i * spec_bytes<T>(p));
@@ -1064,6 +1284,7 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
     PRC_TRY(psi_epilogue(px, py, pz, psi_stride, &es));
     Plan3 p;
     PRC_TRY(make_plan(nmesh, &p));
+    pad_pitch<T>(&p);
     const int nout = los ? 1 : 6;
     // spectra: the forward transform + max(nout, 3) outputs (3 for the final displacements)
     const int nspec = 1 + std::max(nout, 3);
@@ -1152,6 +1373,16 @@ static bool geom_ok(const int32_t* nmesh, const double* boxsize) {
 
 extern "C" {
 
+unsigned int prc_device_fault_flags(int reset) {
+    unsigned int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_fault, sizeof(v)) != cudaSuccess) return 0xffffffffu;
+    if (reset && v != 0) {
+        const unsigned int zero = 0;
+        cudaMemcpyToSymbol(g_fault, &zero, sizeof(zero));
+    }
+    return v;
+}
+
 int prc_fft_supported(const int32_t nmesh[3]) {
     if (!nmesh) return 0;
     Plan3 p;
@@ -1161,7 +1392,12 @@ int prc_fft_supported(const int32_t nmesh[3]) {
 size_t prc_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int nspectra) {
     Plan3 p;
     if (!nmesh || make_plan(nmesh, &p) != PRC_OK) return 0;
-    return (size_t)nspectra * (mesh_bytes == 4 ? spec_bytes<float>(p) : spec_bytes<double>(p));
+    if (mesh_bytes == 4) {
+        pad_pitch<float>(&p);
+        return (size_t)nspectra * spec_bytes<float>(p);
+    }
+    pad_pitch<double>(&p);
+    return (size_t)nspectra * spec_bytes<double>(p);
 }
 
 prc_status_t prc_rfft3d_f32(const void* in, int in_bytes, void* out, const int32_t nmesh[3], void* stream) {

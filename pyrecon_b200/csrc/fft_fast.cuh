@@ -296,53 +296,22 @@ template <typename T, int KT> struct KPoint {
                    // ITER_*, PSI: a = norm / k^2 (0 at k = 0)
 };
 
-// Blocks per SM requested from the register allocator for the FP32 k-space and c2r kernels
-// (tuning knobs PRC_KSPACE_MINB / PRC_C2R_MINB; 1 leaves the allocator free).
-#ifndef PRC_KSPACE_MINB
-#define PRC_KSPACE_MINB 1
-#endif
-#ifndef PRC_C2R_MINB
-#define PRC_C2R_MINB 2
-#endif
-template <typename T, int THREADS, int MINB> struct MinBlocks {
-    static constexpr int value = (sizeof(T) == 4 && THREADS * MINB <= 2048) ? MINB : 1;
-};
-
-template <typename T, int N, int B, int KT>
-__global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE_MINB>::value)) x_kspace(Specs<cplx_t<T>> in, int nin, Specs<cplx_t<T>> out, Dims dims,
-                                                      KOp op) {
+// The k-space step on one x-line held as 8 points per thread (points t + i N/8) at fixed (iy, iz):
+// `setup` computes what does not depend on the output once, `apply` multiplies the forward
+// spectrum v by output o's symmetrised multiplier into u.
+template <typename T, int N, int KT> struct KLine {
     typedef cplx_t<T> C;
-    constexpr int TL = N / 8;
-    extern __shared__ unsigned char smem_raw[];
-    C* tw = (C*)smem_raw;
-    C* buf = tw + N;
-    fill_pass_twiddles<C, N>(tw);
-    __syncthreads();
-    const int n1 = dims.n[1], nh = dims.n[2] / 2 + 1;
-    const int64_t ls = (int64_t)n1 * nh;
-    const int col = threadIdx.x % B, t = threadIdx.x / B;
-    const ColAddr addr{B, col};
-    const int ctiles = (nh + B - 1) / B;
-    const int64_t tiles_per = (int64_t)n1 * ctiles;
-    const int64_t ntiles = tiles_per * nin;
-    const T norm = (T)op.norm, beta = (T)op.beta;
-    const T l0 = (T)op.los[0], l1 = (T)op.los[1], l2 = (T)op.los[2];
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int bi = (int)(tile / tiles_per);
-        const int64_t r = tile % tiles_per;
-        const int iy = (int)(r / ctiles), c0 = (int)(r % ctiles) * B;
-        const int iz = c0 + col;
-        const bool ok = iz < nh;
-        const int64_t off = (int64_t)iy * nh + iz;
-        const C* g = in.p[bi] + off;
-        C v[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) v[i] = ok ? g[(int64_t)(t + i * TL) * ls] : cmake<C>(0, 0);
-        fft_regs<C, N, -1>(v, t, buf, addr, tw);
-        // wavenumbers: ky, kz fixed for this thread, kx per point
-        const T ky = kval<T>(iy, dims.n[1], (T)op.fscale[1]), kz = kval<T>(iz, dims.n[2], (T)op.fscale[2]);
-        const T ty = nyquist(iy, dims.n[1]) ? ky : -ky, tz = nyquist(iz, dims.n[2]) ? kz : -kz;
-        KPoint<T, KT> kp[8];
+    static constexpr int TL = N / 8;
+    T ky, kz, ty, tz;
+    KPoint<T, KT> kp[8];
+
+    __device__ __forceinline__ void setup(const KOp& op, const Dims& dims, int t, int iy, int iz) {
+        const T norm = (T)op.norm, beta = (T)op.beta;
+        const T l0 = (T)op.los[0], l1 = (T)op.los[1], l2 = (T)op.los[2];
+        ky = kval<T>(iy, dims.n[1], (T)op.fscale[1]);
+        kz = kval<T>(iz, dims.n[2], (T)op.fscale[2]);
+        ty = nyquist(iy, dims.n[1]) ? ky : -ky;
+        tz = nyquist(iz, dims.n[2]) ? kz : -kz;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             const int ix = t + i * TL;
@@ -361,37 +330,90 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE
                 kp[i].a = zero ? (T)0 : norm / k2;
             }
         }
+    }
+
+    __device__ __forceinline__ void apply(const KOp& op, const Dims& dims, int t, int o, const C (&v)[8],
+                                          C (&u)[8]) const {
+        const T norm = (T)op.norm;
+        const T l0 = (T)op.los[0], l1 = (T)op.los[1], l2 = (T)op.los[2];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            T re = 0, im = 0;
+            const int ix = t + i * TL;
+            const T kx = kval<T>(ix, dims.n[0], (T)op.fscale[0]);
+            const T tx = nyquist(ix, dims.n[0]) ? kx : -kx;
+            if constexpr (KT == KOP_GAUSS) {
+                re = kp[i].a;
+            } else if constexpr (KT == KOP_PP) {
+                // (i m(k) + conj(i m(k~))) / 2 with m = k_o / (k^2 (1 + beta mu^2))
+                const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
+                im = (T)0.5 * (ko * kp[i].a - to * kp[i].b) * norm;
+            } else if constexpr (KT == KOP_ITER_GLOBAL) {
+                const T kl = kx * l0 + ky * l1 + kz * l2, klt = tx * l0 + ty * l1 + tz * l2;
+                re = (T)0.5 * (kl * kl + klt * klt) * kp[i].a;
+            } else if constexpr (KT == KOP_ITER_LOCAL) {
+                const int ci = o < 3 ? 0 : (o < 5 ? 1 : 2);
+                const int cj = o < 3 ? o : (o < 5 ? o - 2 : 2);
+                const T ki = ci == 0 ? kx : (ci == 1 ? ky : kz), ti = ci == 0 ? tx : (ci == 1 ? ty : tz);
+                const T kj = cj == 0 ? kx : (cj == 1 ? ky : kz), tj = cj == 0 ? tx : (cj == 1 ? ty : tz);
+                re = (T)0.5 * (ki * kj + ti * tj) * kp[i].a;
+            } else if constexpr (KT == KOP_PSI) {
+                const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
+                im = (T)0.5 * (ko - to) * kp[i].a;
+            } else {
+                re = norm;
+            }
+            u[i] = cmake<C>(re * v[i].x - im * v[i].y, re * v[i].y + im * v[i].x);
+        }
+    }
+};
+
+// Blocks per SM requested from the register allocator for the FP32 k-space and c2r kernels
+// (tuning knobs PRC_KSPACE_MINB / PRC_C2R_MINB; 1 leaves the allocator free).
+#ifndef PRC_KSPACE_MINB
+#define PRC_KSPACE_MINB 1
+#endif
+#ifndef PRC_C2R_MINB
+#define PRC_C2R_MINB 2
+#endif
+template <typename T, int THREADS, int MINB> struct MinBlocks {
+    static constexpr int value = (sizeof(T) == 4 && THREADS * MINB <= 2048) ? MINB : 1;
+};
+
+template <typename T, int N, int B, int KT>
+__global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE_MINB>::value)) x_kspace(Specs<cplx_t<T>> in, int nin, Specs<cplx_t<T>> out, Dims dims,
+                                                      int pitch, KOp op) {
+    typedef cplx_t<T> C;
+    constexpr int TL = N / 8;
+    extern __shared__ unsigned char smem_raw[];
+    C* tw = (C*)smem_raw;
+    C* buf = tw + N;
+    fill_pass_twiddles<C, N>(tw);
+    __syncthreads();
+    const int n1 = dims.n[1], nh = dims.n[2] / 2 + 1;
+    const int64_t ls = (int64_t)n1 * pitch;
+    const int col = threadIdx.x % B, t = threadIdx.x / B;
+    const ColAddr addr{B, col};
+    const int ctiles = (nh + B - 1) / B;
+    const int64_t tiles_per = (int64_t)n1 * ctiles;
+    const int64_t ntiles = tiles_per * nin;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int bi = (int)(tile / tiles_per);
+        const int64_t r = tile % tiles_per;
+        const int iy = (int)(r / ctiles), c0 = (int)(r % ctiles) * B;
+        const int iz = c0 + col;
+        const bool ok = iz < nh;
+        const int64_t off = (int64_t)iy * pitch + iz;
+        const C* g = in.p[bi] + off;
+        C v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = ok ? g[(int64_t)(t + i * TL) * ls] : cmake<C>(0, 0);
+        fft_regs<C, N, -1>(v, t, buf, addr, tw);
+        KLine<T, N, KT> kl;
+        kl.setup(op, dims, t, iy, iz);
         for (int o = 0; o < op.nper; o++) {
             C u[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                T re = 0, im = 0;
-                const int ix = t + i * TL;
-                const T kx = kval<T>(ix, dims.n[0], (T)op.fscale[0]);
-                const T tx = nyquist(ix, dims.n[0]) ? kx : -kx;
-                if constexpr (KT == KOP_GAUSS) {
-                    re = kp[i].a;
-                } else if constexpr (KT == KOP_PP) {
-                    // (i m(k) + conj(i m(k~))) / 2 with m = k_o / (k^2 (1 + beta mu^2))
-                    const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
-                    im = (T)0.5 * (ko * kp[i].a - to * kp[i].b) * norm;
-                } else if constexpr (KT == KOP_ITER_GLOBAL) {
-                    const T kl = kx * l0 + ky * l1 + kz * l2, klt = tx * l0 + ty * l1 + tz * l2;
-                    re = (T)0.5 * (kl * kl + klt * klt) * kp[i].a;
-                } else if constexpr (KT == KOP_ITER_LOCAL) {
-                    const int ci = o < 3 ? 0 : (o < 5 ? 1 : 2);
-                    const int cj = o < 3 ? o : (o < 5 ? o - 2 : 2);
-                    const T ki = ci == 0 ? kx : (ci == 1 ? ky : kz), ti = ci == 0 ? tx : (ci == 1 ? ty : tz);
-                    const T kj = cj == 0 ? kx : (cj == 1 ? ky : kz), tj = cj == 0 ? tx : (cj == 1 ? ty : tz);
-                    re = (T)0.5 * (ki * kj + ti * tj) * kp[i].a;
-                } else if constexpr (KT == KOP_PSI) {
-                    const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
-                    im = (T)0.5 * (ko - to) * kp[i].a;
-                } else {
-                    re = norm;
-                }
-                u[i] = cmake<C>(re * v[i].x - im * v[i].y, re * v[i].y + im * v[i].x);
-            }
+            kl.apply(op, dims, t, o, v, u);
             fft_regs<C, N, +1>(u, t, buf, addr, tw);
             C* go = out.p[bi * op.nper + o] + off;
             if (ok) {
@@ -407,9 +429,9 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE
 // CTA = (M / 8) x ROWS threads.
 // ---------------------------------------------------------------------------------------------
 template <typename T, typename TIN, int M, int ROWS>
-__global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T>> out, int nbatch, int64_t rows) {
+__global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T>> out, int nbatch, int64_t rows, int pitch) {
     typedef cplx_t<T> C;
-    constexpr int TL = M / 8, N2 = 2 * M, NH = M + 1, RS = row_stride(M);
+    constexpr int TL = M / 8, N2 = 2 * M, RS = row_stride(M);
     extern __shared__ unsigned char smem_raw[];
     C* tw = (C*)smem_raw;                 // pass table of the M-point transform (M entries)
     C* wk = tw + M;                       // w_{n2}^k, k < M + 1, for the real-FFT unpack
@@ -444,7 +466,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
 #pragma unroll
         for (int i = 0; i < 8; i++) buf[addr(t + i * TL)] = v[i];
         __syncthreads();
-        C* dst = out.p[bi] + row * NH;
+        C* dst = out.p[bi] + row * pitch;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             const int k = t + i * TL;
@@ -506,18 +528,27 @@ __device__ __forceinline__ void row_c2r(const cplx_t<T>* __restrict__ src, bool 
     fft_regs<C, M, +1>(v, t, buf, addr, tw);
 }
 
-template <typename T, int M, int ROWS, int ET>
-__global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_C2R_MINB>::value)) z_c2r(Specs<cplx_t<T>> in, int nin, Dims dims, Epi<T> e) {
+// Input rows read straight from global memory into the row buffer (register kernels).
+template <typename T, int M> struct GlobalRows {
     typedef cplx_t<T> C;
-    constexpr int TL = M / 8, N2 = 2 * M, NH = M + 1, RS = row_stride(M);
+    const Specs<C>& in;
+    int pitch;
+    __device__ __forceinline__ void row(int c, int64_t row, bool ok, int t, C* buf, const RowAddr& addr, const C* tw,
+                                        const C* wk, C (&v)[8]) {
+        row_c2r<T, M>(select6(in, c) + row * pitch, ok, t, buf, addr, tw, wk, v);
+    }
+    __device__ __forceinline__ bool stop() { return false; }
+};
+
+// Inverse z pass over the tiles of ROWS rows, inputs fetched through `src` (GlobalRows, or the
+// TMA-staged rows of fft_tma.cuh), epilogue ET.  tw, wk, buf: pass twiddles, real-FFT roots, the
+// exchange buffer, filled by the caller.
+template <typename T, int M, int ROWS, int ET, class Src>
+__device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, const Epi<T>& e,
+                                           const cplx_t<T>* tw, const cplx_t<T>* wk, cplx_t<T>* buf) {
+    typedef cplx_t<T> C;
+    constexpr int TL = M / 8, N2 = 2 * M, RS = row_stride(M);
     constexpr int NMAX = EpiInputs<ET>::NMAX;
-    extern __shared__ unsigned char smem_raw[];
-    C* tw = (C*)smem_raw;
-    C* wk = tw + M;
-    C* buf = wk + M + 1;
-    fill_pass_twiddles<C, M>(tw);
-    fill_roots(wk, M + 1, N2);
-    __syncthreads();
     const int line = threadIdx.x / TL, t = threadIdx.x % TL;
     const RowAddr addr{line * RS};
     const int64_t rows = (int64_t)dims.n[0] * dims.n[1];
@@ -533,7 +564,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
             for (int c = 0; c < NMAX; c++) {
                 if (c < nin) {
                     C v[8];
-                    row_c2r<T, M>(in.p[c] + row * NH, ok, t, buf, addr, tw, wk, v);
+                    src.row(c, row, ok, t, buf, addr, tw, wk, v);
                     C* o = (C*)(e.out[c] + (ok ? row : 0) * N2);
                     if (ok) {
 #pragma unroll
@@ -544,9 +575,9 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
         } else if constexpr (ET == EPI_STORE4) {
             // three inputs -> one interleaved (x, y, z, 0) quadruple per cell
             C v0[8], v1[8], v2[8];
-            row_c2r<T, M>(in.p[0] + row * NH, ok, t, buf, addr, tw, wk, v0);
-            row_c2r<T, M>(in.p[1] + row * NH, ok, t, buf, addr, tw, wk, v1);
-            row_c2r<T, M>(in.p[2] + row * NH, ok, t, buf, addr, tw, wk, v2);
+            src.row(0, row, ok, t, buf, addr, tw, wk, v0);
+            src.row(1, row, ok, t, buf, addr, tw, wk, v1);
+            src.row(2, row, ok, t, buf, addr, tw, wk, v2);
             if (ok) {
                 typedef typename vec4_of<T>::type V4;
                 V4* o = (V4*)(e.out[0] + row * N2 * 4);
@@ -559,8 +590,8 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
             }
         } else if constexpr (ET == EPI_DENSITY) {
             C d[8], r[8];
-            row_c2r<T, M>(in.p[0] + row * NH, ok, t, buf, addr, tw, wk, d);
-            row_c2r<T, M>(in.p[1] + row * NH, ok, t, buf, addr, tw, wk, r);
+            src.row(0, row, ok, t, buf, addr, tw, wk, d);
+            src.row(1, row, ok, t, buf, addr, tw, wk, r);
             const double sd = e.sums[0], sr = e.sums[1];
             const double alpha = sd * 1. / sr;
             const double threshold = e.ran_min * sr / e.size_randoms;
@@ -576,7 +607,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
             }
         } else if constexpr (ET == EPI_DENSITY_NORANDOMS) {
             C d[8];
-            row_c2r<T, M>(in.p[0] + row * NH, ok, t, buf, addr, tw, wk, d);
+            src.row(0, row, ok, t, buf, addr, tw, wk, d);
             const double mean = e.sums[0] / e.ncells;
             if (ok) {
 #pragma unroll
@@ -609,7 +640,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
 #pragma unroll 1
             for (int c = 0; c < NMAX; c++) {
                 C v[8];
-                row_c2r<T, M>(select6(in, c) + row * NH, ok, t, buf, addr, tw, wk, v);
+                src.row(c, row, ok, t, buf, addr, tw, wk, v);
                 const T fc = (T)select6(e.factor, c) * sc;
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
@@ -635,7 +666,23 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
                 for (int i = 0; i < 8; i++) out0[t + i * TL] = cmake<C>(acc[i][0], acc[i][1]);
             }
         }
+        if (src.stop()) return;
     }
+}
+
+template <typename T, int M, int ROWS, int ET>
+__global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_C2R_MINB>::value))
+    z_c2r(Specs<cplx_t<T>> in, int nin, Dims dims, int pitch, Epi<T> e) {
+    typedef cplx_t<T> C;
+    extern __shared__ unsigned char smem_raw[];
+    C* tw = (C*)smem_raw;
+    C* wk = tw + M;
+    C* buf = wk + M + 1;
+    fill_pass_twiddles<C, M>(tw);
+    fill_roots(wk, M + 1, 2 * M);
+    __syncthreads();
+    GlobalRows<T, M> src{in, pitch};
+    z_c2r_body<T, M, ROWS, ET>(src, nin, dims, e, tw, wk, buf);
 }
 
 }  // namespace fast

@@ -208,6 +208,7 @@ class BaseReconstruction(BaseClass):
             self._shift_call(p, _lib.FIELDS[field], int(shifted), out, obytes)
             low, high = self.info.boxcenter - self.info.boxsize / 2., self.info.boxcenter + self.info.boxsize / 2.
             self._flags.raise_if_set(low, high)
+            _lib.check_device_faults(ReconstructionError)
             return p.output(out)
 
     def read_shifts(self, positions, field='disp+rsd'):

@@ -343,3 +343,27 @@ def test_generic_fft_path_on_power_of_two_sizes():
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     res = subprocess.run([sys.executable, '-c', code], cwd=root, env=env, capture_output=True, text=True, timeout=300)
     assert res.returncode == 0, res.stdout + res.stderr
+
+
+def test_register_fft_path_without_tma():
+    """PRC_FFT_TMA=0 keeps the register-prefetch strided and k-space kernels (the ones user-laid-out
+    FP32 spectra with odd rows always take) checked on the composite entry points too."""
+    import subprocess
+    import sys
+    import os
+    code = ("import sys; sys.path.insert(0, '.'); sys.path.insert(0, 'tests');"
+            "import test_gpu_kernels as T; T.test_fft_against_numpy((16, 16, 16), 'f8'); "
+            "T.test_density_contrast_batched((32, 32, 32), 'f4', True); "
+            "T.test_density_contrast_batched((64, 32, 16), 'f8', True)")
+    env = dict(os.environ, PRC_FFT_TMA='0')
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = subprocess.run([sys.executable, '-c', code], cwd=root, env=env, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+
+
+def test_no_device_faults_after_kernels():
+    """The FFT kernels' bounded waits never ran out in this process."""
+    from pyrecon_b200 import _lib
+    import torch
+    torch.cuda.synchronize()
+    assert _lib.load().prc_device_fault_flags(0) == 0
