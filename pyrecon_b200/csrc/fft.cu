@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_x_fused(Specs<cplx_t<T>> in, 
 // z pass, inverse c2r, with real-space epilogues
 // ---------------------------------------------------------------------------------------------
 enum EpiType { EPI_STORE = 0, EPI_DENSITY = 1, EPI_DENSITY_NORANDOMS = 2, EPI_ITER_GLOBAL = 3, EPI_ITER_LOCAL = 4,
-               EPI_STORE4 = 5 };
+               EPI_STORE4 = 5, EPI_ITER_POLY = 6 };
 
 template <typename T> struct Epi {
     int type;
@@ -796,6 +796,7 @@ template <typename T> struct FastZC2R {
                 case EPI_ITER_GLOBAL: return go<EPI_ITER_GLOBAL>(si, nin, dims, pitch, e, bytes, st);
                 case EPI_ITER_LOCAL: return go<EPI_ITER_LOCAL>(si, nin, dims, pitch, e, bytes, st);
                 case EPI_STORE4: return go<EPI_STORE4>(si, nin, dims, pitch, e, bytes, st);
+                case EPI_ITER_POLY: return go<EPI_ITER_POLY>(si, nin, dims, pitch, e, bytes, st);
                 default: return go<EPI_STORE>(si, nin, dims, pitch, e, bytes, st);
             }
         }
@@ -968,6 +969,35 @@ template <typename T> struct FastXTma {
     };
 };
 
+template <typename T> struct FastHessTma {
+    template <int N> struct K {
+        typedef StridedTmaCfg<T, N> cfg;
+        static int run(const Plan3& p, cplx_t<T>* const* d, cplx_t<T>* const* o, fast::HessGeom h, cudaStream_t st) {
+            typedef fast::TileShape<T, N, cfg::B> TS;
+            tma::Maps maps;
+            for (int i = 0; i < 6; i++)
+                if (!spectrum_map(&maps.m[i], d[i], p, sizeof(cplx_t<T>), cfg::B, TS::BOXL, 1)) return TMA_UNAVAILABLE;
+            Specs<cplx_t<T>> so;
+            for (int i = 0; i < 3; i++) so.p[i] = o[i];
+            Strided s;
+            s.n = p.dims.n[1];
+            s.ls = p.pitch;
+            s.outer = p.dims.n[0];
+            s.os = (int64_t)p.dims.n[1] * p.pitch;
+            s.ncols = p.nh;
+            auto kern = fast::y_hessian_tma<T, N, cfg::B, cfg::S>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
+            const int64_t ntiles = (int64_t)s.outer * ((s.ncols + cfg::B - 1) / cfg::B);
+            const double bytes = 9.0 * spectrum_values(p) * sizeof(cplx_t<T>);
+            PRC_LAUNCH_B("fft_y_inv_hessian", st, bytes,
+                         kern<<<resident_grid(kern, cfg::THREADS, cfg::SMEM, ntiles), cfg::THREADS, cfg::SMEM, st>>>(
+                             maps, so, s, h));
+            PRC_CHECK_LAUNCH();
+            return PRC_OK;
+        }
+    };
+};
+
 template <typename T> struct FastZC2RTma {
     template <int M> struct K {
         typedef RowCfg<T, M> cfg;
@@ -983,6 +1013,7 @@ template <typename T> struct FastZC2RTma {
                 case EPI_ITER_GLOBAL: return go<EPI_ITER_GLOBAL>(p, si, nin, e, bytes, st);
                 case EPI_ITER_LOCAL: return go<EPI_ITER_LOCAL>(p, si, nin, e, bytes, st);
                 case EPI_STORE4: return go<EPI_STORE4>(p, si, nin, e, bytes, st);
+                case EPI_ITER_POLY: return go<EPI_ITER_POLY>(p, si, nin, e, bytes, st);
                 default: return go<EPI_STORE>(p, si, nin, e, bytes, st);
             }
         }
@@ -1314,7 +1345,6 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
         op.type = los ? KOP_ITER_GLOBAL : KOP_ITER_LOCAL;
         op.nper = nout;
         PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));
-        PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, nout, st));
         double base = beta;
         if (it == 0) base /= (1. + beta);
         if (los) {
@@ -1325,6 +1355,27 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
             const int pi[6] = {0, 0, 0, 1, 1, 2}, pj[6] = {0, 1, 2, 1, 2, 2};
             for (int c = 0; c < 6; c++) e.factor[c] = (1. + (pi[c] != pj[c])) * beta / (it == 0 ? (1. + beta) : 1.);
         }
+        if (!los && fast_len(p.dims.n[1]) && !getenv_generic() && tma_enabled()) {
+            // inverse y of the six Hessian spectra combined into the quadratic in x2 (A, B, C over
+            // D00, D01, D02), then the z pass over C, B, A
+            fast::HessGeom h;
+            h.x0_off = e.offset[0];
+            h.x0_cell = e.cell[0];
+            h.x1_off = e.offset[1];
+            h.x1_cell = e.cell[1];
+            for (int c = 0; c < 6; c++) h.f[c] = e.factor[c];
+            cplx_t<T>* outs[3] = {S[1], S[2], S[3]};
+            const int r = dispatch_pow2<FastHessTma<T>::template K>(p.dims.n[1], p, S + 1, outs, h, st);
+            if (r != TMA_UNAVAILABLE) {
+                PRC_TRY(r);
+                Epi<T> ep = e;
+                ep.type = EPI_ITER_POLY;
+                cplx_t<T>* cba[3] = {S[3], S[2], S[1]};
+                PRC_TRY(FFTLaunch<T>::z_c2r(p, cba, 3, ep, st));
+                continue;
+            }
+        }
+        PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, nout, st));
         PRC_TRY(FFTLaunch<T>::z_c2r(p, S + 1, nout, e, st));
     }
     const void* ins[1] = {niter > 0 ? (const void*)dreal : (const void*)delta};

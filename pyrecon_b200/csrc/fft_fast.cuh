@@ -500,7 +500,8 @@ __device__ __forceinline__ double select6(const double (&f)[6], int c) {
 
 template <int ET> struct EpiInputs {
     static constexpr int NMAX =
-        ET == EPI_ITER_LOCAL ? 6 : (ET == EPI_DENSITY ? 2 : ((ET == EPI_STORE || ET == EPI_STORE4) ? 3 : 1));
+        ET == EPI_ITER_LOCAL ? 6
+                             : (ET == EPI_DENSITY ? 2 : ((ET == EPI_STORE || ET == EPI_STORE4 || ET == EPI_ITER_POLY) ? 3 : 1));
 };
 
 // Inverse z transform of one row: returns v[i] = (x[2k], x[2k+1]), k = t + i TL, unscaled.
@@ -615,6 +616,41 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
                     const double o0 = ((double)(d[i].x * sc) / mean - 1.) / e.bias;
                     const double o1 = ((double)(d[i].y * sc) / mean - 1.) / e.bias;
                     out0[t + i * TL] = cmake<C>((T)o0, (T)o1);
+                }
+            }
+        } else if constexpr (ET == EPI_ITER_POLY) {
+            // RSD removal from the quadratic in x2 formed by the Hessian y pass: inputs C, B, A, so
+            // sum_ij f_ij x_i x_j d_ij = (C x2 + B) x2 + A, evaluated by Horner as the rows arrive.
+            const T x0 = (T)(e.offset[0] + e.cell[0] * ix), x1 = (T)(e.offset[1] + e.cell[1] * iy);
+            const T oz = (T)e.offset[2], cz = (T)e.cell[2];
+            T r[8][2];
+#pragma unroll 1
+            for (int c = 0; c < 3; c++) {
+                C v[8];
+                src.row(c, row, ok, t, buf, addr, tw, wk, v);
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const T val = (h ? v[i].y : v[i].x) * sc;
+                        const T xz = oz + cz * (T)(2 * (t + i * TL) + h);
+                        r[i][h] = c == 0 ? val : r[i][h] * xz + val;
+                    }
+                }
+            }
+            if (ok) {
+                const C* dl = (const C*)(e.delta + row * N2);
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const C d0 = dl[t + i * TL];
+                    T o[2];
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const T xz = oz + cz * (T)(2 * (t + i * TL) + h);
+                        const T ix2 = (T)1 / ((x0 * x0 + x1 * x1) + xz * xz);
+                        o[h] = (h ? d0.y : d0.x) - r[i][h] * ix2;
+                    }
+                    out0[t + i * TL] = cmake<C>(o[0], o[1]);
                 }
             }
         } else {

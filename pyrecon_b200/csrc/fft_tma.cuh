@@ -333,4 +333,113 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
     z_c2r_body<T, M, ROWS, ET>(src, nin, dims, e, tw, wk, buf);
 }
 
+// Inverse y pass of the six Hessian spectra D_ij = k_i k_j delta(k) / k^2 of the local-line-of-sight
+// iteration, combined on the fly.  After the inverse x (done) and y transforms, x0 (fixed per tile)
+// and x1 (per point) are known, so the weighted sum over (i, j) of f_ij x_i x_j d_ij, which the
+// real-space update needs, is a quadratic in x2 with coefficients
+//   A = f00 x0^2 D00 + f01 x0 x1 D01 + f11 x1^2 D11,   B = f02 x0 D02 + f12 x1 D12,   C = f22 D22
+// that are formed here, before the inverse z transform (which they commute with, being constant along
+// z).  The three are written in place of D00, D01, D02, so the z pass reads 3 spectra instead of 6
+// and runs 3 row transforms instead of 6.  Inputs stream through S stages in the order
+// D00, D01, D11 | D02, D12 | D22, one accumulator per output.
+struct HessGeom {
+    double x0_off, x0_cell;   // x0 = x0_off + x0_cell * ix (mesh-dtype offset, float64 cell as the epilogue)
+    double x1_off, x1_cell;   // x1 = x1_off + x1_cell * iy
+    double f[6];              // f_ij in the order (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+};
+
+template <typename T, int N, int B, int S>
+__global__ void __launch_bounds__(N / 8 * B) y_hessian_tma(const __grid_constant__ prc::tma::Maps maps,
+                                                           Specs<cplx_t<T>> out, Strided s, HessGeom h) {
+    typedef cplx_t<T> C;
+    typedef TileShape<T, N, B> TS;
+    constexpr int TL = N / 8;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    C* stages = (C*)smem_raw;
+    C* tw = stages + S * TS::ELEMS;
+    uint64_t* bars = (uint64_t*)(tw + N);
+    const int tid = threadIdx.x, col = tid % B, t = tid / B;
+    const ColAddr addr{B, col};
+    if (tid == 0) {
+        for (int i = 0; i < S; i++) prc::tma::barrier_init(&bars[i], 1);
+        prc::tma::fence_barrier_init();
+    }
+    fill_pass_twiddles<C, N>(tw);
+    const int ctiles = (s.ncols + B - 1) / B;
+    const int64_t ntiles = (int64_t)s.outer * ctiles;
+    __syncthreads();
+    if ((prc::tma::smem_addr(stages) & 127) != 0) {
+        if (tid == 0) atomicOr(&prc::g_fault, prc::tma::FAULT_SMEM_ALIGN);
+        return;
+    }
+    // unit u: tile blockIdx.x + (u / 6) gridDim.x, spectrum ORDER[u % 6]
+    auto spectrum_of = [](int k) { return k < 2 ? k : (k == 2 ? 3 : (k == 3 ? 2 : k)); };
+    auto issue = [&](int64_t u) {
+        const int64_t tile = blockIdx.x + (u / 6) * gridDim.x;
+        if (tile >= ntiles) return;
+        const TileAt a = tile_at(tile, ntiles, ctiles, B);
+        issue_tile<T, N, B>(stages + (u % S) * TS::ELEMS, &maps.m[spectrum_of((int)(u % 6))], &bars[u % S], 1, a.o,
+                            a.c0);
+    };
+    if (tid == 0)
+        for (int u = 0; u < S; u++) issue(u);
+    int64_t u = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const TileAt a = tile_at(tile, ntiles, ctiles, B);
+        const T x0 = (T)(h.x0_off + h.x0_cell * a.o);
+        T x1[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x1[i] = (T)(h.x1_off + h.x1_cell * (t + i * TL));
+        const bool store = a.c0 + col < s.ncols;
+        const int64_t off = (int64_t)a.o * s.os + a.c0 + col;
+#pragma unroll 1
+        for (int g = 0; g < 3; g++) {
+            C acc[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) acc[i] = cmake<C>(0, 0);
+            const int nterm = g == 0 ? 3 : (g == 1 ? 2 : 1);
+#pragma unroll 1
+            for (int q = 0; q < nterm; q++, u++) {
+                const int st = (int)(u % S);
+                const bool ok = prc::tma::wait(&bars[st], (uint32_t)((u / S) & 1));
+                if (__syncthreads_or(!ok)) {
+                    if (tid == 0) {
+                        atomicOr(&prc::g_fault, prc::tma::FAULT_WAIT_TIMEOUT);
+                        for (int d = 0; d < S; d++) {
+                            const int64_t uu = u + d;
+                            if ((int64_t)blockIdx.x + (uu / 6) * gridDim.x >= ntiles) break;
+                            prc::tma::wait(&bars[uu % S], (uint32_t)((uu / S) & 1));
+                        }
+                    }
+                    return;
+                }
+                C* sb = stages + st * TS::ELEMS;
+                C v[8];
+#pragma unroll
+                for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
+                __syncthreads();
+                fft_regs<C, N, +1>(v, t, sb, addr, tw);
+                if (tid == 0) {
+                    prc::tma::fence_proxy_async();
+                    issue(u + S);
+                }
+                const int k = g == 0 ? (q == 0 ? 0 : (q == 1 ? 1 : 3)) : (g == 1 ? (q == 0 ? 2 : 4) : 5);
+                const T f = (T)(k == 0 ? h.f[0] : k == 1 ? h.f[1] : k == 2 ? h.f[2] : k == 3 ? h.f[3] : k == 4 ? h.f[4] : h.f[5]);
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    // weight of D_k at this point: f x0^2 | f x0 x1 | f x1^2 | f x0 | f x1 | f
+                    const T w = k == 0 ? f * (x0 * x0) : k == 1 ? f * (x0 * x1[i]) : k == 3 ? f * (x1[i] * x1[i])
+                              : k == 2 ? f * x0 : k == 4 ? f * x1[i] : f;
+                    acc[i] = cmake<C>(acc[i].x + w * v[i].x, acc[i].y + w * v[i].y);
+                }
+            }
+            if (store) {
+                C* o = (g == 0 ? out.p[0] : (g == 1 ? out.p[1] : out.p[2])) + off;
+#pragma unroll
+                for (int i = 0; i < 8; i++) o[(int64_t)(t + i * TL) * s.ls] = acc[i];
+            }
+        }
+    }
+}
+
 }  // namespace fast
