@@ -623,6 +623,11 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
             // sum_ij f_ij x_i x_j d_ij = (C x2 + B) x2 + A, evaluated by Horner as the rows arrive.
             const T x0 = (T)(e.offset[0] + e.cell[0] * ix), x1 = (T)(e.offset[1] + e.cell[1] * iy);
             const T oz = (T)e.offset[2], cz = (T)e.cell[2];
+            // the original density contrast is fetched first, so its latency hides behind the transforms
+            const C* dl = (const C*)(e.delta + (ok ? row : 0) * N2);
+            C dv[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) dv[i] = ok ? dl[t + i * TL] : cmake<C>(0, 0);
             T r[8][2];
 #pragma unroll 1
             for (int c = 0; c < 3; c++) {
@@ -639,10 +644,9 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
                 }
             }
             if (ok) {
-                const C* dl = (const C*)(e.delta + row * N2);
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
-                    const C d0 = dl[t + i * TL];
+                    const C d0 = dv[i];
                     T o[2];
 #pragma unroll
                     for (int h = 0; h < 2; h++) {
