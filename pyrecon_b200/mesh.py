@@ -358,6 +358,10 @@ class BaseMesh(BaseClass):
         new.attrs = dict(self.attrs)
         if copy_value and self.value is not None:
             new.__dict__['value'] = self.value.clone()
+        if '_accum' in new.__dict__:
+            # the copy owns its values; a later paint into it starts a new FP64 accumulator from them
+            new.__dict__['_accum'] = None
+            new.__dict__['_colsums'] = None
         return new
 
     def __repr__(self):
@@ -390,6 +394,23 @@ class RealMesh(BaseMesh):
     @property
     def shape(self):
         return self.info.shape
+
+    def __getattr__(self, name):
+        # An FP32 mesh filled by assign_cic keeps its FP64 sums (what set_density_contrast reads); its
+        # FP32 `value` is made from them on first access only.
+        if name == 'value':
+            accum = self.__dict__.get('_accum')
+            if accum is None:
+                return None
+            value = accum.to(_torch().float32)
+            self.__dict__['value'] = value
+            return value
+        raise AttributeError(name)
+
+    @property
+    def is_set(self):
+        """Whether the mesh holds values (painted or assigned), without materialising them."""
+        return self.__dict__.get('value') is not None or self.__dict__.get('_accum') is not None
 
     def __setattr__(self, name, value):
         if name == 'value' and value is not None:
@@ -435,7 +456,10 @@ class RealMesh(BaseMesh):
                 self._accum.copy_(self.value)
             self._colsums = torch.zeros(int(self.nmesh[0]) * int(self.nmesh[1]), dtype=torch.float64, device=self.device)
         paint(self.info, self._accum, self._colsums, p, wrap, True, self._workspace(), self._flags(), check=check)
-        self.__dict__['value'] = self._accum if self.dtype.itemsize == 8 else self._accum.to(torch.float32)
+        if self.dtype.itemsize == 8:
+            self.__dict__['value'] = self._accum
+        else:
+            self.__dict__.pop('value', None)
 
     def _workspace(self):
         if getattr(self, '_ws', None) is None:

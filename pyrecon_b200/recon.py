@@ -132,7 +132,7 @@ class BaseReconstruction(BaseClass):
 
     def assign_randoms(self, positions, weights=None, check=True):
         """Same as :meth:`assign_data`, for randoms."""
-        if self.mesh_randoms.value is None:
+        if not self.mesh_randoms.is_set:
             self._size_randoms = 0
         with self._stream_ctx():
             self.mesh_randoms.assign_cic(positions, weights=weights, wrap=self.wrap, check=check)
@@ -140,7 +140,7 @@ class BaseReconstruction(BaseClass):
 
     @property
     def has_randoms(self):
-        return self.mesh_randoms.value is not None
+        return self.mesh_randoms.is_set
 
     # -- density contrast (recon.py:198-249) --
 
@@ -156,7 +156,7 @@ class BaseReconstruction(BaseClass):
             radius = _array3(smoothing_radius, self.info._type_float)
             lib = _lib.load()
             st = _lib.stream_of(self.device)
-            if self.mesh_data.value is None:
+            if not self.mesh_data.is_set:
                 raise ReconstructionError('assign_data must be called before set_density_contrast')
             sums = torch.zeros(2, dtype=torch.float64, device=self.device)
             sws = torch.empty(lib.prc_sum_workspace_bytes(0), dtype=torch.uint8, device=self.device)
@@ -195,11 +195,17 @@ class BaseReconstruction(BaseClass):
     def _shift_call(self, particles, field, shifted, out, out_bytes):
         raise NotImplementedError
 
+    # particles per chunk of a read-out from host memory (copies in, kernel, copies out overlap)
+    _read_chunk = 1 << 21
+
     def _read(self, positions, field, shifted):
         import torch
         field = field.lower()
         if field not in ALLOWED_FIELDS:
             raise ReconstructionError('Unknown field {}. Choices are {}'.format(field, ALLOWED_FIELDS))
+        host = not (isinstance(positions, torch.Tensor) and positions.is_cuda)
+        if host and len(positions) > self._read_chunk:
+            return self._read_pipelined(positions, field, shifted)
         with self._stream_ctx():
             p = Particles(positions, self.device)
             pbytes = p.pos_bytes
@@ -210,6 +216,75 @@ class BaseReconstruction(BaseClass):
             self._flags.raise_if_set(low, high)
             _lib.check_device_faults(ReconstructionError)
             return p.output(out)
+
+    def _copy_streams(self):
+        import torch
+        if getattr(self, '_streams', None) is None:
+            self._streams = (torch.cuda.Stream(self.device), torch.cuda.Stream(self.device))
+        return self._streams
+
+    def _read_pipelined(self, positions, field, shifted):
+        """Read-out of host positions in chunks: the host-to-device copy of chunk i + 1, the kernel on
+        chunk i and the device-to-host copy of chunk i - 1 run at once (two copy streams, events
+        between them; the kernels stay on the reconstruction's stream).  Same results as one call."""
+        import torch
+        numpy_in = not isinstance(positions, torch.Tensor)
+        if numpy_in:
+            arr = np.asarray(positions)
+            if arr.dtype not in (np.float32, np.float64):
+                arr = arr.astype('f8')
+            host = torch.from_numpy(np.ascontiguousarray(arr))
+        else:
+            host = positions if positions.dtype in (torch.float32, torch.float64) else positions.double()
+            host = host.contiguous()
+        if host.ndim != 2 or host.shape[1] != 3:
+            raise MeshError('positions must be of shape (N, 3)')
+        n, pbytes = int(host.shape[0]), host.element_size()
+        obytes = max(pbytes, self.info.dtype.itemsize) if (shifted and self.wrap) else pbytes
+        odt = torch_dtype('f4' if obytes == 4 else 'f8')
+        out_host = torch.empty((n, 3), dtype=odt, pin_memory=True)
+        chunk = self._read_chunk
+        s_in, s_out = self._copy_streams()
+        with self._stream_ctx():
+            compute = torch.cuda.current_stream(self.device)
+            nbuf = 2
+            din = [torch.empty((chunk, 3), dtype=host.dtype, device=self.device) for _ in range(nbuf)]
+            dout = [torch.empty((chunk, 3), dtype=odt, device=self.device) for _ in range(nbuf)]
+            for k in range(nbuf):
+                din[k].record_stream(s_in)
+                dout[k].record_stream(s_out)
+            read_done, copied_out = [None] * nbuf, [None] * nbuf
+
+            class _Chunk(object):
+                pass
+
+            for i, a in enumerate(range(0, n, chunk)):
+                k, b = i % nbuf, min(n, a + chunk)
+                m = b - a
+                with torch.cuda.stream(s_in):
+                    if read_done[k] is not None:
+                        s_in.wait_event(read_done[k])
+                    din[k][:m].copy_(host[a:b], non_blocking=True)
+                    arrived = torch.cuda.Event()
+                    arrived.record(s_in)
+                compute.wait_event(arrived)
+                if copied_out[k] is not None:
+                    compute.wait_event(copied_out[k])
+                c = _Chunk()
+                c.pos, c.size, c.pos_bytes = din[k], m, pbytes
+                self._shift_call(c, _lib.FIELDS[field], int(shifted), dout[k], obytes)
+                read_done[k] = torch.cuda.Event()
+                read_done[k].record(compute)
+                with torch.cuda.stream(s_out):
+                    s_out.wait_event(read_done[k])
+                    out_host[a:b].copy_(dout[k][:m], non_blocking=True)
+                    copied_out[k] = torch.cuda.Event()
+                    copied_out[k].record(s_out)
+            s_out.synchronize()
+            low, high = self.info.boxcenter - self.info.boxsize / 2., self.info.boxcenter + self.info.boxsize / 2.
+            self._flags.raise_if_set(low, high)
+            _lib.check_device_faults(ReconstructionError)
+        return out_host.numpy() if numpy_in else out_host
 
     def read_shifts(self, positions, field='disp+rsd'):
         """Displacements at ``positions``: 'disp' (Zeldovich), 'rsd' or 'disp+rsd'."""
