@@ -12,7 +12,8 @@
  * Conditions found while running (positions outside the box, NaN/inf) are OR-ed into the
  * caller's device word `flags` (PRC_FLAG_*); kernels downstream of a raised flag in the same
  * call skip their writes, so the output mesh is left untouched, as the reference leaves it
- * when it raises MeshError (pyrecon/mesh.py:549-553).
+ * when it raises MeshError (pyrecon/mesh.py:549-553); a paint that does not accumulate
+ * (accumulate = 0, the mesh's previous contents unused) writes zeros instead.
  *
  * Meshes are C-ordered (n0, n1, n2); half spectra are (n0, n1, n2/2+1) interleaved complex;
  * positions are (N, 3) row-major float32 or float64 (`pos_bytes` = 4 or 8).  `_f32` / `_f64`

@@ -382,12 +382,20 @@ __global__ void __launch_bounds__(PULL_WARPS * 32) paint_pull(const uint32_t* __
                                                               int accumulate, double* __restrict__ mesh,
                                                               double* __restrict__ column_sums,
                                                               const int32_t* __restrict__ flags) {
-    if (*flags) return;
     extern __shared__ double s_col[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n0 = dims.n[0], n1 = dims.n[1], n2 = dims.n[2];
     double* col = s_col + (size_t)warp * n2;
     const int64_t ncol = (int64_t)n0 * n1;
+    if (*flags) {
+        // bad catalogue: an accumulated mesh is left as it was, a fresh one comes out zero
+        if (!accumulate)
+            for (int64_t c = (int64_t)blockIdx.x * PULL_WARPS + warp; c < ncol; c += (int64_t)gridDim.x * PULL_WARPS) {
+                for (int z = lane; z < n2; z += 32) mesh[c * n2 + z] = 0.;
+                if (column_sums != nullptr && lane == 0) column_sums[c] = 0.;
+            }
+        return;
+    }
     for (int64_t c = (int64_t)blockIdx.x * PULL_WARPS + warp; c < ncol; c += (int64_t)gridDim.x * PULL_WARPS) {
         const int X = (int)(c / n1), Y = (int)(c % n1);
         for (int z = lane; z < n2; z += 32) col[z] = 0.;

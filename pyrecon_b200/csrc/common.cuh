@@ -142,13 +142,20 @@ __host__ __forceinline__ int ceil_div(int64_t a, int64_t b) { return (int)((a + 
 
 int device_sm_count();
 
+// Adds n to the launch counter (kernels replayed inside a CUDA graph launch).
+void add_launches(unsigned long long n);
+// Launches and compulsory bytes recorded by this thread's captures since the last call (reset).
+void capture_tally(unsigned long long* launches, double* bytes);
+
 // Every kernel launch goes through PRC_LAUNCH: it counts launches (prc_launch_count) and, when
 // prc_profile_enable(1) is on, brackets the launch with CUDA events on its stream so the
 // per-kernel device time can be read back with prc_profile_collect.
 // `bytes` is the launch's compulsory DRAM traffic (what it must read and write at least), so
 // the profile reports achieved bandwidth against the HBM roofline.
+// Launches made while the calling thread captures a stream are not counted or timed; they are
+// tallied per thread (capture_tally) so a replayed graph can report them.
 struct KernelScope {
-    KernelScope(const char* name, cudaStream_t st, double bytes = 0.);
+    KernelScope(const char* name, cudaStream_t st, double bytes = 0., bool count = true);
     ~KernelScope();
     const char* name;
     cudaStream_t st;

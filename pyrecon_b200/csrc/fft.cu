@@ -927,7 +927,12 @@ template <typename T, int DIR> struct FastStridedTma {
     };
 };
 
+// PRC_TMA_KSPACE_LEAN=1: FP32 k-space kernel with the spectrum kept in shared memory, two CTAs per SM.
+#ifndef PRC_TMA_KSPACE_LEAN
+#define PRC_TMA_KSPACE_LEAN 0
+#endif
 template <typename T, int N> struct KSpaceTmaCfg {
+    static constexpr bool LEAN = PRC_TMA_KSPACE_LEAN && sizeof(T) == 4;
     static constexpr int B = KSpaceCfg<T, N>::B;
     static constexpr int THREADS = KSpaceCfg<T, N>::THREADS;
     static constexpr int S = 2;
@@ -940,7 +945,7 @@ template <typename T> struct FastXTma {
         static int go(const tma::Maps& maps, int nin, Specs<cplx_t<T>> so, const Plan3& p, KOp op, double bytes,
                       cudaStream_t st) {
             typedef KSpaceTmaCfg<T, N> cfg;
-            auto kern = fast::x_kspace_tma<T, N, cfg::B, cfg::S, KT>;
+            auto kern = fast::x_kspace_tma<T, N, cfg::B, cfg::S, KT, cfg::LEAN>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
             const int64_t ntiles = (int64_t)p.dims.n[1] * ((p.nh + cfg::B - 1) / cfg::B) * nin;
             PRC_LAUNCH_B("fft_x_kspace", st, bytes,

@@ -139,8 +139,11 @@ __global__ void __launch_bounds__(N / 8 * B) strided_tma(const __grid_constant__
     }
 }
 
-template <typename T, int N, int B, int S, int KT>
-__global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE_MINB>::value))
+// LEAN: the forward spectrum is kept in the tile's stage (not in registers) and the per-point
+// multiplier terms are recomputed for every output, so two CTAs fit on an SM (FP32); the stage is
+// re-armed only after the tile's last output.
+template <typename T, int N, int B, int S, int KT, bool LEAN>
+__global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 : PRC_KSPACE_MINB>::value))
     x_kspace_tma(const __grid_constant__ prc::tma::Maps maps, int nin, Specs<cplx_t<T>> out, Dims dims, int pitch,
                  KOp op) {
     typedef cplx_t<T> C;
@@ -189,30 +192,65 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE
         C* sb = stages + st * TS::ELEMS;
         const TileAt a = tile_at(tile, tiles_per, ctiles, B);
         const int iy = a.o, iz = a.c0 + col;
-        C v[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
-        __syncthreads();
-        fft_regs<C, N, -1>(v, t, sb, addr, tw);
-        if (tid == 0) {
-            const int64_t next = tile + (int64_t)S * gridDim.x;
-            if (next < ntiles) {
-                const TileAt b = tile_at(next, tiles_per, ctiles, B);
-                prc::tma::fence_proxy_async();
-                issue_tile<T, N, B>(sb, &maps.m[b.bi], &bars[st], 0, b.o, b.c0);
+        auto refill = [&]() {
+            if (tid == 0) {
+                const int64_t next = tile + (int64_t)S * gridDim.x;
+                if (next < ntiles) {
+                    const TileAt b = tile_at(next, tiles_per, ctiles, B);
+                    prc::tma::fence_proxy_async();
+                    issue_tile<T, N, B>(sb, &maps.m[b.bi], &bars[st], 0, b.o, b.c0);
+                }
             }
-        }
-        KLine<T, N, KT> kl;
-        kl.setup(op, dims, t, iy, iz);
+        };
         const int64_t off = (int64_t)iy * pitch + iz;
-        for (int o = 0; o < op.nper; o++) {
-            C u[8];
-            kl.apply(op, dims, t, o, v, u);
-            fft_regs<C, N, +1>(u, t, xbuf, addr, tw);
-            if (iz < nh) {
-                C* go = out.p[a.bi * op.nper + o] + off;
+        if constexpr (LEAN) {
+            {
+                C v[8];
 #pragma unroll
-                for (int i = 0; i < 8; i++) go[(int64_t)(t + i * TL) * ls] = u[i];
+                for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
+                __syncthreads();
+                fft_regs<C, N, -1>(v, t, sb, addr, tw);
+                if constexpr (Plan<N>::NPASS == 1) __syncthreads();
+#pragma unroll
+                for (int i = 0; i < 8; i++) sb[(t + i * TL) * B + col] = v[i];
+            }
+            for (int o = 0; o < op.nper; o++) {
+                C u[8];
+                {
+                    C v[8];
+#pragma unroll
+                    for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
+                    KLine<T, N, KT> kl;
+                    kl.setup(op, dims, t, iy, iz);
+                    kl.apply(op, dims, t, o, v, u);
+                }
+                fft_regs<C, N, +1>(u, t, xbuf, addr, tw);
+                if (iz < nh) {
+                    C* go = out.p[a.bi * op.nper + o] + off;
+#pragma unroll
+                    for (int i = 0; i < 8; i++) go[(int64_t)(t + i * TL) * ls] = u[i];
+                }
+            }
+            __syncthreads();
+            refill();
+        } else {
+            C v[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
+            __syncthreads();
+            fft_regs<C, N, -1>(v, t, sb, addr, tw);
+            refill();
+            KLine<T, N, KT> kl;
+            kl.setup(op, dims, t, iy, iz);
+            for (int o = 0; o < op.nper; o++) {
+                C u[8];
+                kl.apply(op, dims, t, o, v, u);
+                fft_regs<C, N, +1>(u, t, xbuf, addr, tw);
+                if (iz < nh) {
+                    C* go = out.p[a.bi * op.nper + o] + off;
+#pragma unroll
+                    for (int i = 0; i < 8; i++) go[(int64_t)(t + i * TL) * ls] = u[i];
+                }
             }
         }
     }

@@ -26,21 +26,71 @@ struct TimedLaunch {
 };
 std::mutex g_mutex;
 std::vector<TimedLaunch> g_timed;
+// Recycled timing events per device (creating an event per launch would add host time to every
+// profiled launch).
+std::map<int, std::vector<cudaEvent_t>> g_event_pool;
+
+cudaEvent_t take_event() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lock(g_mutex);
+        auto& pool = g_event_pool[dev];
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+// Caller holds g_mutex.
+void recycle_event(cudaEvent_t e) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    g_event_pool[dev].push_back(e);
+}
 }  // namespace
 
-KernelScope::KernelScope(const char* n, cudaStream_t s, double b) : name(n), st(s), start(nullptr), bytes(b) {
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+void add_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+thread_local unsigned long long t_capture_launches = 0;
+thread_local double t_capture_bytes = 0.;
+}  // namespace
+
+void capture_tally(unsigned long long* launches, double* bytes) {
+    if (launches) *launches = t_capture_launches;
+    if (bytes) *bytes = t_capture_bytes;
+    t_capture_launches = 0;
+    t_capture_bytes = 0.;
+}
+
+KernelScope::KernelScope(const char* n, cudaStream_t s, double b, bool count)
+    : name(n), st(s), start(nullptr), bytes(b) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        // inside a capture: tallied for the graph, neither counted nor timed here
+        t_capture_launches += 1;
+        t_capture_bytes += b;
+        return;
+    }
+    if (count) g_launches.fetch_add(1, std::memory_order_relaxed);
     if (g_profiling.load(std::memory_order_relaxed)) {
-        if (cudaEventCreate(&start) == cudaSuccess) cudaEventRecord(start, st);
-        else start = nullptr;
+        start = take_event();
+        if (start != nullptr) cudaEventRecord(start, st);
     }
 }
 
 KernelScope::~KernelScope() {
     if (start == nullptr) return;
-    cudaEvent_t stop;
-    if (cudaEventCreate(&stop) != cudaSuccess) {
-        cudaEventDestroy(start);
+    cudaEvent_t stop = take_event();
+    if (stop == nullptr) {
+        std::lock_guard<std::mutex> lock(g_mutex);
+        recycle_event(start);
         return;
     }
     cudaEventRecord(stop, st);
@@ -99,8 +149,9 @@ unsigned long long prc_launch_count(void) { return prc::g_launches.load(); }
 void prc_profile_enable(int on) {
     std::lock_guard<std::mutex> lock(prc::g_mutex);
     for (auto& t : prc::g_timed) {
-        cudaEventDestroy(t.start);
-        cudaEventDestroy(t.stop);
+        cudaEventSynchronize(t.stop);
+        prc::recycle_event(t.start);
+        prc::recycle_event(t.stop);
     }
     prc::g_timed.clear();
     prc::g_profiling.store(on ? 1 : 0);
@@ -119,8 +170,8 @@ int prc_profile_collect(char* buf, size_t cap) {
                 a.ms += ms;
                 a.bytes += t.bytes;
             }
-            cudaEventDestroy(t.start);
-            cudaEventDestroy(t.stop);
+            prc::recycle_event(t.start);
+            prc::recycle_event(t.stop);
         }
         prc::g_timed.clear();
     }

@@ -19,6 +19,11 @@
 #include "common.cuh"
 
 #include <algorithm>
+#include <list>
+#include <map>
+#include <mutex>
+#include <stdlib.h>
+#include <string>
 #include <vector>
 
 namespace prc {
@@ -64,6 +69,17 @@ __device__ __forceinline__ void coeffs(const Stencil<S>& s, int x, int y, int z,
     for (int d = 0; d < 3; d++) G[d] = (T)s.ih2[d] + g * p[d] * p[d];
 }
 
+// S(v) from the six axis neighbours and the three edge combinations e_ab = v(+a+b) + v(-a-b) -
+// v(-a+b) - v(+a-b); every kernel evaluates it through this one expression.
+template <typename A>
+__device__ __forceinline__ A stencil_terms(A vxp, A vxm, A vyp, A vym, A vzp, A vzm, A exy, A exz, A eyz, const A p[3],
+                                           A g, const A G[3], int local) {
+    A s = G[0] * (vxp + vxm) + G[1] * (vyp + vym) + G[2] * (vzp + vzm);
+    s += g / (A)2 * (p[0] * p[1] * exy + p[0] * p[2] * exz + p[1] * p[2] * eyz);
+    if (local) s += g * (p[0] * (vxp - vxm) + p[1] * (vyp - vym) + p[2] * (vzp - vzm));
+    return s;
+}
+
 // The neighbour terms of S(v) at one cell, accumulated in type A from a mesh of type V.
 template <typename A, typename V>
 __device__ __forceinline__ A neighbour_sum(const V* __restrict__ v, const int n[3], int x, int y, int z, const A p[3],
@@ -78,20 +94,20 @@ __device__ __forceinline__ A neighbour_sum(const V* __restrict__ v, const int n[
     const A vxp = L(Xp, Y0, z), vxm = L(Xm, Y0, z);
     const A vyp = L(X0, Yp, z), vym = L(X0, Ym, z);
     const A vzp = L(X0, Y0, zp), vzm = L(X0, Y0, zm);
-    A s = G[0] * (vxp + vxm) + G[1] * (vyp + vym) + G[2] * (vzp + vzm);
-    s += g / (A)2 * (p[0] * p[1] * (L(Xp, Yp, z) + L(Xm, Ym, z) - L(Xm, Yp, z) - L(Xp, Ym, z))
-                   + p[0] * p[2] * (L(Xp, Y0, zp) + L(Xm, Y0, zm) - L(Xm, Y0, zp) - L(Xp, Y0, zm))
-                   + p[1] * p[2] * (L(X0, Yp, zp) + L(X0, Ym, zm) - L(X0, Ym, zp) - L(X0, Yp, zm)));
-    if (local) s += g * (p[0] * (vxp - vxm) + p[1] * (vyp - vym) + p[2] * (vzp - vzm));
+    const A exy = L(Xp, Yp, z) + L(Xm, Ym, z) - L(Xm, Yp, z) - L(Xp, Ym, z);
+    const A exz = L(Xp, Y0, zp) + L(Xm, Y0, zm) - L(Xm, Y0, zp) - L(Xp, Y0, zm);
+    const A eyz = L(X0, Yp, zp) + L(X0, Ym, zm) - L(X0, Ym, zp) - L(X0, Yp, zm);
 #undef L
-    return s;
+    return stencil_terms<A>(vxp, vxm, vyp, vym, vzp, vzm, exy, exz, eyz, p, g, G, local);
 }
 
-__device__ __forceinline__ void cell_of(int64_t i, const int n[3], int& x, int& y, int& z) {
-    z = (int)(i % n[2]);
-    int64_t r = i / n[2];
-    y = (int)(r % n[1]);
-    x = (int)(r / n[1]);
+// Kernels run one thread per cell of a 3D launch: (z, y) over the block's (x, y) threads, x over
+// blockIdx.z, so no index division is needed.
+__device__ __forceinline__ bool cell3(const int n[3], int& x, int& y, int& z) {
+    z = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y * blockDim.y + threadIdx.y;
+    x = blockIdx.z;
+    return z < n[2] && y < n[1];
 }
 
 // One damped-Jacobi sweep: vout = (1 - w) v + w (f + S(v)) / (2 sum G).  zero_v: v is
@@ -99,20 +115,137 @@ __device__ __forceinline__ void cell_of(int64_t i, const int n[3], int& x, int& 
 template <typename T, typename FT>
 __global__ void __launch_bounds__(256) jacobi_sweep(const T* __restrict__ v, const FT* __restrict__ f,
                                                     T* __restrict__ vout, Stencil<T> s, T w, int zero_v) {
-    const int64_t N = (int64_t)s.n[0] * s.n[1] * s.n[2];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        cell_of(i, s.n, x, y, z);
-        T p[3], g, G[3];
-        coeffs<T>(s, x, y, z, p, g, G);
-        T jac = (T)f[i];
-        T vc = (T)0;
-        if (!zero_v) {
-            jac += neighbour_sum<T>(v, s.n, x, y, z, p, g, G, s.local);
-            vc = v[i];
+    int x, y, z;
+    if (!cell3(s.n, x, y, z)) return;
+    const int64_t i = ((int64_t)x * s.n[1] + y) * s.n[2] + z;
+    T p[3], g, G[3];
+    coeffs<T>(s, x, y, z, p, g, G);
+    T jac = (T)f[i];
+    T vc = (T)0;
+    if (!zero_v) {
+        jac += neighbour_sum<T>(v, s.n, x, y, z, p, g, G, s.local);
+        vc = v[i];
+    }
+    jac /= (T)2 * (G[0] + G[1] + G[2]);
+    vout[i] = ((T)1 - w) * vc + w * jac;
+}
+
+// ---- four cells along z per thread (n2 % 4 == 0, 16-byte aligned meshes) ----
+// The thread loads the nine (x +- 1, y +- 1) columns it needs once as vectors (the five that need
+// z - 1 and z + 4 as well), so a cell costs ~5 loads instead of 19 and the index arithmetic is
+// shared.  Same expression per cell as the one-cell kernels.
+template <typename T> __device__ __forceinline__ void load4(const T* __restrict__ p, T (&o)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 q = __ldg((const float4*)p);
+        o[0] = q.x, o[1] = q.y, o[2] = q.z, o[3] = q.w;
+    } else {
+        const double2 a = __ldg((const double2*)p), b = __ldg((const double2*)p + 1);
+        o[0] = a.x, o[1] = a.y, o[2] = b.x, o[3] = b.y;
+    }
+}
+// values at z0 - 1 .. z0 + 4 of one column (periodic in z)
+template <typename T> __device__ __forceinline__ void load6(const T* __restrict__ col, int z0, int n2, T (&o)[6]) {
+    T m[4];
+    load4(col + z0, m);
+    o[0] = __ldg(col + (z0 == 0 ? n2 - 1 : z0 - 1));
+    o[1] = m[0], o[2] = m[1], o[3] = m[2], o[4] = m[3];
+    o[5] = __ldg(col + (z0 + 4 == n2 ? 0 : z0 + 4));
+}
+
+struct Quad {
+    int x, y, z0;
+    int64_t c;        // offset of (x, y, 0)
+};
+__device__ __forceinline__ bool quad_of(const int n[3], Quad& q) {
+    q.z0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    q.y = blockIdx.y * blockDim.y + threadIdx.y;
+    q.x = blockIdx.z;
+    q.c = ((int64_t)q.x * n[1] + q.y) * n[2];
+    return q.z0 < n[2] && q.y < n[1];
+}
+
+// S(v) at the four cells of a quad (type A), with their coefficients.
+template <typename A, typename V, typename S>
+__device__ __forceinline__ void quad_stencil(const V* __restrict__ v, const Stencil<S>& s, const Quad& q, A (&sv)[4],
+                                             A (&diag)[4]) {
+    const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
+    const int64_t sx = (int64_t)n1 * n2;
+    const int64_t xp = (int64_t)wrap_up(q.x, n0) * sx, xm = (int64_t)wrap_dn(q.x, n0) * sx, x0 = (int64_t)q.x * sx;
+    const int64_t yp = (int64_t)wrap_up(q.y, n1) * n2, ym = (int64_t)wrap_dn(q.y, n1) * n2, y0 = (int64_t)q.y * n2;
+    V c[6], XP[6], XM[6], YP[6], YM[6], PP[4], MM[4], MP[4], PM[4];
+    load6(v + x0 + y0, q.z0, n2, c);
+    load6(v + xp + y0, q.z0, n2, XP);
+    load6(v + xm + y0, q.z0, n2, XM);
+    load6(v + x0 + yp, q.z0, n2, YP);
+    load6(v + x0 + ym, q.z0, n2, YM);
+    load4(v + xp + yp + q.z0, PP);
+    load4(v + xm + ym + q.z0, MM);
+    load4(v + xm + yp + q.z0, MP);
+    load4(v + xp + ym + q.z0, PM);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        A p[3], g, G[3];
+        coeffs<A>(s, q.x, q.y, q.z0 + k, p, g, G);
+        const A exy = (A)PP[k] + (A)MM[k] - (A)MP[k] - (A)PM[k];
+        const A exz = (A)XP[k + 2] + (A)XM[k] - (A)XM[k + 2] - (A)XP[k];
+        const A eyz = (A)YP[k + 2] + (A)YM[k] - (A)YM[k + 2] - (A)YP[k];
+        sv[k] = stencil_terms<A>((A)XP[k + 1], (A)XM[k + 1], (A)YP[k + 1], (A)YM[k + 1], (A)c[k + 2], (A)c[k], exy, exz,
+                                 eyz, p, g, G, s.local);
+        diag[k] = (A)2 * (G[0] + G[1] + G[2]);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) jacobi_sweep4(const T* __restrict__ v, const T* __restrict__ f,
+                                                     T* __restrict__ vout, Stencil<T> s, T w, int zero_v) {
+    Quad q;
+    if (!quad_of(s.n, q)) return;
+    T fv[4], sv[4], dg[4], vc[4];
+    load4(f + q.c + q.z0, fv);
+    if (zero_v) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            T p[3], g, G[3];
+            coeffs<T>(s, q.x, q.y, q.z0 + k, p, g, G);
+            sv[k] = (T)0;
+            dg[k] = (T)2 * (G[0] + G[1] + G[2]);
+            vc[k] = (T)0;
         }
-        jac /= (T)2 * (G[0] + G[1] + G[2]);
-        vout[i] = ((T)1 - w) * vc + w * jac;
+    } else {
+        quad_stencil<T>(v, s, q, sv, dg);
+        load4(v + q.c + q.z0, vc);
+    }
+    T o[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        T jac = fv[k];
+        if (!zero_v) jac += sv[k];
+        jac /= dg[k];
+        o[k] = ((T)1 - w) * vc[k] + w * jac;
+    }
+    if constexpr (sizeof(T) == 4) {
+        *(float4*)(vout + q.c + q.z0) = make_float4(o[0], o[1], o[2], o[3]);
+    } else {
+        ((double2*)(vout + q.c + q.z0))[0] = make_double2(o[0], o[1]);
+        ((double2*)(vout + q.c + q.z0))[1] = make_double2(o[2], o[3]);
+    }
+}
+
+template <typename A, typename V, typename FT, typename R, typename S>
+__global__ void __launch_bounds__(256) residual_kernel4(const V* __restrict__ v, const FT* __restrict__ f,
+                                                        R* __restrict__ r, Stencil<S> s) {
+    Quad q;
+    if (!quad_of(s.n, q)) return;
+    A sv[4], dg[4];
+    quad_stencil<A>(v, s, q, sv, dg);
+    V vc[4];
+    FT fv[4];
+    load4(v + q.c + q.z0, vc);
+    load4(f + q.c + q.z0, fv);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const A av = dg[k] * (A)vc[k] - sv[k];
+        r[q.c + q.z0 + k] = (R)((A)fv[k] - av);
     }
 }
 
@@ -120,26 +253,24 @@ __global__ void __launch_bounds__(256) jacobi_sweep(const T* __restrict__ v, con
 template <typename A, typename V, typename FT, typename R, typename S>
 __global__ void __launch_bounds__(256) residual_kernel(const V* __restrict__ v, const FT* __restrict__ f,
                                                        R* __restrict__ r, Stencil<S> s) {
-    const int64_t N = (int64_t)s.n[0] * s.n[1] * s.n[2];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        cell_of(i, s.n, x, y, z);
-        A p[3], g, G[3];
-        coeffs<A>(s, x, y, z, p, g, G);
-        const A nb = neighbour_sum<A>(v, s.n, x, y, z, p, g, G, s.local);
-        const A av = (A)2 * (G[0] + G[1] + G[2]) * (A)v[i] - nb;
-        r[i] = (R)((A)f[i] - av);
-    }
+    int x, y, z;
+    if (!cell3(s.n, x, y, z)) return;
+    const int64_t i = ((int64_t)x * s.n[1] + y) * s.n[2] + z;
+    A p[3], g, G[3];
+    coeffs<A>(s, x, y, z, p, g, G);
+    const A nb = neighbour_sum<A>(v, s.n, x, y, z, p, g, G, s.local);
+    const A av = (A)2 * (G[0] + G[1] + G[2]) * (A)v[i] - nb;
+    r[i] = (R)((A)f[i] - av);
 }
 
 // 27-point full weighting, coarse cell (x, y, z) centred on fine (2x, 2y, 2z).
 template <typename A, typename TI, typename TO>
 __global__ void __launch_bounds__(256) reduce_kernel(const TI* __restrict__ fine, TO* __restrict__ coarse, Dims nf) {
     const int nc[3] = {nf.n[0] / 2, nf.n[1] / 2, nf.n[2] / 2};
-    const int64_t N = (int64_t)nc[0] * nc[1] * nc[2];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    {
         int x, y, z;
-        cell_of(i, nc, x, y, z);
+        if (!cell3(nc, x, y, z)) return;
+        const int64_t i = ((int64_t)x * nc[1] + y) * nc[2] + z;
         const int X[3] = {wrap_dn(2 * x, nf.n[0]), 2 * x, wrap_up(2 * x, nf.n[0])};
         const int Y[3] = {wrap_dn(2 * y, nf.n[1]), 2 * y, wrap_up(2 * y, nf.n[1])};
         const int Z[3] = {wrap_dn(2 * z, nf.n[2]), 2 * z, wrap_up(2 * z, nf.n[2])};
@@ -164,11 +295,10 @@ __global__ void __launch_bounds__(256) reduce_kernel(const TI* __restrict__ fine
 // else fine = value.
 template <typename A, typename TI, typename TO, bool ADD>
 __global__ void __launch_bounds__(256) prolong_kernel(const TI* __restrict__ coarse, TO* __restrict__ fine, Dims nc) {
-    const int64_t N = (int64_t)nc.n[0] * nc.n[1] * nc.n[2];
     const int nf1 = 2 * nc.n[1], nf2 = 2 * nc.n[2];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    {
         int x, y, z;
-        cell_of(i, nc.n, x, y, z);
+        if (!cell3(nc.n, x, y, z)) return;
         const int xs[2] = {x, wrap_up(x, nc.n[0])}, ys[2] = {y, wrap_up(y, nc.n[1])}, zs[2] = {z, wrap_up(z, nc.n[2])};
         A c[2][2][2];
 #pragma unroll
@@ -211,6 +341,33 @@ __global__ void add_kernel(TA* __restrict__ acc, const TB* __restrict__ x, int64
 static int grid_for(int64_t n) {
     int64_t blocks = (n + 255) / 256;
     return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)device_sm_count() * 16));
+}
+
+// 3D launch over an (n0, n1, n2) mesh for the cell3 kernels: up to 32 z x 8 y threads per block.
+struct Grid3 {
+    dim3 grid, block;
+};
+static Grid3 grid3(const int n[3]) {
+    int bx = 1, by = 1;
+    while (bx < n[2] && bx < 32) bx <<= 1;
+    while (by < n[1] && bx * by < 256) by <<= 1;
+    Grid3 g;
+    g.block = dim3(bx, by, 1);
+    g.grid = dim3((n[2] + bx - 1) / bx, (n[1] + by - 1) / by, n[0]);
+    return g;
+}
+static Grid3 grid3_coarse(const int nf[3]) {
+    const int nc[3] = {nf[0] / 2, nf[1] / 2, nf[2] / 2};
+    return grid3(nc);
+}
+// Launch of the four-cells-per-thread kernels, usable when n2 % 4 == 0 and the meshes are
+// 16-byte aligned.
+static Grid3 grid3_quad(const int n[3]) {
+    const int nq[3] = {n[0], n[1], n[2] / 4};
+    return grid3(nq);
+}
+static bool quad_ok(const int n[3], const void* a, const void* b, const void* c) {
+    return n[2] % 4 == 0 && (((uintptr_t)a | (uintptr_t)b | (uintptr_t)c) & 15) == 0;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -264,35 +421,52 @@ template <typename T> struct MGRunner {
         return make_stencil<T>(L[l].n, P.boxsize, P.boxcenter, P.beta, P.has_los ? P.los : nullptr);
     }
 
-    // niter sweeps in place on v (ping-pong through tmp); zero_first: v known to be zero.
-    int jacobi(int l, T* v, const T* f, T* tmp, int niter, bool zero_first) {
+    // niter sweeps ping-ponging between v and tmp; on return v points at the result and tmp at the
+    // other buffer (the pointers are swapped instead of copying back).  zero_first: v known zero.
+    int jacobi(int l, T*& v, const T* f, T*& tmp, int niter, bool zero_first) {
         Stencil<T> s = stencil(l);
         const int64_t N = L[l].size();
-        T* src = v;
-        T* dst = tmp;
+        const Grid3 g = grid3(L[l].n);
         if (niter == 0 && zero_first && cudaMemsetAsync(v, 0, N * sizeof(T), st) != cudaSuccess) return PRC_ERR_CUDA;
+        const bool quad = quad_ok(L[l].n, v, f, tmp);
+        const Grid3 gq = grid3_quad(L[l].n);
         for (int it = 0; it < niter; it++) {
-            PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * ((zero_first && it == 0) ? 2 : 3), jacobi_sweep<T, T><<<grid_for(N), 256, 0, st>>>(src, f, dst, s, (T)P.damping, zero_first && it == 0));
-            std::swap(src, dst);
+            const bool z0 = zero_first && it == 0;
+            if (quad)
+                PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
+                             jacobi_sweep4<T><<<gq.grid, gq.block, 0, st>>>(v, f, tmp, s, (T)P.damping, z0));
+            else
+                PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
+                             jacobi_sweep<T, T><<<g.grid, g.block, 0, st>>>(v, f, tmp, s, (T)P.damping, z0));
+            std::swap(v, tmp);
         }
-        if (src != v) cudaMemcpyAsync(v, src, N * sizeof(T), cudaMemcpyDeviceToDevice, st);
         PRC_CHECK_LAUNCH();
         return PRC_OK;
     }
 
-    // Recursive V-cycle on level l: v (B[l].v) with right-hand side f.
-    int vcycle(int l, T* v, const T* f, bool v_zero) {
+    // Recursive V-cycle on level l: v (B[l].v, or the caller's level-0 pointer) with right-hand side f.
+    int vcycle(int l, T*& v, const T* f, bool v_zero) {
         PRC_TRY(jacobi(l, v, f, B[l].tmp, P.jn, v_zero));
         if (l + 1 < (int)L.size()) {
             Stencil<T> s = stencil(l);
             const int64_t N = L[l].size();
-            PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T), residual_kernel<T, T, T, T, T><<<grid_for(N), 256, 0, st>>>(v, f, B[l].r, s));
+            const Grid3 g = grid3(L[l].n), gc = grid3_coarse(L[l].n);
+            if (quad_ok(L[l].n, v, f, B[l].r)) {
+                const Grid3 gq = grid3_quad(L[l].n);
+                PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T),
+                             residual_kernel4<T, T, T, T, T><<<gq.grid, gq.block, 0, st>>>(v, f, B[l].r, s));
+            } else {
+                PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T),
+                             residual_kernel<T, T, T, T, T><<<g.grid, g.block, 0, st>>>(v, f, B[l].r, s));
+            }
             Dims nf = {{L[l].n[0], L[l].n[1], L[l].n[2]}};
-            PRC_LAUNCH_B("mg_reduce", st, (double)(N + L[l + 1].size()) * sizeof(T), reduce_kernel<T, T, T><<<grid_for(L[l + 1].size()), 256, 0, st>>>(B[l].r, B[l + 1].f, nf));
+            PRC_LAUNCH_B("mg_reduce", st, (double)(N + L[l + 1].size()) * sizeof(T),
+                         reduce_kernel<T, T, T><<<gc.grid, gc.block, 0, st>>>(B[l].r, B[l + 1].f, nf));
             PRC_CHECK_LAUNCH();
             PRC_TRY(vcycle(l + 1, B[l + 1].v, B[l + 1].f, true));
             Dims nc = {{L[l + 1].n[0], L[l + 1].n[1], L[l + 1].n[2]}};
-            PRC_LAUNCH_B("mg_prolong_add", st, (double)(2 * N + L[l + 1].size()) * sizeof(T), prolong_kernel<T, T, T, true><<<grid_for(L[l + 1].size()), 256, 0, st>>>(B[l + 1].v, v, nc));
+            PRC_LAUNCH_B("mg_prolong_add", st, (double)(2 * N + L[l + 1].size()) * sizeof(T),
+                         prolong_kernel<T, T, T, true><<<gc.grid, gc.block, 0, st>>>(B[l + 1].v, v, nc));
             PRC_CHECK_LAUNCH();
         }
         return jacobi(l, v, f, B[l].tmp, P.jn, false);
@@ -307,24 +481,30 @@ template <typename T> static int fmg_plain(MGRunner<T>& R, const T* f0, T* v0) {
     R.B[0].f = const_cast<T*>(f0);
     for (int l = 0; l + 1 < nl; l++) {
         Dims nf = {{R.L[l].n[0], R.L[l].n[1], R.L[l].n[2]}};
-        PRC_LAUNCH_B("mg_reduce", st, (double)(R.L[l].size() + R.L[l + 1].size()) * sizeof(T), reduce_kernel<T, T, T><<<grid_for(R.L[l + 1].size()), 256, 0, st>>>(R.B[l].f, R.B[l + 1].f, nf));
+        const Grid3 gc = grid3_coarse(R.L[l].n);
+        PRC_LAUNCH_B("mg_reduce", st, (double)(R.L[l].size() + R.L[l + 1].size()) * sizeof(T),
+                     reduce_kernel<T, T, T><<<gc.grid, gc.block, 0, st>>>(R.B[l].f, R.B[l + 1].f, nf));
     }
     PRC_CHECK_LAUNCH();
-    // the FMG solution of level l lives in fmg_v[l]; level 0 writes straight into v0
+    // the FMG solution of level l >= 1 lives in B[l].v; level 0 starts in v0 and may end in
+    // B[0].tmp (pointer swaps), in which case it is copied to v0 once at the end
+    T* v0cur = v0;
     for (int l = nl - 1; l >= 0; l--) {
-        T* v = l == 0 ? v0 : R.B[l].v;
+        T*& v = l == 0 ? v0cur : R.B[l].v;
         if (l == nl - 1) {
             if (cudaMemsetAsync(v, 0, R.L[l].size() * sizeof(T), st) != cudaSuccess) return PRC_ERR_CUDA;
         } else {
             Dims nc = {{R.L[l + 1].n[0], R.L[l + 1].n[1], R.L[l + 1].n[2]}};
-            PRC_LAUNCH_B("mg_prolong", st, (double)(R.L[l].size() + R.L[l + 1].size()) * sizeof(T), prolong_kernel<T, T, T, false><<<grid_for(R.L[l + 1].size()), 256, 0, st>>>(R.B[l + 1].v, v, nc));
+            const Grid3 gc = grid3(R.L[l + 1].n);
+            PRC_LAUNCH_B("mg_prolong", st, (double)(R.L[l].size() + R.L[l + 1].size()) * sizeof(T),
+                         prolong_kernel<T, T, T, false><<<gc.grid, gc.block, 0, st>>>(R.B[l + 1].v, v, nc));
             PRC_CHECK_LAUNCH();
         }
-        // V-cycles at level l use the coarser levels' v as scratch: keep this level's FMG
-        // solution in `v` and run the recursion with v_zero = false.
-        // the next finer level prolongs from R.B[l].v, which is `v` itself for l >= 1
         for (int it = 0; it < R.P.vn; it++) PRC_TRY(R.vcycle(l, v, R.B[l].f, l == nl - 1 && it == 0));
     }
+    if (v0cur != v0 &&
+        cudaMemcpyAsync(v0, v0cur, R.L[0].size() * sizeof(T), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return PRC_ERR_CUDA;
     return PRC_OK;
 }
 
@@ -440,32 +620,165 @@ int run_mixed(const float* delta, float* phi, const int32_t nmesh[3], const Para
     PRC_LAUNCH_B("mg_convert", st, 12.0 * N0, convert_kernel<float, double><<<grid_for(N0), 256, 0, st>>>(delta, m.f64[0], N0));
     for (int l = 0; l + 1 < nl; l++) {
         Dims nf = {{m.L[l].n[0], m.L[l].n[1], m.L[l].n[2]}};
-        PRC_LAUNCH_B("mg_reduce", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()), reduce_kernel<double, double, double><<<grid_for(m.L[l + 1].size()), 256, 0, st>>>(m.f64[l], m.f64[l + 1], nf));
+        const Grid3 gc = grid3_coarse(m.L[l].n);
+        PRC_LAUNCH_B("mg_reduce", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()),
+                     reduce_kernel<double, double, double><<<gc.grid, gc.block, 0, st>>>(m.f64[l], m.f64[l + 1], nf));
     }
     PRC_CHECK_LAUNCH();
     for (int l = nl - 1; l >= 0; l--) {
         const int64_t N = m.L[l].size();
+        const Grid3 g = grid3(m.L[l].n);
         if (l == nl - 1) {
             if (cudaMemsetAsync(m.v64[l], 0, N * 8, st) != cudaSuccess) return PRC_ERR_CUDA;
         } else {
             Dims nc = {{m.L[l + 1].n[0], m.L[l + 1].n[1], m.L[l + 1].n[2]}};
-            PRC_LAUNCH_B("mg_prolong", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()), prolong_kernel<double, double, double, false><<<grid_for(m.L[l + 1].size()), 256, 0, st>>>(m.v64[l + 1],
-                                                                                                    m.v64[l], nc));
+            const Grid3 gc = grid3(m.L[l + 1].n);
+            PRC_LAUNCH_B("mg_prolong", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()),
+                         prolong_kernel<double, double, double, false><<<gc.grid, gc.block, 0, st>>>(m.v64[l + 1],
+                                                                                                  m.v64[l], nc));
         }
         Stencil<double> s64 = make_stencil<double>(m.L[l].n, P.boxsize, P.boxcenter, P.beta,
                                                    P.has_los ? P.los : nullptr);
         for (int it = 0; it < P.vn; it++) {
             // defect in FP64 (stored FP32 as the inner V-cycle's right-hand side)
-            PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N, residual_kernel<double, double, double, float, double><<<grid_for(N), 256, 0, st>>>(m.v64[l], m.f64[l],
-                                                                                            m.b32[l].f, s64));
+            if (quad_ok(m.L[l].n, m.v64[l], m.f64[l], R.B[l].f)) {
+                const Grid3 gq = grid3_quad(m.L[l].n);
+                PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N,
+                             residual_kernel4<double, double, double, float, double><<<gq.grid, gq.block, 0, st>>>(
+                                 m.v64[l], m.f64[l], R.B[l].f, s64));
+            } else {
+                PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N,
+                             residual_kernel<double, double, double, float, double><<<g.grid, g.block, 0, st>>>(
+                                 m.v64[l], m.f64[l], R.B[l].f, s64));
+            }
             PRC_CHECK_LAUNCH();
-            PRC_TRY(R.vcycle(l, m.b32[l].v, m.b32[l].f, true));
-            PRC_LAUNCH_B("mg_correct_fp64", st, 20.0 * N, add_kernel<double, float><<<grid_for(N), 256, 0, st>>>(m.v64[l], m.b32[l].v, N));
+            PRC_TRY(R.vcycle(l, R.B[l].v, R.B[l].f, true));
+            PRC_LAUNCH_B("mg_correct_fp64", st, 20.0 * N,
+                         add_kernel<double, float><<<grid_for(N), 256, 0, st>>>(m.v64[l], R.B[l].v, N));
             PRC_CHECK_LAUNCH();
         }
     }
     PRC_LAUNCH_B("mg_convert", st, 12.0 * N0, convert_kernel<double, float><<<grid_for(N0), 256, 0, st>>>(m.v64[0], phi, N0));
     PRC_CHECK_LAUNCH();
+    return PRC_OK;
+}
+
+// ---- the whole solve as a CUDA graph ----
+//
+// A solve is a fixed sequence of some thousands of small launches (most on the coarse levels),
+// set by the mesh, the parameters and the buffer addresses.  It is captured once into a CUDA graph
+// and replayed while those stay the same (a small cache keyed on all of them), on a library stream
+// that waits for the caller's stream and is waited for by it.  PRC_MG_GRAPH=0 launches directly.
+struct GraphEntry {
+    std::string key;
+    int device;
+    cudaGraphExec_t exec;
+    unsigned long long launches;
+    double bytes;
+};
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t in = nullptr, out = nullptr;
+};
+std::mutex g_graph_mutex;
+std::list<GraphEntry> g_graphs;
+std::map<int, SideStream> g_side;
+constexpr size_t GRAPH_CACHE = 8;
+
+bool graphs_enabled() {
+    static int cached = -1;
+    if (cached < 0) {
+        const char* v = getenv("PRC_MG_GRAPH");
+        cached = (v != nullptr && v[0] == '0') ? 0 : 1;
+    }
+    return cached == 1;
+}
+
+template <typename V> void key_add(std::string& k, const V& v) { k.append((const char*)&v, sizeof(V)); }
+
+std::string solve_key(int tsize, int mixed, const int32_t nmesh[3], const Params& P, const void* delta,
+                      const void* phi, const void* ws, size_t wsb) {
+    std::string k;
+    key_add(k, tsize);
+    key_add(k, mixed);
+    for (int d = 0; d < 3; d++) {
+        key_add(k, nmesh[d]);
+        key_add(k, P.boxsize[d]);
+        key_add(k, P.boxcenter[d]);
+        key_add(k, P.los[d]);
+    }
+    key_add(k, P.has_los);
+    key_add(k, P.beta);
+    key_add(k, P.damping);
+    key_add(k, P.jn);
+    key_add(k, P.vn);
+    key_add(k, delta);
+    key_add(k, phi);
+    key_add(k, ws);
+    key_add(k, wsb);
+    return k;
+}
+
+template <typename F> int run_graph(const std::string& key, cudaStream_t st, F body) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (!graphs_enabled() || cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+        return body(st);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PRC_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_graph_mutex);
+    SideStream& side = g_side[dev];
+    if (side.s == nullptr) {
+        if (cudaStreamCreateWithFlags(&side.s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&side.in, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&side.out, cudaEventDisableTiming) != cudaSuccess) {
+            side = SideStream();
+            return body(st);
+        }
+    }
+    if (cudaEventRecord(side.in, st) != cudaSuccess || cudaStreamWaitEvent(side.s, side.in, 0) != cudaSuccess)
+        return PRC_ERR_CUDA;
+    auto it = g_graphs.begin();
+    for (; it != g_graphs.end(); ++it)
+        if (it->device == dev && it->key == key) break;
+    if (it != g_graphs.end()) {
+        g_graphs.splice(g_graphs.begin(), g_graphs, it);
+    } else {
+        capture_tally(nullptr, nullptr);
+        if (cudaStreamBeginCapture(side.s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return PRC_ERR_CUDA;
+        const int r = body(side.s);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(side.s, &g);
+        GraphEntry ent;
+        capture_tally(&ent.launches, &ent.bytes);
+        if (r != PRC_OK || e != cudaSuccess || g == nullptr) {
+            if (g != nullptr) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return r != PRC_OK ? r : PRC_ERR_CUDA;
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&ent.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return PRC_ERR_CUDA;
+        ent.key = key;
+        ent.device = dev;
+        g_graphs.push_front(ent);
+        while (g_graphs.size() > GRAPH_CACHE) {
+            const GraphEntry& old = g_graphs.back();
+            int cur = dev;
+            if (old.device != cur) cudaSetDevice(old.device);
+            cudaDeviceSynchronize();
+            cudaGraphExecDestroy(old.exec);
+            if (old.device != cur) cudaSetDevice(cur);
+            g_graphs.pop_back();
+        }
+    }
+    const GraphEntry& ent = g_graphs.front();
+    {
+        KernelScope scope("mg_solve_graph", side.s, ent.bytes, false);
+        if (cudaGraphLaunch(ent.exec, side.s) != cudaSuccess) return PRC_ERR_CUDA;
+    }
+    add_launches(ent.launches);
+    if (cudaEventRecord(side.out, side.s) != cudaSuccess || cudaStreamWaitEvent(st, side.out, 0) != cudaSuccess)
+        return PRC_ERR_CUDA;
     return PRC_OK;
 }
 
@@ -488,8 +801,12 @@ prc_status_t prc_multigrid_f32(const float* delta, float* phi, const int32_t nme
                                size_t workspace_bytes, void* stream) {
     if (!mg_args_ok(delta, phi, nmesh, boxsize, boxcenter, jacobi_niterations, vcycle_niterations)) return PRC_ERR_ARG;
     Params P = make_params(boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los);
-    if (mixed_precision) return run_mixed(delta, phi, nmesh, P, workspace, workspace_bytes, (cudaStream_t)stream);
-    return run_plain<float>(delta, phi, nmesh, P, workspace, workspace_bytes, (cudaStream_t)stream);
+    if (!workspace || workspace_bytes < prc_multigrid_workspace_bytes(nmesh, 4, mixed_precision)) return PRC_ERR_WORKSPACE;
+    const std::string key = solve_key(4, mixed_precision ? 1 : 0, nmesh, P, delta, phi, workspace, workspace_bytes);
+    return run_graph(key, (cudaStream_t)stream, [&](cudaStream_t s) {
+        if (mixed_precision) return run_mixed(delta, phi, nmesh, P, workspace, workspace_bytes, s);
+        return run_plain<float>(delta, phi, nmesh, P, workspace, workspace_bytes, s);
+    });
 }
 
 prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t nmesh[3], const double boxsize[3],
@@ -498,7 +815,10 @@ prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t n
                                void* stream) {
     if (!mg_args_ok(delta, phi, nmesh, boxsize, boxcenter, jacobi_niterations, vcycle_niterations)) return PRC_ERR_ARG;
     Params P = make_params(boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los);
-    return run_plain<double>(delta, phi, nmesh, P, workspace, workspace_bytes, (cudaStream_t)stream);
+    if (!workspace || workspace_bytes < prc_multigrid_workspace_bytes(nmesh, 8, 0)) return PRC_ERR_WORKSPACE;
+    const std::string key = solve_key(8, 0, nmesh, P, delta, phi, workspace, workspace_bytes);
+    return run_graph(key, (cudaStream_t)stream,
+                     [&](cudaStream_t s) { return run_plain<double>(delta, phi, nmesh, P, workspace, workspace_bytes, s); });
 }
 
 #define MG_COMPONENTS(SUF, T)                                                                                        \
@@ -510,7 +830,12 @@ prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t n
         R.L = hierarchy(nmesh);                                                                                      \
         R.P = make_params(boxsize, boxcenter, beta, damping, niterations, 0, los);                                  \
         R.st = (cudaStream_t)stream;                                                                                 \
-        return R.jacobi(0, v, f, scratch, niterations, false);                                                      \
+        T *cur = v, *other = scratch;                                                                                \
+        PRC_TRY(R.jacobi(0, cur, f, other, niterations, false));                                                     \
+        if (cur != v && cudaMemcpyAsync(v, cur, (size_t)R.L[0].size() * sizeof(T), cudaMemcpyDeviceToDevice,       \
+                                        (cudaStream_t)stream) != cudaSuccess)                                        \
+            return PRC_ERR_CUDA;                                                                                     \
+        return PRC_OK;                                                                                               \
     }                                                                                                                \
     prc_status_t prc_mg_residual_##SUF(const T* v, const T* f, T* r, const int32_t nmesh[3],                        \
                                        const double boxsize[3], const double boxcenter[3], double beta,             \
@@ -518,27 +843,24 @@ prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t n
         if (!v || !f || !r || !nmesh || !boxsize || !boxcenter) return PRC_ERR_ARG;                                 \
         int n[3] = {nmesh[0], nmesh[1], nmesh[2]};                                                                   \
         Stencil<T> s = make_stencil<T>(n, boxsize, boxcenter, beta, los);                                            \
-        int64_t N = (int64_t)n[0] * n[1] * n[2];                                                                     \
         PRC_LAUNCH("mg_residual", (cudaStream_t)stream,                                                              \
-                   residual_kernel<T, T, T, T, T><<<grid_for(N), 256, 0, (cudaStream_t)stream>>>(v, f, r, s));     \
+                   residual_kernel<T, T, T, T, T><<<grid3(n).grid, grid3(n).block, 0, (cudaStream_t)stream>>>(v, f, r, s)); \
         PRC_CHECK_LAUNCH();                                                                                          \
         return PRC_OK;                                                                                               \
     }                                                                                                                \
     prc_status_t prc_mg_reduce_##SUF(const T* fine, T* coarse, const int32_t nf[3], void* stream) {                 \
         if (!fine || !coarse || !nf) return PRC_ERR_ARG;                                                             \
         Dims d = {{nf[0], nf[1], nf[2]}};                                                                            \
-        int64_t N = (int64_t)(nf[0] / 2) * (nf[1] / 2) * (nf[2] / 2);                                                \
         PRC_LAUNCH("mg_reduce", (cudaStream_t)stream,                                                                \
-                   reduce_kernel<T, T, T><<<grid_for(N), 256, 0, (cudaStream_t)stream>>>(fine, coarse, d));       \
+                   reduce_kernel<T, T, T><<<grid3_coarse(nf).grid, grid3_coarse(nf).block, 0, (cudaStream_t)stream>>>(fine, coarse, d)); \
         PRC_CHECK_LAUNCH();                                                                                          \
         return PRC_OK;                                                                                               \
     }                                                                                                                \
     prc_status_t prc_mg_prolong_##SUF(const T* coarse, T* fine, const int32_t nc[3], void* stream) {                \
         if (!fine || !coarse || !nc) return PRC_ERR_ARG;                                                             \
         Dims d = {{nc[0], nc[1], nc[2]}};                                                                            \
-        int64_t N = (int64_t)nc[0] * nc[1] * nc[2];                                                                  \
         PRC_LAUNCH("mg_prolong", (cudaStream_t)stream,                                                               \
-                   prolong_kernel<T, T, T, false><<<grid_for(N), 256, 0, (cudaStream_t)stream>>>(coarse, fine, d)); \
+                   prolong_kernel<T, T, T, false><<<grid3(nc).grid, grid3(nc).block, 0, (cudaStream_t)stream>>>(coarse, fine, d)); \
         PRC_CHECK_LAUNCH();                                                                                          \
         return PRC_OK;                                                                                               \
     }

@@ -450,12 +450,16 @@ class RealMesh(BaseMesh):
         """Paint positions with CIC, accumulating (mesh.py:529-568); FP64 sums, deterministic."""
         torch = _torch()
         p = Particles(positions, self.device, weights=weights, weight_dtype=self.dtype)
+        accumulate = True
         if self._accum is None:
-            self._accum = torch.zeros(self.shape, dtype=torch.float64, device=self.device)
+            # a fresh mesh is written (not added to) by the paint, which covers every cell and column sum
+            self._accum = torch.empty(self.shape, dtype=torch.float64, device=self.device)
+            self._colsums = torch.empty(int(self.nmesh[0]) * int(self.nmesh[1]), dtype=torch.float64, device=self.device)
             if self.value is not None:
                 self._accum.copy_(self.value)
-            self._colsums = torch.zeros(int(self.nmesh[0]) * int(self.nmesh[1]), dtype=torch.float64, device=self.device)
-        paint(self.info, self._accum, self._colsums, p, wrap, True, self._workspace(), self._flags(), check=check)
+            else:
+                accumulate = False
+        paint(self.info, self._accum, self._colsums, p, wrap, accumulate, self._workspace(), self._flags(), check=check)
         if self.dtype.itemsize == 8:
             self.__dict__['value'] = self._accum
         else:

@@ -139,6 +139,25 @@ def test_paint_flags_leave_mesh_untouched():
     assert torch().equal(mesh, base)
 
 
+def test_paint_flags_zero_a_fresh_mesh():
+    """A non-accumulating paint of a bad catalogue writes zeros over whatever the buffer held."""
+    geom = pipeline.Geometry(8, 100., 0.)
+    pos = catalog(1000, [100.] * 3, [0.] * 3, seed=5)
+    pos[10, 1] = 60.
+    L, t = lib(), torch()
+    n = geom.shape
+    mesh = t.full(n, 7., dtype=t.float64, device='cuda')
+    colsums = t.full((n[0] * n[1],), 3., dtype=t.float64, device='cuda')
+    fl = flags()
+    nm, bs, bc = L.i3(geom.nmesh), L.d3(geom.boxsize), L.d3(geom.boxcenter)
+    w = ws(L.load().prc_assign_cic_workspace_bytes(nm, len(pos), 8))
+    dpos = dev(pos)
+    L.call('prc_assign_cic', L.ptr(mesh), L.ptr(colsums), nm, bs, bc, 8, L.ptr(dpos), 8, None, 0, len(pos), 0, 0,
+           L.ptr(fl), L.ptr(w), w.numel(), stream())
+    assert int(fl.item()) & L.PRC_FLAG_OUT_OF_BOX
+    assert float(mesh.abs().max()) == 0. and float(colsums.abs().max()) == 0.
+
+
 @pytest.mark.parametrize('mesh_dtype,pos_dtype', [('f8', 'f8'), ('f4', 'f4'), ('f4', 'f8')])
 def test_gathers_bit_exact(mesh_dtype, pos_dtype):
     L = lib()
@@ -367,3 +386,44 @@ def test_no_device_faults_after_kernels():
     import torch
     torch.cuda.synchronize()
     assert _lib.load().prc_device_fault_flags(0) == 0
+
+
+def mg_solve(dtype, mixed, nmesh=(32, 32, 32), los=None, calls=1):
+    """phi of prc_multigrid_* on a fixed random right-hand side, `calls` times on the same buffers."""
+    L, t = lib(), torch()
+    rng = np.random.default_rng(21)
+    delta = dev(rng.standard_normal(nmesh).astype(dtype))
+    phi = t.empty(nmesh, dtype=delta.dtype, device='cuda')
+    nm, bs, bc = L.i3(nmesh), L.d3([800.] * 3), L.d3([0., 0., 1500.])
+    w = ws(L.load().prc_multigrid_workspace_bytes(nm, np.dtype(dtype).itemsize, int(mixed)))
+    args = [L.ptr(delta), L.ptr(phi), nm, bs, bc, 0.4, 0.4, 5, 6, L.opt_d3(los)]
+    if dtype == 'f4':
+        args.append(int(mixed))
+    out = []
+    for _ in range(calls):
+        L.call('prc_multigrid_' + L.suffix(dtype), *args, L.ptr(w), w.numel(), stream())
+        t.cuda.synchronize()
+        out.append(phi.cpu().numpy().copy())
+    return out
+
+
+@pytest.mark.parametrize('dtype,mixed', [('f8', False), ('f4', True), ('f4', False)])
+def test_multigrid_graph_replay_equals_direct_launches(dtype, mixed, tmp_path):
+    """A solve is captured into a CUDA graph on its first call and replayed on the next call with the
+    same buffers; both give the bits of the same solve launched kernel by kernel (PRC_MG_GRAPH=0)."""
+    import subprocess
+    import sys
+    import os
+    L = lib()
+    n0 = L.launch_count()
+    first, second = mg_solve(dtype, mixed, calls=2)
+    assert np.array_equal(first, second)
+    assert L.launch_count() - n0 > 100          # replayed kernels are counted
+    path = str(tmp_path / 'phi.npy')
+    code = ("import sys, numpy; sys.path.insert(0, '.'); sys.path.insert(0, 'tests');"
+            "import test_gpu_kernels as T; numpy.save({!r}, T.mg_solve({!r}, {!r})[0])".format(path, dtype, mixed))
+    env = dict(os.environ, PRC_MG_GRAPH='0')
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = subprocess.run([sys.executable, '-c', code], cwd=root, env=env, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert np.array_equal(np.load(path), first)
