@@ -216,6 +216,23 @@ def reconstruct(w, device, data, wd, randoms, wr, check):
     return out_d, out_r
 
 
+# ncu DRAM-traffic summary of the small case of the iterative FFT workload (profiles/): per kernel, DRAM bytes
+# per launch over the algorithmic bytes of the same launches
+TRAFFIC_PROFILE = os.path.join(ROOT, 'profiles', 'traffic_iterative_fft_256.md')
+
+
+def traffic_ratio(kernel):
+    try:
+        with open(TRAFFIC_PROFILE) as fh:
+            for line in fh:
+                cells = [c.strip() for c in line.strip().strip('|').split('|')]
+                if len(cells) == 5 and cells[0] == kernel:
+                    return float(cells[4])
+    except (OSError, ValueError):
+        return None
+    return None
+
+
 def load_peaks():
     path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
     if os.path.isfile(path):
@@ -318,8 +335,14 @@ def run_gpu_arm(args, w):
     achieved = (kbytes / 1e9) / (kms / 1e3) if kms > 0 else 0.
     kernels = {k: dict(launches=v[0], ms=round(v[1], 3), share=round(v[1] / max(sum(x[1] for x in prof.values()), 1e-9), 4),
                        gbs=round((v[2] / 1e9) / (v[1] / 1e3), 1) if v[1] > 0 else None) for k, v in prof.items()}
+    ratio = traffic_ratio(name) if w['algorithm'] == 'IterativeFFTReconstruction' else None
+    traffic = None if ratio is None else ratio * kbytes / nl
     roofline = dict(bound='hbm', kernel=name, achieved=round(achieved, 1), peak=peak, unit='GB/s',
-                    frac=round(achieved / peak, 4), traffic=None,
+                    frac=round(achieved / peak, 4), traffic=traffic,
+                    traffic_source=None if ratio is None else
+                    'ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at nmesh 256 '
+                    '(profiles/traffic_iterative_fft_256.md), ratio {:.3f} to the algorithmic bytes, '
+                    'scaled to this launch'.format(ratio),
                     bytes_per_launch=kbytes / nl, launch_ms=kms / nl, peak_source=peak_kind + ' (MEASURED_PEAKS.json hbm_gbs)')
 
     cpu = None
