@@ -53,6 +53,25 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = 'iterative_fft_512'
 
+# Many requests at once through the request loop (pyrecon_b200.serving), against the same requests run one
+# after the other on one stream (the plain path).  A step is the whole set of requests.
+MULTI_WORKLOADS = {
+    # BASELINE config: 64 periodic-box mocks, plane-parallel and multigrid mixed, los='z', nmesh in
+    # {128, 192, 256}, boxsize 1000, 0.3M-2M lognormal data each, no randoms
+    'batched_mocks': dict(kind='batched', nrequests=64, algorithms=['PlaneParallelFFTReconstruction',
+                                                                    'MultiGridReconstruction'],
+                          nmesh=[128, 192, 256], ndata=(300_000, 2_000_000), randoms_factor=0, boxsize=1000.,
+                          boxcenter=500., los='z', wrap=True, dtype='f4', slots=16),
+    # BASELINE config: Poisson arrivals at 20 req/s, the three algorithms, nmesh in {128, 256, 384, 512},
+    # 0.5M-8M data with 4x randoms, 150 GB admission budget (100 requests instead of 500: same mix, a
+    # run that fits the bench's time)
+    'serving': dict(kind='serving', nrequests=100, rate=20., algorithms=['MultiGridReconstruction',
+                                                                        'IterativeFFTReconstruction',
+                                                                        'PlaneParallelFFTReconstruction'],
+                    nmesh=[128, 256, 384, 512], ndata=(500_000, 8_000_000), randoms_factor=4, boxsize=2000.,
+                    boxcenter=2000., los=None, wrap=False, dtype='f4', slots=8, hbm_budget=150e9),
+}
+
 
 def workload_name(w):
     return '{algorithm} nmesh={nmesh} boxsize={boxsize:g} boxcenter={boxcenter:g} los={los} f=0.8 bias=2.0 ' \
@@ -367,16 +386,119 @@ def run_gpu_arm(args, w):
     return 0
 
 
+def multi_requests(w, device, seed=0):
+    """The request list of a multi-request workload: catalogues drawn once per nmesh on the device (a request
+    takes a prefix of them, itself a random sample), sizes and algorithms from a seeded generator."""
+    import numpy as np
+    from pyrecon_b200 import mocks
+    from pyrecon_b200.serving import ReconstructionRequest
+    rng = np.random.default_rng(5000 + seed)
+    pool = {}
+    nmax = w['ndata'][1]
+    for i, n in enumerate(w['nmesh']):
+        data = mocks.lognormal_positions_torch(nmax, n, w['boxsize'], w['boxcenter'], seed=6000 + i, field_seed=7000 + i,
+                                               dtype='f4', device=device)
+        randoms = None
+        if w['randoms_factor']:
+            randoms = mocks.uniform_positions_torch(w['randoms_factor'] * nmax, w['boxsize'], w['boxcenter'],
+                                                    seed=8000 + i, dtype='f4', device=device)
+        pool[n] = (data, randoms)
+    reqs = []
+    for r in range(w['nrequests']):
+        algo = w['algorithms'][int(rng.integers(len(w['algorithms'])))]
+        n = int(w['nmesh'][int(rng.integers(len(w['nmesh'])))])
+        nd = int(rng.integers(w['ndata'][0], w['ndata'][1] + 1))
+        data, randoms = pool[n]
+        los = w['los']
+        if algo == 'PlaneParallelFFTReconstruction' and los is None:
+            los = 'z'
+        reqs.append(ReconstructionRequest(algo, data=data[:nd],
+                                          randoms=None if randoms is None else randoms[:w['randoms_factor'] * nd],
+                                          f=0.8, bias=2., los=los, nmesh=n, boxsize=w['boxsize'],
+                                          boxcenter=w['boxcenter'], wrap=w['wrap'], dtype=w['dtype'],
+                                          density_kwargs=dict(smoothing_radius=15.)))
+    return reqs
+
+
+def run_multi_arm(args, w):
+    """Throughput and latency of a multi-request workload: the plain path (requests one after the other on one
+    stream) and the request loop (continuous batching on `slots` streams; for 'serving', submitted at Poisson
+    arrival times).  Wall clock with the device synchronised on both sides."""
+    import torch
+    import numpy as np
+    from pyrecon_b200 import _lib
+    from pyrecon_b200.serving import ReconstructionServer, run_request
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    device = torch.device('cuda', local_rank)
+    reqs = multi_requests(w, device, seed=rank)
+    for r in reqs[:4]:                       # warm-up: kernels, graphs, allocator
+        run_request(r, device=device)
+    torch.cuda.synchronize(device)
+    # plain path
+    lat_plain = []
+    t0 = time.perf_counter()
+    for r in reqs:
+        t = time.perf_counter()
+        run_request(r, device=device)
+        torch.cuda.synchronize(device)
+        lat_plain.append(time.perf_counter() - t)
+    plain_s = time.perf_counter() - t0
+    # request loop
+    rng = np.random.default_rng(9000 + rank)
+    arrivals = np.cumsum(rng.exponential(1. / w['rate'], len(reqs))) if w['kind'] == 'serving' else np.zeros(len(reqs))
+    launches0 = _lib.launch_count()
+    with ClockSampler(local_rank) as clocks:
+        server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=w.get('hbm_budget'))
+        torch.cuda.synchronize(device)
+        start = time.perf_counter()
+        futures = []
+        for r, at in zip(reqs, arrivals):
+            delay = start + at - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            futures.append(server.submit(r))
+        for f in futures:
+            f.result()
+        torch.cuda.synchronize(device)
+        served_s = time.perf_counter() - start
+        stats = server.stats()
+        server.close()
+    launches = _lib.launch_count() - launches0
+    pct = lambda xs, q: 1e3 * sorted(xs)[min(len(xs) - 1, int(round(q / 100. * (len(xs) - 1))))]
+    n = len(reqs)
+    if rank == 0:
+        line = dict(metric=METRIC, value=n / served_s, unit='recons/s', n_gpus=world, steps=1, warmup=4,
+                    ms_per_step=served_s * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None,
+                    dtype=w['dtype'], data='synthetic: seeded lognormal catalogues, one per nmesh, requests take prefixes',
+                    config=dict(workload=args.workload, requests=n, slots=w['slots'],
+                                arrivals='poisson {:g}/s'.format(w['rate']) if w['kind'] == 'serving' else 'all at once',
+                                nmesh=w['nmesh'], algorithms=w['algorithms'], timing='wall clock, device synchronised'),
+                    served=dict(recons_per_s=n / served_s, p50_ms=stats['p50_ms'], p99_ms=stats['p99_ms'],
+                                peak_in_flight=stats['peak_active']),
+                    plain=dict(recons_per_s=n / plain_s, p50_ms=pct(lat_plain, 50), p99_ms=pct(lat_plain, 99)),
+                    served_vs_plain=(n / served_s) / (n / plain_s), gpu_launches=int(launches),
+                    clocks=clocks.summary())
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=10)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(MULTI_WORKLOADS))
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     args = ap.parse_args(argv)
+    if args.workload in MULTI_WORKLOADS:
+        if args.impl == 'reference':
+            print(json.dumps({'impl': 'reference', 'unavailable': 'multi-request workloads compare the request loop '
+                              'with the plain GPU path; the CPU reference is timed on the single-request workloads'}))
+            return 0
+        return run_multi_arm(args, MULTI_WORKLOADS[args.workload])
     w = WORKLOADS[args.workload]
     if args.impl == 'reference':
         return run_reference_arm(args, w)

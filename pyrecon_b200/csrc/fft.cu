@@ -24,6 +24,8 @@
 #include "tma.cuh"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <math.h>
 #include <string.h>
 #include <stdlib.h>
@@ -863,9 +865,23 @@ static bool spectrum_map(CUtensorMap* m, const void* base, const Plan3& p, size_
 // Persistent grid: as many CTAs as fit on the device at once (occupancy of this kernel), at most
 // one per tile.
 template <typename K> static int resident_grid(K kern, int threads, size_t smem, int64_t ntiles) {
+    // occupancy of (kernel, device), looked up once
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> known;
+    int dev = 0;
+    cudaGetDevice(&dev);
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
-        per_sm = 1;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = known.find({(const void*)kern, dev});
+        if (it != known.end()) per_sm = it->second;
+    }
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        std::lock_guard<std::mutex> lock(mu);
+        known[{(const void*)kern, dev}] = per_sm;
+    }
     const int64_t cap = (int64_t)device_sm_count() * per_sm;
     return (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, cap));
 }

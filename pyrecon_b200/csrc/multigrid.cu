@@ -514,7 +514,8 @@ using namespace prc;
 
 namespace {
 
-// Workspace layout for plain FMG in precision T: per level v, f (levels >= 1), r, tmp.
+// Workspace layout for plain FMG in precision T: per level v, f, r, tmp (level 0's f and v receive the
+// caller's right-hand side and return the solution, so the solve itself touches the workspace only).
 template <typename T> size_t plain_layout(const int32_t nmesh[3], char* base, std::vector<LevelBufs<T>>* out,
                                           std::vector<Level>* lv) {
     std::vector<Level> L = hierarchy(nmesh);
@@ -527,8 +528,8 @@ template <typename T> size_t plain_layout(const int32_t nmesh[3], char* base, st
     std::vector<LevelBufs<T>> B(L.size());
     for (size_t l = 0; l < L.size(); l++) {
         size_t b = (size_t)L[l].size() * sizeof(T);
-        B[l].v = l == 0 ? nullptr : (T*)take(b);
-        B[l].f = l == 0 ? nullptr : (T*)take(b);
+        B[l].v = (T*)take(b);
+        B[l].f = (T*)take(b);
         B[l].r = (T*)take(b);
         B[l].tmp = (T*)take(b);
     }
@@ -594,20 +595,20 @@ bool mg_args_ok(const void* delta, const void* phi, const int32_t nmesh[3], cons
     return true;
 }
 
-template <typename T>
-int run_plain(const T* delta, T* phi, const int32_t nmesh[3], const Params& P, void* ws, size_t wsb, cudaStream_t st) {
-    if (!ws || wsb < plain_layout<T>(nmesh, nullptr, nullptr, nullptr)) return PRC_ERR_WORKSPACE;
+// Plain solve of the right-hand side held in the workspace's level-0 f into its level-0 v.
+template <typename T> int solve_plain(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t st) {
     MGRunner<T> R;
     plain_layout<T>(nmesh, (char*)ws, &R.B, &R.L);
     R.P = P;
     R.st = st;
-    return fmg_plain<T>(R, delta, phi);
+    T* f0 = R.B[0].f;
+    T* v0 = R.B[0].v;
+    return fmg_plain<T>(R, f0, v0);
 }
 
-// Mixed precision FMG: every V-cycle is v64 += V32(0, f64 - A v64).
-int run_mixed(const float* delta, float* phi, const int32_t nmesh[3], const Params& P, void* ws, size_t wsb,
-              cudaStream_t st) {
-    if (!ws || wsb < mixed_layout(nmesh, nullptr, nullptr)) return PRC_ERR_WORKSPACE;
+// Mixed precision FMG: every V-cycle is v64 += V32(0, f64 - A v64); the FP64 right-hand side is in the
+// workspace's level-0 f64 and the solution is left in its level-0 v64.
+int solve_mixed(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t st) {
     MixedBufs m;
     mixed_layout(nmesh, (char*)ws, &m);
     const int nl = (int)m.L.size();
@@ -616,8 +617,6 @@ int run_mixed(const float* delta, float* phi, const int32_t nmesh[3], const Para
     R.B = m.b32;
     R.P = P;
     R.st = st;
-    const int64_t N0 = m.L[0].size();
-    PRC_LAUNCH_B("mg_convert", st, 12.0 * N0, convert_kernel<float, double><<<grid_for(N0), 256, 0, st>>>(delta, m.f64[0], N0));
     for (int l = 0; l + 1 < nl; l++) {
         Dims nf = {{m.L[l].n[0], m.L[l].n[1], m.L[l].n[2]}};
         const Grid3 gc = grid3_coarse(m.L[l].n);
@@ -658,17 +657,17 @@ int run_mixed(const float* delta, float* phi, const int32_t nmesh[3], const Para
             PRC_CHECK_LAUNCH();
         }
     }
-    PRC_LAUNCH_B("mg_convert", st, 12.0 * N0, convert_kernel<double, float><<<grid_for(N0), 256, 0, st>>>(m.v64[0], phi, N0));
-    PRC_CHECK_LAUNCH();
     return PRC_OK;
 }
 
 // ---- the whole solve as a CUDA graph ----
 //
 // A solve is a fixed sequence of some thousands of small launches (most on the coarse levels),
-// set by the mesh, the parameters and the buffer addresses.  It is captured once into a CUDA graph
-// and replayed while those stay the same (a small cache keyed on all of them), on a library stream
-// that waits for the caller's stream and is waited for by it.  PRC_MG_GRAPH=0 launches directly.
+// set by the mesh, the parameters and the workspace address (the caller's right-hand side and
+// solution are copied in and out around it, so they are not part of it).  It is captured once into a CUDA graph
+// and replayed while those stay the same (a small cache keyed on all of them), on the caller's stream
+// (on a library stream joined to it by events when the caller gives the legacy default stream, which
+// cannot be captured).  PRC_MG_GRAPH=0 launches directly.
 struct GraphEntry {
     std::string key;
     int device;
@@ -683,7 +682,7 @@ struct SideStream {
 std::mutex g_graph_mutex;
 std::list<GraphEntry> g_graphs;
 std::map<int, SideStream> g_side;
-constexpr size_t GRAPH_CACHE = 8;
+constexpr size_t GRAPH_CACHE = 64;
 
 bool graphs_enabled() {
     static int cached = -1;
@@ -696,8 +695,7 @@ bool graphs_enabled() {
 
 template <typename V> void key_add(std::string& k, const V& v) { k.append((const char*)&v, sizeof(V)); }
 
-std::string solve_key(int tsize, int mixed, const int32_t nmesh[3], const Params& P, const void* delta,
-                      const void* phi, const void* ws, size_t wsb) {
+std::string solve_key(int tsize, int mixed, const int32_t nmesh[3], const Params& P, const void* ws, size_t wsb) {
     std::string k;
     key_add(k, tsize);
     key_add(k, mixed);
@@ -712,8 +710,6 @@ std::string solve_key(int tsize, int mixed, const int32_t nmesh[3], const Params
     key_add(k, P.damping);
     key_add(k, P.jn);
     key_add(k, P.vn);
-    key_add(k, delta);
-    key_add(k, phi);
     key_add(k, ws);
     key_add(k, wsb);
     return k;
@@ -726,8 +722,9 @@ template <typename F> int run_graph(const std::string& key, cudaStream_t st, F b
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return PRC_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_graph_mutex);
+    const bool legacy = st == nullptr || st == cudaStreamLegacy;
     SideStream& side = g_side[dev];
-    if (side.s == nullptr) {
+    if (legacy && side.s == nullptr) {
         if (cudaStreamCreateWithFlags(&side.s, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&side.in, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&side.out, cudaEventDisableTiming) != cudaSuccess) {
@@ -735,7 +732,9 @@ template <typename F> int run_graph(const std::string& key, cudaStream_t st, F b
             return body(st);
         }
     }
-    if (cudaEventRecord(side.in, st) != cudaSuccess || cudaStreamWaitEvent(side.s, side.in, 0) != cudaSuccess)
+    const cudaStream_t run_st = legacy ? side.s : st;
+    if (legacy &&
+        (cudaEventRecord(side.in, st) != cudaSuccess || cudaStreamWaitEvent(side.s, side.in, 0) != cudaSuccess))
         return PRC_ERR_CUDA;
     auto it = g_graphs.begin();
     for (; it != g_graphs.end(); ++it)
@@ -744,10 +743,10 @@ template <typename F> int run_graph(const std::string& key, cudaStream_t st, F b
         g_graphs.splice(g_graphs.begin(), g_graphs, it);
     } else {
         capture_tally(nullptr, nullptr);
-        if (cudaStreamBeginCapture(side.s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return PRC_ERR_CUDA;
-        const int r = body(side.s);
+        if (cudaStreamBeginCapture(run_st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return PRC_ERR_CUDA;
+        const int r = body(run_st);
         cudaGraph_t g = nullptr;
-        const cudaError_t e = cudaStreamEndCapture(side.s, &g);
+        const cudaError_t e = cudaStreamEndCapture(run_st, &g);
         GraphEntry ent;
         capture_tally(&ent.launches, &ent.bytes);
         if (r != PRC_OK || e != cudaSuccess || g == nullptr) {
@@ -773,12 +772,27 @@ template <typename F> int run_graph(const std::string& key, cudaStream_t st, F b
     }
     const GraphEntry& ent = g_graphs.front();
     {
-        KernelScope scope("mg_solve_graph", side.s, ent.bytes, false);
-        if (cudaGraphLaunch(ent.exec, side.s) != cudaSuccess) return PRC_ERR_CUDA;
+        KernelScope scope("mg_solve_graph", run_st, ent.bytes, false);
+        if (cudaGraphLaunch(ent.exec, run_st) != cudaSuccess) return PRC_ERR_CUDA;
     }
     add_launches(ent.launches);
-    if (cudaEventRecord(side.out, side.s) != cudaSuccess || cudaStreamWaitEvent(st, side.out, 0) != cudaSuccess)
+    if (legacy &&
+        (cudaEventRecord(side.out, side.s) != cudaSuccess || cudaStreamWaitEvent(st, side.out, 0) != cudaSuccess))
         return PRC_ERR_CUDA;
+    return PRC_OK;
+}
+
+// Plain solve through the workspace: the caller's right-hand side is copied into level 0's f, the
+// (graph-captured) solve runs on the workspace alone, and level 0's v is copied out.
+template <typename T>
+int run_plain_io(const T* delta, T* phi, const int32_t nmesh[3], const Params& P, void* ws, const std::string& key,
+                 cudaStream_t st) {
+    std::vector<LevelBufs<T>> B;
+    plain_layout<T>(nmesh, (char*)ws, &B, nullptr);
+    const size_t bytes = (size_t)nmesh[0] * nmesh[1] * nmesh[2] * sizeof(T);
+    if (cudaMemcpyAsync(B[0].f, delta, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return PRC_ERR_CUDA;
+    PRC_TRY(run_graph(key, st, [&](cudaStream_t s) { return solve_plain<T>(nmesh, P, ws, s); }));
+    if (cudaMemcpyAsync(phi, B[0].v, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return PRC_ERR_CUDA;
     return PRC_OK;
 }
 
@@ -802,11 +816,20 @@ prc_status_t prc_multigrid_f32(const float* delta, float* phi, const int32_t nme
     if (!mg_args_ok(delta, phi, nmesh, boxsize, boxcenter, jacobi_niterations, vcycle_niterations)) return PRC_ERR_ARG;
     Params P = make_params(boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los);
     if (!workspace || workspace_bytes < prc_multigrid_workspace_bytes(nmesh, 4, mixed_precision)) return PRC_ERR_WORKSPACE;
-    const std::string key = solve_key(4, mixed_precision ? 1 : 0, nmesh, P, delta, phi, workspace, workspace_bytes);
-    return run_graph(key, (cudaStream_t)stream, [&](cudaStream_t s) {
-        if (mixed_precision) return run_mixed(delta, phi, nmesh, P, workspace, workspace_bytes, s);
-        return run_plain<float>(delta, phi, nmesh, P, workspace, workspace_bytes, s);
-    });
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t N = (int64_t)nmesh[0] * nmesh[1] * nmesh[2];
+    const std::string key = solve_key(4, mixed_precision ? 1 : 0, nmesh, P, workspace, workspace_bytes);
+    if (mixed_precision) {
+        MixedBufs m;
+        mixed_layout(nmesh, (char*)workspace, &m);
+        PRC_LAUNCH_B("mg_convert", st, 12.0 * N, convert_kernel<float, double><<<grid_for(N), 256, 0, st>>>(delta, m.f64[0], N));
+        PRC_CHECK_LAUNCH();
+        PRC_TRY(run_graph(key, st, [&](cudaStream_t s) { return solve_mixed(nmesh, P, workspace, s); }));
+        PRC_LAUNCH_B("mg_convert", st, 12.0 * N, convert_kernel<double, float><<<grid_for(N), 256, 0, st>>>(m.v64[0], phi, N));
+        PRC_CHECK_LAUNCH();
+        return PRC_OK;
+    }
+    return run_plain_io<float>(delta, phi, nmesh, P, workspace, key, st);
 }
 
 prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t nmesh[3], const double boxsize[3],
@@ -816,9 +839,8 @@ prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t n
     if (!mg_args_ok(delta, phi, nmesh, boxsize, boxcenter, jacobi_niterations, vcycle_niterations)) return PRC_ERR_ARG;
     Params P = make_params(boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los);
     if (!workspace || workspace_bytes < prc_multigrid_workspace_bytes(nmesh, 8, 0)) return PRC_ERR_WORKSPACE;
-    const std::string key = solve_key(8, 0, nmesh, P, delta, phi, workspace, workspace_bytes);
-    return run_graph(key, (cudaStream_t)stream,
-                     [&](cudaStream_t s) { return run_plain<double>(delta, phi, nmesh, P, workspace, workspace_bytes, s); });
+    const std::string key = solve_key(8, 0, nmesh, P, workspace, workspace_bytes);
+    return run_plain_io<double>(delta, phi, nmesh, P, workspace, key, (cudaStream_t)stream);
 }
 
 #define MG_COMPONENTS(SUF, T)                                                                                        \

@@ -38,7 +38,8 @@ class BaseReconstruction(BaseClass):
         return nmesh.copy()
 
     def __init__(self, f=0., bias=1., los=None, fft_engine='numpy', fft_wisdom=None, save_fft_wisdom=None,
-                 fft_plan='measure', wrap=False, device=None, mixed_precision=True, stream=None, **kwargs):
+                 fft_plan='measure', wrap=False, device=None, mixed_precision=True, stream=None, workspace=None,
+                 **kwargs):
         """
         Parameters are the reference's (recon.py:66-120): growth rate ``f``, ``bias``, line of sight
         ``los`` (None / 'local' for a varying one, 'x' / 'y' / 'z' or a 3-vector), ``wrap`` and the
@@ -47,7 +48,9 @@ class BaseReconstruction(BaseClass):
         compatibility and ignored (the FFTs are this library's CUDA kernels).
 
         Extra: ``device`` (CUDA device, default current), ``mixed_precision`` (dtype 'f4' multigrid
-        with FP64 defect correction, default True), ``stream`` (torch.cuda.Stream to enqueue on).
+        with FP64 defect correction, default True), ``stream`` (torch.cuda.Stream to enqueue on),
+        ``workspace`` (a scratch buffer object kept from an earlier reconstruction, so successive
+        reconstructions reuse the same device scratch; see :mod:`pyrecon_b200.serving`).
         """
         import torch
         self.set_cosmo(f=f, bias=bias)
@@ -64,7 +67,7 @@ class BaseReconstruction(BaseClass):
                             'the last one even)'.format(self.info.nmesh))
         self.fft_engine = 'cuda'
         self.fft_wisdom = None
-        self._ws = _Workspace(self.device)
+        self._ws = workspace if workspace is not None else _Workspace(self.device)
         self._flags = _Flags(self.device)
         self._size_randoms = 0
         with self._stream_ctx():

@@ -1,0 +1,208 @@
+"""
+Serving many reconstructions on one GPU: continuous batching of independent requests.
+
+    server = ReconstructionServer(slots=8, hbm_budget=150e9)
+    fut = server.submit(ReconstructionRequest('PlaneParallelFFTReconstruction', data=positions,
+                                              nmesh=256, boxsize=1000., boxcenter=500., los='z', wrap=True))
+    shifted = fut.result()['shifted_data']
+    print(server.stats())          # throughput, p50 / p99 latency, peak concurrency
+    server.close()
+
+Requests are admitted in arrival order as soon as a slot (a CUDA stream with its own resident device
+scratch) is free and their estimated device memory fits in what the budget has left; each admitted
+request runs the plain
+pipeline (constructor, assign_data, assign_randoms, set_density_contrast, run,
+read_shifted_positions) on its own stream from a worker thread, so the kernels of the requests
+in flight overlap on the device while requests keep arriving.  A request's result does not depend
+on what else is running: every kernel is deterministic and requests share no device buffers.
+"""
+import threading
+import time
+import collections
+import concurrent.futures
+
+import numpy as np
+
+from . import _lib
+from .mesh import _device_of
+
+
+class ReconstructionRequest(object):
+    """One reconstruction: the algorithm class name, its constructor keywords (f, bias, los, nmesh,
+    boxsize, boxcenter, wrap, dtype, ...), the catalogues (numpy arrays or torch tensors), the
+    keywords of set_density_contrast and of run."""
+
+    def __init__(self, algorithm, data, data_weights=None, randoms=None, randoms_weights=None,
+                 density_kwargs=None, run_kwargs=None, **kwargs):
+        self.algorithm = algorithm
+        self.data, self.data_weights = data, data_weights
+        self.randoms, self.randoms_weights = randoms, randoms_weights
+        self.density_kwargs = dict(density_kwargs or {})
+        self.run_kwargs = dict(run_kwargs or {})
+        self.kwargs = dict(kwargs)
+        self.submitted = None
+
+
+def _size(x):
+    return 0 if x is None else int(len(x))
+
+
+def estimate_device_bytes(request):
+    """Device memory a request holds at its peak (meshes, workspaces, catalogues, outputs), from the
+    library's own workspace queries; used for admission."""
+    import pyrecon_b200
+    from .multigrid import OriginalMultiGridReconstruction
+    from .mesh import MeshInfo
+    lib = _lib.load()
+    cls = getattr(pyrecon_b200, request.algorithm)
+    kw = dict(request.kwargs)
+    geometry = ('nmesh', 'boxsize', 'boxcenter', 'cellsize', 'positions', 'boxpad', 'dtype')
+    info = MeshInfo(select_nmesh=cls._select_nmesh, **{k: kw[k] for k in geometry if k in kw})
+    n = int(np.prod(info.nmesh))
+    item = info.dtype.itemsize
+    nm = _lib.i3(info.nmesh)
+    npart = _size(request.data) + _size(request.randoms)
+    nmeshes = 2 if request.randoms is not None else 1
+    total = 8 * n * nmeshes + 8 * int(info.nmesh[0] * info.nmesh[1]) * nmeshes           # FP64 paint meshes
+    total += lib.prc_assign_cic_workspace_bytes(nm, max(_size(request.data), _size(request.randoms)), item)
+    total += lib.prc_density_contrast_workspace_bytes(nm, item, int(request.randoms is not None))
+    total += n * item                                                                     # delta
+    if issubclass(cls, OriginalMultiGridReconstruction):
+        total += lib.prc_multigrid_workspace_bytes(nm, item, 1) + n * item                # hierarchy, phi
+    elif request.algorithm == 'IterativeFFTReconstruction':
+        total += lib.prc_iterative_fft_workspace_bytes(nm, item, int(kw.get('los') is None)) + 4 * n * item
+    else:
+        total += lib.prc_plane_parallel_workspace_bytes(nm, item) + 4 * n * item
+    total += npart * 3 * 8 * 3                                                            # positions, outputs
+    return int(total)
+
+
+def run_request(request, device=None, stream=None, workspace=None):
+    """The plain pipeline for one request on `stream`; returns {'shifted_data', 'shifted_randoms'}.
+    `workspace`: scratch kept across requests (a slot's), so its address, and with it the multigrid
+    solve's captured CUDA graph, is reused."""
+    import pyrecon_b200
+    cls = getattr(pyrecon_b200, request.algorithm)
+    rec = cls(device=device, stream=stream, workspace=workspace, **request.kwargs)
+    rec.assign_data(request.data, request.data_weights)
+    if request.randoms is not None:
+        rec.assign_randoms(request.randoms, request.randoms_weights)
+    rec.set_density_contrast(**request.density_kwargs)
+    rec.run(**request.run_kwargs)
+    out = {'shifted_data': rec.read_shifted_positions(request.data)}
+    if request.randoms is not None:
+        out['shifted_randoms'] = rec.read_shifted_positions(request.randoms)
+    return out
+
+
+class ReconstructionServer(object):
+    """Continuous-batching request loop on one GPU (see the module docstring).
+
+    slots: requests in flight at most (one CUDA stream each).  hbm_budget: bytes of device memory
+    the requests in flight may hold together (default: 90% of the free memory at start).
+    """
+
+    def __init__(self, device=None, slots=8, hbm_budget=None):
+        import torch
+        self.device = _device_of(device)
+        _lib.load()
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            hbm_budget = 0.9 * free
+        self.hbm_budget = float(hbm_budget)
+        from .mesh import _Workspace
+        self._streams = [torch.cuda.Stream(self.device) for _ in range(slots)]
+        # device scratch resident per slot: reused by every request the slot runs
+        self._workspaces = [_Workspace(self.device) for _ in range(slots)]
+        self._free_streams = list(range(slots))
+        self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=slots)
+        self._cv = threading.Condition()
+        self._queue = collections.deque()
+        self._in_use = 0.
+        self._active = 0
+        self.peak_active = 0
+        self.latencies = []
+        self._first_submit = None
+        self._last_done = None
+        self._closed = False
+        self._dispatcher = threading.Thread(target=self._loop, name='pyrecon-b200-dispatch', daemon=True)
+        self._dispatcher.start()
+
+    def submit(self, request):
+        """Queue a request; returns a concurrent.futures.Future of run_request's result."""
+        need = estimate_device_bytes(request)
+        if need > self.hbm_budget:
+            raise ValueError('request needs ~{:.1f} GB, above the HBM budget of {:.1f} GB'.format(need / 1e9,
+                                                                                                self.hbm_budget / 1e9))
+        fut = concurrent.futures.Future()
+        with self._cv:
+            if self._closed:
+                raise RuntimeError('server is closed')
+            request.submitted = time.perf_counter()
+            if self._first_submit is None:
+                self._first_submit = request.submitted
+            self._queue.append((request, need, fut))
+            self._cv.notify_all()
+        return fut
+
+    def _loop(self):
+        while True:
+            with self._cv:
+                while True:
+                    if self._queue and self._free_streams and self._in_use + self._queue[0][1] <= self.hbm_budget:
+                        break
+                    if self._closed and not self._queue:
+                        return
+                    self._cv.wait()
+                request, need, fut = self._queue.popleft()
+                slot = self._free_streams.pop()
+                self._in_use += need
+                self._active += 1
+                self.peak_active = max(self.peak_active, self._active)
+            self._pool.submit(self._work, request, need, fut, slot)
+
+    def _work(self, request, need, fut, slot):
+        import torch
+        stream = self._streams[slot]
+        try:
+            with torch.cuda.device(self.device):
+                out = run_request(request, device=self.device, stream=stream, workspace=self._workspaces[slot])
+                stream.synchronize()
+        except BaseException as exc:
+            fut.set_exception(exc)
+        else:
+            done = time.perf_counter()
+            with self._cv:
+                self.latencies.append(done - request.submitted)
+                self._last_done = done
+            fut.set_result(out)
+        finally:
+            with self._cv:
+                self._in_use -= need
+                self._active -= 1
+                self._free_streams.append(slot)
+                self._cv.notify_all()
+
+    def stats(self):
+        """Throughput (completed requests / s from the first submission to the last completion) and
+        latency percentiles (submission to result, ms)."""
+        with self._cv:
+            lat = sorted(self.latencies)
+            span = (self._last_done - self._first_submit) if lat else 0.
+        pct = lambda q: 1e3 * lat[min(len(lat) - 1, int(round(q / 100. * (len(lat) - 1))))] if lat else None
+        return dict(completed=len(lat), recons_per_s=len(lat) / span if span > 0 else None, p50_ms=pct(50),
+                    p99_ms=pct(99), peak_active=self.peak_active)
+
+    def close(self, wait=True):
+        with self._cv:
+            self._closed = True
+            self._cv.notify_all()
+        if wait:
+            self._dispatcher.join()
+            self._pool.shutdown(wait=True)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
