@@ -90,6 +90,15 @@ PRC_API prc_status_t prc_assign_cic(double *mesh, double *column_sums, const int
                             const void *positions, int pos_bytes, const void *weights,
                             int weight_bytes, int64_t npos, int wrap, int accumulate,
                             int32_t *flags, void *workspace, size_t workspace_bytes, void *stream);
+/* prc_assign_cic that also writes `order` (npos uint32): the particles' indices sorted by base cell
+ * (stable), the order in which the paint summed them; a read-out of the same positions given it
+ * gathers in cell order (prc_read_shifts_*). */
+PRC_API prc_status_t prc_assign_cic_order(double *mesh, double *column_sums, const int32_t nmesh[3],
+                                  const double boxsize[3], const double boxcenter[3], int mesh_bytes,
+                                  const void *positions, int pos_bytes, const void *weights,
+                                  int weight_bytes, int64_t npos, int wrap, int accumulate,
+                                  int32_t *flags, void *workspace, size_t workspace_bytes, void *stream,
+                                  uint32_t *order);
 
 /* Allocation-free variant of prc_assign_cic, with no counterpart in the reference.  For callers
  * that cannot allocate device memory (no allocator of their own, or code running where a
@@ -149,28 +158,31 @@ PRC_API prc_status_t prc_read_finite_difference_cic_f64(const double *mesh, cons
  * Replaces BaseReconstruction.read_shifts / read_shifted_positions (pyrecon/recon.py:255-325).
  * psi_stride: 1 for three separate meshes, 4 for one interleaved (x, y, z, 0) mesh with
  * psi_y = psi_x + 1, psi_z = psi_x + 2 (one vector load per CIC corner).
- * out is (npos, 3) in `out_bytes` precision. */
+ * out is (npos, 3) in `out_bytes` precision.  `order` (may be NULL) is a permutation of 0..npos-1
+ * in which to visit the particles, e.g. the cell order prc_assign_cic_order returned when these
+ * positions were painted: neighbouring threads then gather neighbouring cells.  Results do not
+ * depend on it. */
 PRC_API prc_status_t prc_read_shifts_psi_f32(const float *psi_x, const float *psi_y, const float *psi_z, int psi_stride,
                                      const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
-                                     int64_t npos, double f, const double *los, int field, int shifted,
-                                     int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                     int64_t npos, const uint32_t *order, double f, const double *los, int field,
+                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
 PRC_API prc_status_t prc_read_shifts_psi_f64(const double *psi_x, const double *psi_y, const double *psi_z,
                                      int psi_stride, const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
-                                     int64_t npos, double f, const double *los, int field, int shifted,
-                                     int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                     int64_t npos, const uint32_t *order, double f, const double *los, int field,
+                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
 
 /* Same for the multigrid potential: finite-difference CIC gradient of phi, RSD direction from
  * the UNWRAPPED positions (pyrecon/multigrid.py:137-158). */
 PRC_API prc_status_t prc_read_shifts_phi_f32(const float *phi, const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
-                                     int64_t npos, double f, const double *los, int field, int shifted,
-                                     int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                     int64_t npos, const uint32_t *order, double f, const double *los, int field,
+                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
 PRC_API prc_status_t prc_read_shifts_phi_f64(const double *phi, const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
-                                     int64_t npos, double f, const double *los, int field, int shifted,
-                                     int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                     int64_t npos, const uint32_t *order, double f, const double *los, int field,
+                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
 
 /* Device fault word of the FFT kernels on the current device (no counterpart in the reference,
  * whose FFTs run on the host): PRC_FAULT_WAIT_TIMEOUT when a kernel gave up a bounded wait for its

@@ -37,6 +37,8 @@ _SIGNATURES = {
     'prc_device_fault_flags': (ctypes.c_uint, [c_int]),
     'prc_assign_cic_workspace_bytes': (c_size, [I3, c_i64, c_int]),
     'prc_assign_cic': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size, _p]),
+    'prc_assign_cic_order': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size,
+                                     _p, _p]),
     'prc_cic_cell_order': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, c_i64, c_int, _p, _p, c_size, _p]),
     'prc_assign_cic_noalloc': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p]),
     'prc_sum_workspace_bytes': (c_size, [c_i64]),
@@ -51,10 +53,10 @@ for _s in ['f32', 'f64']:
     _SIGNATURES.update({
         'prc_read_cic_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, c_int, _p, _p, _p]),
         'prc_read_finite_difference_cic_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, c_int, _p, _p, _p]),
-        'prc_read_shifts_psi_' + _s: (c_int, [_p, _p, _p, c_int, I3, D3, D3, _p, c_int, c_i64, c_double, DP, c_int,
-                                              c_int, c_int, _p, c_int, _p, _p]),
-        'prc_read_shifts_phi_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, c_double, DP, c_int, c_int, c_int, _p,
-                                              c_int, _p, _p]),
+        'prc_read_shifts_psi_' + _s: (c_int, [_p, _p, _p, c_int, I3, D3, D3, _p, c_int, c_i64, _p, c_double, DP,
+                                              c_int, c_int, c_int, _p, c_int, _p, _p]),
+        'prc_read_shifts_phi_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, _p, c_double, DP, c_int, c_int, c_int,
+                                              _p, c_int, _p, _p]),
         'prc_rfft3d_' + _s: (c_int, [_p, c_int, _p, I3, _p]),
         'prc_irfft3d_' + _s: (c_int, [_p, _p, I3, _p]),
         'prc_smooth_gaussian_' + _s: (c_int, [_p, c_int, _p, I3, D3, D3, _p, c_size, _p]),

@@ -446,8 +446,10 @@ class RealMesh(BaseMesh):
         low, high = self.boxcenter - self.boxsize / 2., self.boxcenter + self.boxsize / 2.
         return low, high
 
-    def assign_cic(self, positions, weights=None, wrap=False, check=True):
-        """Paint positions with CIC, accumulating (mesh.py:529-568); FP64 sums, deterministic."""
+    def assign_cic(self, positions, weights=None, wrap=False, check=True, order_out=None):
+        """Paint positions with CIC, accumulating (mesh.py:529-568); FP64 sums, deterministic.
+        ``order_out``: optional int32 device tensor of len(positions) that receives the particles'
+        indices in the (cell-sorted) order the paint summed them."""
         torch = _torch()
         p = Particles(positions, self.device, weights=weights, weight_dtype=self.dtype)
         accumulate = True
@@ -459,7 +461,8 @@ class RealMesh(BaseMesh):
                 self._accum.copy_(self.value)
             else:
                 accumulate = False
-        paint(self.info, self._accum, self._colsums, p, wrap, accumulate, self._workspace(), self._flags(), check=check)
+        paint(self.info, self._accum, self._colsums, p, wrap, accumulate, self._workspace(), self._flags(), check=check,
+              order_out=order_out)
         if self.dtype.itemsize == 8:
             self.__dict__['value'] = self._accum
         else:
@@ -575,16 +578,19 @@ class ComplexMesh(BaseMesh):
         return RealMesh(out, info=self.info, device=self.device, attrs=self.attrs)
 
 
-def paint(info, accum, colsums, particles, wrap, accumulate, workspace, flags, check=True):
+def paint(info, accum, colsums, particles, wrap, accumulate, workspace, flags, check=True, order_out=None):
     """Deterministic CIC paint of ``particles`` into the FP64 ``accum`` mesh (C ABI prc_assign_cic)."""
     nm, bs, bc = info.c_geometry()
     lib = _lib.load()
     ws = workspace.get(lib.prc_assign_cic_workspace_bytes(nm, particles.size, info.dtype.itemsize))
     w = particles.weights
-    _lib.call('prc_assign_cic', _lib.ptr(accum), _lib.ptr(colsums), nm, bs, bc, info.dtype.itemsize,
-              _lib.ptr(particles.pos), particles.pos_bytes, _lib.ptr(w), 0 if w is None else w.element_size(),
-              particles.size, int(bool(wrap)), int(bool(accumulate)), flags.ptr, _lib.ptr(ws), ws.numel(),
-              _lib.stream_of(accum.device), error=MeshError)
+    args = [_lib.ptr(accum), _lib.ptr(colsums), nm, bs, bc, info.dtype.itemsize, _lib.ptr(particles.pos),
+            particles.pos_bytes, _lib.ptr(w), 0 if w is None else w.element_size(), particles.size, int(bool(wrap)),
+            int(bool(accumulate)), flags.ptr, _lib.ptr(ws), ws.numel(), _lib.stream_of(accum.device)]
+    if order_out is not None:
+        _lib.call('prc_assign_cic_order', *args, _lib.ptr(order_out), error=MeshError)
+    else:
+        _lib.call('prc_assign_cic', *args, error=MeshError)
     if check:
         low, high = info.boxcenter - info.boxsize / 2., info.boxcenter + info.boxsize / 2.
         flags.raise_if_set(low, high)

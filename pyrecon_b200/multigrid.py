@@ -54,7 +54,8 @@ class OriginalMultiGridReconstruction(BaseReconstruction):
             raise ReconstructionError('run() must be called before reading shifts')
         nm, bs, bc = self._geometry_args()
         _lib.call('prc_read_shifts_phi_' + _lib.suffix(self.info.dtype), _lib.ptr(self.mesh_phi.value), nm, bs, bc,
-                  _lib.ptr(p.pos), p.pos_bytes, p.size, float(self.f), self._los_arg(), field, shifted, int(self.wrap),
+                  _lib.ptr(p.pos), p.pos_bytes, p.size, _lib.ptr(getattr(p, 'order', None)), float(self.f),
+                  self._los_arg(), field, shifted, int(self.wrap),
                   _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device), error=MeshError)
 
 

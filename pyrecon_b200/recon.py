@@ -131,15 +131,47 @@ class BaseReconstruction(BaseClass):
         """Paint data (accumulates over calls, e.g. slab by slab).  ``check=False`` defers the
         box / NaN check (no host synchronisation)."""
         with self._stream_ctx():
-            self.mesh_data.assign_cic(positions, weights=weights, wrap=self.wrap, check=check)
+            order = self._new_order(positions)
+            self.mesh_data.assign_cic(positions, weights=weights, wrap=self.wrap, check=check, order_out=order)
+            self._keep_order(positions, order)
 
     def assign_randoms(self, positions, weights=None, check=True):
         """Same as :meth:`assign_data`, for randoms."""
         if not self.mesh_randoms.is_set:
             self._size_randoms = 0
         with self._stream_ctx():
-            self.mesh_randoms.assign_cic(positions, weights=weights, wrap=self.wrap, check=check)
+            order = self._new_order(positions)
+            self.mesh_randoms.assign_cic(positions, weights=weights, wrap=self.wrap, check=check, order_out=order)
+            self._keep_order(positions, order)
         self._size_randoms += len(positions)
+
+    # Device-resident catalogues keep the cell order their paint used: a later read-out of the same
+    # tensor visits the particles in that order, so the gathers of neighbouring threads hit
+    # neighbouring cells.  Any permutation gives the same results; the key (address, length) only
+    # picks which one.
+
+    @staticmethod
+    def _order_key(positions):
+        import torch
+        if isinstance(positions, torch.Tensor) and positions.is_cuda and positions.ndim == 2:
+            return (positions.data_ptr(), int(positions.shape[0]))
+        return None
+
+    def _new_order(self, positions):
+        import torch
+        if self._order_key(positions) is None or len(positions) == 0:
+            return None
+        return torch.empty(len(positions), dtype=torch.int32, device=self.device)
+
+    def _keep_order(self, positions, order):
+        if order is not None:
+            if not hasattr(self, '_orders'):
+                self._orders = {}
+            self._orders[self._order_key(positions)] = order
+
+    def _order_for(self, positions):
+        key = self._order_key(positions)
+        return None if key is None else getattr(self, '_orders', {}).get(key)
 
     @property
     def has_randoms(self):
@@ -211,6 +243,7 @@ class BaseReconstruction(BaseClass):
             return self._read_pipelined(positions, field, shifted)
         with self._stream_ctx():
             p = Particles(positions, self.device)
+            p.order = self._order_for(positions)
             pbytes = p.pos_bytes
             obytes = max(pbytes, self.info.dtype.itemsize) if (shifted and self.wrap) else pbytes
             out = torch.empty((p.size, 3), dtype=torch_dtype('f4' if obytes == 4 else 'f8'), device=self.device)
@@ -329,5 +362,6 @@ class FFTShiftsMixin(object):
             raise ReconstructionError('run() must be called before reading shifts')
         nm, bs, bc = self._geometry_args()
         _lib.call('prc_read_shifts_psi_' + _lib.suffix(self.info.dtype), *self._psi_pointers(self._psi4), 4, nm, bs,
-                  bc, _lib.ptr(p.pos), p.pos_bytes, p.size, float(self.f), self._los_arg(), field, shifted,
+                  bc, _lib.ptr(p.pos), p.pos_bytes, p.size, _lib.ptr(getattr(p, 'order', None)), float(self.f),
+                  self._los_arg(), field, shifted,
                   int(self.wrap), _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device), error=MeshError)

@@ -93,3 +93,31 @@ def test_chunked_host_readout_equals_device_readout(kind):
     disp = rec.read_shifts(pos, field='disp')
     disp = disp if kind == 'numpy' else disp.numpy()
     assert np.array_equal(disp, out['shifts_disp'])
+
+
+@pytest.mark.parametrize('name', ['ifft_f4_local', 'mg_f8_local'])
+def test_readout_in_paint_order_equals_plain_readout(name):
+    """Device catalogues are read out in the cell order of their paint; a copy of the same positions
+    (no order remembered) gives the same bits."""
+    import torch
+    import pyrecon_b200
+    from _util import ALGOS
+    g = load_golden(name)
+    m = g['meta']
+    Cls = getattr(pyrecon_b200, ALGOS[m['algorithm']])
+    rec = Cls(f=m['f'], bias=m['bias'], los=m['los'], nmesh=m['nmesh'], boxsize=m['boxsize'],
+              boxcenter=m['boxcenter'], dtype=m['dtype'], wrap=m['wrap'])
+    data = torch.from_numpy(g['data']).cuda()
+    rec.assign_data(data, None if g['wdata'] is None else torch.from_numpy(g['wdata']).cuda())
+    randoms = None
+    if m['randoms']:
+        randoms = torch.from_numpy(g['randoms']).cuda()
+        rec.assign_randoms(randoms, None if g['wrandoms'] is None else torch.from_numpy(g['wrandoms']).cuda())
+    rec.set_density_contrast(smoothing_radius=m['smoothing_radius'])
+    rec.run()
+    assert rec._order_for(data) is not None
+    for cat in [data] + ([randoms] if randoms is not None else []):
+        ordered = rec.read_shifted_positions(cat)
+        plain = rec.read_shifted_positions(cat.clone())
+        assert torch.equal(ordered, plain)
+        assert torch.equal(rec.read_shifts(cat, field='rsd'), rec.read_shifts(cat.clone(), field='rsd'))
