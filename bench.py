@@ -284,6 +284,18 @@ def percentile(xs, q):
     return xs[f] + (xs[c] - xs[f]) * (k - f)
 
 
+def reduce_max(x, world, device):
+    """Max of a per-rank number over the ranks of the default process group (the timing of an N-replica run is
+    the slowest rank's); the tensor lives on `device` (the GPU for NCCL, the CPU for gloo)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_gpu_arm(args, w):
     import torch
     import torch.distributed as dist
@@ -300,11 +312,7 @@ def run_gpu_arm(args, w):
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, world, device)
 
     data, wd, randoms, wr = make_catalogs(w, device, rank)
     step = lambda: reconstruct(w, device, data, wd, randoms, wr, check=False)

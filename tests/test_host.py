@@ -98,3 +98,37 @@ def test_fft_engine_kwargs_accepted():
     params = inspect.signature(BaseReconstruction.__init__).parameters
     for name in ['f', 'bias', 'los', 'fft_engine', 'fft_wisdom', 'save_fft_wisdom', 'fft_plan', 'wrap']:
         assert name in params
+
+
+def _replica_worker(rank, world, port, out):
+    import os
+    import torch.distributed as dist
+    import bench
+    os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        # rank r "timed" 10 (r + 1) ms: every rank must see the slowest one, as bench.py reports it
+        ms = bench.reduce_max(10. * (rank + 1), world, 'cpu')
+        dist.barrier()
+        out[rank] = ms
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replicas_timing_is_the_max_over_ranks_gloo():
+    """The N>1 host logic of bench.py (independent replicas, max over ranks) on two gloo ranks."""
+    import socket
+    import torch.multiprocessing as mp
+    s = socket.socket()
+    s.bind(('127.0.0.1', 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context('spawn')
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_replica_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert dict(out) == {0: 20., 1: 20.}
