@@ -50,6 +50,9 @@ WORKLOADS = {
     'plane_parallel_512': dict(algorithm='PlaneParallelFFTReconstruction', nmesh=512, boxsize=2000., boxcenter=2000.,
                                los='z', ndata=5_000_000, nrandoms=20_000_000, pos_dtype='f4', dtype='f4', weights=None,
                                run_kwargs={}),
+    'iterative_fft_particle_512': dict(algorithm='IterativeFFTParticleReconstruction', nmesh=512, boxsize=2000.,
+                                       boxcenter=2000., los=None, ndata=5_000_000, nrandoms=20_000_000, pos_dtype='f4',
+                                       dtype='f4', weights=None, run_kwargs=dict(niterations=3)),
 }
 DEFAULT_WORKLOAD = 'iterative_fft_512'
 
@@ -96,7 +99,8 @@ def reference_sample(w, seed=0):
     n = w['nmesh'] // 2
     nd, nr = w['ndata'] // 8, w['nrandoms'] // 8
     algo = {'IterativeFFTReconstruction': 'iterative_fft', 'MultiGridReconstruction': 'multigrid',
-            'PlaneParallelFFTReconstruction': 'plane_parallel_fft'}[w['algorithm']]
+            'PlaneParallelFFTReconstruction': 'plane_parallel_fft',
+            'IterativeFFTParticleReconstruction': 'iterative_fft_particle'}[w['algorithm']]
     data = mocks.lognormal_positions_numpy(nd, n, w['boxsize'], w['boxcenter'], seed=2002 + seed,
                                            field_seed=1002 + seed, dtype=w['pos_dtype'])
     randoms = mocks.uniform_positions_numpy(nr, w['boxsize'], w['boxcenter'], seed=3002 + seed, dtype=w['pos_dtype'])

@@ -184,6 +184,61 @@ PRC_API prc_status_t prc_read_shifts_phi_f64(const double *phi, const int32_t nm
                                      int64_t npos, const uint32_t *order, double f, const double *los, int field,
                                      int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
 
+/* Sum of a float mesh accumulated in float64 (deterministic, as prc_sum_f64); replaces np.sum of the
+ * smoothed meshes in IterativeFFTParticleReconstruction.set_density_contrast
+ * (pyrecon/iterative_fft_particle.py:52). */
+PRC_API prc_status_t prc_sum_f32(const float *x, int64_t n, double *out, void *workspace, size_t workspace_bytes,
+                                 void *stream);
+
+/* Density contrast of meshes that are already smoothed (IterativeFFTParticleReconstruction.set_density_contrast,
+ * pyrecon/iterative_fft_particle.py:35-63): delta = (d - alpha r) / (b alpha r) where r > ran_min * sum(r) /
+ * size_randoms (else 0), alpha = sum(d) / sum(r); without randoms (mesh_randoms NULL) delta = (d / mean(d) - 1) / b.
+ * Inputs of `in_bytes` precision (8: the paint accumulators, 4: FP32 meshes); sums = device {sum d, sum r}. */
+PRC_API prc_status_t prc_delta_from_meshes_f32(const void *mesh_data, const void *mesh_randoms, int in_bytes,
+                                               const double *sums, const int32_t nmesh[3], double bias, double ran_min,
+                                               double size_randoms, float *delta, void *stream);
+PRC_API prc_status_t prc_delta_from_meshes_f64(const void *mesh_data, const void *mesh_randoms, int in_bytes,
+                                               const double *sums, const int32_t nmesh[3], double bias, double ran_min,
+                                               double size_randoms, double *delta, void *stream);
+
+/* Zeldovich displacement of a density contrast, psi_a = IFFT(i k_a delta_k / k^2) with delta_k(0) = 0
+ * (pyrecon/iterative_fft.py:71-82, pyrecon/iterative_fft_particle.py:93-108); psi_stride as for
+ * prc_read_shifts_psi_*. */
+PRC_API size_t prc_zeldovich_psi_workspace_bytes(const int32_t nmesh[3], int mesh_bytes);
+PRC_API prc_status_t prc_zeldovich_psi_f32(const float *delta, const int32_t nmesh[3], const double boxsize[3],
+                                           float *psi_x, float *psi_y, float *psi_z, int psi_stride, void *workspace,
+                                           size_t workspace_bytes, void *stream);
+PRC_API prc_status_t prc_zeldovich_psi_f64(const double *delta, const int32_t nmesh[3], const double boxsize[3],
+                                           double *psi_x, double *psi_y, double *psi_z, int psi_stride,
+                                           void *workspace, size_t workspace_bytes, void *stream);
+
+/* One iteration's particle update of IterativeFFTParticleReconstruction (pyrecon/iterative_fft_particle.py:106-139):
+ * s = CIC read of the interleaved (x, y, z, 0) displacement psi4 at the wrapped pos_rec; on the first iteration
+ * s -= beta / (1 + beta) (s.l) l; then pos_rec = x - f (s.l) l, with x = pos_data (wrapped when wrap_data) and
+ * l = los (global, unit 3-vector) or x / |x| (los = NULL).  Float64 arithmetic, stored in the positions dtype. */
+PRC_API prc_status_t prc_ifftp_update_f32(const float *psi4, const int32_t nmesh[3], const double boxsize[3],
+                                          const double boxcenter[3], const void *pos_data, void *pos_rec, int pos_bytes,
+                                          int64_t npos, double f, double beta, int first, const double *los,
+                                          int wrap_data, int32_t *flags, void *stream);
+PRC_API prc_status_t prc_ifftp_update_f64(const double *psi4, const int32_t nmesh[3], const double boxsize[3],
+                                          const double boxcenter[3], const void *pos_data, void *pos_rec, int pos_bytes,
+                                          int64_t npos, double f, double beta, int first, const double *los,
+                                          int wrap_data, int32_t *flags, void *stream);
+
+/* Shift read-out of IterativeFFTParticleReconstruction (pyrecon/iterative_fft_particle.py:148-244).  With
+ * pos_rec (the data, `positions` = the data positions): shifts at the reconstructed positions and
+ * RSD = data - reconstructed.  Without: at positions p (wrapped when wrap), disp = psi(p),
+ * rsd = f (disp.l) l, disp+rsd = psi(p - rsd, wrapped) + rsd.  `shifted`: positions - shifts, wrapped
+ * when wrap.  out (npos, 3) in `out_bytes` precision. */
+PRC_API prc_status_t prc_ifftp_read_f32(const float *psi4, const int32_t nmesh[3], const double boxsize[3],
+                                        const double boxcenter[3], const void *positions, const void *pos_rec,
+                                        int pos_bytes, int64_t npos, double f, const double *los, int field,
+                                        int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+PRC_API prc_status_t prc_ifftp_read_f64(const double *psi4, const int32_t nmesh[3], const double boxsize[3],
+                                        const double boxcenter[3], const void *positions, const void *pos_rec,
+                                        int pos_bytes, int64_t npos, double f, const double *los, int field,
+                                        int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+
 /* Device fault word of the FFT kernels on the current device (no counterpart in the reference,
  * whose FFTs run on the host): PRC_FAULT_WAIT_TIMEOUT when a kernel gave up a bounded wait for its
  * own tile copies (its outputs are then incomplete), PRC_FAULT_SMEM_ALIGN when shared memory was

@@ -258,8 +258,9 @@ class OracleReconstruction(object):
     """One reconstruction, step by step as the reference runs it.
 
     algorithm: 'multigrid' (MultiGridReconstruction, pyrecon/multigrid.py:99-167),
-    'iterative_fft' (pyrecon/iterative_fft.py:12-82) or 'plane_parallel_fft'
-    (pyrecon/plane_parallel_fft.py:27-55).
+    'iterative_fft' (pyrecon/iterative_fft.py:12-82), 'plane_parallel_fft'
+    (pyrecon/plane_parallel_fft.py:27-55) or 'iterative_fft_particle'
+    (IterativeFFTParticleReconstruction, pyrecon/iterative_fft_particle.py:9-244).
     """
 
     def __init__(self, algorithm, f=0., bias=1., los=None, nmesh=None, boxsize=None, boxcenter=None,
@@ -318,6 +319,17 @@ class OracleReconstruction(object):
         return mesh
 
     def assign_data(self, positions, weights=None):
+        if self.algorithm == 'iterative_fft_particle':
+            # keeps the (wrapped) positions and weights for run (iterative_fft_particle.py:16-33)
+            if weights is None:
+                weights = np.ones_like(positions, shape=(len(positions),))
+            if self.wrap:
+                positions = self.geom.wrap(positions)
+            if self.mesh_data is None:
+                self._positions_data, self._weights_data = positions, weights
+            else:
+                self._positions_data = np.concatenate([self._positions_data, positions], axis=0)
+                self._weights_data = np.concatenate([self._weights_data, weights], axis=0)
         self.mesh_data = self._assign(self.mesh_data, positions, weights)
 
     def assign_randoms(self, positions, weights=None):
@@ -357,6 +369,11 @@ class OracleReconstruction(object):
     # -- density contrast (recon.py:198-249) --
 
     def set_density_contrast(self, ran_min=0.01, smoothing_radius=15.):
+        if self.algorithm == 'iterative_fft_particle':
+            # the meshes are smoothed by run (iterative_fft_particle.py:35-63)
+            self.ran_min, self.smoothing_radius = ran_min, smoothing_radius
+            self._delta_from_meshes()
+            return
         data = self.smooth_gaussian(self.mesh_data, smoothing_radius)
         if self.has_randoms:
             randoms = self.smooth_gaussian(self.mesh_randoms, smoothing_radius)
@@ -372,6 +389,112 @@ class OracleReconstruction(object):
             delta = self._cast(delta / self.bias)
         self.mesh_delta = delta
         self.mesh_data = self.mesh_randoms = None
+
+    def _delta_from_meshes(self):
+        """OriginalIterativeFFTParticleReconstruction.set_density_contrast body, on the current meshes."""
+        data = self.mesh_data
+        if self.has_randoms:
+            randoms = self.mesh_randoms
+            sum_data, sum_randoms = np.sum(data), np.sum(randoms)
+            alpha = sum_data * 1. / sum_randoms
+            delta = self._cast(data - alpha * randoms)
+            threshold = self.ran_min * sum_randoms / self._size_randoms
+            mask = randoms > threshold
+            delta[mask] /= (self.bias * alpha * randoms[mask])
+            delta[~mask] = 0.
+        else:
+            delta = self._cast(data / np.mean(data) - 1.)
+            delta = self._cast(delta / self.bias)
+        self.mesh_delta = delta
+
+    def _read_cic_wrap(self, mesh, positions):
+        """RealMesh.read_cic(positions, wrap=True) (mesh.py:570-610)."""
+        g = self.geom
+        dtype = positions.dtype
+        values = self.kernels.read_cic(mesh, g.nmesh, g.to_index(g.wrap(positions)))
+        return values.astype(dtype, copy=False)
+
+    def _run_iterative_fft_particle(self, niterations=3):
+        """OriginalIterativeFFTParticleReconstruction.run/_iterate (iterative_fft_particle.py:65-146)."""
+        self._iter = 0
+        self.mesh_data = self.smooth_gaussian(self.mesh_data, self.smoothing_radius)
+        if self.has_randoms:
+            self.mesh_randoms = self.smooth_gaussian(self.mesh_randoms, self.smoothing_radius)
+        self._positions_rec_data = self._positions_data.copy()
+        for it in range(niterations):
+            self.mesh_psi = self._iterate_particle(return_psi=it == niterations - 1)
+
+    def _iterate_particle(self, return_psi=False):
+        g = self.geom
+        if self._iter > 0:
+            wrap = self.wrap
+            self.wrap = True                               # painting always wraps here
+            self.mesh_data = self._assign(None, self._positions_rec_data, self._weights_data)
+            self.wrap = wrap
+            self.mesh_data = self.smooth_gaussian(self.mesh_data, self.smoothing_radius)
+        self._delta_from_meshes()
+        self.mesh_data = None
+        delta_k = self._to_complex(self.mesh_delta)
+        self.mesh_delta = None
+        kc = g.k_coords()
+        k = broadcast(*kc)
+        self._prod_sum_complex(delta_k, [kk ** 2 for kk in kc], exp=-1)
+        delta_k[0, 0, 0] = 0.
+        shifts = np.empty_like(self._positions_rec_data)
+        psis = []
+        for iaxis in range(3):
+            if not return_psi and self.los is not None and self.los[iaxis] == 0:
+                shifts[:, iaxis] = 0.
+                continue
+            psi = self._to_real(self._ccast(delta_k * 1j * k[iaxis]))
+            shifts[:, iaxis] = self._read_cic_wrap(psi, self._positions_rec_data)
+            if return_psi:
+                psis.append(psi)
+        if self.los is None:
+            los = self._positions_data / distance(self._positions_data)[:, None]
+        else:
+            los = self.los
+        if self._iter == 0:
+            shifts -= self.beta / (1 + self.beta) * np.sum(shifts * los, axis=-1)[:, None] * los
+        self._positions_rec_data = self._positions_data - self.f * np.sum(shifts * los, axis=-1)[:, None] * los
+        self._iter += 1
+        if return_psi:
+            return psis
+
+    def _read_shifts_particle(self, positions, field):
+        """OriginalIterativeFFTParticleReconstruction.read_shifts (iterative_fft_particle.py:148-218)."""
+        g = self.geom
+
+        def read(pos, wrap):
+            shifts = np.empty_like(pos)
+            for iaxis, psi in enumerate(self.mesh_psi):
+                if wrap:
+                    shifts[:, iaxis] = self._read_cic_wrap(psi, pos)
+                else:
+                    shifts[:, iaxis] = self._read_cic(psi, pos)
+            return shifts
+
+        if isinstance(positions, str) and positions == 'data':
+            shifts = read(self._positions_rec_data, True)
+            if field == 'disp':
+                return shifts
+            rsd = self._positions_data - self._positions_rec_data
+            if field == 'rsd':
+                return rsd
+            shifts += rsd
+            return shifts
+        if self.wrap:
+            positions = g.wrap(positions)
+        shifts = read(positions, False)
+        if field == 'disp':
+            return shifts
+        los = positions / distance(positions)[:, None] if self.los is None else self.los
+        rsd = self.f * np.sum(shifts * los, axis=-1)[:, None] * los
+        if field == 'rsd':
+            return rsd
+        real_positions = positions - rsd
+        shifts = read(real_positions, True)
+        return shifts + rsd
 
     # -- solvers --
 
@@ -462,6 +585,8 @@ class OracleReconstruction(object):
         field = field.lower()
         if field not in ['disp', 'rsd', 'disp+rsd']:
             raise OracleError('Unknown field {}'.format(field))
+        if self.algorithm == 'iterative_fft_particle':
+            return self._read_shifts_particle(positions, field)
         g = self.geom
         if self.algorithm == 'multigrid':
             dtype = positions.dtype
@@ -489,6 +614,8 @@ class OracleReconstruction(object):
 
     def read_shifted_positions(self, positions, field='disp+rsd'):
         shifts = self.read_shifts(positions, field=field)
+        if isinstance(positions, str) and positions == 'data':
+            positions = self._positions_data
         positions = positions - shifts
         if self.wrap:
             positions = self.geom.wrap(positions)

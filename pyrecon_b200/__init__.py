@@ -9,8 +9,10 @@ from .recon import BaseReconstruction, ReconstructionError
 from .multigrid import OriginalMultiGridReconstruction, MultiGridReconstruction
 from .iterative_fft import IterativeFFTReconstruction
 from .plane_parallel_fft import PlaneParallelFFTReconstruction
+from .iterative_fft_particle import OriginalIterativeFFTParticleReconstruction, IterativeFFTParticleReconstruction
 from .utils import setup_logging
 
 __all__ = ['MeshInfo', 'RealMesh', 'ComplexMesh', 'MeshError', 'BaseReconstruction', 'ReconstructionError',
            'OriginalMultiGridReconstruction', 'MultiGridReconstruction', 'IterativeFFTReconstruction',
-           'PlaneParallelFFTReconstruction', 'setup_logging']
+           'PlaneParallelFFTReconstruction', 'OriginalIterativeFFTParticleReconstruction',
+           'IterativeFFTParticleReconstruction', 'setup_logging']

@@ -34,6 +34,8 @@ _SIGNATURES = {
     'prc_profile_enable': (None, [c_int]),
     'prc_profile_collect': (c_int, [ctypes.c_char_p, c_size]),
     'prc_fft_supported': (c_int, [I3]),
+    'prc_sum_f32': (c_int, [_p, c_i64, _p, _p, c_size, _p]),
+    'prc_zeldovich_psi_workspace_bytes': (c_size, [I3, c_int]),
     'prc_device_fault_flags': (ctypes.c_uint, [c_int]),
     'prc_assign_cic_workspace_bytes': (c_size, [I3, c_i64, c_int]),
     'prc_assign_cic': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size, _p]),
@@ -57,6 +59,12 @@ for _s in ['f32', 'f64']:
                                               c_int, c_int, c_int, _p, c_int, _p, _p]),
         'prc_read_shifts_phi_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, _p, c_double, DP, c_int, c_int, c_int,
                                               _p, c_int, _p, _p]),
+        'prc_delta_from_meshes_' + _s: (c_int, [_p, _p, c_int, _p, I3, c_double, c_double, c_double, _p, _p]),
+        'prc_zeldovich_psi_' + _s: (c_int, [_p, I3, D3, _p, _p, _p, c_int, _p, c_size, _p]),
+        'prc_ifftp_update_' + _s: (c_int, [_p, I3, D3, D3, _p, _p, c_int, c_i64, c_double, c_double, c_int, DP, c_int,
+                                           _p, _p]),
+        'prc_ifftp_read_' + _s: (c_int, [_p, I3, D3, D3, _p, _p, c_int, c_i64, c_double, DP, c_int, c_int, c_int, _p,
+                                         c_int, _p, _p]),
         'prc_rfft3d_' + _s: (c_int, [_p, c_int, _p, I3, _p]),
         'prc_irfft3d_' + _s: (c_int, [_p, _p, I3, _p]),
         'prc_smooth_gaussian_' + _s: (c_int, [_p, c_int, _p, I3, D3, D3, _p, c_size, _p]),

@@ -462,7 +462,8 @@ __global__ void __launch_bounds__(PULL_WARPS * 32) paint_pull(const uint32_t* __
 constexpr int SUM_THREADS = 256;
 constexpr int SUM_BLOCKS = 512;
 
-__global__ void __launch_bounds__(SUM_THREADS) sum_partials(const double* __restrict__ x, int64_t n,
+template <typename X>
+__global__ void __launch_bounds__(SUM_THREADS) sum_partials(const X* __restrict__ x, int64_t n,
                                                             double* __restrict__ partial) {
     __shared__ double s[SUM_THREADS];
     double acc = 0.;
@@ -710,6 +711,181 @@ __global__ void __launch_bounds__(256) read_shifts_kernel(const F* __restrict__ 
             }
         }
         raise_flags(flags, bad & PRC_FLAG_OUT_OF_BOX);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// IterativeFFTParticleReconstruction (pyrecon/iterative_fft_particle.py): density contrast of
+// already smoothed meshes, the per-iteration particle update and the particle read-out.
+// Arithmetic of the particle steps in float64, results stored in the positions dtype.
+// ---------------------------------------------------------------------------------------------
+
+// delta of set_density_contrast (iterative_fft_particle.py:50-63) from meshes of type X.
+template <typename X, typename T>
+__global__ void __launch_bounds__(256) delta_meshes_kernel(const X* __restrict__ d, const X* __restrict__ r,
+                                                           const double* __restrict__ sums, int64_t n, double bias,
+                                                           double ran_min, double size_randoms, T* __restrict__ delta) {
+    const double sd = sums[0];
+    const double sr = r ? sums[1] : 0.;
+    const double alpha = r ? sd * 1. / sr : 0.;
+    const double threshold = r ? ran_min * sr / size_randoms : 0.;
+    const double mean = sd / (double)n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double dv = (double)d[i];
+        double o;
+        if (r) {
+            const double rv = (double)r[i];
+            o = rv > threshold ? (dv - alpha * rv) / (bias * alpha * rv) : 0.;
+        } else {
+            o = (dv / mean - 1.) / bias;
+        }
+        delta[i] = (T)o;
+    }
+}
+
+// Displacement (3 components, in P) at coordinates p, read with RealMesh.read_cic's wrap (wrap = 1)
+// or its box check (wrap = 0); NaN where invalid.
+template <typename P, typename F>
+__device__ __forceinline__ void psi_at(const typename vec4_of<F>::type* __restrict__ psi, const BoxGeom& g,
+                                       const P (&p)[3], int wrap, P (&s)[3], int* bad) {
+    F q[3] = {0, 0, 0};
+    const bool ok = particle_index<P, F>(p, 0, g, wrap, q, bad);
+    F d[3] = {(F)NAN, (F)NAN, (F)NAN};
+    if (ok) cic_read3<F>(psi, cic_setup(q, g.n), g.n, d);
+#pragma unroll
+    for (int a = 0; a < 3; a++) s[a] = (P)d[a];
+}
+
+// Line of sight: the global one (mesh dtype) or the unit vector of x.
+__device__ __forceinline__ void los_of(int global, double l0, double l1, double l2, const double (&x)[3],
+                                       double (&l)[3]) {
+    if (global) {
+        l[0] = l0, l[1] = l1, l[2] = l2;
+        return;
+    }
+    const double dist = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+#pragma unroll
+    for (int a = 0; a < 3; a++) l[a] = x[a] / dist;
+}
+
+__device__ __forceinline__ double dot3(const double (&a)[3], const double (&b)[3]) {
+    return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
+}
+
+// One iteration's update (iterative_fft_particle.py:106-139): shifts read at the current
+// reconstructed positions (wrapped), the first iteration's RSD correction, then
+// x_rec = x_data - f (s.l) l with l from the data positions (wrapped when wrap_data).
+template <typename P, typename F>
+__global__ void __launch_bounds__(256) ifftp_update_kernel(const typename vec4_of<F>::type* __restrict__ psi, BoxGeom g,
+                                                           const P* __restrict__ pos_data, P* __restrict__ pos_rec,
+                                                           int64_t n, double f, double beta, int first, int global_los,
+                                                           double l0, double l1, double l2, int wrap_data,
+                                                           int32_t* flags) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t nround = (n + stride - 1) / stride;
+    for (int64_t r = 0; r < nround; r++) {
+        const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + r * stride;
+        int bad = 0;
+        if (i < n) {
+            const P pr[3] = {pos_rec[3 * i], pos_rec[3 * i + 1], pos_rec[3 * i + 2]};
+            P s[3];
+            psi_at<P, F>(psi, g, pr, 1, s, &bad);
+            double x[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+                x[a] = wrap_data ? (double)(P)wrap_position<P, F>(pos_data[3 * i + a], g, a) : (double)pos_data[3 * i + a];
+            double l[3];
+            los_of(global_los, l0, l1, l2, x, l);
+            double sd[3] = {(double)s[0], (double)s[1], (double)s[2]};
+            double dot = dot3(sd, l);
+            if (first) {
+                const double c = beta / (1. + beta) * dot;
+#pragma unroll
+                for (int a = 0; a < 3; a++) sd[a] = (double)(P)(sd[a] - c * l[a]);
+                dot = dot3(sd, l);
+            }
+            const double fd = f * dot;
+#pragma unroll
+            for (int a = 0; a < 3; a++) pos_rec[3 * i + a] = (P)(x[a] - fd * l[a]);
+        }
+        raise_flags(flags, bad & PRC_FLAG_NONFINITE);
+    }
+}
+
+// Read-out (iterative_fft_particle.py:148-244).  data mode (pos_rec != NULL, pos = the data):
+// shifts at the reconstructed positions, RSD = data - reconstructed.  Otherwise, at positions p
+// (wrapped when wrap): disp = psi(p); rsd = f (disp.l) l; disp+rsd = psi(p - rsd, wrapped) + rsd.
+// shifted: input positions - shifts, wrapped when wrap.
+template <typename P, typename F, typename O>
+__global__ void __launch_bounds__(256) ifftp_read_kernel(const typename vec4_of<F>::type* __restrict__ psi, BoxGeom g,
+                                                         const P* __restrict__ pos, const P* __restrict__ pos_rec,
+                                                         int64_t n, double f, int global_los, double l0, double l1,
+                                                         double l2, int field, int shifted, int wrap,
+                                                         O* __restrict__ out, int32_t* flags) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t nround = (n + stride - 1) / stride;
+    for (int64_t r = 0; r < nround; r++) {
+        const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + r * stride;
+        int bad = 0;
+        if (i < n) {
+            double base[3], sh[3];
+            if (pos_rec != nullptr) {
+                const P pr[3] = {pos_rec[3 * i], pos_rec[3 * i + 1], pos_rec[3 * i + 2]};
+                P s[3];
+                psi_at<P, F>(psi, g, pr, 1, s, &bad);
+                P pd[3];
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    pd[a] = wrap ? (P)wrap_position<P, F>(pos[3 * i + a], g, a) : pos[3 * i + a];
+                    base[a] = (double)pd[a];
+                    const P rsd = (P)(pd[a] - pr[a]);
+                    sh[a] = field == PRC_FIELD_DISP ? (double)s[a]
+                          : (field == PRC_FIELD_RSD ? (double)rsd : (double)(P)(s[a] + rsd));
+                }
+            } else {
+                P p[3];
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    base[a] = (double)pos[3 * i + a];
+                    p[a] = wrap ? (P)wrap_position<P, F>(pos[3 * i + a], g, a) : pos[3 * i + a];
+                }
+                P s[3];
+                psi_at<P, F>(psi, g, p, 0, s, &bad);
+                if (field == PRC_FIELD_DISP) {
+#pragma unroll
+                    for (int a = 0; a < 3; a++) sh[a] = (double)s[a];
+                } else {
+                    double x[3] = {(double)p[0], (double)p[1], (double)p[2]}, l[3];
+                    los_of(global_los, l0, l1, l2, x, l);
+                    const double sd[3] = {(double)s[0], (double)s[1], (double)s[2]};
+                    const double fd = f * dot3(sd, l);
+                    P rsd[3];
+#pragma unroll
+                    for (int a = 0; a < 3; a++) rsd[a] = (P)(fd * l[a]);
+                    if (field == PRC_FIELD_RSD) {
+#pragma unroll
+                        for (int a = 0; a < 3; a++) sh[a] = (double)rsd[a];
+                    } else {
+                        P real[3], s2[3];
+#pragma unroll
+                        for (int a = 0; a < 3; a++) real[a] = (P)(p[a] - rsd[a]);
+                        psi_at<P, F>(psi, g, real, 1, s2, &bad);
+#pragma unroll
+                        for (int a = 0; a < 3; a++) sh[a] = (double)(P)(s2[a] + rsd[a]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                if (shifted) {
+                    const P v = (P)(base[a] - sh[a]);
+                    out[3 * i + a] = wrap ? (O)wrap_position<P, F>(v, g, a) : (O)v;
+                } else {
+                    out[3 * i + a] = (O)sh[a];
+                }
+            }
+        }
+        raise_flags(flags, bad);
     }
 }
 
@@ -1038,7 +1214,17 @@ prc_status_t prc_sum_f64(const double* x, int64_t n, double* out, void* workspac
     if (!out || n < 0 || (n > 0 && !x)) return PRC_ERR_ARG;
     if (!workspace || workspace_bytes < prc_sum_workspace_bytes(n)) return PRC_ERR_WORKSPACE;
     cudaStream_t st = (cudaStream_t)stream;
-    PRC_LAUNCH("sum", st, sum_partials<<<SUM_BLOCKS, SUM_THREADS, 0, st>>>(x, n, (double*)workspace));
+    PRC_LAUNCH("sum", st, sum_partials<double><<<SUM_BLOCKS, SUM_THREADS, 0, st>>>(x, n, (double*)workspace));
+    PRC_LAUNCH("sum", st, sum_final<<<1, SUM_THREADS, 0, st>>>((const double*)workspace, out));
+    PRC_CHECK_LAUNCH();
+    return PRC_OK;
+}
+
+prc_status_t prc_sum_f32(const float* x, int64_t n, double* out, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!out || n < 0 || (n > 0 && !x)) return PRC_ERR_ARG;
+    if (!workspace || workspace_bytes < prc_sum_workspace_bytes(n)) return PRC_ERR_WORKSPACE;
+    cudaStream_t st = (cudaStream_t)stream;
+    PRC_LAUNCH("sum", st, sum_partials<float><<<SUM_BLOCKS, SUM_THREADS, 0, st>>>(x, n, (double*)workspace));
     PRC_LAUNCH("sum", st, sum_final<<<1, SUM_THREADS, 0, st>>>((const double*)workspace, out));
     PRC_CHECK_LAUNCH();
     return PRC_OK;
@@ -1138,5 +1324,110 @@ READ_SHIFTS_IMPL(prc_read_shifts_phi_f64, double, true,
                   const double* los, int field, int shifted, int wrap, void* out, int out_bytes, int32_t* flags,
                   void* stream),
                  phi, phi, phi, 1)
+
+
+// ---- IterativeFFTParticleReconstruction ----
+
+#define DELTA_MESHES_IMPL(NAME, T)                                                                                    \
+    prc_status_t NAME(const void* mesh_data, const void* mesh_randoms, int in_bytes, const double* sums,            \
+                      const int32_t nmesh[3], double bias, double ran_min, double size_randoms, T* delta,           \
+                      void* stream) {                                                                             \
+        if (!mesh_data || !sums || !delta || !valid_nmesh(nmesh) || (in_bytes != 4 && in_bytes != 8))             \
+            return PRC_ERR_ARG;                                                                                   \
+        cudaStream_t st = (cudaStream_t)stream;                                                                   \
+        const int64_t n = (int64_t)nmesh[0] * nmesh[1] * nmesh[2];                                                \
+        const int grid = particle_grid(n);                                                                        \
+        const double bytes = (double)n * (in_bytes * (mesh_randoms ? 2 : 1) + sizeof(T));                         \
+        if (in_bytes == 8)                                                                                        \
+            PRC_LAUNCH_B("delta_meshes", st, bytes, delta_meshes_kernel<double, T><<<grid, 256, 0, st>>>(          \
+                (const double*)mesh_data, (const double*)mesh_randoms, sums, n, bias, ran_min, size_randoms, delta)); \
+        else                                                                                                      \
+            PRC_LAUNCH_B("delta_meshes", st, bytes, delta_meshes_kernel<float, T><<<grid, 256, 0, st>>>(           \
+                (const float*)mesh_data, (const float*)mesh_randoms, sums, n, bias, ran_min, size_randoms, delta));  \
+        PRC_CHECK_LAUNCH();                                                                                       \
+        return PRC_OK;                                                                                            \
+    }
+DELTA_MESHES_IMPL(prc_delta_from_meshes_f32, float)
+DELTA_MESHES_IMPL(prc_delta_from_meshes_f64, double)
+
+static int ifftp_args_ok(const void* psi4, size_t fsize, const int32_t nmesh[3], const double* boxsize,
+                         const double* boxcenter, const int32_t* flags, int pos_bytes, int64_t npos) {
+    if (!psi4 || !valid_nmesh(nmesh) || !boxsize || !boxcenter || !flags || npos < 0) return PRC_ERR_ARG;
+    if (pos_bytes != 4 && pos_bytes != 8) return PRC_ERR_ARG;
+    if (((uintptr_t)psi4 % (4 * fsize)) != 0) return PRC_ERR_ARG;
+    return PRC_OK;
+}
+
+#define IFFTP_UPDATE_IMPL(NAME, F)                                                                                    \
+    prc_status_t NAME(const F* psi4, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],     \
+                      const void* pos_data, void* pos_rec, int pos_bytes, int64_t npos, double f, double beta,       \
+                      int first, const double* los, int wrap_data, int32_t* flags, void* stream) {                   \
+        PRC_TRY(ifftp_args_ok(psi4, sizeof(F), nmesh, boxsize, boxcenter, flags, pos_bytes, npos));                         \
+        if (npos > 0 && (!pos_data || !pos_rec)) return PRC_ERR_ARG;                                              \
+        cudaStream_t st = (cudaStream_t)stream;                                                                   \
+        if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return PRC_ERR_CUDA;                  \
+        if (npos == 0) return PRC_OK;                                                                             \
+        BoxGeom g = make_geom(nmesh, boxsize, boxcenter);                                                         \
+        double l[3] = {0, 0, 0};                                                                                  \
+        if (los)                                                                                                  \
+            for (int a = 0; a < 3; a++) l[a] = (double)(F)los[a];                                                 \
+        typedef typename vec4_of<F>::type V4;                                                                     \
+        const double bytes = (double)npos * 9 * pos_bytes + 8.0 * npos * 4 * sizeof(F);                           \
+        if (pos_bytes == 4)                                                                                       \
+            PRC_LAUNCH_B("ifftp_update", st, bytes, ifftp_update_kernel<float, F><<<particle_grid(npos), 256, 0, st>>>( \
+                (const V4*)psi4, g, (const float*)pos_data, (float*)pos_rec, npos, f, beta, first, los != nullptr,  \
+                l[0], l[1], l[2], wrap_data, flags));                                                             \
+        else                                                                                                      \
+            PRC_LAUNCH_B("ifftp_update", st, bytes, ifftp_update_kernel<double, F><<<particle_grid(npos), 256, 0, st>>>( \
+                (const V4*)psi4, g, (const double*)pos_data, (double*)pos_rec, npos, f, beta, first,               \
+                los != nullptr, l[0], l[1], l[2], wrap_data, flags));                                             \
+        PRC_CHECK_LAUNCH();                                                                                       \
+        return PRC_OK;                                                                                            \
+    }
+IFFTP_UPDATE_IMPL(prc_ifftp_update_f32, float)
+IFFTP_UPDATE_IMPL(prc_ifftp_update_f64, double)
+
+#define IFFTP_READ_IMPL(NAME, F)                                                                                      \
+    prc_status_t NAME(const F* psi4, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],     \
+                      const void* positions, const void* pos_rec, int pos_bytes, int64_t npos, double f,             \
+                      const double* los, int field, int shifted, int wrap, void* out, int out_bytes, int32_t* flags, \
+                      void* stream) {                                                                             \
+        PRC_TRY(ifftp_args_ok(psi4, sizeof(F), nmesh, boxsize, boxcenter, flags, pos_bytes, npos));                         \
+        if (npos > 0 && (!positions || !out)) return PRC_ERR_ARG;                                                 \
+        if ((out_bytes != 4 && out_bytes != 8) || field < PRC_FIELD_DISP || field > PRC_FIELD_DISP_RSD)           \
+            return PRC_ERR_ARG;                                                                                   \
+        cudaStream_t st = (cudaStream_t)stream;                                                                   \
+        if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return PRC_ERR_CUDA;                  \
+        if (npos == 0) return PRC_OK;                                                                             \
+        BoxGeom g = make_geom(nmesh, boxsize, boxcenter);                                                         \
+        double l[3] = {0, 0, 0};                                                                                  \
+        if (los)                                                                                                  \
+            for (int a = 0; a < 3; a++) l[a] = (double)(F)los[a];                                                 \
+        typedef typename vec4_of<F>::type V4;                                                                     \
+        const int grid = particle_grid(npos);                                                                     \
+        const double bytes = (double)npos * (3 * pos_bytes * (pos_rec ? 2 : 1) + 3 * out_bytes) +                 \
+                             8.0 * npos * 4 * sizeof(F) * (field == PRC_FIELD_DISP_RSD && !pos_rec ? 2 : 1);     \
+        const int gl = los != nullptr;                                                                            \
+        if (pos_bytes == 4 && out_bytes == 4)                                                                     \
+            PRC_LAUNCH_B("ifftp_read", st, bytes, ifftp_read_kernel<float, F, float><<<grid, 256, 0, st>>>(        \
+                (const V4*)psi4, g, (const float*)positions, (const float*)pos_rec, npos, f, gl, l[0], l[1], l[2],  \
+                field, shifted, wrap, (float*)out, flags));                                                       \
+        else if (pos_bytes == 4)                                                                                  \
+            PRC_LAUNCH_B("ifftp_read", st, bytes, ifftp_read_kernel<float, F, double><<<grid, 256, 0, st>>>(       \
+                (const V4*)psi4, g, (const float*)positions, (const float*)pos_rec, npos, f, gl, l[0], l[1], l[2],  \
+                field, shifted, wrap, (double*)out, flags));                                                      \
+        else if (out_bytes == 4)                                                                                  \
+            PRC_LAUNCH_B("ifftp_read", st, bytes, ifftp_read_kernel<double, F, float><<<grid, 256, 0, st>>>(       \
+                (const V4*)psi4, g, (const double*)positions, (const double*)pos_rec, npos, f, gl, l[0], l[1],      \
+                l[2], field, shifted, wrap, (float*)out, flags));                                                 \
+        else                                                                                                      \
+            PRC_LAUNCH_B("ifftp_read", st, bytes, ifftp_read_kernel<double, F, double><<<grid, 256, 0, st>>>(      \
+                (const V4*)psi4, g, (const double*)positions, (const double*)pos_rec, npos, f, gl, l[0], l[1],      \
+                l[2], field, shifted, wrap, (double*)out, flags));                                                \
+        PRC_CHECK_LAUNCH();                                                                                       \
+        return PRC_OK;                                                                                            \
+    }
+IFFTP_READ_IMPL(prc_ifftp_read_f32, float)
+IFFTP_READ_IMPL(prc_ifftp_read_f64, double)
 
 }  // extern "C"

@@ -1408,6 +1408,31 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
     return FFTLaunch<T>::z_c2r(p, S + 1, 3, es, st);
 }
 
+// Zeldovich displacement of a density contrast, psi_a = IFFT(i k_a delta_k / k^2), delta_k(0) = 0
+// (iterative_fft.py:71-82, iterative_fft_particle.py:93-108).
+template <typename T>
+static int psi_impl(const T* delta, const int32_t nmesh[3], const double boxsize[3], T* px, T* py, T* pz,
+                    int psi_stride, void* ws, size_t wsb, cudaStream_t st) {
+    Epi<T> es;
+    PRC_TRY(psi_epilogue(px, py, pz, psi_stride, &es));
+    Plan3 p;
+    PRC_TRY(make_plan(nmesh, &p));
+    pad_pitch<T>(&p);
+    const size_t sb = spec_bytes<T>(p);
+    if (!ws || wsb < 4 * sb) return PRC_ERR_WORKSPACE;
+    cplx_t<T>* S[4];
+    for (int i = 0; i < 4; i++) S[i] = (cplx_t<T>*)((char*)ws + i * sb);
+    KOp op;
+    fill_kop_geometry(&op, p, boxsize, sizeof(T));
+    const void* ins[1] = {delta};
+    PRC_TRY((forward_zy<T, T>(p, ins, S, 1, st)));
+    op.type = KOP_PSI;
+    op.nper = 3;
+    PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));
+    PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, 3, st));
+    return FFTLaunch<T>::z_c2r(p, S + 1, 3, es, st);
+}
+
 template <typename T>
 static int rfft_impl(const void* in, int in_bytes, void* out, const int32_t nmesh[3], cudaStream_t st) {
     Plan3 p;
@@ -1566,6 +1591,26 @@ prc_status_t prc_iterative_fft_f64(const double* delta, const int32_t nmesh[3], 
         return PRC_ERR_ARG;
     return iter_impl<double>(delta, nmesh, boxsize, boxcenter, beta, los, niterations, psi_x, psi_y, psi_z, psi_stride,
                              workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+
+size_t prc_zeldovich_psi_workspace_bytes(const int32_t nmesh[3], int mesh_bytes) {
+    return prc_fft_workspace_bytes(nmesh, mesh_bytes, 4);
+}
+
+prc_status_t prc_zeldovich_psi_f32(const float* delta, const int32_t nmesh[3], const double boxsize[3], float* psi_x,
+                                   float* psi_y, float* psi_z, int psi_stride, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+    if (!delta || !geom_ok(nmesh, boxsize) || !psi_x || !psi_y || !psi_z) return PRC_ERR_ARG;
+    return psi_impl<float>(delta, nmesh, boxsize, psi_x, psi_y, psi_z, psi_stride, workspace, workspace_bytes,
+                           (cudaStream_t)stream);
+}
+prc_status_t prc_zeldovich_psi_f64(const double* delta, const int32_t nmesh[3], const double boxsize[3],
+                                   double* psi_x, double* psi_y, double* psi_z, int psi_stride, void* workspace,
+                                   size_t workspace_bytes, void* stream) {
+    if (!delta || !geom_ok(nmesh, boxsize) || !psi_x || !psi_y || !psi_z) return PRC_ERR_ARG;
+    return psi_impl<double>(delta, nmesh, boxsize, psi_x, psi_y, psi_z, psi_stride, workspace, workspace_bytes,
+                            (cudaStream_t)stream);
 }
 
 }  // extern "C"

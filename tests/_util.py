@@ -8,7 +8,8 @@ from conftest import GOLDEN
 from oracle import pipeline
 
 ALGOS = {'multigrid': 'MultiGridReconstruction', 'iterative_fft': 'IterativeFFTReconstruction',
-         'plane_parallel_fft': 'PlaneParallelFFTReconstruction'}
+         'plane_parallel_fft': 'PlaneParallelFFTReconstruction',
+         'iterative_fft_particle': 'IterativeFFTParticleReconstruction'}
 
 
 def load_golden(name):
@@ -52,6 +53,10 @@ def run_oracle(g, dtype=None, kernels='oracle'):
     out['shifted_data'] = rec.read_shifted_positions(data)
     if m['randoms']:
         out['shifted_randoms'] = rec.read_shifted_positions(randoms)
+    if m['algorithm'] == 'iterative_fft_particle':
+        out['shifts_data_disp'] = rec.read_shifts('data', field='disp')
+        out['shifts_data_rsd'] = rec.read_shifts('data', field='rsd')
+        out['shifted_data_str'] = rec.read_shifted_positions('data')
     return out
 
 
@@ -82,6 +87,10 @@ def run_gpu(g, dtype=None, **kwargs):
     out['shifted_data'] = rec.read_shifted_positions(data)
     if m['randoms']:
         out['shifted_randoms'] = rec.read_shifted_positions(randoms)
+    if m['algorithm'] == 'iterative_fft_particle':
+        out['shifts_data_disp'] = rec.read_shifts('data', field='disp')
+        out['shifts_data_rsd'] = rec.read_shifts('data', field='rsd')
+        out['shifted_data_str'] = rec.read_shifted_positions('data')
     return out, rec
 
 

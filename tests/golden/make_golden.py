@@ -69,6 +69,14 @@ CASES = [
     dict(name='pp_f4_losx', algorithm='plane_parallel_fft', dtype='f4', los='x', nmesh=16, boxsize=800., boxcenter=1600.),
     dict(name='pp_f8_box_wrap', algorithm='plane_parallel_fft', dtype='f8', los=[1., 2., 2.], nmesh=16, boxsize=800.,
          boxcenter=400., wrap=True, randoms=False),
+    dict(name='ifftp_f8_local', algorithm='iterative_fft_particle', dtype='f8', los=None, nmesh=16, boxsize=800.,
+         boxcenter=1600.),
+    dict(name='ifftp_f4_local', algorithm='iterative_fft_particle', dtype='f4', los=None, nmesh=16, boxsize=800.,
+         boxcenter=1600.),
+    dict(name='ifftp_f8_losvec', algorithm='iterative_fft_particle', dtype='f8', los=[0.3, -0.5, 0.8], nmesh=16,
+         boxsize=800., boxcenter=1600.),
+    dict(name='ifftp_f8_box_wrap', algorithm='iterative_fft_particle', dtype='f8', los='z', nmesh=16, boxsize=800.,
+         boxcenter=400., wrap=True, randoms=False),
 ]
 
 NDATA, NRANDOMS = 1500, 4000
@@ -98,7 +106,8 @@ def make_inputs(case, seed):
 
 def run_case(pyrecon, case, seed):
     Cls = {'multigrid': pyrecon.MultiGridReconstruction, 'iterative_fft': pyrecon.IterativeFFTReconstruction,
-           'plane_parallel_fft': pyrecon.PlaneParallelFFTReconstruction}[case['algorithm']]
+           'plane_parallel_fft': pyrecon.PlaneParallelFFTReconstruction,
+           'iterative_fft_particle': pyrecon.IterativeFFTParticleReconstruction}[case['algorithm']]
     data, wdata, randoms, wrandoms = make_inputs(case, seed)
     with_randoms = case.get('randoms', True)
     wrap = case.get('wrap', False)
@@ -129,6 +138,11 @@ def run_case(pyrecon, case, seed):
     out['shifted_data'] = recon.read_shifted_positions(data)
     if with_randoms:
         out['shifted_randoms'] = recon.read_shifted_positions(randoms)
+    if case['algorithm'] == 'iterative_fft_particle':
+        # the data at their own reconstructed real-space positions (iterative_fft_particle.py:176-186)
+        out['shifts_data_disp'] = recon.read_shifts('data', field='disp')
+        out['shifts_data_rsd'] = recon.read_shifts('data', field='rsd')
+        out['shifted_data_str'] = recon.read_shifted_positions('data')
     meta = dict(case)
     meta.update(f=0.8, bias=2., smoothing_radius=SMOOTHING, randoms=with_randoms, wrap=wrap,
                 reference_version=pyrecon.__version__)

@@ -27,7 +27,8 @@ def test_f8_matches_reference(name):
     assert maxrel(out['mesh_delta'], g['mesh_delta']) < 1e-10, name
     key = 'mesh_phi' if 'mesh_phi' in g else 'mesh_psi'
     assert maxrel(out[key], g[key]) < 1e-9, name
-    for k in ['shifts_disp', 'shifts_rsd', 'shifted_data', 'shifted_randoms']:
+    for k in ['shifts_disp', 'shifts_rsd', 'shifted_data', 'shifted_randoms', 'shifts_data_disp', 'shifts_data_rsd',
+              'shifted_data_str']:
         if k in g:
             assert out[k].dtype == g[k].dtype, k
             assert maxabs(out[k], g[k]) < 1e-6, (name, k, maxabs(out[k], g[k]))
@@ -43,7 +44,7 @@ def test_f4_within_1e3_of_f8_oracle(name):
     ref = run_oracle(g, dtype='f8')
     out, rec = run_gpu(g, dtype='f4')
     assert maxrel(out['mesh_data'], ref['mesh_data']) < 1e-5   # float index coordinates, as the reference's f4
-    for k in ['shifted_data', 'shifted_randoms']:
+    for k in ['shifted_data', 'shifted_randoms', 'shifted_data_str']:
         if k in ref:
             assert out[k].dtype == np.float32
             assert maxabs(out[k], ref[k]) < 1e-3, (name, k, maxabs(out[k], ref[k]))

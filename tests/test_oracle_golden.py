@@ -45,6 +45,10 @@ def run_oracle(g, kernels='oracle', dtype=None):
     out['shifted_data'] = rec.read_shifted_positions(g['data'])
     if m['randoms']:
         out['shifted_randoms'] = rec.read_shifted_positions(g['randoms'])
+    if m['algorithm'] == 'iterative_fft_particle':
+        out['shifts_data_disp'] = rec.read_shifts('data', field='disp')
+        out['shifts_data_rsd'] = rec.read_shifts('data', field='rsd')
+        out['shifted_data_str'] = rec.read_shifted_positions('data')
     return out
 
 
@@ -61,7 +65,7 @@ def test_oracle_matches_reference_golden(name):
     tol = tolerances(g['meta']['dtype'])
     np.testing.assert_array_equal(out['keys_data'], g['keys_data'])   # cell indices: bit-exact
     for key in ['mesh_data', 'mesh_randoms', 'mesh_delta', 'mesh_phi', 'mesh_psi', 'shifts_disp', 'shifts_rsd',
-                'shifted_data', 'shifted_randoms']:
+                'shifted_data', 'shifted_randoms', 'shifts_data_disp', 'shifts_data_rsd', 'shifted_data_str']:
         if key not in g:
             continue
         ref = g[key]
