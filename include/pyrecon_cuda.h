@@ -273,6 +273,40 @@ PRC_API prc_status_t prc_smooth_gaussian_f64(const void *in, int in_bytes, doubl
                                      const double boxsize[3], const double radius[3], void *workspace,
                                      size_t workspace_bytes, void *stream);
 
+/* Gaussian smoothing in real space: periodic convolution with exp(-r^2 / 2) truncated at r < nsigmas,
+ * normalised by the sum of its taps.  Replaces RealMesh.smooth_gaussian(method='real')
+ * (pyrecon/mesh.py:684-695) and the reference C smooth_gaussian / convolve (src/mesh.c:66-143), whose
+ * arguments it keeps: `radius` in units of the box side per axis (the reference's radius / boxsize,
+ * rounded to the mesh precision), `nsigmas` (rounded likewise).  Outputs equal the reference's bit for
+ * bit.  Out of place (in != out).  The taps are built on the host and copied into the workspace
+ * (from pageable memory: not for stream capture).  PRC_ERR_UNSUPPORTED when a half-width
+ * nsigmas * radius * nmesh exceeds 2047 cells.  The reference's kernel array is only fully written
+ * when its x and z widths agree; elsewhere this uses the layout its convolution reads. */
+PRC_API size_t prc_smooth_gaussian_real_workspace_bytes(const int32_t nmesh[3], const double radius[3], double nsigmas,
+                                                        int mesh_bytes);
+PRC_API prc_status_t prc_smooth_gaussian_real_f32(const float *in, float *out, const int32_t nmesh[3],
+                                                  const double radius[3], double nsigmas, void *workspace,
+                                                  size_t workspace_bytes, void *stream);
+PRC_API prc_status_t prc_smooth_gaussian_real_f64(const double *in, double *out, const int32_t nmesh[3],
+                                                  const double radius[3], double nsigmas, void *workspace,
+                                                  size_t workspace_bytes, void *stream);
+
+/* Martin's density contrast of OriginalMultiGridReconstruction.set_density_contrast
+ * (pyrecon/multigrid.py:49-97), before its smoothing, from the FP64 data and randoms paint meshes
+ * (randoms may be NULL): data set to 0 where 0 < randoms < ran_min, alpha = sum(data) / sum of
+ * randoms >= ran_min, delta = (data / (alpha randoms) - 1) / bias where randoms >= ran_min, else 0,
+ * then the mean of the non-zero delta removed from them.  Without randoms delta = (data / mean - 1) /
+ * bias.  The caller smooths delta afterwards (prc_smooth_gaussian_* or prc_smooth_gaussian_real_*). */
+PRC_API size_t prc_density_contrast_original_workspace_bytes(void);
+PRC_API prc_status_t prc_density_contrast_original_f32(const double *mesh_data, const double *mesh_randoms,
+                                                       const int32_t nmesh[3], double bias, double ran_min,
+                                                       float *delta, void *workspace, size_t workspace_bytes,
+                                                       void *stream);
+PRC_API prc_status_t prc_density_contrast_original_f64(const double *mesh_data, const double *mesh_randoms,
+                                                       const int32_t nmesh[3], double bias, double ran_min,
+                                                       double *delta, void *workspace, size_t workspace_bytes,
+                                                       void *stream);
+
 /* set_density_contrast of BaseReconstruction (pyrecon/recon.py:198-249): smooths the FP64 data
  * (and randoms, may be NULL) meshes, then delta = (d - alpha r) / (bias alpha r) where
  * r > ran_min * sum_r / size_randoms, else 0 (no randoms: d / mean(d) - 1, / bias).

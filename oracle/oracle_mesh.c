@@ -16,6 +16,7 @@
  */
 #include <stddef.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <math.h>
 
 #ifdef ORACLE_F32
@@ -173,5 +174,71 @@ int oracle_prod_sum(real_t *mesh, const int64_t *n, const real_t *coords, int ex
 #endif
             }
         }
+    return 0;
+}
+
+/*
+ * Gaussian smoothing by brute-force periodic convolution, in place.
+ * Follows src/mesh.c:117-143 (smooth_gaussian) and :66-115 (convolve):
+ * half-width rad = (size_t)(nsigmas * radius * n + 1.0) cells per axis
+ * (radius in box units; the product in real_t, the + 1.0 in double),
+ * fact = 1 / (n radius)^2 rounded to real_t, tap exp(-r2 / 2) evaluated in
+ * double where r2 = sum fact dx^2 < nsigmas^2 (else 0); every output is the
+ * sum of tap * input over dx, dy, dz ascending, in real_t, divided by the sum
+ * of all taps.  Neighbours wrap as ((i + d + n) mod 2^64) % n.  The taps are
+ * stored in the order the convolution reads them.
+ */
+int oracle_smooth_gaussian(real_t *mesh, const int64_t *n, const real_t *radius, real_t nsigmas)
+{
+    int64_t rad[3], nk[3];
+    real_t fact[3];
+    for (int a = 0; a < 3; a++) {
+        rad[a] = (int64_t)(size_t)((double)(nsigmas * radius[a] * (real_t)n[a]) + 1.0);
+        nk[a] = 2 * rad[a] + 1;
+        real_t nr = (real_t)n[a] * radius[a];
+        fact[a] = (real_t)(1.0 / (double)nr / (double)nr);
+    }
+    size_t ntaps = (size_t)(nk[0] * nk[1] * nk[2]);
+    real_t *taps = (real_t *)malloc(ntaps * sizeof(real_t));
+    size_t size = (size_t)(n[0] * n[1] * n[2]);
+    real_t *copy = (real_t *)malloc(size * sizeof(real_t));
+    if (!taps || !copy) {
+        free(taps);
+        free(copy);
+        return -1;
+    }
+    real_t total = 0;
+    size_t it = 0;
+    for (int64_t dx = -rad[0]; dx <= rad[0]; dx++)
+        for (int64_t dy = -rad[1]; dy <= rad[1]; dy++)
+            for (int64_t dz = -rad[2]; dz <= rad[2]; dz++) {
+                real_t r2 = fact[0] * (real_t)dx * (real_t)dx + fact[1] * (real_t)dy * (real_t)dy
+                            + fact[2] * (real_t)dz * (real_t)dz;
+                real_t k = 0;
+                if (r2 < nsigmas * nsigmas) k = (real_t)exp((double)(-r2 / (real_t)2));
+                taps[it++] = k;
+                total += k;
+            }
+    for (size_t i = 0; i < size; i++) copy[i] = mesh[i];
+    for (int64_t ix = 0; ix < n[0]; ix++)
+        for (int64_t iy = 0; iy < n[1]; iy++)
+            for (int64_t iz = 0; iz < n[2]; iz++) {
+                real_t acc = 0;
+                size_t t = 0;
+                for (int64_t dx = -rad[0]; dx <= rad[0]; dx++) {
+                    size_t jx = (size_t)(ix + dx + n[0]) % (size_t)n[0];
+                    for (int64_t dy = -rad[1]; dy <= rad[1]; dy++) {
+                        size_t jy = (size_t)(iy + dy + n[1]) % (size_t)n[1];
+                        for (int64_t dz = -rad[2]; dz <= rad[2]; dz++) {
+                            size_t jz = (size_t)(iz + dz + n[2]) % (size_t)n[2];
+                            real_t prod = taps[t++] * copy[flat(n, jx, jy, jz)];
+                            acc += prod;
+                        }
+                    }
+                }
+                mesh[flat(n, (size_t)ix, (size_t)iy, (size_t)iz)] = acc / total;
+            }
+    free(taps);
+    free(copy);
     return 0;
 }

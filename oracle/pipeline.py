@@ -71,13 +71,14 @@ class _Kernels(object):
             lib = ctypes.CDLL(name, mode=ctypes.RTLD_LOCAL)
             self._mesh, self._mg = lib, lib
             self._names = dict(assign='oracle_assign_cic', read='oracle_read_cic',
-                               fd='oracle_read_finite_difference_cic', prod='oracle_prod_sum', fmg='oracle_fmg')
+                               fd='oracle_read_finite_difference_cic', prod='oracle_prod_sum', fmg='oracle_fmg',
+                               smooth='oracle_smooth_gaussian')
         elif source == 'reference':
             prec = 'float' if self.dtype.itemsize == 4 else 'double'
             self._mesh = ctypes.CDLL(os.path.join(REF_DIR, 'mesh_{}.so'.format(prec)), mode=ctypes.RTLD_LOCAL)
             self._mg = ctypes.CDLL(os.path.join(REF_DIR, 'multigrid_{}.so'.format(prec)), mode=ctypes.RTLD_LOCAL)
             self._names = dict(assign='assign_cic', read='read_cic', fd='read_finite_difference_cic',
-                               prod='prod_sum', fmg='fmg')
+                               prod='prod_sum', fmg='fmg', smooth='smooth_gaussian')
         else:
             raise ValueError('unknown kernel source {}'.format(source))
 
@@ -129,6 +130,15 @@ class _Kernels(object):
         f.argtypes = (self._ptr(flat_real.size), ctypeslib.ndpointer(np.uint64, shape=3), self._ptr(coords.size), ctypes.c_int)
         f.restype = ctypes.c_int
         f(flat_real, self._sizes(shape), coords, int(exp))
+
+    def smooth_gaussian(self, mesh, nmesh, radius, nsigmas):
+        """In-place real-space smoothing; radius in box units (mesh.py:684-695, mesh.c:117-143)."""
+        f = getattr(self._mesh, self._names['smooth'])
+        f.argtypes = (self._ptr(mesh.size), ctypeslib.ndpointer(np.uint64, shape=3), self._ptr(3), self._ctype)
+        f.restype = ctypes.c_int
+        flat = mesh.reshape(-1)
+        if f(flat, self._sizes(nmesh), np.ascontiguousarray(radius, dtype=self.dtype), self.dtype.type(nsigmas)) != 0:
+            raise OracleError('smooth_gaussian failed')
 
     def fmg(self, delta, nmesh, boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los):
         phi = np.zeros(delta.size, dtype=self.dtype)
@@ -257,7 +267,8 @@ def sorted_cell_order(positions, geom, wrap=False):
 class OracleReconstruction(object):
     """One reconstruction, step by step as the reference runs it.
 
-    algorithm: 'multigrid' (MultiGridReconstruction, pyrecon/multigrid.py:99-167),
+    algorithm: 'multigrid' (MultiGridReconstruction, pyrecon/multigrid.py:99-167), 'multigrid_original'
+    (OriginalMultiGridReconstruction, pyrecon/multigrid.py:13-158, Martin's density contrast),
     'iterative_fft' (pyrecon/iterative_fft.py:12-82), 'plane_parallel_fft'
     (pyrecon/plane_parallel_fft.py:27-55) or 'iterative_fft_particle'
     (IterativeFFTParticleReconstruction, pyrecon/iterative_fft_particle.py:9-244).
@@ -357,10 +368,14 @@ class OracleReconstruction(object):
     def _to_real(self, valuek):
         return self._cast(self.fft.backward(valuek, self.geom.ctype).real)
 
-    def smooth_gaussian(self, value, radius):
-        """RealMesh.smooth_gaussian(method='fft') (mesh.py:655-680)."""
+    def smooth_gaussian(self, value, radius, method='fft', nsigmas=2.5):
+        """RealMesh.smooth_gaussian (mesh.py:655-695): by FFT, or (method='real') by the C convolution."""
         radius_ = np.empty_like(self.geom.boxsize, order='C')
         radius_[:] = radius
+        if method != 'fft':
+            out = np.array(value, dtype=self.dtype, order='C')
+            self.kernels.smooth_gaussian(out, self.geom.nmesh, radius_ / self.geom.boxsize, nsigmas)
+            return out
         valuek = self._to_complex(value)
         k2 = sum(-0.5 * (r * k) ** 2 for r, k in zip(radius_, broadcast(*self.geom.k_coords())))
         valuek *= np.exp(k2)
@@ -368,15 +383,20 @@ class OracleReconstruction(object):
 
     # -- density contrast (recon.py:198-249) --
 
-    def set_density_contrast(self, ran_min=0.01, smoothing_radius=15.):
+    def set_density_contrast(self, ran_min=None, smoothing_radius=15., **kwargs):
+        if self.algorithm == 'multigrid_original':
+            self._density_contrast_original(0.75 if ran_min is None else ran_min, smoothing_radius, **kwargs)
+            return
+        if ran_min is None:
+            ran_min = 0.01
         if self.algorithm == 'iterative_fft_particle':
             # the meshes are smoothed by run (iterative_fft_particle.py:35-63)
             self.ran_min, self.smoothing_radius = ran_min, smoothing_radius
             self._delta_from_meshes()
             return
-        data = self.smooth_gaussian(self.mesh_data, smoothing_radius)
+        data = self.smooth_gaussian(self.mesh_data, smoothing_radius, **kwargs)
         if self.has_randoms:
-            randoms = self.smooth_gaussian(self.mesh_randoms, smoothing_radius)
+            randoms = self.smooth_gaussian(self.mesh_randoms, smoothing_radius, **kwargs)
             sum_data, sum_randoms = np.sum(data), np.sum(randoms)
             alpha = sum_data * 1. / sum_randoms
             delta = self._cast(data - alpha * randoms)
@@ -388,6 +408,27 @@ class OracleReconstruction(object):
             delta = self._cast(data / np.mean(data) - 1.)
             delta = self._cast(delta / self.bias)
         self.mesh_delta = delta
+        self.mesh_data = self.mesh_randoms = None
+
+    def _density_contrast_original(self, ran_min, smoothing_radius, **kwargs):
+        """OriginalMultiGridReconstruction.set_density_contrast, Martin's recipe (multigrid.py:49-97)."""
+        data = self.mesh_data.copy()
+        if not self.has_randoms:
+            delta = self._cast(data / np.mean(data) - 1.)
+            delta = self._cast(delta / self.bias)
+        else:
+            randoms = self.mesh_randoms
+            mask = randoms >= ran_min
+            data[(randoms > 0) & (randoms < ran_min)] = 0.
+            alpha = np.sum(data) / np.sum(randoms[mask])
+            data[mask] /= alpha * randoms[mask]
+            delta = data
+            delta -= 1
+            delta[~mask] = 0.
+            delta /= self.bias
+            mask = delta != 0.
+            delta[mask] -= np.mean(delta[mask])
+        self.mesh_delta = self.smooth_gaussian(delta, smoothing_radius, **kwargs)
         self.mesh_data = self.mesh_randoms = None
 
     def _delta_from_meshes(self):
@@ -572,6 +613,8 @@ class OracleReconstruction(object):
                                          jacobi_damping_factor, jacobi_niterations, vcycle_niterations, self.los)
         self.mesh_delta = None
 
+    _run_multigrid_original = _run_multigrid
+
     # -- shifts (recon.py:255-325, multigrid.py:137-158, mesh.py:570-653) --
 
     def _read_cic(self, mesh, positions):
@@ -588,7 +631,7 @@ class OracleReconstruction(object):
         if self.algorithm == 'iterative_fft_particle':
             return self._read_shifts_particle(positions, field)
         g = self.geom
-        if self.algorithm == 'multigrid':
+        if self.algorithm in ('multigrid', 'multigrid_original'):
             dtype = positions.dtype
             p = g.wrap(positions) if self.wrap else positions
             if not self.wrap:

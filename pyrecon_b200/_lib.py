@@ -50,6 +50,8 @@ _SIGNATURES = {
     'prc_plane_parallel_workspace_bytes': (c_size, [I3, c_int]),
     'prc_iterative_fft_workspace_bytes': (c_size, [I3, c_int, c_int]),
     'prc_multigrid_workspace_bytes': (c_size, [I3, c_int, c_int]),
+    'prc_smooth_gaussian_real_workspace_bytes': (c_size, [I3, D3, c_double, c_int]),
+    'prc_density_contrast_original_workspace_bytes': (c_size, []),
 }
 for _s in ['f32', 'f64']:
     _SIGNATURES.update({
@@ -68,6 +70,8 @@ for _s in ['f32', 'f64']:
         'prc_rfft3d_' + _s: (c_int, [_p, c_int, _p, I3, _p]),
         'prc_irfft3d_' + _s: (c_int, [_p, _p, I3, _p]),
         'prc_smooth_gaussian_' + _s: (c_int, [_p, c_int, _p, I3, D3, D3, _p, c_size, _p]),
+        'prc_smooth_gaussian_real_' + _s: (c_int, [_p, _p, I3, D3, c_double, _p, c_size, _p]),
+        'prc_density_contrast_original_' + _s: (c_int, [_p, _p, I3, c_double, c_double, _p, _p, c_size, _p]),
         'prc_density_contrast_' + _s: (c_int, [_p, _p, _p, I3, D3, D3, c_double, c_double, c_double, _p, _p, c_size, _p]),
         'prc_plane_parallel_fft_' + _s: (c_int, [_p, I3, D3, c_double, D3, _p, _p, _p, c_int, _p, c_size, _p]),
         'prc_iterative_fft_' + _s: (c_int, [_p, I3, D3, D3, c_double, DP, c_int, _p, _p, _p, c_int, _p, c_size, _p]),

@@ -508,18 +508,30 @@ class RealMesh(BaseMesh):
     # -- spectral --
 
     def smooth_gaussian(self, radius, method='fft', nsigmas=2.5, **kwargs):
-        """Gaussian smoothing by FFT (mesh.py:655-680)."""
-        if method != 'fft':
-            raise MeshError("smooth_gaussian(method='{}') is not provided by pyrecon_b200; use method='fft'".format(method))
+        """Gaussian smoothing (mesh.py:655-695): by FFT (``method='fft'``), else by the real-space
+        convolution truncated at ``nsigmas``, whose output equals the reference's bit for bit."""
         torch = _torch()
         radius_ = _array3(radius, self.info._type_float)
         nm, bs, _ = self.info.c_geometry()
-        src = self._accum if self._accum is not None else self.value
+        lib = _lib.load()
         out = torch.empty(self.shape, dtype=torch_dtype(self.dtype), device=self.device)
-        ws = self._workspace().get(_lib.load().prc_fft_workspace_bytes(nm, self.dtype.itemsize, 1))
-        _lib.call('prc_smooth_gaussian_' + _lib.suffix(self.dtype), _lib.ptr(src), src.element_size(), _lib.ptr(out),
-                  nm, bs, _lib.d3(radius_), _lib.ptr(ws), ws.numel(), _lib.stream_of(self.device), error=MeshError)
+        if method == 'fft':
+            src = self._accum if self._accum is not None else self.value
+            ws = self._workspace().get(lib.prc_fft_workspace_bytes(nm, self.dtype.itemsize, 1))
+            _lib.call('prc_smooth_gaussian_' + _lib.suffix(self.dtype), _lib.ptr(src), src.element_size(), _lib.ptr(out),
+                      nm, bs, _lib.d3(radius_), _lib.ptr(ws), ws.numel(), _lib.stream_of(self.device), error=MeshError)
+        else:
+            src = self.value                                   # in the mesh dtype, as the reference smooths it
+            box = radius_ / self.info.boxsize                  # box units, in the mesh dtype (mesh.py:685)
+            nsig = float(self.info._type_float.type(nsigmas))
+            nbytes = lib.prc_smooth_gaussian_real_workspace_bytes(nm, _lib.d3(box), nsig, self.dtype.itemsize)
+            if nbytes == 0:
+                raise MeshError('smooth_gaussian: invalid radius {} or nsigmas {}'.format(radius, nsigmas))
+            ws = self._workspace().get(nbytes)
+            _lib.call('prc_smooth_gaussian_real_' + _lib.suffix(self.dtype), _lib.ptr(src), _lib.ptr(out), nm,
+                      _lib.d3(box), nsig, _lib.ptr(ws), ws.numel(), _lib.stream_of(self.device), error=MeshError)
         self._accum = None
+        self._colsums = None
         self.__dict__['value'] = out
 
     def to_complex(self):

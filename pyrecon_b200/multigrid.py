@@ -28,6 +28,39 @@ class OriginalMultiGridReconstruction(BaseReconstruction):
             out.append(ntries[iclosest])
         return np.array(out, dtype='i8')
 
+    def set_density_contrast(self, ran_min=0.75, smoothing_radius=15., **kwargs):
+        r"""Martin's density contrast (multigrid.py:49-97): cells whose (unsmoothed) randoms are below
+        ``ran_min`` get :math:`\delta = 0` (their data is left out of the normalisation where randoms are
+        positive), elsewhere :math:`\delta = (d / (\alpha r) - 1) / b`; the mean of the non-zero
+        :math:`\delta` is removed, then :math:`\delta` is smoothed (``kwargs``: :meth:`RealMesh.smooth_gaussian`).
+        Without randoms :math:`\delta = (d / \bar{d} - 1) / b`, smoothed."""
+        import torch
+        with self._stream_ctx():
+            if not self.mesh_data.is_set:
+                from .recon import ReconstructionError
+                raise ReconstructionError('assign_data must be called before set_density_contrast')
+            lib = _lib.load()
+            nm, _, _ = self.info.c_geometry()
+
+            def fp64(mesh):
+                return mesh._accum if mesh._accum is not None else mesh.value.to(torch.float64)
+
+            has_randoms = self.has_randoms
+            data = fp64(self.mesh_data)
+            randoms = fp64(self.mesh_randoms) if has_randoms else None
+            delta = RealMesh(info=self.info, device=self.device)
+            delta._ws = self._ws
+            delta.__dict__['value'] = torch.empty(self.info.shape, dtype=torch_dtype(self.info.dtype), device=self.device)
+            ws = self._ws.get(lib.prc_density_contrast_original_workspace_bytes())
+            _lib.call('prc_density_contrast_original_' + _lib.suffix(self.info.dtype), _lib.ptr(data),
+                      _lib.ptr(randoms), nm, float(self.bias), float(ran_min), _lib.ptr(delta.value), _lib.ptr(ws),
+                      ws.numel(), _lib.stream_of(self.device), error=MeshError)
+            if has_randoms:
+                del self.mesh_data
+                del self.mesh_randoms
+            delta.smooth_gaussian(smoothing_radius, **kwargs)
+            self.mesh_delta = delta
+
     def run(self, jacobi_damping_factor=0.4, jacobi_niterations=5, vcycle_niterations=6):
         """Compute the displacement potential :attr:`mesh_phi` (multigrid.py:99-135)."""
         import torch

@@ -185,7 +185,7 @@ class BaseReconstruction(BaseClass):
         import torch
         method = kwargs.pop('method', 'fft')
         if method != 'fft':
-            raise MeshError("set_density_contrast(method='{}') is not provided by pyrecon_b200; use 'fft'".format(method))
+            return self._density_contrast_real(ran_min, smoothing_radius, check, **kwargs)
         with self._stream_ctx():
             nm, bs, _ = self.info.c_geometry()
             radius = _array3(smoothing_radius, self.info._type_float)
@@ -217,6 +217,39 @@ class BaseReconstruction(BaseClass):
                 s = sums.cpu().numpy()
                 threshold = ran_min * s[1] / self._size_randoms
                 self.log_info('Smoothed random threshold is (ran_min * mean weight) = {:.4f}.'.format(threshold))
+            self._sums = sums
+            self.mesh_delta = delta
+            del self.mesh_data
+            del self.mesh_randoms
+
+    def _density_contrast_real(self, ran_min, smoothing_radius, check, nsigmas=2.5, **kwargs):
+        """set_density_contrast with real-space smoothing (recon.py:220-249, mesh.py:684-695): both meshes
+        smoothed in the mesh dtype by the truncated convolution, then the contrast from their sums."""
+        import torch
+        with self._stream_ctx():
+            if not self.mesh_data.is_set:
+                raise ReconstructionError('assign_data must be called before set_density_contrast')
+            lib = _lib.load()
+            st = _lib.stream_of(self.device)
+            nm, _, _ = self.info.c_geometry()
+            self.mesh_data.smooth_gaussian(smoothing_radius, method='real', nsigmas=nsigmas)
+            data, randoms = self.mesh_data.value, None
+            if self.has_randoms:
+                if check and int((self.mesh_randoms.value > 0.).sum()) < 2:
+                    raise ValueError('Very few randoms!')
+                self.mesh_randoms.smooth_gaussian(smoothing_radius, method='real', nsigmas=nsigmas)
+                randoms = self.mesh_randoms.value
+            sums = torch.zeros(2, dtype=torch.float64, device=self.device)
+            ws = self._ws.get(lib.prc_sum_workspace_bytes(0))
+            for i, m in enumerate([data, randoms]):
+                if m is not None:
+                    _lib.call('prc_sum_' + _lib.suffix(self.info.dtype), _lib.ptr(m), m.numel(),
+                              _lib.c_void_p(sums.data_ptr() + 8 * i), _lib.ptr(ws), ws.numel(), st)
+            delta = RealMesh(info=self.info, device=self.device)
+            delta.__dict__['value'] = torch.empty(self.info.shape, dtype=torch_dtype(self.info.dtype), device=self.device)
+            _lib.call('prc_delta_from_meshes_' + _lib.suffix(self.info.dtype), _lib.ptr(data), _lib.ptr(randoms),
+                      data.element_size(), _lib.ptr(sums), nm, float(self.bias), float(ran_min),
+                      float(self._size_randoms), _lib.ptr(delta.value), st, error=MeshError)
             self._sums = sums
             self.mesh_delta = delta
             del self.mesh_data

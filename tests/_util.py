@@ -9,7 +9,8 @@ from oracle import pipeline
 
 ALGOS = {'multigrid': 'MultiGridReconstruction', 'iterative_fft': 'IterativeFFTReconstruction',
          'plane_parallel_fft': 'PlaneParallelFFTReconstruction',
-         'iterative_fft_particle': 'IterativeFFTParticleReconstruction'}
+         'iterative_fft_particle': 'IterativeFFTParticleReconstruction',
+         'multigrid_original': 'OriginalMultiGridReconstruction'}
 
 
 def load_golden(name):
@@ -41,10 +42,10 @@ def run_oracle(g, dtype=None, kernels='oracle'):
         randoms = g['randoms'].astype(dtype) if dtype else g['randoms']
         rec.assign_randoms(randoms, g['wrandoms'])
         out['mesh_randoms'] = rec.mesh_randoms.copy()
-    rec.set_density_contrast(smoothing_radius=m['smoothing_radius'])
+    rec.set_density_contrast(smoothing_radius=m['smoothing_radius'], **m.get('density_kwargs', {}))
     out['mesh_delta'] = rec.mesh_delta.copy()
     rec.run()
-    if m['algorithm'] == 'multigrid':
+    if m['algorithm'] in ('multigrid', 'multigrid_original'):
         out['mesh_phi'] = rec.mesh_phi
     else:
         out['mesh_psi'] = np.stack(rec.mesh_psi)
@@ -75,10 +76,10 @@ def run_gpu(g, dtype=None, **kwargs):
         randoms = g['randoms'].astype(dtype) if dtype else g['randoms']
         rec.assign_randoms(randoms, g['wrandoms'])
         out['mesh_randoms'] = rec.mesh_randoms._accum.cpu().numpy()
-    rec.set_density_contrast(smoothing_radius=m['smoothing_radius'])
+    rec.set_density_contrast(smoothing_radius=m['smoothing_radius'], **m.get('density_kwargs', {}))
     out['mesh_delta'] = np.asarray(rec.mesh_delta)
     rec.run()
-    if m['algorithm'] == 'multigrid':
+    if m['algorithm'] in ('multigrid', 'multigrid_original'):
         out['mesh_phi'] = np.asarray(rec.mesh_phi)
     else:
         out['mesh_psi'] = np.stack([np.asarray(p) for p in rec.mesh_psi])

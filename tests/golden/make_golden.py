@@ -18,7 +18,7 @@ the inputs and every intermediate the drop-in exposes:
 
 plus mesh-level kernel outputs in mesh_kernels.npz.  The fixtures are small
 (nmesh <= 24, a few thousand particles) so the oracle reproduces them in
-seconds.  Usage:  python tests/golden/make_golden.py
+seconds.  Usage:  python tests/golden/make_golden.py [name ...]   (all by default)
 """
 
 import os
@@ -77,6 +77,20 @@ CASES = [
          boxsize=800., boxcenter=1600.),
     dict(name='ifftp_f8_box_wrap', algorithm='iterative_fft_particle', dtype='f8', los='z', nmesh=16, boxsize=800.,
          boxcenter=400., wrap=True, randoms=False),
+    # OriginalMultiGridReconstruction: Martin's density contrast (multigrid.py:49-97)
+    dict(name='omg_f8_local', algorithm='multigrid_original', dtype='f8', los=None, nmesh=16, boxsize=800.,
+         boxcenter=1600.),
+    dict(name='omg_f4_local', algorithm='multigrid_original', dtype='f4', los=None, nmesh=16, boxsize=800.,
+         boxcenter=1600.),
+    dict(name='omg_f8_box_wrap', algorithm='multigrid_original', dtype='f8', los='z', nmesh=16, boxsize=800.,
+         boxcenter=400., wrap=True, randoms=False),
+    dict(name='omg_f8_real', algorithm='multigrid_original', dtype='f8', los=None, nmesh=16, boxsize=800.,
+         boxcenter=1600., density_kwargs=dict(method='real')),
+    # base density contrast with real-space smoothing (recon.py:220-226, mesh.py:684-695)
+    dict(name='mg_f8_real', algorithm='multigrid', dtype='f8', los=None, nmesh=16, boxsize=800., boxcenter=1600.,
+         density_kwargs=dict(method='real')),
+    dict(name='ifft_f4_real', algorithm='iterative_fft', dtype='f4', los=None, nmesh=16, boxsize=800., boxcenter=1600.,
+         density_kwargs=dict(method='real', nsigmas=3.)),
 ]
 
 NDATA, NRANDOMS = 1500, 4000
@@ -106,6 +120,7 @@ def make_inputs(case, seed):
 
 def run_case(pyrecon, case, seed):
     Cls = {'multigrid': pyrecon.MultiGridReconstruction, 'iterative_fft': pyrecon.IterativeFFTReconstruction,
+           'multigrid_original': pyrecon.multigrid.OriginalMultiGridReconstruction,
            'plane_parallel_fft': pyrecon.PlaneParallelFFTReconstruction,
            'iterative_fft_particle': pyrecon.IterativeFFTParticleReconstruction}[case['algorithm']]
     data, wdata, randoms, wrandoms = make_inputs(case, seed)
@@ -126,10 +141,10 @@ def run_case(pyrecon, case, seed):
         out.update(randoms=randoms, wrandoms=wrandoms)
         recon.assign_randoms(randoms, wrandoms)
         out['mesh_randoms'] = np.array(recon.mesh_randoms.value)
-    recon.set_density_contrast(smoothing_radius=SMOOTHING)
+    recon.set_density_contrast(smoothing_radius=SMOOTHING, **case.get('density_kwargs', {}))
     out['mesh_delta'] = np.array(recon.mesh_delta.value)
     recon.run()
-    if case['algorithm'] == 'multigrid':
+    if case['algorithm'] in ('multigrid', 'multigrid_original'):
         out['mesh_phi'] = np.array(recon.mesh_phi.value)
     else:
         out['mesh_psi'] = np.stack([np.array(p.value) for p in recon.mesh_psi])
@@ -174,18 +189,37 @@ def mesh_kernels(pyrecon):
         out['prod_in_' + dtype] = np.array(cmesh.value)
         cmesh.prod_sum(arrays, exp=-1)
         out['prod_out_' + dtype] = np.array(cmesh.value)
+    # real-space Gaussian smoothing (mesh.py:684-695): isotropic, anisotropic, and a kernel wider
+    # than the mesh (neighbour indices wrap through the C code's unsigned arithmetic)
+    rng = np.random.default_rng(43)
+    smooth = [dict(nmesh=16, boxsize=1000., radius=90., nsigmas=2.5),
+              dict(nmesh=16, boxsize=1000., radius=[70., 90., 80.], nsigmas=3.),
+              dict(nmesh=6, boxsize=600., radius=250., nsigmas=2.5)]
+    out['smooth_cases'] = np.array(json.dumps(smooth))
+    for i, c in enumerate(smooth):
+        value = rng.uniform(-1., 3., (c['nmesh'],) * 3)
+        out['smooth_in_{:d}'.format(i)] = value
+        for dtype in ['f4', 'f8']:
+            mesh = pyrecon.RealMesh(boxsize=c['boxsize'], boxcenter=0., nmesh=c['nmesh'], dtype=dtype)
+            mesh.value = value.astype(dtype)
+            mesh.smooth_gaussian(c['radius'], method='real', nsigmas=c['nsigmas'])
+            out['smooth_real_{}_{:d}'.format(dtype, i)] = np.array(mesh.value)
     return out
 
 
-def main():
+def main(names=None):
+    """Write every fixture, or only those named (case names, 'mesh_kernels')."""
     with tempfile.TemporaryDirectory() as tmp:
         pyrecon = import_reference(tmp)
-        np.savez_compressed(os.path.join(HERE, 'mesh_kernels.npz'), **mesh_kernels(pyrecon))
+        if not names or 'mesh_kernels' in names:
+            np.savez_compressed(os.path.join(HERE, 'mesh_kernels.npz'), **mesh_kernels(pyrecon))
         for seed, case in enumerate(CASES):
+            if names and case['name'] not in names:
+                continue
             out = run_case(pyrecon, case, seed)
             np.savez_compressed(os.path.join(HERE, case['name'] + '.npz'), **out)
             print('wrote', case['name'])
 
 
 if __name__ == '__main__':
-    main()
+    main(sys.argv[1:])

@@ -427,3 +427,80 @@ def test_multigrid_graph_replay_equals_direct_launches(dtype, mixed, tmp_path):
     res = subprocess.run([sys.executable, '-c', code], cwd=root, env=env, capture_output=True, text=True, timeout=300)
     assert res.returncode == 0, res.stdout + res.stderr
     assert np.array_equal(np.load(path), first)
+
+
+def _smooth_real_gpu(value, radius_box, nsigmas, dtype):
+    L = lib()
+    t = torch()
+    nm = L.i3(value.shape)
+    src = dev(value.astype(dtype))
+    out = t.empty_like(src)
+    nbytes = L.load().prc_smooth_gaussian_real_workspace_bytes(nm, L.d3(radius_box), float(nsigmas), np.dtype(dtype).itemsize)
+    assert nbytes > 0
+    w = ws(nbytes)
+    L.call('prc_smooth_gaussian_real_' + L.suffix(dtype), L.ptr(src), L.ptr(out), nm, L.d3(radius_box),
+           float(nsigmas), L.ptr(w), w.numel(), stream())
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+def test_real_space_smoothing_bit_exact(dtype):
+    """RealMesh.smooth_gaussian(method='real') equals the reference's output bit for bit (golden
+    vectors: isotropic, anisotropic, and a kernel wider than the mesh), twice in a row."""
+    import json
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, 'mesh_kernels.npz'))
+    for i, c in enumerate(json.loads(str(z['smooth_cases']))):
+        radius = pipeline._array3(c['radius'], dtype) / pipeline._array3(c['boxsize'], dtype)
+        nsig = np.dtype(dtype).type(c['nsigmas'])
+        ref = z['smooth_real_{}_{:d}'.format(dtype, i)]
+        for _ in range(2):
+            out = _smooth_real_gpu(z['smooth_in_{:d}'.format(i)], radius, nsig, dtype)
+            assert out.dtype == ref.dtype
+            np.testing.assert_array_equal(out, ref, err_msg=str(c))
+
+
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+def test_real_space_smoothing_matches_oracle_noncubic(dtype):
+    """Non-cubic mesh, widths differing per axis, tiles cut by the mesh edge: bit-exact against the C oracle."""
+    rng = np.random.default_rng(7)
+    nmesh = (37, 30, 45)
+    value = rng.uniform(-1., 3., nmesh).astype(dtype)
+    radius = np.array([0.09, 0.12, 0.07], dtype=dtype)
+    k = pipeline._Kernels(dtype)
+    ref = value.copy()
+    k.smooth_gaussian(ref, np.array(nmesh), radius, 2.5)
+    out = _smooth_real_gpu(value, radius, np.dtype(dtype).type(2.5), dtype)
+    np.testing.assert_array_equal(out, ref)
+
+
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+@pytest.mark.parametrize('randoms', [True, False])
+def test_density_contrast_original_matches_numpy(dtype, randoms):
+    """Martin's density contrast (before smoothing) against its numpy restatement in FP64."""
+    L = lib()
+    t = torch()
+    rng = np.random.default_rng(11)
+    nmesh = (48, 40, 36)
+    d = rng.gamma(2., 1., nmesh)
+    r = rng.gamma(1.5, 0.6, nmesh) * (rng.uniform(size=nmesh) > 0.2) if randoms else None
+    bias, ran_min = 1.7, 0.75
+    if randoms:
+        mask = r >= ran_min
+        dd = np.where((r > 0) & (r < ran_min), 0., d)
+        alpha = dd.sum() / r[mask].sum()
+        ref = np.where(mask, (dd / (alpha * np.where(mask, r, 1.)) - 1.) / bias, 0.).astype(dtype)
+        nz = ref != 0
+        ref[nz] = (ref[nz].astype('f8') - ref[nz].astype('f8').mean()).astype(dtype)
+    else:
+        ref = ((d / d.mean() - 1.) / bias).astype(dtype)
+    out = t.empty(nmesh, dtype=t.float32 if dtype == 'f4' else t.float64, device='cuda')
+    w = ws(L.load().prc_density_contrast_original_workspace_bytes())
+    d_dev, r_dev = dev(d), (dev(r) if randoms else None)        # kept alive until the kernel has run
+    L.call('prc_density_contrast_original_' + L.suffix(dtype), L.ptr(d_dev), L.ptr(r_dev), L.i3(nmesh), bias, ran_min,
+           L.ptr(out), L.ptr(w), w.numel(), stream())
+    out = out.cpu().numpy()
+    assert np.array_equal(out == 0, ref == 0)
+    tol = 1e-12 if dtype == 'f8' else 1e-6
+    assert maxrel(out, ref) < tol

@@ -48,6 +48,17 @@ def test_host_only_entry_points():
     # argument checks run before anything touches a device
     assert lib.prc_assign_cic(None, None, _lib.i3((8, 8, 8)), _lib.d3([1.] * 3), _lib.d3([0.] * 3), 8, None, 8, None, 0,
                               0, 0, 0, None, None, 0, None) == 1
+    # real-space smoothing: taps of a half-width (2.5 * 0.09 * 64 + 1 -> 15 cells) stored as rows + weights
+    nm64 = _lib.i3((64, 64, 64))
+    small = lib.prc_smooth_gaussian_real_workspace_bytes(nm64, _lib.d3([0.09] * 3), 2.5, 4)
+    assert 4 * 4 * 31 * 31 * 0.5 < small < 256 + 16 * 31 * 31 + 4 * 31 ** 3
+    assert lib.prc_smooth_gaussian_real_workspace_bytes(nm64, _lib.d3([0.09] * 3), 2.5, 8) > small
+    assert lib.prc_smooth_gaussian_real_workspace_bytes(nm64, _lib.d3([40.] * 3), 2.5, 4) == 0      # too wide
+    assert lib.prc_smooth_gaussian_real_workspace_bytes(nm64, _lib.d3([0., 0.1, 0.1]), 2.5, 4) == 0  # no radius
+    buf = ctypes.c_void_p(4096)
+    assert lib.prc_smooth_gaussian_real_f32(buf, buf, nm64, _lib.d3([0.09] * 3), 2.5, None, 0, None) == 1  # in place
+    assert lib.prc_density_contrast_original_workspace_bytes() >= 4 * 8
+    assert lib.prc_density_contrast_original_f64(None, None, nm64, 2., 0.75, None, None, 0, None) == 1
 
 
 def test_meshinfo_semantics():

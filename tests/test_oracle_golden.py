@@ -33,10 +33,10 @@ def run_oracle(g, kernels='oracle', dtype=None):
     if m['randoms']:
         rec.assign_randoms(g['randoms'], g['wrandoms'])
         out['mesh_randoms'] = rec.mesh_randoms.copy()
-    rec.set_density_contrast(smoothing_radius=m['smoothing_radius'])
+    rec.set_density_contrast(smoothing_radius=m['smoothing_radius'], **m.get('density_kwargs', {}))
     out['mesh_delta'] = rec.mesh_delta.copy()
     rec.run()
-    if m['algorithm'] == 'multigrid':
+    if m['algorithm'] in ('multigrid', 'multigrid_original'):
         out['mesh_phi'] = rec.mesh_phi
     else:
         out['mesh_psi'] = np.stack(rec.mesh_psi)
@@ -75,7 +75,7 @@ def test_oracle_matches_reference_golden(name):
 
 
 @pytest.mark.skipif(not pipeline.reference_kernels_available(), reason='reference C kernels not compiled here')
-@pytest.mark.parametrize('name', ['mg_f8_local', 'ifft_f8_local', 'pp_f8_losz'])
+@pytest.mark.parametrize('name', ['mg_f8_local', 'ifft_f8_local', 'pp_f8_losz', 'omg_f8_local', 'mg_f8_real'])
 def test_reference_kernel_backend_matches_golden(name):
     """The CPU-baseline back-end (reference C compiled from source, oracle/_ref) reproduces the golden run."""
     g = load(name)
@@ -107,6 +107,30 @@ def test_mesh_kernels_golden():
         rec.dtype, rec.kernels = np.dtype(dtype), k
         rec._prod_sum_complex(val, arrays, exp=-1)
         np.testing.assert_allclose(val, z['prod_out_' + dtype], **tol)
+
+
+def smooth_cases():
+    z = np.load(os.path.join(GOLDEN, 'mesh_kernels.npz'))
+    return z, json.loads(str(z['smooth_cases']))
+
+
+@pytest.mark.parametrize('kernels', ['oracle', 'reference'])
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+def test_real_space_smoothing_bit_exact(dtype, kernels):
+    """RealMesh.smooth_gaussian(method='real'): the C restatement (and the reference C compiled here)
+    equal the reference's output bit for bit, kernels wider than the mesh included."""
+    if kernels == 'reference' and not pipeline.reference_kernels_available():
+        pytest.skip('reference C kernels not compiled here')
+    z, cases = smooth_cases()
+    for i, c in enumerate(cases):
+        geom = pipeline.Geometry(c['nmesh'], c['boxsize'], 0., dtype=dtype)
+        rec = pipeline.OracleReconstruction.__new__(pipeline.OracleReconstruction)
+        rec.geom, rec.dtype, rec.kernels = geom, geom.dtype, pipeline._Kernels(dtype, source=kernels)
+        out = rec.smooth_gaussian(z['smooth_in_{:d}'.format(i)].astype(dtype), c['radius'], method='real',
+                                  nsigmas=c['nsigmas'])
+        ref = z['smooth_real_{}_{:d}'.format(dtype, i)]
+        assert out.dtype == ref.dtype
+        np.testing.assert_array_equal(out, ref, err_msg=str(c))
 
 
 def test_cell_order_is_stable_sort():
