@@ -53,6 +53,13 @@ WORKLOADS = {
     'iterative_fft_particle_512': dict(algorithm='IterativeFFTParticleReconstruction', nmesh=512, boxsize=2000.,
                                        boxcenter=2000., los=None, ndata=5_000_000, nrandoms=20_000_000, pos_dtype='f4',
                                        dtype='f4', weights=None, run_kwargs=dict(niterations=3)),
+    # OriginalMultiGridReconstruction (Martin's density contrast) with the real-space (truncated convolution)
+    # smoothing, on the multigrid_256 catalogues; the reference sample runs at full size (the convolution's
+    # cost grows with the cube of the mesh size at a fixed radius, so a smaller mesh would not scale)
+    'original_multigrid_real_256': dict(algorithm='OriginalMultiGridReconstruction', nmesh=256, boxsize=2000.,
+                                        boxcenter=2000., los=None, ndata=2_000_000, nrandoms=10_000_000,
+                                        pos_dtype='f8', dtype='f4', weights=(0.5, 1.5), run_kwargs={},
+                                        density_kwargs=dict(method='real'), reference_scale=1),
 }
 DEFAULT_WORKLOAD = 'iterative_fft_512'
 
@@ -77,8 +84,11 @@ MULTI_WORKLOADS = {
 
 
 def workload_name(w):
-    return '{algorithm} nmesh={nmesh} boxsize={boxsize:g} boxcenter={boxcenter:g} los={los} f=0.8 bias=2.0 ' \
+    name = '{algorithm} nmesh={nmesh} boxsize={boxsize:g} boxcenter={boxcenter:g} los={los} f=0.8 bias=2.0 ' \
            'smoothing_radius=15 data={ndata} lognormal randoms={nrandoms} uniform positions={pos_dtype}'.format(**w)
+    if w.get('density_kwargs'):
+        name += ' ' + ' '.join('{}={}'.format(k, v) for k, v in sorted(w['density_kwargs'].items()))
+    return name
 
 
 def dist_env():
@@ -96,11 +106,13 @@ def reference_sample(w, seed=0):
     from pyrecon_b200 import mocks
     cores = os.cpu_count() or 1
     kernels = 'reference' if pipeline.reference_kernels_available() else 'oracle'
-    n = w['nmesh'] // 2
-    nd, nr = w['ndata'] // 8, w['nrandoms'] // 8
+    scale = w.get('reference_scale', 8)
+    n = w['nmesh'] // (2 if scale == 8 else 1)
+    nd, nr = w['ndata'] // scale, w['nrandoms'] // scale
     algo = {'IterativeFFTReconstruction': 'iterative_fft', 'MultiGridReconstruction': 'multigrid',
             'PlaneParallelFFTReconstruction': 'plane_parallel_fft',
-            'IterativeFFTParticleReconstruction': 'iterative_fft_particle'}[w['algorithm']]
+            'IterativeFFTParticleReconstruction': 'iterative_fft_particle',
+            'OriginalMultiGridReconstruction': 'multigrid_original'}[w['algorithm']]
     data = mocks.lognormal_positions_numpy(nd, n, w['boxsize'], w['boxcenter'], seed=2002 + seed,
                                            field_seed=1002 + seed, dtype=w['pos_dtype'])
     randoms = mocks.uniform_positions_numpy(nr, w['boxsize'], w['boxcenter'], seed=3002 + seed, dtype=w['pos_dtype'])
@@ -114,15 +126,16 @@ def reference_sample(w, seed=0):
                                         fft_engine='scipy', nthreads=cores)
     rec.assign_data(data, wd)
     rec.assign_randoms(randoms, wr)
-    rec.set_density_contrast(smoothing_radius=15.)
+    rec.set_density_contrast(smoothing_radius=15., **w.get('density_kwargs', {}))
     rec.run(**w['run_kwargs'])
     rec.read_shifted_positions(data)
     rec.read_shifted_positions(randoms)
     dt = time.perf_counter() - t0
-    info = dict(cores=cores, kind='reference' if kernels == 'reference' else 'port',
-                sample='reference CPU path ({} C kernels with OpenMP x{}, numpy glue, scipy pocketfft x{}) on a 1/8 '
-                       'sample: nmesh {} and {} + {} particles, time x8'.format(
-                           'reference' if kernels == 'reference' else 'restated', cores, cores, n, nd, nr))
+    what = '1/8 sample: nmesh {} and {} + {} particles, time x8'.format(n, nd, nr) if scale == 8 else \
+        'full-size run: nmesh {} and {} + {} particles'.format(n, nd, nr)
+    info = dict(cores=cores, kind='reference' if kernels == 'reference' else 'port', scale=scale,
+                sample='reference CPU path ({} C kernels with OpenMP x{}, numpy glue, scipy pocketfft x{}) on a {}'.format(
+                    'reference' if kernels == 'reference' else 'restated', cores, cores, what))
     return dt, info
 
 
@@ -136,7 +149,7 @@ def run_reference_arm(args, w):
     for i in range(args.warmup + args.steps):
         dt, info = reference_sample(w, seed=i)
         if i >= args.warmup:
-            times.append(dt * 8.)
+            times.append(dt * info['scale'])
         if time.perf_counter() - t_start > budget and len(times) >= 1:
             break
     sec = statistics.median(times)
@@ -232,7 +245,7 @@ def reconstruct(w, device, data, wd, randoms, wr, check):
               dtype=w['dtype'], device=device)
     rec.assign_data(data, wd, check=check)
     rec.assign_randoms(randoms, wr, check=check)
-    rec.set_density_contrast(smoothing_radius=15.)
+    rec.set_density_contrast(smoothing_radius=15., **w.get('density_kwargs', {}))
     rec.run(**w['run_kwargs'])
     out_d = rec.read_shifted_positions(data)
     out_r = rec.read_shifted_positions(randoms)
@@ -379,7 +392,7 @@ def run_gpu_arm(args, w):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sec, info = reference_sample(w)
-        cpu = dict(value=1. / (8. * sec), unit='recons/s', cores=info['cores'], kind=info['kind'], sample=info['sample'])
+        cpu = dict(value=1. / (info['scale'] * sec), unit='recons/s', cores=info['cores'], kind=info['kind'], sample=info['sample'])
 
     if rank == 0:
         line = dict(metric=METRIC, value=value, unit='recons/s', n_gpus=world, steps=args.steps, warmup=args.warmup,
@@ -495,6 +508,60 @@ def run_multi_arm(args, w):
     return 0
 
 
+# Single-kernel timings through the C ABI (one launch per step, inputs above L2), for the per-kernel
+# roofline and for ncu captures of one kernel: name -> (mesh dtype, nmesh).
+KERNELS = {
+    'mg_jacobi': ('f4', 512),          # damped-Jacobi sweeps (two per step), local line of sight, FP32
+    'mg_jacobi_f64': ('f8', 384),
+    'mg_residual': ('f4', 512),
+    'smooth_real': ('f4', 256),        # truncated real-space Gaussian, radius 15 Mpc/h on 7.8 Mpc/h cells
+}
+
+
+def run_kernel_arm(args):
+    import torch
+    import numpy as np
+    from pyrecon_b200 import _lib
+    device = torch.device('cuda', 0)
+    torch.cuda.set_device(device)
+    dtype, n = KERNELS[args.kernel]
+    tdt = torch.float32 if dtype == 'f4' else torch.float64
+    item = 4 if dtype == 'f4' else 8
+    g = torch.Generator(device=device).manual_seed(5)
+    v = torch.rand((n, n, n), generator=g, device=device, dtype=tdt)
+    f = torch.rand((n, n, n), generator=g, device=device, dtype=tdt)
+    out = torch.empty_like(v)
+    nm, bs, bc = _lib.i3((n, n, n)), _lib.d3([2000.] * 3), _lib.d3([2000.] * 3)
+    st = _lib.stream_of(device)
+    N = n ** 3
+    if args.kernel.startswith('mg_jacobi'):
+        # two sweeps per step (v -> out -> v), so the result lands back in v without a copy
+        name, nbytes = 'prc_mg_jacobi_' + _lib.suffix(dtype), 2 * 3 * N * item
+        call = lambda: _lib.call(name, _lib.ptr(v), _lib.ptr(f), _lib.ptr(out), nm, bs, bc, 0.4, 0.4, 2, None, st)
+    elif args.kernel == 'mg_residual':
+        name, nbytes = 'prc_mg_residual_' + _lib.suffix(dtype), 3 * N * item
+        call = lambda: _lib.call(name, _lib.ptr(v), _lib.ptr(f), _lib.ptr(out), nm, bs, bc, 0.4, None, st)
+    else:
+        box = np.array([15. / 2000.] * 3, dtype=dtype)
+        ws = torch.empty(_lib.load().prc_smooth_gaussian_real_workspace_bytes(nm, _lib.d3(box), 2.5, item),
+                         dtype=torch.uint8, device=device)
+        name, nbytes = 'prc_smooth_gaussian_real_' + _lib.suffix(dtype), 2 * N * item
+        call = lambda: _lib.call(name, _lib.ptr(v), _lib.ptr(out), nm, _lib.d3(box), 2.5, _lib.ptr(ws), ws.numel(), st)
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize(device)
+    with ClockSampler(0) as clocks:
+        time.sleep(1.0)
+        total_ms, per = timed_loop(call, args.steps, device)
+    peak, peak_kind = load_peaks()
+    ms = total_ms / args.steps
+    gbs = nbytes / 1e9 / (ms / 1e3)
+    print(json.dumps(dict(kernel=args.kernel, entry_point=name, nmesh=n, dtype=dtype, steps=args.steps, ms=ms,
+                          p50_ms=percentile(per, 50), algorithmic_bytes=nbytes, gbs=gbs, peak=peak, frac=gbs / peak,
+                          peak_source=peak_kind, clocks=clocks.summary())), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -504,7 +571,11 @@ def main(argv=None):
     ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(MULTI_WORKLOADS))
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--kernel', default=None, choices=sorted(KERNELS),
+                    help='time one kernel through the C ABI instead of a workload')
     args = ap.parse_args(argv)
+    if args.kernel is not None:
+        return run_kernel_arm(args)
     if args.workload in MULTI_WORKLOADS:
         if args.impl == 'reference':
             print(json.dumps({'impl': 'reference', 'unavailable': 'multi-request workloads compare the request loop '

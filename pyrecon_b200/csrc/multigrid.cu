@@ -164,10 +164,15 @@ __device__ __forceinline__ bool quad_of(const int n[3], Quad& q) {
     return q.z0 < n[2] && q.y < n[1];
 }
 
-// S(v) at the four cells of a quad (type A), with their coefficients.
-template <typename A, typename V, typename S>
-__device__ __forceinline__ void quad_stencil(const V* __restrict__ v, const Stencil<S>& s, const Quad& q, A (&sv)[4],
-                                             A (&diag)[4]) {
+// The operator at the four cells of a quad, rearranged so that a cell needs one division.  With
+// q = sum_a h_a^2 p_a^2 (so g = beta / q) and P = sum_a p_a^2:
+//   U = sum_a (v+a + v-a) / h_a^2
+//   W = sum_a p_a^2 (v+a + v-a) + 1/2 sum_{a<b} p_a p_b e_ab [+ sum_a p_a (v+a - v-a), local]
+//   S(v) = U + g W,   2 sum_a G_a = 2 (sum_a 1/h_a^2 + g P).
+// x and y are fixed for the thread, so the p_0, p_1 terms are computed once for its four cells.
+template <typename A, typename V, typename S, bool LOCAL>
+__device__ __forceinline__ void quad_terms(const V* __restrict__ v, const Stencil<S>& s, const Quad& q, A (&U)[4],
+                                           A (&W)[4], A (&qq)[4], A (&P)[4]) {
     const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
     const int64_t sx = (int64_t)n1 * n2;
     const int64_t xp = (int64_t)wrap_up(q.x, n0) * sx, xm = (int64_t)wrap_dn(q.x, n0) * sx, x0 = (int64_t)q.x * sx;
@@ -182,46 +187,77 @@ __device__ __forceinline__ void quad_stencil(const V* __restrict__ v, const Sten
     load4(v + xm + ym + q.z0, MM);
     load4(v + xm + yp + q.z0, MP);
     load4(v + xp + ym + q.z0, PM);
+    const A ih0 = (A)s.ih2[0], ih1 = (A)s.ih2[1], ih2 = (A)s.ih2[2];
+    A p0, p1, p2b;
+    if (LOCAL) {
+        p0 = (A)q.x + (A)s.off[0];
+        p1 = (A)q.y + (A)s.off[1];
+        p2b = (A)q.z0 + (A)s.off[2];
+    } else {
+        p0 = (A)s.losh[0];
+        p1 = (A)s.losh[1];
+        p2b = (A)s.losh[2];
+    }
+    const A s0 = p0 * p0, s1 = p1 * p1;
+    const A q01 = (A)s.h2[0] * s0 + (A)s.h2[1] * s1, P01 = s0 + s1;
+    const A e01 = (A)0.5 * p0 * p1, hp0 = (A)0.5 * p0, hp1 = (A)0.5 * p1;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        A p[3], g, G[3];
-        coeffs<A>(s, q.x, q.y, q.z0 + k, p, g, G);
-        const A exy = (A)PP[k] + (A)MM[k] - (A)MP[k] - (A)PM[k];
-        const A exz = (A)XP[k + 2] + (A)XM[k] - (A)XM[k + 2] - (A)XP[k];
-        const A eyz = (A)YP[k + 2] + (A)YM[k] - (A)YM[k + 2] - (A)YP[k];
-        sv[k] = stencil_terms<A>((A)XP[k + 1], (A)XM[k + 1], (A)YP[k + 1], (A)YM[k + 1], (A)c[k + 2], (A)c[k], exy, exz,
-                                 eyz, p, g, G, s.local);
-        diag[k] = (A)2 * (G[0] + G[1] + G[2]);
+        const A p2 = LOCAL ? p2b + (A)k : p2b;
+        const A s2 = p2 * p2;
+        const A xpv = (A)XP[k + 1], xmv = (A)XM[k + 1], ypv = (A)YP[k + 1], ymv = (A)YM[k + 1];
+        const A zpv = (A)c[k + 2], zmv = (A)c[k];
+        const A exy = ((A)PP[k] + (A)MM[k]) - ((A)MP[k] + (A)PM[k]);
+        const A exz = ((A)XP[k + 2] + (A)XM[k]) - ((A)XM[k + 2] + (A)XP[k]);
+        const A eyz = ((A)YP[k + 2] + (A)YM[k]) - ((A)YM[k + 2] + (A)YP[k]);
+        U[k] = ih0 * (xpv + xmv) + ih1 * (ypv + ymv) + ih2 * (zpv + zmv);
+        A w;
+        if (LOCAL)
+            w = (s0 + p0) * xpv + (s0 - p0) * xmv + (s1 + p1) * ypv + (s1 - p1) * ymv + (s2 + p2) * zpv +
+                (s2 - p2) * zmv;
+        else
+            w = s0 * (xpv + xmv) + s1 * (ypv + ymv) + s2 * (zpv + zmv);
+        W[k] = w + e01 * exy + hp0 * p2 * exz + hp1 * p2 * eyz;
+        qq[k] = q01 + (A)s.h2[2] * s2;
+        P[k] = P01 + s2;
     }
 }
 
-template <typename T>
+template <typename T> __device__ __forceinline__ T quotient(T a, T b) {
+    if constexpr (sizeof(T) == 4) return __fdividef(a, b);   // FP32 sweeps: fast reciprocal (2 ulp)
+    else return a / b;
+}
+
+// Damped-Jacobi sweep of four cells per thread:
+//   jac = (f + S) / (2 sum G) = (q (f + U) + beta W) / (2 (q sum 1/h^2 + beta P)),
+//   vout = v + w (jac - v).
+template <typename T, bool LOCAL>
 __global__ void __launch_bounds__(256) jacobi_sweep4(const T* __restrict__ v, const T* __restrict__ f,
                                                      T* __restrict__ vout, Stencil<T> s, T w, int zero_v) {
     Quad q;
     if (!quad_of(s.n, q)) return;
-    T fv[4], sv[4], dg[4], vc[4];
+    T fv[4], vc[4], U[4], W[4], qq[4], P[4];
     load4(f + q.c + q.z0, fv);
     if (zero_v) {
+        const T p0 = LOCAL ? (T)q.x + s.off[0] : s.losh[0], p1 = LOCAL ? (T)q.y + s.off[1] : s.losh[1];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            T p[3], g, G[3];
-            coeffs<T>(s, q.x, q.y, q.z0 + k, p, g, G);
-            sv[k] = (T)0;
-            dg[k] = (T)2 * (G[0] + G[1] + G[2]);
-            vc[k] = (T)0;
+            const T p2 = LOCAL ? (T)(q.z0 + k) + s.off[2] : s.losh[2];
+            const T s2 = p2 * p2;
+            qq[k] = s.h2[0] * p0 * p0 + s.h2[1] * p1 * p1 + s.h2[2] * s2;
+            P[k] = p0 * p0 + p1 * p1 + s2;
+            U[k] = W[k] = vc[k] = (T)0;
         }
     } else {
-        quad_stencil<T>(v, s, q, sv, dg);
+        quad_terms<T, T, T, LOCAL>(v, s, q, U, W, qq, P);
         load4(v + q.c + q.z0, vc);
     }
+    const T sih = s.ih2[0] + s.ih2[1] + s.ih2[2];
     T o[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        T jac = fv[k];
-        if (!zero_v) jac += sv[k];
-        jac /= dg[k];
-        o[k] = ((T)1 - w) * vc[k] + w * jac;
+        const T jac = quotient<T>(qq[k] * (fv[k] + U[k]) + s.beta * W[k], (T)2 * (qq[k] * sih + s.beta * P[k]));
+        o[k] = vc[k] + w * (jac - vc[k]);
     }
     if constexpr (sizeof(T) == 4) {
         *(float4*)(vout + q.c + q.z0) = make_float4(o[0], o[1], o[2], o[3]);
@@ -231,21 +267,24 @@ __global__ void __launch_bounds__(256) jacobi_sweep4(const T* __restrict__ v, co
     }
 }
 
-template <typename A, typename V, typename FT, typename R, typename S>
+// r = f - A v = (f + U - 2 v sum 1/h^2) + g (W - 2 P v), g = beta / q, evaluated in type A.
+template <typename A, typename V, typename FT, typename R, typename S, bool LOCAL>
 __global__ void __launch_bounds__(256) residual_kernel4(const V* __restrict__ v, const FT* __restrict__ f,
                                                         R* __restrict__ r, Stencil<S> s) {
     Quad q;
     if (!quad_of(s.n, q)) return;
-    A sv[4], dg[4];
-    quad_stencil<A>(v, s, q, sv, dg);
+    A U[4], W[4], qq[4], P[4];
+    quad_terms<A, V, S, LOCAL>(v, s, q, U, W, qq, P);
     V vc[4];
     FT fv[4];
     load4(v + q.c + q.z0, vc);
     load4(f + q.c + q.z0, fv);
+    const A sih2 = (A)2 * ((A)s.ih2[0] + (A)s.ih2[1] + (A)s.ih2[2]);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        const A av = dg[k] * (A)vc[k] - sv[k];
-        r[q.c + q.z0 + k] = (R)((A)fv[k] - av);
+        const A g = quotient<A>((A)s.beta, qq[k]);
+        const A x = (A)vc[k];
+        r[q.c + q.z0 + k] = (R)(((A)fv[k] + U[k] - sih2 * x) + g * (W[k] - (A)2 * P[k] * x));
     }
 }
 
@@ -434,7 +473,8 @@ template <typename T> struct MGRunner {
             const bool z0 = zero_first && it == 0;
             if (quad)
                 PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
-                             jacobi_sweep4<T><<<gq.grid, gq.block, 0, st>>>(v, f, tmp, s, (T)P.damping, z0));
+                             (s.local ? jacobi_sweep4<T, true> : jacobi_sweep4<T, false>)<<<gq.grid, gq.block, 0, st>>>(
+                                 v, f, tmp, s, (T)P.damping, z0));
             else
                 PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
                              jacobi_sweep<T, T><<<g.grid, g.block, 0, st>>>(v, f, tmp, s, (T)P.damping, z0));
@@ -454,7 +494,8 @@ template <typename T> struct MGRunner {
             if (quad_ok(L[l].n, v, f, B[l].r)) {
                 const Grid3 gq = grid3_quad(L[l].n);
                 PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T),
-                             residual_kernel4<T, T, T, T, T><<<gq.grid, gq.block, 0, st>>>(v, f, B[l].r, s));
+                             (s.local ? residual_kernel4<T, T, T, T, T, true> : residual_kernel4<T, T, T, T, T, false>)
+                                 <<<gq.grid, gq.block, 0, st>>>(v, f, B[l].r, s));
             } else {
                 PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T),
                              residual_kernel<T, T, T, T, T><<<g.grid, g.block, 0, st>>>(v, f, B[l].r, s));
@@ -643,8 +684,9 @@ int solve_mixed(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t 
             if (quad_ok(m.L[l].n, m.v64[l], m.f64[l], R.B[l].f)) {
                 const Grid3 gq = grid3_quad(m.L[l].n);
                 PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N,
-                             residual_kernel4<double, double, double, float, double><<<gq.grid, gq.block, 0, st>>>(
-                                 m.v64[l], m.f64[l], R.B[l].f, s64));
+                             (s64.local ? residual_kernel4<double, double, double, float, double, true>
+                                        : residual_kernel4<double, double, double, float, double, false>)
+                                 <<<gq.grid, gq.block, 0, st>>>(m.v64[l], m.f64[l], R.B[l].f, s64));
             } else {
                 PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N,
                              residual_kernel<double, double, double, float, double><<<g.grid, g.block, 0, st>>>(
@@ -865,8 +907,15 @@ prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t n
         if (!v || !f || !r || !nmesh || !boxsize || !boxcenter) return PRC_ERR_ARG;                                 \
         int n[3] = {nmesh[0], nmesh[1], nmesh[2]};                                                                   \
         Stencil<T> s = make_stencil<T>(n, boxsize, boxcenter, beta, los);                                            \
-        PRC_LAUNCH("mg_residual", (cudaStream_t)stream,                                                              \
-                   residual_kernel<T, T, T, T, T><<<grid3(n).grid, grid3(n).block, 0, (cudaStream_t)stream>>>(v, f, r, s)); \
+        const double bytes = 3.0 * sizeof(T) * n[0] * n[1] * n[2];                                                   \
+        if (quad_ok(n, v, f, r))                                                                                     \
+            PRC_LAUNCH_B("mg_residual", (cudaStream_t)stream, bytes,                                                 \
+                         (s.local ? residual_kernel4<T, T, T, T, T, true> : residual_kernel4<T, T, T, T, T, false>)  \
+                             <<<grid3_quad(n).grid, grid3_quad(n).block, 0, (cudaStream_t)stream>>>(v, f, r, s));     \
+        else                                                                                                         \
+            PRC_LAUNCH_B("mg_residual", (cudaStream_t)stream, bytes,                                                 \
+                         residual_kernel<T, T, T, T, T><<<grid3(n).grid, grid3(n).block, 0, (cudaStream_t)stream>>>(  \
+                             v, f, r, s));                                                                           \
         PRC_CHECK_LAUNCH();                                                                                          \
         return PRC_OK;                                                                                               \
     }                                                                                                                \
