@@ -337,7 +337,11 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_strided(Specs<cplx_t<T>> data
 // ---------------------------------------------------------------------------------------------
 // k-space operators (applied between forward and inverse x transforms)
 // ---------------------------------------------------------------------------------------------
-enum KOpType { KOP_IDENTITY = 0, KOP_GAUSS = 1, KOP_PP = 2, KOP_ITER_GLOBAL = 3, KOP_ITER_LOCAL = 4, KOP_PSI = 5 };
+// KOP_HESS3 (TMA passes only): the three x-transformed spectra of the local-line-of-sight iteration,
+// E, s_x E and k_x^2 E with E = delta / k^2, plus the two Nyquist lines written to `side` (see
+// fast::y_hessian_tma).
+enum KOpType { KOP_IDENTITY = 0, KOP_GAUSS = 1, KOP_PP = 2, KOP_ITER_GLOBAL = 3, KOP_ITER_LOCAL = 4, KOP_PSI = 5,
+               KOP_HESS3 = 6 };
 
 struct KOp {
     int type;
@@ -348,6 +352,7 @@ struct KOp {
     double los[3];
     double beta;
     double norm;         // overall scale (1 / (n0 n1 n2) when the inverse follows)
+    void* side;          // KOP_HESS3: nh + n1 complex values (the Nyquist lines Q01, L02)
 };
 
 __device__ __forceinline__ double kvalue(int i, int n, double fscale) {
@@ -984,6 +989,7 @@ template <typename T> struct FastXTma {
                 case KOP_ITER_GLOBAL: return go<KOP_ITER_GLOBAL>(maps, nin, so, p, op, bytes, st);
                 case KOP_ITER_LOCAL: return go<KOP_ITER_LOCAL>(maps, nin, so, p, op, bytes, st);
                 case KOP_PSI: return go<KOP_PSI>(maps, nin, so, p, op, bytes, st);
+                case KOP_HESS3: return go<KOP_HESS3>(maps, nin, so, p, op, bytes, st);
                 default: return go<KOP_IDENTITY>(maps, nin, so, p, op, bytes, st);
             }
         }
@@ -993,11 +999,14 @@ template <typename T> struct FastXTma {
 template <typename T> struct FastHessTma {
     template <int N> struct K {
         typedef StridedTmaCfg<T, N> cfg;
-        static int run(const Plan3& p, cplx_t<T>* const* d, cplx_t<T>* const* o, fast::HessGeom h, cudaStream_t st) {
+        // probe: only check that the tensor maps can be made (nothing is launched)
+        static int run(const Plan3& p, cplx_t<T>* const* d, cplx_t<T>* const* o, fast::HessGeom h, cudaStream_t st,
+                       bool probe) {
             typedef fast::TileShape<T, N, cfg::B> TS;
             tma::Maps maps;
-            for (int i = 0; i < 6; i++)
+            for (int i = 0; i < 3; i++)
                 if (!spectrum_map(&maps.m[i], d[i], p, sizeof(cplx_t<T>), cfg::B, TS::BOXL, 1)) return TMA_UNAVAILABLE;
+            if (probe) return PRC_OK;
             Specs<cplx_t<T>> so;
             for (int i = 0; i < 3; i++) so.p[i] = o[i];
             Strided s;
@@ -1007,11 +1016,12 @@ template <typename T> struct FastHessTma {
             s.os = (int64_t)p.dims.n[1] * p.pitch;
             s.ncols = p.nh;
             auto kern = fast::y_hessian_tma<T, N, cfg::B, cfg::S>;
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
+            const size_t smem = cfg::SMEM + 2 * N * sizeof(T);     // + the x1 and k_y tables
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             const int64_t ntiles = (int64_t)s.outer * ((s.ncols + cfg::B - 1) / cfg::B);
-            const double bytes = 9.0 * spectrum_values(p) * sizeof(cplx_t<T>);
+            const double bytes = 6.0 * spectrum_values(p) * sizeof(cplx_t<T>);
             PRC_LAUNCH_B("fft_y_inv_hessian", st, bytes,
-                         kern<<<resident_grid(kern, cfg::THREADS, cfg::SMEM, ntiles), cfg::THREADS, cfg::SMEM, st>>>(
+                         kern<<<resident_grid(kern, cfg::THREADS, smem, ntiles), cfg::THREADS, smem, st>>>(
                              maps, so, s, h));
             PRC_CHECK_LAUNCH();
             return PRC_OK;
@@ -1167,6 +1177,17 @@ template <typename T> struct FFTLaunch {
         return PRC_OK;
     }
 
+    // The TMA x pass only (TMA_UNAVAILABLE, with nothing launched, where it cannot run).
+    static int x_fused_tma(const Plan3& p, C* const* in, int nin, C* const* out, const KOp& op, cudaStream_t st) {
+        const int n0 = p.dims.n[0];
+        if (!fast_len(n0) || getenv_generic() || !tma_enabled()) return TMA_UNAVAILABLE;
+        Specs<C> si, so;
+        for (int i = 0; i < nin; i++) si.p[i] = in[i];
+        for (int i = 0; i < nin * op.nper; i++) so.p[i] = out[i];
+        const double bytes = (double)nin * (1 + op.nper) * spectrum_values(p) * CS;
+        return dispatch_pow2<FastXTma<T>::template K>(n0, p, si, nin, so, op, bytes, st);
+    }
+
     static int z_c2r(const Plan3& p, C* const* in, int nin, const Epi<T>& e, cudaStream_t st) {
         const int M = p.dims.n[2] / 2, nh = M + 1;
         if (fast_len(M) && !getenv_generic()) {
@@ -1210,6 +1231,7 @@ static void fill_kop_geometry(KOp* op, const Plan3& p, const double boxsize[3], 
     op->beta = 0.;
     op->nper = 1;
     op->norm = 1.0 / ((double)p.dims.n[0] * p.dims.n[1] * p.dims.n[2]);
+    op->side = nullptr;
 }
 
 template <typename T> static Epi<T> epi_default() {
@@ -1342,10 +1364,12 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
     const int nspec = 1 + std::max(nout, 3);
     const size_t sb = spec_bytes<T>(p);
     const size_t mesh_b = ((size_t)p.dims.size() * sizeof(T) + 255) & ~(size_t)255;
-    if (!ws || wsb < (size_t)nspec * sb + mesh_b) return PRC_ERR_WORKSPACE;
+    const size_t side_b = los ? 0 : (((size_t)(p.nh + p.dims.n[1]) * sizeof(cplx_t<T>) + 255) & ~(size_t)255);
+    if (!ws || wsb < (size_t)nspec * sb + mesh_b + side_b) return PRC_ERR_WORKSPACE;
     cplx_t<T>* S[7];
     for (int i = 0; i < nspec; i++) S[i] = (cplx_t<T>*)((char*)ws + i * sb);
     T* dreal = (T*)((char*)ws + nspec * sb);
+    cplx_t<T>* side = los ? nullptr : (cplx_t<T>*)((char*)ws + nspec * sb + mesh_b);
     KOp op;
     fill_kop_geometry(&op, p, boxsize, sizeof(T));
     if (los)
@@ -1363,9 +1387,6 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
     for (int it = 0; it < niter; it++) {
         const void* ins[1] = {it == 0 ? (const void*)delta : (const void*)dreal};
         PRC_TRY((forward_zy<T, T>(p, ins, S, 1, st)));
-        op.type = los ? KOP_ITER_GLOBAL : KOP_ITER_LOCAL;
-        op.nper = nout;
-        PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));
         double base = beta;
         if (it == 0) base /= (1. + beta);
         if (los) {
@@ -1377,25 +1398,44 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
             for (int c = 0; c < 6; c++) e.factor[c] = (1. + (pi[c] != pj[c])) * beta / (it == 0 ? (1. + beta) : 1.);
         }
         if (!los && fast_len(p.dims.n[1]) && !getenv_generic() && tma_enabled()) {
-            // inverse y of the six Hessian spectra combined into the quadratic in x2 (A, B, C over
-            // D00, D01, D02), then the z pass over C, B, A
+            // x pass to the three spectra E, s_x E, k_x^2 E (S1..S3), inverse y forming the six
+            // Hessian terms and combining them into the quadratic in x2 (A, B, C in S4..S6), then
+            // the z pass over C, B, A
             fast::HessGeom h;
             h.x0_off = e.offset[0];
             h.x0_cell = e.cell[0];
             h.x1_off = e.offset[1];
             h.x1_cell = e.cell[1];
             for (int c = 0; c < 6; c++) h.f[c] = e.factor[c];
-            cplx_t<T>* outs[3] = {S[1], S[2], S[3]};
-            const int r = dispatch_pow2<FastHessTma<T>::template K>(p.dims.n[1], p, S + 1, outs, h, st);
+            h.fscale_y = op.fscale[1];
+            h.fscale_z = op.fscale[2];
+            h.ny = p.dims.n[1];
+            h.nz = p.dims.n[2];
+            const bool even_x = p.dims.n[0] % 2 == 0;
+            h.q01 = even_x && p.dims.n[1] % 2 == 0 ? side : nullptr;
+            h.l02 = even_x && p.dims.n[2] % 2 == 0 ? side + p.nh : nullptr;
+            cplx_t<T>* outs[3] = {S[4], S[5], S[6]};
+            int r = dispatch_pow2<FastHessTma<T>::template K>(p.dims.n[1], p, S + 1, outs, h, st, true);
+            if (r == PRC_OK) {
+                op.type = KOP_HESS3;
+                op.nper = 3;
+                op.side = side;
+                r = FFTLaunch<T>::x_fused_tma(p, S, 1, S + 1, op, st);
+                op.side = nullptr;
+            }
             if (r != TMA_UNAVAILABLE) {
                 PRC_TRY(r);
+                PRC_TRY(dispatch_pow2<FastHessTma<T>::template K>(p.dims.n[1], p, S + 1, outs, h, st, false));
                 Epi<T> ep = e;
                 ep.type = EPI_ITER_POLY;
-                cplx_t<T>* cba[3] = {S[3], S[2], S[1]};
+                cplx_t<T>* cba[3] = {S[6], S[5], S[4]};
                 PRC_TRY(FFTLaunch<T>::z_c2r(p, cba, 3, ep, st));
                 continue;
             }
         }
+        op.type = los ? KOP_ITER_GLOBAL : KOP_ITER_LOCAL;
+        op.nper = nout;
+        PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));
         PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, nout, st));
         PRC_TRY(FFTLaunch<T>::z_c2r(p, S + 1, nout, e, st));
     }
@@ -1571,7 +1611,9 @@ size_t prc_iterative_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes,
     Plan3 p;
     if (!nmesh || make_plan(nmesh, &p) != PRC_OK) return 0;
     size_t mesh_b = ((size_t)p.dims.size() * mesh_bytes + 255) & ~(size_t)255;
-    return prc_fft_workspace_bytes(nmesh, mesh_bytes, local_los ? 7 : 4) + mesh_b;
+    // local line of sight: the two Nyquist lines of the three-spectrum Hessian pass
+    size_t side_b = local_los ? (((size_t)(p.nh + p.dims.n[1]) * 2 * mesh_bytes + 255) & ~(size_t)255) : 0;
+    return prc_fft_workspace_bytes(nmesh, mesh_bytes, local_los ? 7 : 4) + mesh_b + side_b;
 }
 
 prc_status_t prc_iterative_fft_f32(const float* delta, const int32_t nmesh[3], const double boxsize[3],

@@ -360,11 +360,29 @@ template <typename T, int N, int KT> struct KLine {
             } else if constexpr (KT == KOP_PSI) {
                 const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
                 im = (T)0.5 * (ko - to) * kp[i].a;
+            } else if constexpr (KT == KOP_HESS3) {
+                // E, s_x E, k_x^2 E with E = norm delta / k^2 (s_x = k_x, 0 on the Nyquist index)
+                re = (o == 0 ? (T)1 : (o == 1 ? (T)0.5 * (kx - tx) : kx * kx)) * kp[i].a;
             } else {
                 re = norm;
             }
             u[i] = cmake<C>(re * v[i].x - im * v[i].y, re * v[i].y + im * v[i].x);
         }
+    }
+
+    // KOP_HESS3: the line's point at the x Nyquist index (held by thread 0 as its point 4, since
+    // N / 2 = 4 N / 8) feeds the y pass's Nyquist terms: q01[iz] = k_x k_y E on the y Nyquist index,
+    // l02[iy] = k_x k_z E on the z Nyquist index (op.side = q01, then l02 after nh values).
+    __device__ __forceinline__ void nyquist_lines(const KOp& op, const Dims& dims, int t, int iy, int iz,
+                                                  const C (&v)[8]) const {
+        if (t != 0 || op.side == nullptr) return;
+        const int n1 = dims.n[1], n2 = dims.n[2], nh = n2 / 2 + 1;
+        if (iz >= nh) return;
+        const T kx = kval<T>(N / 2, N, (T)op.fscale[0]);
+        const C e = cmake<C>(kp[4].a * v[4].x, kp[4].a * v[4].y);
+        C* side = (C*)op.side;
+        if (n1 % 2 == 0 && iy == n1 / 2) side[iz] = cmake<C>(kx * ky * e.x, kx * ky * e.y);
+        if (n2 % 2 == 0 && iz == n2 / 2) side[nh + iy] = cmake<C>(kx * kz * e.x, kx * kz * e.y);
     }
 };
 

@@ -222,6 +222,8 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 :
                     for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
                     KLine<T, N, KT> kl;
                     kl.setup(op, dims, t, iy, iz);
+                    if constexpr (KT == KOP_HESS3)
+                        if (o == 0) kl.nyquist_lines(op, dims, t, iy, iz, v);
                     kl.apply(op, dims, t, o, v, u);
                 }
                 fft_regs<C, N, +1>(u, t, xbuf, addr, tw);
@@ -242,6 +244,7 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 :
             refill();
             KLine<T, N, KT> kl;
             kl.setup(op, dims, t, iy, iz);
+            if constexpr (KT == KOP_HESS3) kl.nyquist_lines(op, dims, t, iy, iz, v);
             for (int o = 0; o < op.nper; o++) {
                 C u[8];
                 kl.apply(op, dims, t, o, v, u);
@@ -371,19 +374,34 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
     z_c2r_body<T, M, ROWS, ET>(src, nin, dims, e, tw, wk, buf);
 }
 
-// Inverse y pass of the six Hessian spectra D_ij = k_i k_j delta(k) / k^2 of the local-line-of-sight
-// iteration, combined on the fly.  After the inverse x (done) and y transforms, x0 (fixed per tile)
-// and x1 (per point) are known, so the weighted sum over (i, j) of f_ij x_i x_j d_ij, which the
-// real-space update needs, is a quadratic in x2 with coefficients
+// Inverse y pass of the local-line-of-sight iteration.  The update needs the six Hessian fields
+// d_ij = IFFT(k_i k_j E), E = delta(k) / k^2, weighted by f_ij x_i x_j.  Along an x line k_y and k_z are
+// constant, so the x pass only transforms three spectra
+//   F0 = IFFT_x(E),  F1 = IFFT_x(s_x E),  F2 = IFFT_x(k_x^2 E)
+// (s_a = k_a, or 0 on the Nyquist plane of axis a, which is what the symmetrised multiplier of an odd
+// factor reduces to), and the six follow in y-k space as D00 = F2, D01 = s_y F1, D02 = s_z F1,
+// D11 = k_y^2 F0, D12 = s_y s_z F0, D22 = k_z^2 F0 (k_z constant along y).  After the inverse y
+// transforms, x0 (fixed per tile) and x1 (per point) are known, so the weighted sum is a quadratic in
+// x2 with coefficients
 //   A = f00 x0^2 D00 + f01 x0 x1 D01 + f11 x1^2 D11,   B = f02 x0 D02 + f12 x1 D12,   C = f22 D22
-// that are formed here, before the inverse z transform (which they commute with, being constant along
-// z).  The three are written in place of D00, D01, D02, so the z pass reads 3 spectra instead of 6
-// and runs 3 row transforms instead of 6.  Inputs stream through S stages in the order
-// D00, D01, D11 | D02, D12 | D22, one accumulator per output.
+// formed here, before the inverse z transform (which they commute with, being constant along z); the
+// z pass then reads 3 spectra and runs 3 row transforms.  Where two axes are both at their Nyquist
+// index the symmetrised k_a k_b is not s_a s_b but k_a k_b: D01 gains q01[iz] (-1)^(x + y) (the
+// single mode at the x and y Nyquist indices, transformed), D02 on the z-Nyquist column is
+// IFFT_y((-1)^x l02) and D12 on it is k_z IFFT_y(k_y [y Nyquist] F0).  Six units per tile stream through S stages:
+// (F2, 1) (F1, s_y) (F0, k_y^2) -> A | (F1, 1) (F0, s_y) -> B | (F0, 1) -> C; a tile's second and third
+// reads of F0 / F1 come from L2.
 struct HessGeom {
     double x0_off, x0_cell;   // x0 = x0_off + x0_cell * ix (mesh-dtype offset, float64 cell as the epilogue)
     double x1_off, x1_cell;   // x1 = x1_off + x1_cell * iy
     double f[6];              // f_ij in the order (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+    double fscale_y, fscale_z; // numpy fftfreq spacing of the y and z wavenumbers
+    int ny, nz;
+    // Nyquist lines written by the x pass (null where an axis is odd): q01[iz] = k_x k_y E at
+    // (x, y Nyquist), l02[iy] = k_x k_z E at (x, z Nyquist).  The symmetrised multiplier of k_a k_b is
+    // k_a k_b where a and b are both Nyquist or both not, so D01 and D02 need these beyond s_a s_b.
+    const void* q01;
+    const void* l02;
 };
 
 template <typename T, int N, int B, int S>
@@ -396,6 +414,8 @@ __global__ void __launch_bounds__(N / 8 * B) y_hessian_tma(const __grid_constant
     C* stages = (C*)smem_raw;
     C* tw = stages + S * TS::ELEMS;
     uint64_t* bars = (uint64_t*)(tw + N);
+    T* x1tab = (T*)(bars + S);     // x1 and k_y of every y index (2 N values after the barriers)
+    T* kytab = x1tab + N;
     const int tid = threadIdx.x, col = tid % B, t = tid / B;
     const ColAddr addr{B, col};
     if (tid == 0) {
@@ -403,6 +423,10 @@ __global__ void __launch_bounds__(N / 8 * B) y_hessian_tma(const __grid_constant
         prc::tma::fence_barrier_init();
     }
     fill_pass_twiddles<C, N>(tw);
+    for (int i = tid; i < N; i += blockDim.x) {
+        x1tab[i] = (T)(h.x1_off + h.x1_cell * i);
+        kytab[i] = kval<T>(i, h.ny, (T)h.fscale_y);
+    }
     const int ctiles = (s.ncols + B - 1) / B;
     const int64_t ntiles = (int64_t)s.outer * ctiles;
     __syncthreads();
@@ -410,26 +434,31 @@ __global__ void __launch_bounds__(N / 8 * B) y_hessian_tma(const __grid_constant
         if (tid == 0) atomicOr(&prc::g_fault, prc::tma::FAULT_SMEM_ALIGN);
         return;
     }
-    // unit u: tile blockIdx.x + (u / 6) gridDim.x, spectrum ORDER[u % 6]
-    auto spectrum_of = [](int k) { return k < 2 ? k : (k == 2 ? 3 : (k == 3 ? 2 : k)); };
+    // unit u: tile blockIdx.x + (u / 6) gridDim.x, input spectrum F[2, 1, 0, 1, 0, 0][u % 6]
+    auto input_of = [](int q) { return q == 0 ? 2 : (q == 1 || q == 3 ? 1 : 0); };
     auto issue = [&](int64_t u) {
         const int64_t tile = blockIdx.x + (u / 6) * gridDim.x;
         if (tile >= ntiles) return;
         const TileAt a = tile_at(tile, ntiles, ctiles, B);
-        issue_tile<T, N, B>(stages + (u % S) * TS::ELEMS, &maps.m[spectrum_of((int)(u % 6))], &bars[u % S], 1, a.o,
+        issue_tile<T, N, B>(stages + (u % S) * TS::ELEMS, &maps.m[input_of((int)(u % 6))], &bars[u % S], 1, a.o,
                             a.c0);
     };
     if (tid == 0)
         for (int u = 0; u < S; u++) issue(u);
+    const int ynyq = h.ny % 2 == 0 ? h.ny / 2 : -1;
+    const C* q01 = (const C*)h.q01;
+    const C* l02 = (const C*)h.l02;
     int64_t u = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const TileAt a = tile_at(tile, ntiles, ctiles, B);
         const T x0 = (T)(h.x0_off + h.x0_cell * a.o);
-        T x1[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) x1[i] = (T)(h.x1_off + h.x1_cell * (t + i * TL));
-        const bool store = a.c0 + col < s.ncols;
-        const int64_t off = (int64_t)a.o * s.os + a.c0 + col;
+        const int iz = a.c0 + col;
+        const T kz = kval<T>(iz, h.nz, (T)h.fscale_z);
+        const bool znyq = nyquist(iz, h.nz);
+        const T sz = znyq ? (T)0 : kz;
+        const bool store = iz < s.ncols;
+        const T xsign = (a.o & 1) ? (T)-1 : (T)1;     // (-1)^x
+        const int64_t off = (int64_t)a.o * s.os + iz;
 #pragma unroll 1
         for (int g = 0; g < 3; g++) {
             C acc[8];
@@ -437,7 +466,7 @@ __global__ void __launch_bounds__(N / 8 * B) y_hessian_tma(const __grid_constant
             for (int i = 0; i < 8; i++) acc[i] = cmake<C>(0, 0);
             const int nterm = g == 0 ? 3 : (g == 1 ? 2 : 1);
 #pragma unroll 1
-            for (int q = 0; q < nterm; q++, u++) {
+            for (int j = 0; j < nterm; j++, u++) {
                 const int st = (int)(u % S);
                 const bool ok = prc::tma::wait(&bars[st], (uint32_t)((u / S) & 1));
                 if (__syncthreads_or(!ok)) {
@@ -451,23 +480,53 @@ __global__ void __launch_bounds__(N / 8 * B) y_hessian_tma(const __grid_constant
                     }
                     return;
                 }
+                const int q = (int)(u % 6);
                 C* sb = stages + st * TS::ELEMS;
+                // D02 on the z-Nyquist column: the x-Nyquist mode of the line, (-1)^x l02
+                const bool sub02 = q == 3 && znyq && l02 != nullptr;
                 C v[8];
 #pragma unroll
-                for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
+                for (int i = 0; i < 8; i++) {
+                    if (sub02) {
+                        const C x = l02[t + i * TL];
+                        v[i] = cmake<C>(xsign * x.x, xsign * x.y);
+                    } else {
+                        const C x = sb[(t + i * TL) * B + col];
+                        T yf = (T)1;
+                        if (q == 1 || q == 2 || q == 4) {
+                            // k_y^2 (D11), s_y (D01, D12), k_y on the Nyquist index only (D12, z Nyquist)
+                            const int iy = t + i * TL;
+                            const T ky = kytab[iy];
+                            const bool yn = iy == ynyq;
+                            yf = q == 2 ? ky * ky : ((q == 4 && znyq) == yn ? ky : (T)0);
+                        }
+                        v[i] = cmake<C>(yf * x.x, yf * x.y);
+                    }
+                }
                 __syncthreads();
                 fft_regs<C, N, +1>(v, t, sb, addr, tw);
                 if (tid == 0) {
                     prc::tma::fence_proxy_async();
                     issue(u + S);
                 }
-                const int k = g == 0 ? (q == 0 ? 0 : (q == 1 ? 1 : 3)) : (g == 1 ? (q == 0 ? 2 : 4) : 5);
-                const T f = (T)(k == 0 ? h.f[0] : k == 1 ? h.f[1] : k == 2 ? h.f[2] : k == 3 ? h.f[3] : k == 4 ? h.f[4] : h.f[5]);
+                if (q == 1 && q01 != nullptr && iz < s.ncols) {
+                    // D01 at the x and y Nyquist indices: q01[iz] (-1)^(x + y)
+                    const C c = q01[iz];
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const T sg = ((t + i * TL) & 1) ? -xsign : xsign;
+                        v[i] = cmake<C>(v[i].x + sg * c.x, v[i].y + sg * c.y);
+                    }
+                }
+                // weight at this point: f00 x0^2 | f01 x0 x1 | f11 x1^2 | f02 x0 s_z (1 where substituted) |
+                // f12 x1 k_z | f22 k_z^2
+                const T f = (T)(q == 0 ? h.f[0] : q == 1 ? h.f[1] : q == 2 ? h.f[3] : q == 3 ? h.f[2] : q == 4 ? h.f[4] : h.f[5]);
+                const T z3 = sub02 ? (T)1 : sz;
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
-                    // weight of D_k at this point: f x0^2 | f x0 x1 | f x1^2 | f x0 | f x1 | f
-                    const T w = k == 0 ? f * (x0 * x0) : k == 1 ? f * (x0 * x1[i]) : k == 3 ? f * (x1[i] * x1[i])
-                              : k == 2 ? f * x0 : k == 4 ? f * x1[i] : f;
+                    const T x1 = x1tab[t + i * TL];
+                    const T w = q == 0 ? f * (x0 * x0) : q == 1 ? f * (x0 * x1) : q == 2 ? f * (x1 * x1)
+                              : q == 3 ? f * x0 * z3 : q == 4 ? f * x1 * kz : f * (kz * kz);
                     acc[i] = cmake<C>(acc[i].x + w * v[i].x, acc[i].y + w * v[i].y);
                 }
             }
