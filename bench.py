@@ -71,7 +71,7 @@ MULTI_WORKLOADS = {
     'batched_mocks': dict(kind='batched', nrequests=64, algorithms=['PlaneParallelFFTReconstruction',
                                                                     'MultiGridReconstruction'],
                           nmesh=[128, 192, 256], ndata=(300_000, 2_000_000), randoms_factor=0, boxsize=1000.,
-                          boxcenter=500., los='z', wrap=True, dtype='f4', slots=16),
+                          boxcenter=500., los='z', wrap=True, dtype='f4', slots=4),
     # BASELINE config: Poisson arrivals at 20 req/s, the three algorithms, nmesh in {128, 256, 384, 512},
     # 0.5M-8M data with 4x randoms, 150 GB admission budget (100 requests instead of 500: same mix, a
     # run that fits the bench's time)
@@ -79,7 +79,7 @@ MULTI_WORKLOADS = {
                                                                         'IterativeFFTReconstruction',
                                                                         'PlaneParallelFFTReconstruction'],
                     nmesh=[128, 256, 384, 512], ndata=(500_000, 8_000_000), randoms_factor=4, boxsize=2000.,
-                    boxcenter=2000., los=None, wrap=False, dtype='f4', slots=8, hbm_budget=150e9),
+                    boxcenter=2000., los=None, wrap=False, dtype='f4', slots=4, hbm_budget=150e9),
 }
 
 
@@ -448,7 +448,9 @@ def multi_requests(w, device, seed=0):
 def run_multi_arm(args, w):
     """Throughput and latency of a multi-request workload: the plain path (requests one after the other on one
     stream) and the request loop (continuous batching on `slots` streams; for 'serving', submitted at Poisson
-    arrival times).  Wall clock with the device synchronised on both sides."""
+    arrival times, where throughput is bounded by the arrival rate and the comparison is the latency against
+    the plain path serving the same arrivals first come, first served).  Both warmed up by one pass over the
+    requests.  Wall clock with the device synchronised on both sides."""
     import torch
     import numpy as np
     from pyrecon_b200 import _lib
@@ -457,11 +459,13 @@ def run_multi_arm(args, w):
     torch.cuda.set_device(local_rank)
     device = torch.device('cuda', local_rank)
     reqs = multi_requests(w, device, seed=rank)
-    for r in reqs[:4]:                       # warm-up: kernels, graphs, allocator
+    # warm-up of the plain path: every request once (kernels, multigrid graphs, allocator)
+    for r in reqs:
         run_request(r, device=device)
     torch.cuda.synchronize(device)
-    # plain path
+    # plain path (kernel times recorded: how busy the device is when requests run one at a time)
     lat_plain = []
+    _lib.profile_enable(True)
     t0 = time.perf_counter()
     for r in reqs:
         t = time.perf_counter()
@@ -469,12 +473,28 @@ def run_multi_arm(args, w):
         torch.cuda.synchronize(device)
         lat_plain.append(time.perf_counter() - t)
     plain_s = time.perf_counter() - t0
+    prof = _lib.profile_collect()
+    _lib.profile_enable(False)
+    plain_kernel_ms = sum(v[1] for v in prof.values())
+    top = sorted(prof.items(), key=lambda kv: -kv[1][1])[:6]
     # request loop
     rng = np.random.default_rng(9000 + rank)
     arrivals = np.cumsum(rng.exponential(1. / w['rate'], len(reqs))) if w['kind'] == 'serving' else np.zeros(len(reqs))
-    launches0 = _lib.launch_count()
+    # the plain path serving the same arrivals one request at a time (first come, first served): latency =
+    # waiting + its measured service time
+    fifo, free_at = [], 0.
+    for at, dt in zip(arrivals, lat_plain):
+        free_at = max(free_at, at) + dt
+        fifo.append(free_at - at)
+    launches0 = None
     with ClockSampler(local_rank) as clocks:
         server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=w.get('hbm_budget'))
+        # warm-up of the request loop: the whole request set once, all at once (each slot's scratch and
+        # multigrid graphs, the streams' allocator pools), as a long-running server would be
+        for f in [server.submit(r) for r in reqs]:
+            f.result()
+        server.reset_stats()
+        launches0 = _lib.launch_count()
         torch.cuda.synchronize(device)
         start = time.perf_counter()
         futures = []
@@ -493,7 +513,7 @@ def run_multi_arm(args, w):
     pct = lambda xs, q: 1e3 * sorted(xs)[min(len(xs) - 1, int(round(q / 100. * (len(xs) - 1))))]
     n = len(reqs)
     if rank == 0:
-        line = dict(metric=METRIC, value=n / served_s, unit='recons/s', n_gpus=world, steps=1, warmup=4,
+        line = dict(metric=METRIC, value=n / served_s, unit='recons/s', n_gpus=world, steps=1, warmup=1,
                     ms_per_step=served_s * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None,
                     dtype=w['dtype'], data='synthetic: seeded lognormal catalogues, one per nmesh, requests take prefixes',
                     config=dict(workload=args.workload, requests=n, slots=w['slots'],
@@ -501,7 +521,10 @@ def run_multi_arm(args, w):
                                 nmesh=w['nmesh'], algorithms=w['algorithms'], timing='wall clock, device synchronised'),
                     served=dict(recons_per_s=n / served_s, p50_ms=stats['p50_ms'], p99_ms=stats['p99_ms'],
                                 peak_in_flight=stats['peak_active']),
-                    plain=dict(recons_per_s=n / plain_s, p50_ms=pct(lat_plain, 50), p99_ms=pct(lat_plain, 99)),
+                    plain=dict(recons_per_s=n / plain_s, p50_ms=pct(lat_plain, 50), p99_ms=pct(lat_plain, 99),
+                               fifo_p50_ms=pct(fifo, 50), fifo_p99_ms=pct(fifo, 99),
+                               kernel_ms=plain_kernel_ms, wall_ms=plain_s * 1e3,
+                               top_kernels={k: round(v[1], 2) for k, v in top}),
                     served_vs_plain=(n / served_s) / (n / plain_s), gpu_launches=int(launches),
                     clocks=clocks.summary())
         print(json.dumps(line), flush=True)

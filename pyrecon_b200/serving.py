@@ -183,6 +183,14 @@ class ReconstructionServer(object):
                 self._free_streams.append(slot)
                 self._cv.notify_all()
 
+    def reset_stats(self):
+        """Forget the latencies and the throughput window so far (e.g. after a warm-up)."""
+        with self._cv:
+            self.latencies = []
+            self._first_submit = None
+            self._last_done = None
+            self.peak_active = self._active
+
     def stats(self):
         """Throughput (completed requests / s from the first submission to the last completion) and
         latency percentiles (submission to result, ms)."""
