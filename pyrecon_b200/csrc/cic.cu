@@ -32,6 +32,7 @@ constexpr int ITEMS = 16;                      // per thread
 constexpr int TILE = THREADS * ITEMS;          // 4096 items per tile
 constexpr int MAXBITS = 9;
 constexpr int MAXRADIX = 1 << MAXBITS;
+static_assert(2 * THREADS >= MAXRADIX, "downsweep scans two digits per thread");
 
 __global__ void __launch_bounds__(THREADS) upsweep(const uint32_t* __restrict__ keys, int64_t n, int shift,
                                                    int radix, int ntiles, uint32_t* __restrict__ hist) {
@@ -127,16 +128,21 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_add(uint32_t* __restrict__ 
 
 // Stable scatter of one tile: each warp ranks its contiguous 512-item slice chunk by chunk
 // (__match_any_sync groups equal digits; lanes keep input order), warps are then offset by the
-// counts of the warps before them, and the tile by the scanned histogram.
-__global__ void __launch_bounds__(THREADS) downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+// counts of the warps before them.  The tile is first reordered by digit in shared memory, so the
+// writes to the output run over consecutive addresses of each digit's range (coalesced) instead of
+// scattering single items; the tile's base in each digit's range comes from the scanned histogram.
+__global__ void __launch_bounds__(THREADS, 3) downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                      uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                      int64_t n, int shift, int radix, int ntiles,
                                                      const uint32_t* __restrict__ offsets) {
     extern __shared__ uint32_t smem[];
     uint32_t* s_key = smem;                       // TILE
     uint32_t* s_val = s_key + TILE;               // TILE
-    uint32_t* s_rank = s_val + TILE;              // TILE
+    uint32_t* s_rank = s_val + TILE;              // TILE: rank in the warp's digit group, then local index
     uint32_t* s_cnt = s_rank + TILE;              // WARPS * radix
+    uint32_t* s_loc = s_cnt + WARPS * radix;      // radix: first local index of each digit
+    uint32_t* s_glob = s_loc + radix;             // radix: the tile's first output index of each digit
+    __shared__ uint32_t s_warp[32];
     const uint32_t mask = (uint32_t)radix - 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
@@ -168,19 +174,54 @@ __global__ void __launch_bounds__(THREADS) downsweep(const uint32_t* __restrict_
             __syncwarp();
         }
         __syncthreads();
-        for (int d = threadIdx.x; d < radix; d += THREADS) {
-            uint32_t run = offsets[(int64_t)d * ntiles + tile];
-            for (int w = 0; w < WARPS; w++) {
-                uint32_t c = s_cnt[w * radix + d];
-                s_cnt[w * radix + d] = run;
-                run += c;
+        // per digit: offsets of the warps within the digit's group, and the group size
+        uint32_t tot[2] = {0u, 0u};
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int d = 2 * threadIdx.x + j;
+            if (d < radix) {
+                uint32_t run = 0u;
+                for (int w = 0; w < WARPS; w++) {
+                    uint32_t c = s_cnt[w * radix + d];
+                    s_cnt[w * radix + d] = run;
+                    run += c;
+                }
+                tot[j] = run;
+                s_glob[d] = offsets[(int64_t)d * ntiles + tile];
+            }
+        }
+        // local start of every digit: exclusive scan of the group sizes (2 digits per thread)
+        const uint32_t ex = block_exclusive_scan(tot[0] + tot[1], s_warp, nullptr);
+        if (2 * threadIdx.x < radix) s_loc[2 * threadIdx.x] = ex;
+        if (2 * threadIdx.x + 1 < radix) s_loc[2 * threadIdx.x + 1] = ex + tot[0];
+        __syncthreads();
+        // local index of every item (its own slot of s_rank), then the reorder through registers
+        uint32_t rk[ITEMS], rv[ITEMS], ri[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const int k = j * THREADS + threadIdx.x;
+            if (k < valid) {
+                const uint32_t key = s_key[k];
+                const uint32_t d = (key >> shift) & mask;
+                rk[j] = key;
+                rv[j] = s_val[k];
+                ri[j] = s_loc[d] + s_cnt[(k / SLICE) * radix + d] + s_rank[k];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const int k = j * THREADS + threadIdx.x;
+            if (k < valid) {
+                s_key[ri[j]] = rk[j];
+                s_val[ri[j]] = rv[j];
             }
         }
         __syncthreads();
         for (int k = threadIdx.x; k < valid; k += THREADS) {
-            uint32_t key = s_key[k];
-            uint32_t d = (key >> shift) & mask;
-            uint32_t pos = s_cnt[(k / SLICE) * radix + d] + s_rank[k];
+            const uint32_t key = s_key[k];
+            const uint32_t d = (key >> shift) & mask;
+            const uint32_t pos = s_glob[d] + ((uint32_t)k - s_loc[d]);
             kout[pos] = key;
             vout[pos] = s_val[k];
         }
@@ -188,7 +229,7 @@ __global__ void __launch_bounds__(THREADS) downsweep(const uint32_t* __restrict_
     }
 }
 
-inline size_t downsweep_smem(int radix) { return (size_t)(3 * TILE + WARPS * radix) * sizeof(uint32_t); }
+inline size_t downsweep_smem(int radix) { return (size_t)(3 * TILE + WARPS * radix + 2 * radix) * sizeof(uint32_t); }
 
 inline int num_tiles(int64_t n) { return (int)((n + TILE - 1) / TILE); }
 

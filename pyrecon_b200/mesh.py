@@ -169,6 +169,31 @@ def torch_dtype(dtype):
     return {4: torch.float32, 8: torch.float64}[np.dtype(dtype).itemsize]
 
 
+_copy_streams = {}
+
+
+def _upload(t, device):
+    """Device copy of `t`.  From pinned host memory the copy runs on a copy stream of the device, so it
+    overlaps the kernels already queued on the current stream (e.g. the paint of the previous
+    catalogue); the current stream waits for it before any later use."""
+    torch = _torch()
+    if t.is_cuda or not t.is_pinned():
+        return t.to(device, non_blocking=True).contiguous()
+    t = t.contiguous()
+    compute = torch.cuda.current_stream(device)
+    copy = _copy_streams.get(device)
+    if copy is None:
+        copy = _copy_streams[device] = torch.cuda.Stream(device)
+    with torch.cuda.stream(copy):
+        out = torch.empty(t.shape, dtype=t.dtype, device=device)     # from the copy stream's pool
+        out.copy_(t, non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(copy)
+    compute.wait_event(done)
+    out.record_stream(compute)          # not reused before the current stream's work on it is done
+    return out
+
+
 class Particles(object):
     """Positions (and optional weights) resident on the device, with how to return results."""
 
@@ -190,7 +215,7 @@ class Particles(object):
         if t.ndim != 2 or t.shape[1] != 3:
             raise MeshError('positions must be of shape (N, 3)')
         self.size = int(t.shape[0])
-        self.pos = t.to(device, non_blocking=True).contiguous()
+        self.pos = _upload(t, device)
         self.weights = None
         if weights is not None:
             w = weights if isinstance(weights, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(weights))
@@ -198,7 +223,7 @@ class Particles(object):
                 w = w.to(torch_dtype(weight_dtype or 'f8'))
             if w.shape[0] != self.size:
                 raise MeshError('weights must have the same length as positions')
-            self.weights = w.to(device, non_blocking=True).contiguous().reshape(-1)
+            self.weights = _upload(w.reshape(-1), device)
 
     @property
     def pos_bytes(self):
