@@ -71,7 +71,7 @@ MULTI_WORKLOADS = {
     'batched_mocks': dict(kind='batched', nrequests=64, algorithms=['PlaneParallelFFTReconstruction',
                                                                     'MultiGridReconstruction'],
                           nmesh=[128, 192, 256], ndata=(300_000, 2_000_000), randoms_factor=0, boxsize=1000.,
-                          boxcenter=500., los='z', wrap=True, dtype='f4', slots=4),
+                          boxcenter=500., los='z', wrap=True, dtype='f4', slots=2, max_batch=8),
     # BASELINE config: Poisson arrivals at 20 req/s, the three algorithms, nmesh in {128, 256, 384, 512},
     # 0.5M-8M data with 4x randoms, 150 GB admission budget (100 requests instead of 500: same mix, a
     # run that fits the bench's time)
@@ -79,7 +79,7 @@ MULTI_WORKLOADS = {
                                                                         'IterativeFFTReconstruction',
                                                                         'PlaneParallelFFTReconstruction'],
                     nmesh=[128, 256, 384, 512], ndata=(500_000, 8_000_000), randoms_factor=4, boxsize=2000.,
-                    boxcenter=2000., los=None, wrap=False, dtype='f4', slots=4, hbm_budget=150e9),
+                    boxcenter=2000., los=None, wrap=False, dtype='f4', slots=4, max_batch=8, hbm_budget=150e9),
 }
 
 
@@ -488,7 +488,8 @@ def run_multi_arm(args, w):
         fifo.append(free_at - at)
     launches0 = None
     with ClockSampler(local_rank) as clocks:
-        server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=w.get('hbm_budget'))
+        server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=w.get('hbm_budget'),
+                                      max_batch=w.get('max_batch', 1))
         # warm-up of the request loop: the whole request set once, all at once (each slot's scratch and
         # multigrid graphs, the streams' allocator pools), as a long-running server would be
         for f in [server.submit(r) for r in reqs]:
@@ -516,7 +517,7 @@ def run_multi_arm(args, w):
         line = dict(metric=METRIC, value=n / served_s, unit='recons/s', n_gpus=world, steps=1, warmup=1,
                     ms_per_step=served_s * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None,
                     dtype=w['dtype'], data='synthetic: seeded lognormal catalogues, one per nmesh, requests take prefixes',
-                    config=dict(workload=args.workload, requests=n, slots=w['slots'],
+                    config=dict(workload=args.workload, requests=n, slots=w['slots'], max_batch=w.get('max_batch', 1),
                                 arrivals='poisson {:g}/s'.format(w['rate']) if w['kind'] == 'serving' else 'all at once',
                                 nmesh=w['nmesh'], algorithms=w['algorithms'], timing='wall clock, device synchronised'),
                     served=dict(recons_per_s=n / served_s, p50_ms=stats['p50_ms'], p99_ms=stats['p99_ms'],

@@ -374,6 +374,24 @@ PRC_API prc_status_t prc_multigrid_f64(const double *delta, double *phi, const i
                                int vcycle_niterations, const double *los, void *workspace,
                                size_t workspace_bytes, void *stream);
 
+/* `count` solves of the same mesh and parameters at once (several OriginalMultiGridReconstruction.run,
+ * pyrecon/multigrid.py:99-135, of catalogues in the same box): every kernel of the schedule runs over
+ * all of them in one launch (count * nmesh[0] <= 65535).  delta and phi are host arrays of `count`
+ * device pointers; results equal `count` separate calls. */
+PRC_API size_t prc_multigrid_batch_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int mixed_precision,
+                                                   int count);
+PRC_API prc_status_t prc_multigrid_batch_f32(const float *const *delta, float *const *phi, int count,
+                                             const int32_t nmesh[3], const double boxsize[3],
+                                             const double boxcenter[3], double beta, double damping,
+                                             int jacobi_niterations, int vcycle_niterations, const double *los,
+                                             int mixed_precision, void *workspace, size_t workspace_bytes,
+                                             void *stream);
+PRC_API prc_status_t prc_multigrid_batch_f64(const double *const *delta, double *const *phi, int count,
+                                             const int32_t nmesh[3], const double boxsize[3],
+                                             const double boxcenter[3], double beta, double damping,
+                                             int jacobi_niterations, int vcycle_niterations, const double *los,
+                                             void *workspace, size_t workspace_bytes, void *stream);
+
 /* Components, one level (jacobi: src/multigrid.c:44-104, residual :107-164, prolong :167-209,
  * reduce :212-266).  jacobi runs `niterations` sweeps in place on v using `scratch` (one mesh). */
 PRC_API prc_status_t prc_mg_jacobi_f32(float *v, const float *f, float *scratch, const int32_t nmesh[3],

@@ -83,6 +83,16 @@ for _s in ['f32', 'f64']:
     })
 _SIGNATURES['prc_multigrid_f32'] = (c_int, [_p, _p, I3, D3, D3, c_double, c_double, c_int, c_int, DP, c_int, _p, c_size, _p])
 _SIGNATURES['prc_multigrid_f64'] = (c_int, [_p, _p, I3, D3, D3, c_double, c_double, c_int, c_int, DP, _p, c_size, _p])
+_SIGNATURES['prc_multigrid_batch_workspace_bytes'] = (c_size, [I3, c_int, c_int, c_int])
+_SIGNATURES['prc_multigrid_batch_f32'] = (c_int, [_p, _p, c_int, I3, D3, D3, c_double, c_double, c_int, c_int, DP, c_int,
+                                                  _p, c_size, _p])
+_SIGNATURES['prc_multigrid_batch_f64'] = (c_int, [_p, _p, c_int, I3, D3, D3, c_double, c_double, c_int, c_int, DP, _p,
+                                                  c_size, _p])
+
+
+def pointer_array(tensors):
+    """Host array of the device pointers of `tensors` (a `const T* const*` argument)."""
+    return (c_void_p * len(tensors))(*[t.data_ptr() for t in tensors])
 
 
 class LibraryError(RuntimeError):

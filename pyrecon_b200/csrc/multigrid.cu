@@ -102,12 +102,18 @@ __device__ __forceinline__ A neighbour_sum(const V* __restrict__ v, const int n[
 }
 
 // Kernels run one thread per cell of a 3D launch: (z, y) over the block's (x, y) threads, x over
-// blockIdx.z, so no index division is needed.
+// blockIdx.z.  A batch of `count` problems of the same shape, stored one after the other, is one
+// launch with count n0 planes along blockIdx.z: problem blockIdx.z / n0, plane blockIdx.z % n0.
 __device__ __forceinline__ bool cell3(const int n[3], int& x, int& y, int& z) {
     z = blockIdx.x * blockDim.x + threadIdx.x;
     y = blockIdx.y * blockDim.y + threadIdx.y;
-    x = blockIdx.z;
+    x = blockIdx.z % n[0];
     return z < n[2] && y < n[1];
+}
+
+// Offset of this block's problem in a batch of meshes of shape n.
+__device__ __forceinline__ int64_t batch_offset(const int n[3]) {
+    return (int64_t)(blockIdx.z / n[0]) * ((int64_t)n[0] * n[1] * n[2]);
 }
 
 // One damped-Jacobi sweep: vout = (1 - w) v + w (f + S(v)) / (2 sum G).  zero_v: v is
@@ -117,6 +123,8 @@ __global__ void __launch_bounds__(256) jacobi_sweep(const T* __restrict__ v, con
                                                     T* __restrict__ vout, Stencil<T> s, T w, int zero_v) {
     int x, y, z;
     if (!cell3(s.n, x, y, z)) return;
+    const int64_t bo = batch_offset(s.n);
+    v += bo, f += bo, vout += bo;
     const int64_t i = ((int64_t)x * s.n[1] + y) * s.n[2] + z;
     T p[3], g, G[3];
     coeffs<T>(s, x, y, z, p, g, G);
@@ -159,7 +167,7 @@ struct Quad {
 __device__ __forceinline__ bool quad_of(const int n[3], Quad& q) {
     q.z0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
     q.y = blockIdx.y * blockDim.y + threadIdx.y;
-    q.x = blockIdx.z;
+    q.x = blockIdx.z % n[0];
     q.c = ((int64_t)q.x * n[1] + q.y) * n[2];
     return q.z0 < n[2] && q.y < n[1];
 }
@@ -236,6 +244,8 @@ __global__ void __launch_bounds__(256) jacobi_sweep4(const T* __restrict__ v, co
                                                      T* __restrict__ vout, Stencil<T> s, T w, int zero_v) {
     Quad q;
     if (!quad_of(s.n, q)) return;
+    const int64_t bo = batch_offset(s.n);
+    v += bo, f += bo, vout += bo;
     T fv[4], vc[4], U[4], W[4], qq[4], P[4];
     load4(f + q.c + q.z0, fv);
     if (zero_v) {
@@ -273,6 +283,8 @@ __global__ void __launch_bounds__(256) residual_kernel4(const V* __restrict__ v,
                                                         R* __restrict__ r, Stencil<S> s) {
     Quad q;
     if (!quad_of(s.n, q)) return;
+    const int64_t bo = batch_offset(s.n);
+    v += bo, f += bo, r += bo;
     A U[4], W[4], qq[4], P[4];
     quad_terms<A, V, S, LOCAL>(v, s, q, U, W, qq, P);
     V vc[4];
@@ -294,6 +306,8 @@ __global__ void __launch_bounds__(256) residual_kernel(const V* __restrict__ v, 
                                                        R* __restrict__ r, Stencil<S> s) {
     int x, y, z;
     if (!cell3(s.n, x, y, z)) return;
+    const int64_t bo = batch_offset(s.n);
+    v += bo, f += bo, r += bo;
     const int64_t i = ((int64_t)x * s.n[1] + y) * s.n[2] + z;
     A p[3], g, G[3];
     coeffs<A>(s, x, y, z, p, g, G);
@@ -309,6 +323,8 @@ __global__ void __launch_bounds__(256) reduce_kernel(const TI* __restrict__ fine
     {
         int x, y, z;
         if (!cell3(nc, x, y, z)) return;
+        const int64_t bc = batch_offset(nc);
+        fine += 8 * bc, coarse += bc;
         const int64_t i = ((int64_t)x * nc[1] + y) * nc[2] + z;
         const int X[3] = {wrap_dn(2 * x, nf.n[0]), 2 * x, wrap_up(2 * x, nf.n[0])};
         const int Y[3] = {wrap_dn(2 * y, nf.n[1]), 2 * y, wrap_up(2 * y, nf.n[1])};
@@ -338,6 +354,8 @@ __global__ void __launch_bounds__(256) prolong_kernel(const TI* __restrict__ coa
     {
         int x, y, z;
         if (!cell3(nc.n, x, y, z)) return;
+        const int64_t bc = batch_offset(nc.n);
+        coarse += bc, fine += 8 * bc;
         const int xs[2] = {x, wrap_up(x, nc.n[0])}, ys[2] = {y, wrap_up(y, nc.n[1])}, zs[2] = {z, wrap_up(z, nc.n[2])};
         A c[2][2][2];
 #pragma unroll
@@ -386,24 +404,25 @@ static int grid_for(int64_t n) {
 struct Grid3 {
     dim3 grid, block;
 };
-static Grid3 grid3(const int n[3]) {
+// `count` problems of that shape: count n0 blocks along z (see cell3).
+static Grid3 grid3(const int n[3], int count = 1) {
     int bx = 1, by = 1;
     while (bx < n[2] && bx < 32) bx <<= 1;
     while (by < n[1] && bx * by < 256) by <<= 1;
     Grid3 g;
     g.block = dim3(bx, by, 1);
-    g.grid = dim3((n[2] + bx - 1) / bx, (n[1] + by - 1) / by, n[0]);
+    g.grid = dim3((n[2] + bx - 1) / bx, (n[1] + by - 1) / by, n[0] * count);
     return g;
 }
-static Grid3 grid3_coarse(const int nf[3]) {
+static Grid3 grid3_coarse(const int nf[3], int count = 1) {
     const int nc[3] = {nf[0] / 2, nf[1] / 2, nf[2] / 2};
-    return grid3(nc);
+    return grid3(nc, count);
 }
 // Launch of the four-cells-per-thread kernels, usable when n2 % 4 == 0 and the meshes are
 // 16-byte aligned.
-static Grid3 grid3_quad(const int n[3]) {
+static Grid3 grid3_quad(const int n[3], int count = 1) {
     const int nq[3] = {n[0], n[1], n[2] / 4};
-    return grid3(nq);
+    return grid3(nq, count);
 }
 static bool quad_ok(const int n[3], const void* a, const void* b, const void* c) {
     return n[2] % 4 == 0 && (((uintptr_t)a | (uintptr_t)b | (uintptr_t)c) & 15) == 0;
@@ -452,9 +471,10 @@ struct Params {
 
 template <typename T> struct MGRunner {
     std::vector<Level> L;
-    std::vector<LevelBufs<T>> B;
+    std::vector<LevelBufs<T>> B;     // per level: count problems one after the other in each buffer
     Params P;
     cudaStream_t st;
+    int count = 1;
 
     Stencil<T> stencil(int l) const {
         return make_stencil<T>(L[l].n, P.boxsize, P.boxcenter, P.beta, P.has_los ? P.los : nullptr);
@@ -464,11 +484,11 @@ template <typename T> struct MGRunner {
     // other buffer (the pointers are swapped instead of copying back).  zero_first: v known zero.
     int jacobi(int l, T*& v, const T* f, T*& tmp, int niter, bool zero_first) {
         Stencil<T> s = stencil(l);
-        const int64_t N = L[l].size();
-        const Grid3 g = grid3(L[l].n);
+        const int64_t N = L[l].size() * count;
+        const Grid3 g = grid3(L[l].n, count);
         if (niter == 0 && zero_first && cudaMemsetAsync(v, 0, N * sizeof(T), st) != cudaSuccess) return PRC_ERR_CUDA;
         const bool quad = quad_ok(L[l].n, v, f, tmp);
-        const Grid3 gq = grid3_quad(L[l].n);
+        const Grid3 gq = grid3_quad(L[l].n, count);
         for (int it = 0; it < niter; it++) {
             const bool z0 = zero_first && it == 0;
             if (quad)
@@ -489,10 +509,10 @@ template <typename T> struct MGRunner {
         PRC_TRY(jacobi(l, v, f, B[l].tmp, P.jn, v_zero));
         if (l + 1 < (int)L.size()) {
             Stencil<T> s = stencil(l);
-            const int64_t N = L[l].size();
-            const Grid3 g = grid3(L[l].n), gc = grid3_coarse(L[l].n);
+            const int64_t N = L[l].size() * count;
+            const Grid3 g = grid3(L[l].n, count), gc = grid3_coarse(L[l].n, count);
             if (quad_ok(L[l].n, v, f, B[l].r)) {
-                const Grid3 gq = grid3_quad(L[l].n);
+                const Grid3 gq = grid3_quad(L[l].n, count);
                 PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T),
                              (s.local ? residual_kernel4<T, T, T, T, T, true> : residual_kernel4<T, T, T, T, T, false>)
                                  <<<gq.grid, gq.block, 0, st>>>(v, f, B[l].r, s));
@@ -501,12 +521,12 @@ template <typename T> struct MGRunner {
                              residual_kernel<T, T, T, T, T><<<g.grid, g.block, 0, st>>>(v, f, B[l].r, s));
             }
             Dims nf = {{L[l].n[0], L[l].n[1], L[l].n[2]}};
-            PRC_LAUNCH_B("mg_reduce", st, (double)(N + L[l + 1].size()) * sizeof(T),
+            PRC_LAUNCH_B("mg_reduce", st, (double)(N + L[l + 1].size() * count) * sizeof(T),
                          reduce_kernel<T, T, T><<<gc.grid, gc.block, 0, st>>>(B[l].r, B[l + 1].f, nf));
             PRC_CHECK_LAUNCH();
             PRC_TRY(vcycle(l + 1, B[l + 1].v, B[l + 1].f, true));
             Dims nc = {{L[l + 1].n[0], L[l + 1].n[1], L[l + 1].n[2]}};
-            PRC_LAUNCH_B("mg_prolong_add", st, (double)(2 * N + L[l + 1].size()) * sizeof(T),
+            PRC_LAUNCH_B("mg_prolong_add", st, (double)(2 * N + L[l + 1].size() * count) * sizeof(T),
                          prolong_kernel<T, T, T, true><<<gc.grid, gc.block, 0, st>>>(B[l + 1].v, v, nc));
             PRC_CHECK_LAUNCH();
         }
@@ -520,10 +540,11 @@ template <typename T> static int fmg_plain(MGRunner<T>& R, const T* f0, T* v0) {
     cudaStream_t st = R.st;
     // right-hand sides at every level
     R.B[0].f = const_cast<T*>(f0);
+    const int cnt = R.count;
     for (int l = 0; l + 1 < nl; l++) {
         Dims nf = {{R.L[l].n[0], R.L[l].n[1], R.L[l].n[2]}};
-        const Grid3 gc = grid3_coarse(R.L[l].n);
-        PRC_LAUNCH_B("mg_reduce", st, (double)(R.L[l].size() + R.L[l + 1].size()) * sizeof(T),
+        const Grid3 gc = grid3_coarse(R.L[l].n, cnt);
+        PRC_LAUNCH_B("mg_reduce", st, (double)(R.L[l].size() + R.L[l + 1].size()) * cnt * sizeof(T),
                      reduce_kernel<T, T, T><<<gc.grid, gc.block, 0, st>>>(R.B[l].f, R.B[l + 1].f, nf));
     }
     PRC_CHECK_LAUNCH();
@@ -533,18 +554,18 @@ template <typename T> static int fmg_plain(MGRunner<T>& R, const T* f0, T* v0) {
     for (int l = nl - 1; l >= 0; l--) {
         T*& v = l == 0 ? v0cur : R.B[l].v;
         if (l == nl - 1) {
-            if (cudaMemsetAsync(v, 0, R.L[l].size() * sizeof(T), st) != cudaSuccess) return PRC_ERR_CUDA;
+            if (cudaMemsetAsync(v, 0, R.L[l].size() * cnt * sizeof(T), st) != cudaSuccess) return PRC_ERR_CUDA;
         } else {
             Dims nc = {{R.L[l + 1].n[0], R.L[l + 1].n[1], R.L[l + 1].n[2]}};
-            const Grid3 gc = grid3(R.L[l + 1].n);
-            PRC_LAUNCH_B("mg_prolong", st, (double)(R.L[l].size() + R.L[l + 1].size()) * sizeof(T),
+            const Grid3 gc = grid3(R.L[l + 1].n, cnt);
+            PRC_LAUNCH_B("mg_prolong", st, (double)(R.L[l].size() + R.L[l + 1].size()) * cnt * sizeof(T),
                          prolong_kernel<T, T, T, false><<<gc.grid, gc.block, 0, st>>>(R.B[l + 1].v, v, nc));
             PRC_CHECK_LAUNCH();
         }
         for (int it = 0; it < R.P.vn; it++) PRC_TRY(R.vcycle(l, v, R.B[l].f, l == nl - 1 && it == 0));
     }
     if (v0cur != v0 &&
-        cudaMemcpyAsync(v0, v0cur, R.L[0].size() * sizeof(T), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        cudaMemcpyAsync(v0, v0cur, R.L[0].size() * cnt * sizeof(T), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return PRC_ERR_CUDA;
     return PRC_OK;
 }
@@ -558,7 +579,7 @@ namespace {
 // Workspace layout for plain FMG in precision T: per level v, f, r, tmp (level 0's f and v receive the
 // caller's right-hand side and return the solution, so the solve itself touches the workspace only).
 template <typename T> size_t plain_layout(const int32_t nmesh[3], char* base, std::vector<LevelBufs<T>>* out,
-                                          std::vector<Level>* lv) {
+                                          std::vector<Level>* lv, int count = 1) {
     std::vector<Level> L = hierarchy(nmesh);
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -568,7 +589,7 @@ template <typename T> size_t plain_layout(const int32_t nmesh[3], char* base, st
     };
     std::vector<LevelBufs<T>> B(L.size());
     for (size_t l = 0; l < L.size(); l++) {
-        size_t b = (size_t)L[l].size() * sizeof(T);
+        size_t b = (size_t)L[l].size() * count * sizeof(T);
         B[l].v = (T*)take(b);
         B[l].f = (T*)take(b);
         B[l].r = (T*)take(b);
@@ -586,7 +607,7 @@ struct MixedBufs {
     std::vector<Level> L;
 };
 
-size_t mixed_layout(const int32_t nmesh[3], char* base, MixedBufs* mb) {
+size_t mixed_layout(const int32_t nmesh[3], char* base, MixedBufs* mb, int count = 1) {
     std::vector<Level> L = hierarchy(nmesh);
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -600,7 +621,7 @@ size_t mixed_layout(const int32_t nmesh[3], char* base, MixedBufs* mb) {
     m.v64.resize(L.size());
     m.b32.resize(L.size());
     for (size_t l = 0; l < L.size(); l++) {
-        size_t n = (size_t)L[l].size();
+        size_t n = (size_t)L[l].size() * count;
         m.f64[l] = (double*)take(n * 8);
         m.v64[l] = (double*)take(n * 8);
         m.b32[l].v = (float*)take(n * 4);
@@ -637,11 +658,13 @@ bool mg_args_ok(const void* delta, const void* phi, const int32_t nmesh[3], cons
 }
 
 // Plain solve of the right-hand side held in the workspace's level-0 f into its level-0 v.
-template <typename T> int solve_plain(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t st) {
+template <typename T> int solve_plain(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t st,
+                                      int count = 1) {
     MGRunner<T> R;
-    plain_layout<T>(nmesh, (char*)ws, &R.B, &R.L);
+    plain_layout<T>(nmesh, (char*)ws, &R.B, &R.L, count);
     R.P = P;
     R.st = st;
+    R.count = count;
     T* f0 = R.B[0].f;
     T* v0 = R.B[0].v;
     return fmg_plain<T>(R, f0, v0);
@@ -649,31 +672,32 @@ template <typename T> int solve_plain(const int32_t nmesh[3], const Params& P, v
 
 // Mixed precision FMG: every V-cycle is v64 += V32(0, f64 - A v64); the FP64 right-hand side is in the
 // workspace's level-0 f64 and the solution is left in its level-0 v64.
-int solve_mixed(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t st) {
+int solve_mixed(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t st, int count = 1) {
     MixedBufs m;
-    mixed_layout(nmesh, (char*)ws, &m);
+    mixed_layout(nmesh, (char*)ws, &m, count);
     const int nl = (int)m.L.size();
     MGRunner<float> R;
     R.L = m.L;
     R.B = m.b32;
     R.P = P;
     R.st = st;
+    R.count = count;
     for (int l = 0; l + 1 < nl; l++) {
         Dims nf = {{m.L[l].n[0], m.L[l].n[1], m.L[l].n[2]}};
-        const Grid3 gc = grid3_coarse(m.L[l].n);
-        PRC_LAUNCH_B("mg_reduce", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()),
+        const Grid3 gc = grid3_coarse(m.L[l].n, count);
+        PRC_LAUNCH_B("mg_reduce", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()) * count,
                      reduce_kernel<double, double, double><<<gc.grid, gc.block, 0, st>>>(m.f64[l], m.f64[l + 1], nf));
     }
     PRC_CHECK_LAUNCH();
     for (int l = nl - 1; l >= 0; l--) {
-        const int64_t N = m.L[l].size();
-        const Grid3 g = grid3(m.L[l].n);
+        const int64_t N = m.L[l].size() * count;
+        const Grid3 g = grid3(m.L[l].n, count);
         if (l == nl - 1) {
             if (cudaMemsetAsync(m.v64[l], 0, N * 8, st) != cudaSuccess) return PRC_ERR_CUDA;
         } else {
             Dims nc = {{m.L[l + 1].n[0], m.L[l + 1].n[1], m.L[l + 1].n[2]}};
-            const Grid3 gc = grid3(m.L[l + 1].n);
-            PRC_LAUNCH_B("mg_prolong", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()),
+            const Grid3 gc = grid3(m.L[l + 1].n, count);
+            PRC_LAUNCH_B("mg_prolong", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()) * count,
                          prolong_kernel<double, double, double, false><<<gc.grid, gc.block, 0, st>>>(m.v64[l + 1],
                                                                                                   m.v64[l], nc));
         }
@@ -682,7 +706,7 @@ int solve_mixed(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t 
         for (int it = 0; it < P.vn; it++) {
             // defect in FP64 (stored FP32 as the inner V-cycle's right-hand side)
             if (quad_ok(m.L[l].n, m.v64[l], m.f64[l], R.B[l].f)) {
-                const Grid3 gq = grid3_quad(m.L[l].n);
+                const Grid3 gq = grid3_quad(m.L[l].n, count);
                 PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N,
                              (s64.local ? residual_kernel4<double, double, double, float, double, true>
                                         : residual_kernel4<double, double, double, float, double, false>)
@@ -737,10 +761,12 @@ bool graphs_enabled() {
 
 template <typename V> void key_add(std::string& k, const V& v) { k.append((const char*)&v, sizeof(V)); }
 
-std::string solve_key(int tsize, int mixed, const int32_t nmesh[3], const Params& P, const void* ws, size_t wsb) {
+std::string solve_key(int tsize, int mixed, const int32_t nmesh[3], const Params& P, const void* ws, size_t wsb,
+                      int count) {
     std::string k;
     key_add(k, tsize);
     key_add(k, mixed);
+    key_add(k, count);
     for (int d = 0; d < 3; d++) {
         key_add(k, nmesh[d]);
         key_add(k, P.boxsize[d]);
@@ -824,65 +850,107 @@ template <typename F> int run_graph(const std::string& key, cudaStream_t st, F b
     return PRC_OK;
 }
 
-// Plain solve through the workspace: the caller's right-hand side is copied into level 0's f, the
-// (graph-captured) solve runs on the workspace alone, and level 0's v is copied out.
+// Solve through the workspace: each problem's right-hand side is copied into its slot of level 0's f
+// (FP64 f for the mixed precision solve), the (graph-captured) solve runs on the workspace alone,
+// and each slot of level 0's v is copied out.
 template <typename T>
-int run_plain_io(const T* delta, T* phi, const int32_t nmesh[3], const Params& P, void* ws, const std::string& key,
-                 cudaStream_t st) {
+int run_plain_io(const T* const* delta, T* const* phi, int count, const int32_t nmesh[3], const Params& P, void* ws,
+                 const std::string& key, cudaStream_t st) {
     std::vector<LevelBufs<T>> B;
-    plain_layout<T>(nmesh, (char*)ws, &B, nullptr);
-    const size_t bytes = (size_t)nmesh[0] * nmesh[1] * nmesh[2] * sizeof(T);
-    if (cudaMemcpyAsync(B[0].f, delta, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return PRC_ERR_CUDA;
-    PRC_TRY(run_graph(key, st, [&](cudaStream_t s) { return solve_plain<T>(nmesh, P, ws, s); }));
-    if (cudaMemcpyAsync(phi, B[0].v, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return PRC_ERR_CUDA;
+    plain_layout<T>(nmesh, (char*)ws, &B, nullptr, count);
+    const int64_t N = (int64_t)nmesh[0] * nmesh[1] * nmesh[2];
+    for (int b = 0; b < count; b++)
+        if (cudaMemcpyAsync(B[0].f + b * N, delta[b], N * sizeof(T), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return PRC_ERR_CUDA;
+    PRC_TRY(run_graph(key, st, [&](cudaStream_t s) { return solve_plain<T>(nmesh, P, ws, s, count); }));
+    for (int b = 0; b < count; b++)
+        if (cudaMemcpyAsync(phi[b], B[0].v + b * N, N * sizeof(T), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return PRC_ERR_CUDA;
     return PRC_OK;
 }
+
+int run_mixed_io(const float* const* delta, float* const* phi, int count, const int32_t nmesh[3], const Params& P,
+                 void* ws, const std::string& key, cudaStream_t st) {
+    MixedBufs m;
+    mixed_layout(nmesh, (char*)ws, &m, count);
+    const int64_t N = (int64_t)nmesh[0] * nmesh[1] * nmesh[2];
+    for (int b = 0; b < count; b++)
+        PRC_LAUNCH_B("mg_convert", st, 12.0 * N,
+                     convert_kernel<float, double><<<grid_for(N), 256, 0, st>>>(delta[b], m.f64[0] + b * N, N));
+    PRC_CHECK_LAUNCH();
+    PRC_TRY(run_graph(key, st, [&](cudaStream_t s) { return solve_mixed(nmesh, P, ws, s, count); }));
+    for (int b = 0; b < count; b++)
+        PRC_LAUNCH_B("mg_convert", st, 12.0 * N,
+                     convert_kernel<double, float><<<grid_for(N), 256, 0, st>>>(m.v64[0] + b * N, phi[b], N));
+    PRC_CHECK_LAUNCH();
+    return PRC_OK;
+}
+
+// The batch shares one launch per step along z: count n0 planes (see cell3).
+bool batch_ok(const int32_t nmesh[3], int count) { return count >= 1 && (int64_t)nmesh[0] * count <= 65535; }
 
 }  // namespace
 
 extern "C" {
 
-size_t prc_multigrid_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int mixed_precision) {
-    if (!nmesh) return 0;
+size_t prc_multigrid_batch_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int mixed_precision, int count) {
+    if (!nmesh || count < 1) return 0;
     for (int d = 0; d < 3; d++)
         if (nmesh[d] < 1) return 0;
-    if (mesh_bytes == 4 && mixed_precision) return mixed_layout(nmesh, nullptr, nullptr);
-    if (mesh_bytes == 4) return plain_layout<float>(nmesh, nullptr, nullptr, nullptr);
-    return plain_layout<double>(nmesh, nullptr, nullptr, nullptr);
+    if (mesh_bytes == 4 && mixed_precision) return mixed_layout(nmesh, nullptr, nullptr, count);
+    if (mesh_bytes == 4) return plain_layout<float>(nmesh, nullptr, nullptr, nullptr, count);
+    return plain_layout<double>(nmesh, nullptr, nullptr, nullptr, count);
+}
+
+size_t prc_multigrid_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int mixed_precision) {
+    return prc_multigrid_batch_workspace_bytes(nmesh, mesh_bytes, mixed_precision, 1);
+}
+
+prc_status_t prc_multigrid_batch_f32(const float* const* delta, float* const* phi, int count, const int32_t nmesh[3],
+                                     const double boxsize[3], const double boxcenter[3], double beta, double damping,
+                                     int jacobi_niterations, int vcycle_niterations, const double* los,
+                                     int mixed_precision, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!delta || !phi || !batch_ok(nmesh, count)) return PRC_ERR_ARG;
+    for (int b = 0; b < count; b++)
+        if (!mg_args_ok(delta[b], phi[b], nmesh, boxsize, boxcenter, jacobi_niterations, vcycle_niterations))
+            return PRC_ERR_ARG;
+    Params P = make_params(boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los);
+    if (!workspace || workspace_bytes < prc_multigrid_batch_workspace_bytes(nmesh, 4, mixed_precision, count))
+        return PRC_ERR_WORKSPACE;
+    cudaStream_t st = (cudaStream_t)stream;
+    const std::string key = solve_key(4, mixed_precision ? 1 : 0, nmesh, P, workspace, workspace_bytes, count);
+    if (mixed_precision) return run_mixed_io(delta, phi, count, nmesh, P, workspace, key, st);
+    return run_plain_io<float>(delta, phi, count, nmesh, P, workspace, key, st);
+}
+
+prc_status_t prc_multigrid_batch_f64(const double* const* delta, double* const* phi, int count,
+                                     const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
+                                     double beta, double damping, int jacobi_niterations, int vcycle_niterations,
+                                     const double* los, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!delta || !phi || !batch_ok(nmesh, count)) return PRC_ERR_ARG;
+    for (int b = 0; b < count; b++)
+        if (!mg_args_ok(delta[b], phi[b], nmesh, boxsize, boxcenter, jacobi_niterations, vcycle_niterations))
+            return PRC_ERR_ARG;
+    Params P = make_params(boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los);
+    if (!workspace || workspace_bytes < prc_multigrid_batch_workspace_bytes(nmesh, 8, 0, count)) return PRC_ERR_WORKSPACE;
+    const std::string key = solve_key(8, 0, nmesh, P, workspace, workspace_bytes, count);
+    return run_plain_io<double>(delta, phi, count, nmesh, P, workspace, key, (cudaStream_t)stream);
 }
 
 prc_status_t prc_multigrid_f32(const float* delta, float* phi, const int32_t nmesh[3], const double boxsize[3],
                                const double boxcenter[3], double beta, double damping, int jacobi_niterations,
                                int vcycle_niterations, const double* los, int mixed_precision, void* workspace,
                                size_t workspace_bytes, void* stream) {
-    if (!mg_args_ok(delta, phi, nmesh, boxsize, boxcenter, jacobi_niterations, vcycle_niterations)) return PRC_ERR_ARG;
-    Params P = make_params(boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los);
-    if (!workspace || workspace_bytes < prc_multigrid_workspace_bytes(nmesh, 4, mixed_precision)) return PRC_ERR_WORKSPACE;
-    cudaStream_t st = (cudaStream_t)stream;
-    const int64_t N = (int64_t)nmesh[0] * nmesh[1] * nmesh[2];
-    const std::string key = solve_key(4, mixed_precision ? 1 : 0, nmesh, P, workspace, workspace_bytes);
-    if (mixed_precision) {
-        MixedBufs m;
-        mixed_layout(nmesh, (char*)workspace, &m);
-        PRC_LAUNCH_B("mg_convert", st, 12.0 * N, convert_kernel<float, double><<<grid_for(N), 256, 0, st>>>(delta, m.f64[0], N));
-        PRC_CHECK_LAUNCH();
-        PRC_TRY(run_graph(key, st, [&](cudaStream_t s) { return solve_mixed(nmesh, P, workspace, s); }));
-        PRC_LAUNCH_B("mg_convert", st, 12.0 * N, convert_kernel<double, float><<<grid_for(N), 256, 0, st>>>(m.v64[0], phi, N));
-        PRC_CHECK_LAUNCH();
-        return PRC_OK;
-    }
-    return run_plain_io<float>(delta, phi, nmesh, P, workspace, key, st);
+    return prc_multigrid_batch_f32(&delta, &phi, 1, nmesh, boxsize, boxcenter, beta, damping, jacobi_niterations,
+                                   vcycle_niterations, los, mixed_precision, workspace, workspace_bytes, stream);
 }
 
 prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t nmesh[3], const double boxsize[3],
                                const double boxcenter[3], double beta, double damping, int jacobi_niterations,
                                int vcycle_niterations, const double* los, void* workspace, size_t workspace_bytes,
                                void* stream) {
-    if (!mg_args_ok(delta, phi, nmesh, boxsize, boxcenter, jacobi_niterations, vcycle_niterations)) return PRC_ERR_ARG;
-    Params P = make_params(boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los);
-    if (!workspace || workspace_bytes < prc_multigrid_workspace_bytes(nmesh, 8, 0)) return PRC_ERR_WORKSPACE;
-    const std::string key = solve_key(8, 0, nmesh, P, workspace, workspace_bytes);
-    return run_plain_io<double>(delta, phi, nmesh, P, workspace, key, (cudaStream_t)stream);
+    return prc_multigrid_batch_f64(&delta, &phi, 1, nmesh, boxsize, boxcenter, beta, damping, jacobi_niterations,
+                                   vcycle_niterations, los, workspace, workspace_bytes, stream);
 }
 
 #define MG_COMPONENTS(SUF, T)                                                                                        \

@@ -92,6 +92,60 @@ class OriginalMultiGridReconstruction(BaseReconstruction):
                   _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device), error=MeshError)
 
 
+def run_batch(recons, jacobi_damping_factor=0.4, jacobi_niterations=5, vcycle_niterations=6):
+    """:meth:`OriginalMultiGridReconstruction.run` of several reconstructions at once: one batched solve
+    (every kernel of the multigrid schedule runs over all of them in one launch), on the first
+    reconstruction's stream and workspace.  They must share the mesh (nmesh, boxsize, boxcenter, dtype),
+    the line of sight, beta, the precision mode and the device, and have their density contrast set.
+    Results equal separate :meth:`run` calls."""
+    import torch
+    recons = list(recons)
+    if not recons:
+        return
+    r0 = recons[0]
+    key = lambda r: (tuple(r.info.nmesh), tuple(r.info.boxsize), tuple(r.info.boxcenter), r.info.dtype,
+                     None if r.los is None else tuple(float(x) for x in r.los), float(r.beta),
+                     bool(r.mixed_precision), str(r.device))
+    for r in recons:
+        if not isinstance(r, OriginalMultiGridReconstruction):
+            raise ValueError('run_batch takes multigrid reconstructions')
+        if key(r) != key(r0):
+            raise ValueError('run_batch needs the same mesh, line of sight, beta, precision and device')
+        if getattr(r, 'mesh_delta', None) is None:
+            from .recon import ReconstructionError
+            raise ReconstructionError('set_density_contrast must be called before run')
+    streams = [r.stream if r.stream is not None else torch.cuda.current_stream(r.device) for r in recons]
+    with r0._stream_ctx():
+        st0 = streams[0]
+        for st in streams[1:]:
+            if st != st0:
+                st0.wait_stream(st)         # the other reconstructions' density contrasts are done
+        nm, bs, bc = r0.info.c_geometry()
+        lib = _lib.load()
+        item = r0.info.dtype.itemsize
+        count = len(recons)
+        deltas = [r.mesh_delta.value for r in recons]
+        phis = []
+        for r in recons:
+            phi = RealMesh(info=r.info, device=r.device)
+            phi.__dict__['value'] = torch.empty(r.info.shape, dtype=torch_dtype(r.info.dtype), device=r.device)
+            phis.append(phi)
+        ws = r0._ws.get(lib.prc_multigrid_batch_workspace_bytes(nm, item, int(r0.mixed_precision), count))
+        args = [_lib.pointer_array(deltas), _lib.pointer_array([p.value for p in phis]), count, nm, bs, bc,
+                float(r0.beta), float(jacobi_damping_factor), int(jacobi_niterations), int(vcycle_niterations),
+                r0._los_arg()]
+        if item == 4:
+            args.append(int(r0.mixed_precision))
+        _lib.call('prc_multigrid_batch_' + _lib.suffix(r0.info.dtype), *args, _lib.ptr(ws), ws.numel(),
+                  _lib.stream_of(r0.device), error=MeshError)
+        for r, st, phi in zip(recons, streams, phis):
+            if st != st0:
+                st.wait_stream(st0)         # later work on that reconstruction's stream sees its phi
+                phi.value.record_stream(st)
+            del r.mesh_delta
+            r.mesh_phi = phi
+
+
 class MultiGridReconstruction(OriginalMultiGridReconstruction):
     """Multigrid reconstruction with the base class's density contrast (multigrid.py:161-167)."""
 

@@ -13,8 +13,11 @@ scratch) is free and their estimated device memory fits in what the budget has l
 request runs the plain
 pipeline (constructor, assign_data, assign_randoms, set_density_contrast, run,
 read_shifted_positions) on its own stream from a worker thread, so the kernels of the requests
-in flight overlap on the device while requests keep arriving.  A request's result does not depend
-on what else is running: every kernel is deterministic and requests share no device buffers.
+in flight overlap on the device while requests keep arriving.  Queued multigrid requests of the same
+mesh and settings are admitted together (up to max_batch) and their solves run as one batched solve,
+every kernel of the multigrid schedule covering all of them in one launch.  A request's result does
+not depend on what else is running: every kernel is deterministic, requests share no device buffers
+and a batched solve gives each problem the bits of its own solve.
 """
 import threading
 import time
@@ -77,10 +80,8 @@ def estimate_device_bytes(request):
     return int(total)
 
 
-def run_request(request, device=None, stream=None, workspace=None):
-    """The plain pipeline for one request on `stream`; returns {'shifted_data', 'shifted_randoms'}.
-    `workspace`: scratch kept across requests (a slot's), so its address, and with it the multigrid
-    solve's captured CUDA graph, is reused."""
+def prepare_request(request, device=None, stream=None, workspace=None):
+    """Constructor, paints and density contrast of one request on `stream`; returns the reconstruction."""
     import pyrecon_b200
     cls = getattr(pyrecon_b200, request.algorithm)
     rec = cls(device=device, stream=stream, workspace=workspace, **request.kwargs)
@@ -88,21 +89,62 @@ def run_request(request, device=None, stream=None, workspace=None):
     if request.randoms is not None:
         rec.assign_randoms(request.randoms, request.randoms_weights)
     rec.set_density_contrast(**request.density_kwargs)
-    rec.run(**request.run_kwargs)
+    return rec
+
+
+def finish_request(request, rec):
+    """The shifted positions of a request whose reconstruction has run."""
     out = {'shifted_data': rec.read_shifted_positions(request.data)}
     if request.randoms is not None:
         out['shifted_randoms'] = rec.read_shifted_positions(request.randoms)
     return out
 
 
+def run_request(request, device=None, stream=None, workspace=None):
+    """The plain pipeline for one request on `stream`; returns {'shifted_data', 'shifted_randoms'}.
+    `workspace`: scratch kept across requests (a slot's), so its address, and with it the multigrid
+    solve's captured CUDA graph, is reused."""
+    rec = prepare_request(request, device=device, stream=stream, workspace=workspace)
+    rec.run(**request.run_kwargs)
+    return finish_request(request, rec)
+
+
+def batch_key(request):
+    """Requests with the same key can share one batched multigrid solve (same algorithm, mesh, line of
+    sight, cosmology, precision and solver settings; the catalogues may differ); None: not batchable."""
+    import pyrecon_b200
+    from .multigrid import OriginalMultiGridReconstruction
+    cls = getattr(pyrecon_b200, request.algorithm)
+    kw = request.kwargs
+    if not issubclass(cls, OriginalMultiGridReconstruction) or 'positions' in kw:
+        return None
+    if not all(k in kw for k in ('nmesh', 'boxsize', 'boxcenter')) and not ('cellsize' in kw and 'boxsize' in kw):
+        return None
+    norm = lambda d: repr(sorted((k, np.asarray(v).tolist() if isinstance(v, (list, tuple, np.ndarray)) else v)
+                                 for k, v in d.items()))
+    return (request.algorithm, norm(kw), norm(request.density_kwargs), norm(request.run_kwargs))
+
+
+def run_batch_requests(requests, device=None, stream=None, workspace=None):
+    """Several batchable requests (same batch_key) on one stream: each is prepared, the multigrid solves
+    run as one batched solve, then each is read out; returns their outputs in order."""
+    from .multigrid import run_batch
+    recs = [prepare_request(r, device=device, stream=stream, workspace=workspace) for r in requests]
+    run_batch(recs, **requests[0].run_kwargs)
+    return [finish_request(r, rec) for r, rec in zip(requests, recs)]
+
+
 class ReconstructionServer(object):
     """Continuous-batching request loop on one GPU (see the module docstring).
 
-    slots: requests in flight at most (one CUDA stream each).  hbm_budget: bytes of device memory
-    the requests in flight may hold together (default: 90% of the free memory at start).
+    slots: jobs in flight at most (one CUDA stream each).  hbm_budget: bytes of device memory the
+    requests in flight may hold together (default: 90% of the free memory at start).  max_batch:
+    queued multigrid requests with the same mesh and settings (batch_key) are taken together as one
+    job of up to this many, whose solves run as one batched solve (a power of two, so the slot's
+    captured solves are reused); 1 disables.
     """
 
-    def __init__(self, device=None, slots=8, hbm_budget=None):
+    def __init__(self, device=None, slots=8, hbm_budget=None, max_batch=8):
         import torch
         self.device = _device_of(device)
         _lib.load()
@@ -110,6 +152,7 @@ class ReconstructionServer(object):
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = 0.9 * free
         self.hbm_budget = float(hbm_budget)
+        self.max_batch = max(1, int(max_batch))
         from .mesh import _Workspace
         self._streams = [torch.cuda.Stream(self.device) for _ in range(slots)]
         # device scratch resident per slot: reused by every request the slot runs
@@ -141,7 +184,7 @@ class ReconstructionServer(object):
             request.submitted = time.perf_counter()
             if self._first_submit is None:
                 self._first_submit = request.submitted
-            self._queue.append((request, need, fut))
+            self._queue.append((request, need, fut, batch_key(request) if self.max_batch > 1 else None))
             self._cv.notify_all()
         return fut
 
@@ -154,32 +197,58 @@ class ReconstructionServer(object):
                     if self._closed and not self._queue:
                         return
                     self._cv.wait()
-                request, need, fut = self._queue.popleft()
+                job = [self._queue.popleft()]
+                key = job[0][3]
+                if key is not None:
+                    # queued requests of the same batch key join, while the budget allows
+                    room = self.hbm_budget - self._in_use - job[0][1]
+                    for item in list(self._queue):
+                        if len(job) >= self.max_batch:
+                            break
+                        if item[3] == key and item[1] <= room:
+                            job.append(item)
+                            room -= item[1]
+                    n = 1
+                    while 2 * n <= len(job):
+                        n *= 2
+                    job = job[:n]
+                    for item in job[1:]:
+                        self._queue.remove(item)
                 slot = self._free_streams.pop()
+                need = sum(item[1] for item in job)
                 self._in_use += need
-                self._active += 1
+                self._active += len(job)
                 self.peak_active = max(self.peak_active, self._active)
-            self._pool.submit(self._work, request, need, fut, slot)
+            self._pool.submit(self._work, job, need, slot)
 
-    def _work(self, request, need, fut, slot):
+    def _work(self, job, need, slot):
         import torch
         stream = self._streams[slot]
+        requests = [item[0] for item in job]
         try:
             with torch.cuda.device(self.device):
-                out = run_request(request, device=self.device, stream=stream, workspace=self._workspaces[slot])
+                if len(requests) == 1:
+                    outs = [run_request(requests[0], device=self.device, stream=stream,
+                                        workspace=self._workspaces[slot])]
+                else:
+                    outs = run_batch_requests(requests, device=self.device, stream=stream,
+                                              workspace=self._workspaces[slot])
                 stream.synchronize()
         except BaseException as exc:
-            fut.set_exception(exc)
+            for item in job:
+                item[2].set_exception(exc)
         else:
             done = time.perf_counter()
             with self._cv:
-                self.latencies.append(done - request.submitted)
+                for r in requests:
+                    self.latencies.append(done - r.submitted)
                 self._last_done = done
-            fut.set_result(out)
+            for item, out in zip(job, outs):
+                item[2].set_result(out)
         finally:
             with self._cv:
                 self._in_use -= need
-                self._active -= 1
+                self._active -= len(job)
                 self._free_streams.append(slot)
                 self._cv.notify_all()
 

@@ -429,6 +429,31 @@ def test_multigrid_graph_replay_equals_direct_launches(dtype, mixed, tmp_path):
     assert np.array_equal(np.load(path), first)
 
 
+@pytest.mark.parametrize('dtype,mixed,los', [('f8', False, None), ('f4', True, None), ('f4', False, [0., 0., 1.]),
+                                             ('f8', False, [0.3, -0.5, 0.8])])
+def test_multigrid_batch_equals_separate_solves(dtype, mixed, los):
+    """prc_multigrid_batch_*: three problems in one batched solve give the bits of three separate solves."""
+    L, t = lib(), torch()
+    nmesh = (24, 16, 32)
+    rng = np.random.default_rng(31)
+    deltas = [dev(rng.standard_normal(nmesh).astype(dtype)) for _ in range(3)]
+    nm, bs, bc = L.i3(nmesh), L.d3([800., 600., 900.]), L.d3([0., 100., 1500.])
+    sfx, item = L.suffix(dtype), np.dtype(dtype).itemsize
+    tail = [nm, bs, bc, 0.4, 0.4, 5, 6, L.opt_d3(los)] + ([int(mixed)] if dtype == 'f4' else [])
+    alone = []
+    for d in deltas:
+        phi = t.empty_like(d)
+        w = ws(L.load().prc_multigrid_workspace_bytes(nm, item, int(mixed)))
+        L.call('prc_multigrid_' + sfx, L.ptr(d), L.ptr(phi), *tail, L.ptr(w), w.numel(), stream())
+        alone.append(phi.cpu().numpy())
+    phis = [t.empty_like(d) for d in deltas]
+    w = ws(L.load().prc_multigrid_batch_workspace_bytes(nm, item, int(mixed), 3))
+    L.call('prc_multigrid_batch_' + sfx, L.pointer_array(deltas), L.pointer_array(phis), 3, *tail, L.ptr(w), w.numel(),
+           stream())
+    for a, p in zip(alone, phis):
+        assert np.array_equal(a, p.cpu().numpy())
+
+
 def _smooth_real_gpu(value, radius_box, nsigmas, dtype):
     L = lib()
     t = torch()

@@ -68,3 +68,23 @@ def test_admission_keeps_requests_within_the_budget():
             big = _requests()[4]
             big.kwargs['nmesh'] = 1024
             server.submit(big)
+
+
+def test_batched_multigrid_requests_equal_requests_alone():
+    """Queued multigrid requests of the same mesh and settings run as one job with a batched solve;
+    each result has the bits of the same request run alone."""
+    from pyrecon_b200.serving import ReconstructionRequest, ReconstructionServer, run_request, batch_key
+    reqs = []
+    for i in range(5):
+        data = mocks.lognormal_positions_numpy(10000 + 3000 * i, 32, 1000., 500., seed=100 + i, field_seed=110 + i)
+        reqs.append(ReconstructionRequest('MultiGridReconstruction', data=data, f=0.8, bias=2., los='z', nmesh=32,
+                                          boxsize=1000., boxcenter=500., wrap=True, dtype='f4',
+                                          density_kwargs=dict(smoothing_radius=15.)))
+    assert len(set(batch_key(r) for r in reqs)) == 1
+    alone = [run_request(r) for r in reqs]
+    with ReconstructionServer(slots=1, max_batch=4) as server:
+        futures = [server.submit(r) for r in reqs]
+        mixed = [f.result(timeout=300) for f in futures]
+        assert server.peak_active >= 2          # at least one batch of several requests
+    for a, b in zip(alone, mixed):
+        _same(a, b)
