@@ -536,6 +536,7 @@ def run_multi_arm(args, w):
 # roofline and for ncu captures of one kernel: name -> (mesh dtype, nmesh).
 KERNELS = {
     'mg_jacobi': ('f4', 512),          # damped-Jacobi sweeps (two per step), local line of sight, FP32
+    'mg_jacobi_256': ('f4', 256),
     'mg_jacobi_f64': ('f8', 384),
     'mg_residual': ('f4', 512),
     'smooth_real': ('f4', 256),        # truncated real-space Gaussian, radius 15 Mpc/h on 7.8 Mpc/h cells

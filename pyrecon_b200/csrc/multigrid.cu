@@ -107,12 +107,13 @@ __device__ __forceinline__ A neighbour_sum(const V* __restrict__ v, const int n[
 __device__ __forceinline__ bool cell3(const int n[3], int& x, int& y, int& z) {
     z = blockIdx.x * blockDim.x + threadIdx.x;
     y = blockIdx.y * blockDim.y + threadIdx.y;
-    x = blockIdx.z % n[0];
+    x = gridDim.z == (unsigned)n[0] ? (int)blockIdx.z : (int)(blockIdx.z % n[0]);   // no division unbatched
     return z < n[2] && y < n[1];
 }
 
 // Offset of this block's problem in a batch of meshes of shape n.
 __device__ __forceinline__ int64_t batch_offset(const int n[3]) {
+    if (gridDim.z == (unsigned)n[0]) return 0;
     return (int64_t)(blockIdx.z / n[0]) * ((int64_t)n[0] * n[1] * n[2]);
 }
 
@@ -167,7 +168,7 @@ struct Quad {
 __device__ __forceinline__ bool quad_of(const int n[3], Quad& q) {
     q.z0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
     q.y = blockIdx.y * blockDim.y + threadIdx.y;
-    q.x = blockIdx.z % n[0];
+    q.x = gridDim.z == (unsigned)n[0] ? (int)blockIdx.z : (int)(blockIdx.z % n[0]);
     q.c = ((int64_t)q.x * n[1] + q.y) * n[2];
     return q.z0 < n[2] && q.y < n[1];
 }
