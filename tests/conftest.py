@@ -15,7 +15,8 @@ def pytest_configure(config):
 
 
 def golden_cases():
-    return sorted(fn[:-4] for fn in os.listdir(GOLDEN) if fn.endswith('.npz') and fn != 'mesh_kernels.npz')
+    return sorted(fn[:-4] for fn in os.listdir(GOLDEN) if fn.endswith('.npz') and fn not in ('mesh_kernels.npz',
+                                                                                              'utils.npz'))
 
 
 @pytest.fixture(scope='session')

@@ -207,12 +207,42 @@ def mesh_kernels(pyrecon):
     return out
 
 
+def distance_of_z(z):
+    """A smooth distance-redshift relation for the DistanceToRedshift fixture."""
+    return 2997.92458 * z / (1. + 0.6 * z) ** 0.5
+
+
+def utils_fixture(pyrecon):
+    """pyrecon.utils conversions: sky <-> Cartesian (f4, f8), DistanceToRedshift, random_box_positions."""
+    from pyrecon import utils
+    out = {}
+    rng = np.random.default_rng(44)
+    for dtype in ['f4', 'f8']:
+        pos = (rng.normal(size=(500, 3)) * 800.).astype(dtype)
+        out['pos_' + dtype] = pos
+        for degree in [True, False]:
+            for wrap in [True, False]:
+                d, ra, dec = utils.cartesian_to_sky(pos, wrap=wrap, degree=degree)
+                tag = '{}_{:d}{:d}'.format(dtype, degree, wrap)
+                out['dist_' + tag], out['ra_' + tag], out['dec_' + tag] = d, ra, dec
+            d, ra, dec = utils.cartesian_to_sky(pos, degree=degree)
+            out['xyz_{}_{:d}'.format(dtype, degree)] = utils.sky_to_cartesian(d, ra, dec, degree=degree)
+    d2z = utils.DistanceToRedshift(distance_of_z)
+    r = np.linspace(0., 5000., 301)
+    out['d2z_r'], out['d2z_z'] = r, d2z(r)
+    out['box'] = utils.random_box_positions(1000., boxcenter=[100., 0., -50.], size=200, seed=42, dtype='f4')
+    out['box_nbar'] = utils.random_box_positions([10., 20., 30.], nbar=0.5, seed=7)
+    return out
+
+
 def main(names=None):
     """Write every fixture, or only those named (case names, 'mesh_kernels')."""
     with tempfile.TemporaryDirectory() as tmp:
         pyrecon = import_reference(tmp)
         if not names or 'mesh_kernels' in names:
             np.savez_compressed(os.path.join(HERE, 'mesh_kernels.npz'), **mesh_kernels(pyrecon))
+        if not names or 'utils' in names:
+            np.savez_compressed(os.path.join(HERE, 'utils.npz'), **utils_fixture(pyrecon))
         for seed, case in enumerate(CASES):
             if names and case['name'] not in names:
                 continue

@@ -122,3 +122,20 @@ def test_readout_in_paint_order_equals_plain_readout(name):
         plain = rec.read_shifted_positions(cat.clone())
         assert torch.equal(ordered, plain)
         assert torch.equal(rec.read_shifts(cat, field='rsd'), rec.read_shifts(cat.clone(), field='rsd'))
+
+
+def test_sky_conversions_on_device():
+    """utils.cartesian_to_sky / sky_to_cartesian on CUDA tensors agree with the numpy (reference) path."""
+    import torch
+    from pyrecon_b200 import utils
+    rng = np.random.default_rng(3)
+    for dtype, tol in [('f8', 1e-12), ('f4', 2e-6)]:
+        pos = (rng.normal(size=(10000, 3)) * 800.).astype(dtype)
+        t = torch.from_numpy(pos).cuda()
+        ref = utils.cartesian_to_sky(pos)
+        out = utils.cartesian_to_sky(t)
+        for a, b in zip(out, ref):
+            assert a.is_cuda
+            assert maxrel(a.cpu().numpy(), b) < tol
+        xyz = utils.sky_to_cartesian(*out)
+        assert xyz.is_cuda and maxrel(xyz.cpu().numpy(), pos) < 10 * tol

@@ -143,3 +143,54 @@ def test_replicas_timing_is_the_max_over_ranks_gloo():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert dict(out) == {0: 20., 1: 20.}
+
+
+def _utils_fixture():
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, 'utils.npz'))
+    return {k: z[k] for k in z.files}
+
+
+def test_sky_cartesian_match_reference():
+    """cartesian_to_sky / sky_to_cartesian equal the reference's outputs (numpy, f4 and f8)."""
+    from pyrecon_b200 import utils
+    g = _utils_fixture()
+    for dtype in ['f4', 'f8']:
+        pos = g['pos_' + dtype]
+        for degree in [True, False]:
+            for wrap in [True, False]:
+                tag = '{}_{:d}{:d}'.format(dtype, degree, wrap)
+                d, ra, dec = utils.cartesian_to_sky(pos, wrap=wrap, degree=degree)
+                for name, v in zip(['dist_', 'ra_', 'dec_'], [d, ra, dec]):
+                    assert v.dtype == g[name + tag].dtype
+                    np.testing.assert_array_equal(v, g[name + tag])
+            d, ra, dec = utils.cartesian_to_sky(pos, degree=degree)
+            xyz = utils.sky_to_cartesian(d, ra, dec, degree=degree)
+            ref = g['xyz_{}_{:d}'.format(dtype, degree)]
+            assert xyz.dtype == ref.dtype
+            np.testing.assert_array_equal(xyz, ref)
+
+
+def test_distance_to_redshift_and_box_positions_match_reference():
+    from pyrecon_b200 import utils
+    g = _utils_fixture()
+    d2z = utils.DistanceToRedshift(lambda z: 2997.92458 * z / (1. + 0.6 * z) ** 0.5)
+    np.testing.assert_allclose(d2z(g['d2z_r']), g['d2z_z'], rtol=1e-12, atol=1e-14)
+    box = utils.random_box_positions(1000., boxcenter=[100., 0., -50.], size=200, seed=42, dtype='f4')
+    assert box.dtype == g['box'].dtype
+    np.testing.assert_array_equal(box, g['box'])
+    np.testing.assert_array_equal(utils.random_box_positions([10., 20., 30.], nbar=0.5, seed=7), g['box_nbar'])
+    with pytest.raises(ValueError):
+        utils.random_box_positions(10.)
+
+
+def test_memory_monitor_and_mkdir(tmp_path, capsys):
+    from pyrecon_b200 import utils
+    d = str(tmp_path / 'a' / 'b')
+    utils.mkdir(d)
+    utils.mkdir(d)                      # existing: no error
+    assert os.path.isdir(d)
+    with utils.MemoryMonitor() as mem:
+        mem('step')
+    out = capsys.readouterr().out
+    assert '[step] using' in out and 'increase of' in out
