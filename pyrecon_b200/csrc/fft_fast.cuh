@@ -237,57 +237,6 @@ __device__ __forceinline__ T kval(int i, int n, T fscale) {
     return (T)6.283185307179586 * ((T)s * fscale);
 }
 
-// Symmetrised multiplier (re, im) of output o (see kmultiplier in fft.cu), in precision T,
-// for the compile-time operator KT.
-template <typename T, int KT>
-__device__ __forceinline__ void kmult(const KOp& op, int o, int ix, int iy, int iz, T& re, T& im) {
-    const int idx[3] = {ix, iy, iz};
-    T k[3], kt[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        k[a] = kval<T>(idx[a], op.n[a], (T)op.fscale[a]);
-        kt[a] = nyquist(idx[a], op.n[a]) ? k[a] : -k[a];
-    }
-    const T k2 = (k[1] * k[1] + k[0] * k[0]) + k[2] * k[2];
-    const bool zero = (ix == 0 && iy == 0 && iz == 0);
-    const T norm = (T)op.norm;
-    re = 0;
-    im = 0;
-    if constexpr (KT == KOP_GAUSS) {
-        T e = 0;
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const T rk = (T)op.radius[a] * k[a];
-            e += (T)-0.5 * (rk * rk);
-        }
-        re = exp(e) * norm;
-    } else if constexpr (KT == KOP_PP) {
-        if (zero) return;
-        const T l0 = (T)op.los[0], l1 = (T)op.los[1], l2 = (T)op.los[2];
-        const T kl = k[0] * l0 + k[1] * l1 + k[2] * l2;
-        const T klt = kt[0] * l0 + kt[1] * l1 + kt[2] * l2;
-        const T m = k[o] / (k2 * ((T)1 + (T)op.beta * (kl * kl / k2)));
-        const T mt = kt[o] / (k2 * ((T)1 + (T)op.beta * (klt * klt / k2)));
-        im = (T)0.5 * (m - mt) * norm;
-    } else if constexpr (KT == KOP_ITER_GLOBAL) {
-        if (zero) return;
-        const T l0 = (T)op.los[0], l1 = (T)op.los[1], l2 = (T)op.los[2];
-        const T kl = k[0] * l0 + k[1] * l1 + k[2] * l2;
-        const T klt = kt[0] * l0 + kt[1] * l1 + kt[2] * l2;
-        re = (T)0.5 * (kl * kl + klt * klt) / k2 * norm;
-    } else if constexpr (KT == KOP_ITER_LOCAL) {
-        if (zero) return;
-        const int i = o < 3 ? 0 : (o < 5 ? 1 : 2);
-        const int j = o < 3 ? o : (o < 5 ? o - 2 : 2);
-        re = (T)0.5 * (k[i] * k[j] + kt[i] * kt[j]) / k2 * norm;
-    } else if constexpr (KT == KOP_PSI) {
-        if (zero) return;
-        im = (T)0.5 * (k[o] - kt[o]) / k2 * norm;
-    } else {
-        re = norm;
-    }
-}
-
 // Per-point quantities of the multiplier that do not depend on the output: computed once after the
 // forward x transform and reused by every output (one division per point instead of one per
 // point and output).
