@@ -618,7 +618,9 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
 #pragma unroll
                     for (int h = 0; h < 2; h++) {
                         const T xz = oz + cz * (T)(2 * (t + i * TL) + h);
-                        const T ix2 = (T)1 / ((x0 * x0 + x1 * x1) + xz * xz);
+                        const T x2 = (x0 * x0 + x1 * x1) + xz * xz;
+                        // FP32: fast reciprocal (2 ulp, far inside the FP32 mode's tolerance); FP64: exact
+                        const T ix2 = sizeof(T) == 4 ? (T)__fdividef(1.f, (float)x2) : (T)1 / x2;
                         o[h] = (h ? d0.y : d0.x) - r[i][h] * ix2;
                     }
                     out0[t + i * TL] = cmake<C>(o[0], o[1]);
