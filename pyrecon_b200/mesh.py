@@ -360,6 +360,50 @@ class BaseMesh(BaseClass):
     def __rtruediv__(self, other): return self._binary(other, lambda a, b: b / a)
     def __neg__(self): return self._binary(0, lambda a, b: -a)
 
+    def __pow__(self, other): return self._binary(other, lambda a, b: a ** b)
+    def __rpow__(self, other): return self._binary(other, lambda a, b: b ** a)
+
+    # comparisons give boolean device tensors (the reference's ufuncs give boolean arrays, not meshes)
+    def _compare(self, other, op):
+        return op(self.value, other.value if isinstance(other, BaseMesh) else other)
+
+    def __gt__(self, other): return self._compare(other, lambda a, b: a > b)
+    def __ge__(self, other): return self._compare(other, lambda a, b: a >= b)
+    def __lt__(self, other): return self._compare(other, lambda a, b: a < b)
+    def __le__(self, other): return self._compare(other, lambda a, b: a <= b)
+
+    __array_priority__ = 100
+
+    def __array_ufunc__(self, ufunc, method, *inputs, **kwargs):
+        """numpy ufuncs on meshes (mesh.py:185-225): evaluated on host copies of the values; a result of the
+        mesh's shape that is not boolean comes back as a mesh of this kind, anything else as an array."""
+        if kwargs.get('out'):
+            return NotImplemented
+        args = [np.asarray(x) if isinstance(x, BaseMesh) else x for x in inputs]
+        result = getattr(ufunc, method)(*args, **kwargs)
+
+        def cast(r):
+            if not isinstance(r, np.ndarray) or r.dtype == np.bool_ or r.shape != tuple(self.shape):
+                return r
+            new = self.deepcopy(copy_value=False)
+            new.value = r
+            return new
+
+        return tuple(cast(r) for r in result) if isinstance(result, tuple) else cast(result)
+
+    # FFT-engine and thread-count settings of the reference's CPU meshes: accepted, without effect
+    # (the transforms are this library's CUDA kernels)
+    nthreads = None
+
+    def set_num_threads(self, nthreads=None):
+        self.nthreads = nthreads
+
+    def get_fft_engine(self, engine='numpy', **kwargs):
+        return engine
+
+    def set_fft_engine(self, engine='numpy', **kwargs):
+        self.fft_engine = self.get_fft_engine(engine=engine, **kwargs)
+
     def __iadd__(self, other):
         self.value += other.value if isinstance(other, BaseMesh) else other
         return self
@@ -596,6 +640,16 @@ class ComplexMesh(BaseMesh):
     def shape(self):
         n = self.info.shape
         return (n[0], n[1], n[2] // 2 + 1)
+
+    @property
+    def hshape(self):
+        """Shape of the Hermitian half (the stored shape)."""
+        return self.shape
+
+    @property
+    def fundamental_freq(self):
+        """Fundamental frequency 2 pi / boxsize along each axis (mesh.py:806-810)."""
+        return 2 * np.pi / self.boxsize
 
     def coords(self):
         """Wavenumbers along each axis, fftfreq / rfftfreq (mesh.py:812-820)."""

@@ -139,3 +139,25 @@ def test_sky_conversions_on_device():
             assert maxrel(a.cpu().numpy(), b) < tol
         xyz = utils.sky_to_cartesian(*out)
         assert xyz.is_cuda and maxrel(xyz.cpu().numpy(), pos) < 10 * tol
+
+
+def test_mesh_numpy_interop():
+    """numpy ufuncs on meshes return meshes of the same kind (booleans and reductions return arrays),
+    arithmetic and comparisons run on the device, FFT-engine settings are accepted."""
+    import torch
+    from pyrecon_b200 import RealMesh
+    rng = np.random.default_rng(5)
+    value = rng.uniform(0.5, 2., (8, 6, 4))
+    mesh = RealMesh(value, boxsize=100., boxcenter=0., dtype='f8')
+    e = np.exp(mesh)
+    assert isinstance(e, RealMesh) and np.allclose(np.asarray(e), np.exp(value))
+    assert np.allclose(np.asarray(mesh ** 2), value ** 2) and np.allclose(np.asarray(2. ** mesh), 2. ** value)
+    gt = mesh > 1.
+    assert isinstance(gt, torch.Tensor) and gt.dtype == torch.bool
+    assert np.array_equal(gt.cpu().numpy(), value > 1.)
+    assert isinstance(np.greater(mesh, 1.), np.ndarray)
+    assert np.isclose(np.mean(mesh), value.mean())
+    mesh.set_fft_engine('fftw', nthreads=4)
+    mesh.set_num_threads(4)
+    c = mesh.to_complex()
+    assert np.allclose(c.fundamental_freq, 2 * np.pi / 100.) and c.hshape == (8, 6, 3)
