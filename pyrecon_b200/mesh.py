@@ -454,6 +454,9 @@ class RealMesh(BaseMesh):
             dtype = 'f8'
         if dtype is not None:
             kwargs['dtype'] = dtype
+        if info is None and value is not None and np.ndim(value) == 3:
+            kwargs.setdefault('nmesh', tuple(value.shape))              # mesh shape from the values (mesh.py:384-389)
+            kwargs.setdefault('dtype', _to_numpy(value.reshape(-1)[:0]).dtype if hasattr(value, 'reshape') else 'f8')
         super(RealMesh, self).__init__(value=None, info=info, device=device, attrs=attrs, **kwargs)
         if 'float' not in self.dtype.name:
             raise MeshError('Provide float dtype')
