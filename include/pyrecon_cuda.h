@@ -229,15 +229,18 @@ PRC_API prc_status_t prc_ifftp_update_f64(const double *psi4, const int32_t nmes
  * pos_rec (the data, `positions` = the data positions): shifts at the reconstructed positions and
  * RSD = data - reconstructed.  Without: at positions p (wrapped when wrap), disp = psi(p),
  * rsd = f (disp.l) l, disp+rsd = psi(p - rsd, wrapped) + rsd.  `shifted`: positions - shifts, wrapped
- * when wrap.  out (npos, 3) in `out_bytes` precision. */
+ * when wrap.  out (npos, 3) in `out_bytes` precision.  `order` (may be NULL): the particles' indices in the
+ * cell order of their paint (prc_assign_cic_order), the order the gathers visit them in (same results). */
 PRC_API prc_status_t prc_ifftp_read_f32(const float *psi4, const int32_t nmesh[3], const double boxsize[3],
                                         const double boxcenter[3], const void *positions, const void *pos_rec,
                                         int pos_bytes, int64_t npos, double f, const double *los, int field,
-                                        int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                        int shifted, int wrap, void *out, int out_bytes, int32_t *flags,
+                                        const uint32_t *order, void *stream);
 PRC_API prc_status_t prc_ifftp_read_f64(const double *psi4, const int32_t nmesh[3], const double boxsize[3],
                                         const double boxcenter[3], const void *positions, const void *pos_rec,
                                         int pos_bytes, int64_t npos, double f, const double *los, int field,
-                                        int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                        int shifted, int wrap, void *out, int out_bytes, int32_t *flags,
+                                        const uint32_t *order, void *stream);
 
 /* Device fault word of the FFT kernels on the current device (no counterpart in the reference,
  * whose FFTs run on the host): PRC_FAULT_WAIT_TIMEOUT when a kernel gave up a bounded wait for its

@@ -66,7 +66,7 @@ for _s in ['f32', 'f64']:
         'prc_ifftp_update_' + _s: (c_int, [_p, I3, D3, D3, _p, _p, c_int, c_i64, c_double, c_double, c_int, DP, c_int,
                                            _p, _p]),
         'prc_ifftp_read_' + _s: (c_int, [_p, I3, D3, D3, _p, _p, c_int, c_i64, c_double, DP, c_int, c_int, c_int, _p,
-                                         c_int, _p, _p]),
+                                         c_int, _p, _p, _p]),
         'prc_rfft3d_' + _s: (c_int, [_p, c_int, _p, I3, _p]),
         'prc_irfft3d_' + _s: (c_int, [_p, _p, I3, _p]),
         'prc_smooth_gaussian_' + _s: (c_int, [_p, c_int, _p, I3, D3, D3, _p, c_size, _p]),

@@ -862,13 +862,16 @@ __global__ void __launch_bounds__(256) ifftp_read_kernel(const typename vec4_of<
                                                          const P* __restrict__ pos, const P* __restrict__ pos_rec,
                                                          int64_t n, double f, int global_los, double l0, double l1,
                                                          double l2, int field, int shifted, int wrap,
-                                                         O* __restrict__ out, int32_t* flags) {
+                                                         O* __restrict__ out, int32_t* flags,
+                                                         const uint32_t* __restrict__ order) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t nround = (n + stride - 1) / stride;
     for (int64_t r = 0; r < nround; r++) {
-        const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + r * stride;
+        const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + r * stride;
         int bad = 0;
-        if (i < n) {
+        if (k < n) {
+            // particles visited in `order` when given (the cell order of their paint), as read_shifts_kernel
+            const int64_t i = order != nullptr ? (int64_t)order[k] : k;
             double base[3], sh[3];
             if (pos_rec != nullptr) {
                 const P pr[3] = {pos_rec[3 * i], pos_rec[3 * i + 1], pos_rec[3 * i + 2]};
@@ -1432,7 +1435,7 @@ IFFTP_UPDATE_IMPL(prc_ifftp_update_f64, double)
     prc_status_t NAME(const F* psi4, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],     \
                       const void* positions, const void* pos_rec, int pos_bytes, int64_t npos, double f,             \
                       const double* los, int field, int shifted, int wrap, void* out, int out_bytes, int32_t* flags, \
-                      void* stream) {                                                                             \
+                      const uint32_t* order, void* stream) {                                                      \
         PRC_TRY(ifftp_args_ok(psi4, sizeof(F), nmesh, boxsize, boxcenter, flags, pos_bytes, npos));                         \
         if (npos > 0 && (!positions || !out)) return PRC_ERR_ARG;                                                 \
         if ((out_bytes != 4 && out_bytes != 8) || field < PRC_FIELD_DISP || field > PRC_FIELD_DISP_RSD)           \
@@ -1452,19 +1455,19 @@ IFFTP_UPDATE_IMPL(prc_ifftp_update_f64, double)
         if (pos_bytes == 4 && out_bytes == 4)                                                                     \
             PRC_LAUNCH_B("ifftp_read", st, bytes, ifftp_read_kernel<float, F, float><<<grid, 256, 0, st>>>(        \
                 (const V4*)psi4, g, (const float*)positions, (const float*)pos_rec, npos, f, gl, l[0], l[1], l[2],  \
-                field, shifted, wrap, (float*)out, flags));                                                       \
+                field, shifted, wrap, (float*)out, flags, order));                                                       \
         else if (pos_bytes == 4)                                                                                  \
             PRC_LAUNCH_B("ifftp_read", st, bytes, ifftp_read_kernel<float, F, double><<<grid, 256, 0, st>>>(       \
                 (const V4*)psi4, g, (const float*)positions, (const float*)pos_rec, npos, f, gl, l[0], l[1], l[2],  \
-                field, shifted, wrap, (double*)out, flags));                                                      \
+                field, shifted, wrap, (double*)out, flags, order));                                                      \
         else if (out_bytes == 4)                                                                                  \
             PRC_LAUNCH_B("ifftp_read", st, bytes, ifftp_read_kernel<double, F, float><<<grid, 256, 0, st>>>(       \
                 (const V4*)psi4, g, (const double*)positions, (const double*)pos_rec, npos, f, gl, l[0], l[1],      \
-                l[2], field, shifted, wrap, (float*)out, flags));                                                 \
+                l[2], field, shifted, wrap, (float*)out, flags, order));                                                 \
         else                                                                                                      \
             PRC_LAUNCH_B("ifftp_read", st, bytes, ifftp_read_kernel<double, F, double><<<grid, 256, 0, st>>>(      \
                 (const V4*)psi4, g, (const double*)positions, (const double*)pos_rec, npos, f, gl, l[0], l[1],      \
-                l[2], field, shifted, wrap, (double*)out, flags));                                                \
+                l[2], field, shifted, wrap, (double*)out, flags, order));                                                \
         PRC_CHECK_LAUNCH();                                                                                       \
         return PRC_OK;                                                                                            \
     }

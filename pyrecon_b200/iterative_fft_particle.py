@@ -35,7 +35,9 @@ class OriginalIterativeFFTParticleReconstruction(FFTShiftsMixin, BaseReconstruct
             else:
                 self._positions_data = torch.cat([self._positions_data, p.pos.to(self._positions_data.dtype)], dim=0)
                 self._weights_data = torch.cat([self._weights_data, w.to(self._weights_data.dtype)], dim=0)
-            self.mesh_data.assign_cic(p.pos, weights=w, wrap=self.wrap, check=check)
+            order = self._new_order(positions)
+            self.mesh_data.assign_cic(p.pos, weights=w, wrap=self.wrap, check=check, order_out=order)
+            self._keep_order(positions, order)
 
     def set_density_contrast(self, ran_min=0.01, smoothing_radius=15., check=False, **kwargs):
         """Keep ``ran_min`` and ``smoothing_radius`` for :meth:`run` and set :attr:`mesh_delta` from the
@@ -145,18 +147,20 @@ class OriginalIterativeFFTParticleReconstruction(FFTShiftsMixin, BaseReconstruct
         if data_mode and positions != 'data':
             raise ReconstructionError('positions must be an array or "data"')
         with self._stream_ctx():
+            order = None
             if data_mode:
                 pos, rec, kind = self._positions_data, self._positions_rec_data, self._data_kind
                 n, pbytes = len(pos), pos.element_size()
             else:
                 kind = Particles(positions, self.device)
                 pos, rec, n, pbytes = kind.pos, None, kind.size, kind.pos_bytes
+                order = self._order_for(positions)
             obytes = max(pbytes, self.info.dtype.itemsize) if (shifted and self.wrap) else pbytes
             out = torch.empty((n, 3), dtype=torch_dtype('f4' if obytes == 4 else 'f8'), device=self.device)
             _lib.call('prc_ifftp_read_' + _lib.suffix(self.info.dtype), _lib.ptr(self._psi4), nm, bs, bc, _lib.ptr(pos),
                       _lib.ptr(rec), pbytes, n, float(self.f), self._los_arg(), _lib.FIELDS[field], int(shifted),
-                      int(self.wrap), _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device),
-                      error=MeshError)
+                      int(self.wrap), _lib.ptr(out), obytes, self._flags.ptr, _lib.ptr(order),
+                      _lib.stream_of(self.device), error=MeshError)
             low, high = self.info.boxcenter - self.info.boxsize / 2., self.info.boxcenter + self.info.boxsize / 2.
             self._flags.raise_if_set(low, high)
             _lib.check_device_faults(ReconstructionError)

@@ -96,7 +96,7 @@ def test_chunked_host_readout_equals_device_readout(kind):
     assert np.array_equal(disp, out['shifts_disp'])
 
 
-@pytest.mark.parametrize('name', ['ifft_f4_local', 'mg_f8_local'])
+@pytest.mark.parametrize('name', ['ifft_f4_local', 'mg_f8_local', 'ifftp_f8_local', 'ifftp_f4_local'])
 def test_readout_in_paint_order_equals_plain_readout(name):
     """Device catalogues are read out in the cell order of their paint; a copy of the same positions
     (no order remembered) gives the same bits."""
