@@ -996,9 +996,27 @@ template <typename T> struct FastXTma {
     };
 };
 
+// Columns per tile (FP32; FP64 half as many; 0 = as the strided passes) and CTAs per SM the inverse y pass
+// of the local-line-of-sight iteration is compiled for.  Two CTAs of 8 columns per SM (64 registers a
+// thread) measured 4.30 ms per nmesh-512 reconstruction against 4.57 for one CTA of 16 columns.
+#ifndef PRC_HESS_B
+#define PRC_HESS_B 8
+#endif
+#ifndef PRC_HESS_MINB
+#define PRC_HESS_MINB 2
+#endif
+template <typename T, int N> struct HessTmaCfg {
+    static constexpr int B0 = PRC_HESS_B == 0 ? StridedTmaB<T, N>::value
+                                              : (sizeof(T) == 4 ? PRC_HESS_B : PRC_HESS_B / 2);
+    static constexpr int B = (N / 8) * B0 <= 1024 ? B0 : 1024 / (N / 8);
+    static constexpr int THREADS = (N / 8) * B;
+    static constexpr int S = StageCount<(int)(PRC_TMA_STAGE_KB * 1024 / fast::TileShape<T, N, B>::BYTES)>::value;
+    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, 0>::BYTES;
+};
+
 template <typename T> struct FastHessTma {
     template <int N> struct K {
-        typedef StridedTmaCfg<T, N> cfg;
+        typedef HessTmaCfg<T, N> cfg;
         // probe: only check that the tensor maps can be made (nothing is launched)
         static int run(const Plan3& p, cplx_t<T>* const* d, cplx_t<T>* const* o, fast::HessGeom h, cudaStream_t st,
                        bool probe) {
@@ -1015,7 +1033,7 @@ template <typename T> struct FastHessTma {
             s.outer = p.dims.n[0];
             s.os = (int64_t)p.dims.n[1] * p.pitch;
             s.ncols = p.nh;
-            auto kern = fast::y_hessian_tma<T, N, cfg::B, cfg::S>;
+            auto kern = fast::y_hessian_tma<T, N, cfg::B, cfg::S, PRC_HESS_MINB>;
             const size_t smem = cfg::SMEM + 2 * N * sizeof(T);     // + the x1 and k_y tables
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             const int64_t ntiles = (int64_t)s.outer * ((s.ncols + cfg::B - 1) / cfg::B);

@@ -404,8 +404,8 @@ struct HessGeom {
     const void* l02;
 };
 
-template <typename T, int N, int B, int S>
-__global__ void __launch_bounds__(N / 8 * B) y_hessian_tma(const __grid_constant__ prc::tma::Maps maps,
+template <typename T, int N, int B, int S, int MINB>
+__global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, MINB>::value)) y_hessian_tma(const __grid_constant__ prc::tma::Maps maps,
                                                            Specs<cplx_t<T>> out, Strided s, HessGeom h) {
     typedef cplx_t<T> C;
     typedef TileShape<T, N, B> TS;
@@ -485,23 +485,31 @@ __global__ void __launch_bounds__(N / 8 * B) y_hessian_tma(const __grid_constant
                 // D02 on the z-Nyquist column: the x-Nyquist mode of the line, (-1)^x l02
                 const bool sub02 = q == 3 && znyq && l02 != nullptr;
                 C v[8];
+                // y factor before the transform (q is the same for the whole CTA, so each case is one
+                // uniform branch): k_y^2 (D11), s_y (D01, D12), k_y on the Nyquist index only (D12, z Nyquist)
+                if (q == 2) {
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    if (sub02) {
+                    for (int i = 0; i < 8; i++) {
+                        const T ky = kytab[t + i * TL];
+                        v[i] = cscale(sb[(t + i * TL) * B + col], ky * ky);
+                    }
+                } else if (q == 1 || q == 4) {
+                    const bool on_nyq = q == 4 && znyq;
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const int iy = t + i * TL;
+                        const T yf = (on_nyq == (iy == ynyq)) ? kytab[iy] : (T)0;
+                        v[i] = cscale(sb[iy * B + col], yf);
+                    }
+                } else if (sub02) {
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
                         const C x = l02[t + i * TL];
                         v[i] = cmake<C>(xsign * x.x, xsign * x.y);
-                    } else {
-                        const C x = sb[(t + i * TL) * B + col];
-                        T yf = (T)1;
-                        if (q == 1 || q == 2 || q == 4) {
-                            // k_y^2 (D11), s_y (D01, D12), k_y on the Nyquist index only (D12, z Nyquist)
-                            const int iy = t + i * TL;
-                            const T ky = kytab[iy];
-                            const bool yn = iy == ynyq;
-                            yf = q == 2 ? ky * ky : ((q == 4 && znyq) == yn ? ky : (T)0);
-                        }
-                        v[i] = cmake<C>(yf * x.x, yf * x.y);
                     }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
                 }
                 __syncthreads();
                 fft_regs<C, N, +1>(v, t, sb, addr, tw);
@@ -520,14 +528,19 @@ __global__ void __launch_bounds__(N / 8 * B) y_hessian_tma(const __grid_constant
                 }
                 // weight at this point: f00 x0^2 | f01 x0 x1 | f11 x1^2 | f02 x0 s_z (1 where substituted) |
                 // f12 x1 k_z | f22 k_z^2
-                const T f = (T)(q == 0 ? h.f[0] : q == 1 ? h.f[1] : q == 2 ? h.f[3] : q == 3 ? h.f[2] : q == 4 ? h.f[4] : h.f[5]);
-                const T z3 = sub02 ? (T)1 : sz;
+                if (q == 1 || q == 2 || q == 4) {
+                    const T f = (T)(q == 1 ? h.f[1] : q == 2 ? h.f[3] : h.f[4]);
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const T x1 = x1tab[t + i * TL];
-                    const T w = q == 0 ? f * (x0 * x0) : q == 1 ? f * (x0 * x1) : q == 2 ? f * (x1 * x1)
-                              : q == 3 ? f * x0 * z3 : q == 4 ? f * x1 * kz : f * (kz * kz);
-                    acc[i] = cmake<C>(acc[i].x + w * v[i].x, acc[i].y + w * v[i].y);
+                    for (int i = 0; i < 8; i++) {
+                        const T x1 = x1tab[t + i * TL];
+                        const T w = q == 1 ? f * (x0 * x1) : q == 2 ? f * (x1 * x1) : f * x1 * kz;
+                        acc[i] = cmake<C>(acc[i].x + w * v[i].x, acc[i].y + w * v[i].y);
+                    }
+                } else {
+                    const T f = (T)(q == 0 ? h.f[0] : q == 3 ? h.f[2] : h.f[5]);
+                    const T w = q == 0 ? f * (x0 * x0) : q == 3 ? f * x0 * (sub02 ? (T)1 : sz) : f * (kz * kz);
+#pragma unroll
+                    for (int i = 0; i < 8; i++) acc[i] = cmake<C>(acc[i].x + w * v[i].x, acc[i].y + w * v[i].y);
                 }
             }
             if (store) {
