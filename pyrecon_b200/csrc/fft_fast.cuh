@@ -285,6 +285,23 @@ template <typename T, int N, int KT> struct KLine {
                                           C (&u)[8]) const {
         const T norm = (T)op.norm;
         const T l0 = (T)op.los[0], l1 = (T)op.los[1], l2 = (T)op.los[2];
+        if constexpr (KT == KOP_HESS3) {
+            // E, s_x E, k_x^2 E with E = norm delta / k^2 (s_x = k_x, 0 on the Nyquist index); o is the
+            // same for the whole CTA, so each output is one uniform branch
+            if (o == 0) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) u[i] = cscale(v[i], kp[i].a);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int ix = t + i * TL;
+                    const T kx = kval<T>(ix, dims.n[0], (T)op.fscale[0]);
+                    const T tx = nyquist(ix, dims.n[0]) ? kx : -kx;
+                    u[i] = cscale(v[i], (o == 1 ? (T)0.5 * (kx - tx) : kx * kx) * kp[i].a);
+                }
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             T re = 0, im = 0;
@@ -309,13 +326,12 @@ template <typename T, int N, int KT> struct KLine {
             } else if constexpr (KT == KOP_PSI) {
                 const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
                 im = (T)0.5 * (ko - to) * kp[i].a;
-            } else if constexpr (KT == KOP_HESS3) {
-                // E, s_x E, k_x^2 E with E = norm delta / k^2 (s_x = k_x, 0 on the Nyquist index)
-                re = (o == 0 ? (T)1 : (o == 1 ? (T)0.5 * (kx - tx) : kx * kx)) * kp[i].a;
             } else {
                 re = norm;
             }
-            u[i] = cmake<C>(re * v[i].x - im * v[i].y, re * v[i].y + im * v[i].x);
+            // the multiplier is real or imaginary: one product per component
+            if constexpr (KT == KOP_PP || KT == KOP_PSI) u[i] = cmake<C>(-(im * v[i].y), im * v[i].x);
+            else u[i] = cmake<C>(re * v[i].x, re * v[i].y);
         }
     }
 
