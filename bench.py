@@ -540,6 +540,8 @@ KERNELS = {
     'mg_jacobi_f64': ('f8', 384),
     'mg_residual': ('f4', 512),
     'smooth_real': ('f4', 256),        # truncated real-space Gaussian, radius 15 Mpc/h on 7.8 Mpc/h cells
+    'iterative_fft': ('f4', 512),      # the FFT pipeline of IterativeFFTReconstruction.run on a mesh (3 iterations,
+                                       # local line of sight), no particles: the FFT passes alone, ~6.5 GB on the device
 }
 
 
@@ -559,7 +561,15 @@ def run_kernel_arm(args):
     nm, bs, bc = _lib.i3((n, n, n)), _lib.d3([2000.] * 3), _lib.d3([2000.] * 3)
     st = _lib.stream_of(device)
     N = n ** 3
-    if args.kernel.startswith('mg_jacobi'):
+    if args.kernel == 'iterative_fft':
+        del f
+        psi4 = torch.empty((n, n, n, 4), device=device, dtype=tdt)
+        ws = torch.empty(_lib.load().prc_iterative_fft_workspace_bytes(nm, item, 1), dtype=torch.uint8, device=device)
+        base = psi4.data_ptr()
+        psis = [_lib.c_void_p(base + a * item) for a in range(3)]
+        name, nbytes = 'prc_iterative_fft_' + _lib.suffix(dtype), None
+        call = lambda: _lib.call(name, _lib.ptr(v), nm, bs, bc, 0.4, None, 3, *psis, 4, _lib.ptr(ws), ws.numel(), st)
+    elif args.kernel.startswith('mg_jacobi'):
         # two sweeps per step (v -> out -> v), so the result lands back in v without a copy
         name, nbytes = 'prc_mg_jacobi_' + _lib.suffix(dtype), 2 * 3 * N * item
         call = lambda: _lib.call(name, _lib.ptr(v), _lib.ptr(f), _lib.ptr(out), nm, bs, bc, 0.4, 0.4, 2, None, st)
@@ -577,13 +587,22 @@ def run_kernel_arm(args):
     torch.cuda.synchronize(device)
     with ClockSampler(0) as clocks:
         time.sleep(1.0)
+        _lib.profile_enable(True)
         total_ms, per = timed_loop(call, args.steps, device)
+    prof = _lib.profile_collect()
+    _lib.profile_enable(False)
     peak, peak_kind = load_peaks()
     ms = total_ms / args.steps
-    gbs = nbytes / 1e9 / (ms / 1e3)
-    print(json.dumps(dict(kernel=args.kernel, entry_point=name, nmesh=n, dtype=dtype, steps=args.steps, ms=ms,
-                          p50_ms=percentile(per, 50), algorithmic_bytes=nbytes, gbs=gbs, peak=peak, frac=gbs / peak,
-                          peak_source=peak_kind, clocks=clocks.summary())), flush=True)
+    line = dict(kernel=args.kernel, entry_point=name, nmesh=n, dtype=dtype, steps=args.steps, ms=ms,
+                p50_ms=percentile(per, 50), peak=peak, peak_source=peak_kind, clocks=clocks.summary())
+    if nbytes is not None:
+        gbs = nbytes / 1e9 / (ms / 1e3)
+        line.update(algorithmic_bytes=nbytes, gbs=gbs, frac=gbs / peak)
+    # per launched kernel: launches, ms per step, algorithmic GB/s
+    line['kernels'] = {k: dict(launches=v[0], ms_per_step=round(v[1] / args.steps, 4),
+                               gbs=round((v[2] / 1e9) / (v[1] / 1e3), 1) if v[1] > 0 else None)
+                       for k, v in sorted(prof.items())}
+    print(json.dumps(line), flush=True)
     return 0
 
 

@@ -957,7 +957,7 @@ template <typename T, int N> struct KSpaceTmaCfg {
     static constexpr int B = KSpaceCfg<T, N>::B;
     static constexpr int THREADS = KSpaceCfg<T, N>::THREADS;
     static constexpr int S = 2;
-    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, 1>::BYTES;
+    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, fast::KSpacePP<T, N, B, S, LEAN>::value ? 2 : 1>::BYTES;
 };
 
 template <typename T> struct FastXTma {
@@ -998,20 +998,33 @@ template <typename T> struct FastXTma {
 
 // Columns per tile (FP32; FP64 half as many; 0 = as the strided passes) and CTAs per SM the inverse y pass
 // of the local-line-of-sight iteration is compiled for.  Two CTAs of 8 columns per SM (64 registers a
-// thread) measured 4.30 ms per nmesh-512 reconstruction against 4.57 for one CTA of 16 columns.
+// thread) measured 4.30 ms per nmesh-512 reconstruction against 4.57 for one CTA of 16 columns, and
+// the ping-pong exchanges below 3.82.
 #ifndef PRC_HESS_B
 #define PRC_HESS_B 8
 #endif
 #ifndef PRC_HESS_MINB
 #define PRC_HESS_MINB 2
 #endif
+// PRC_HESS_PP: exchanges through a scratch tile and the consumed stage in turn (half the barriers), with
+// PRC_HESS_PP_S stages
+#ifndef PRC_HESS_PP
+#define PRC_HESS_PP 1
+#endif
+#ifndef PRC_HESS_PP_S
+#define PRC_HESS_PP_S 2
+#endif
 template <typename T, int N> struct HessTmaCfg {
     static constexpr int B0 = PRC_HESS_B == 0 ? StridedTmaB<T, N>::value
                                               : (sizeof(T) == 4 ? PRC_HESS_B : PRC_HESS_B / 2);
     static constexpr int B = (N / 8) * B0 <= 1024 ? B0 : 1024 / (N / 8);
     static constexpr int THREADS = (N / 8) * B;
-    static constexpr int S = StageCount<(int)(PRC_TMA_STAGE_KB * 1024 / fast::TileShape<T, N, B>::BYTES)>::value;
-    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, 0>::BYTES;
+    static constexpr int MINB = THREADS * PRC_HESS_MINB <= 1024 ? PRC_HESS_MINB : 1;
+    static constexpr bool PP =
+        PRC_HESS_PP != 0 && fast::TmaSmem<T, N, B, PRC_HESS_PP_S, 1>::BYTES + 2 * N * sizeof(T) <= 227 * 1024;
+    static constexpr int S = PP ? PRC_HESS_PP_S
+                                : StageCount<(int)(PRC_TMA_STAGE_KB * 1024 / fast::TileShape<T, N, B>::BYTES)>::value;
+    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, PP ? 1 : 0>::BYTES;
 };
 
 template <typename T> struct FastHessTma {
@@ -1033,7 +1046,7 @@ template <typename T> struct FastHessTma {
             s.outer = p.dims.n[0];
             s.os = (int64_t)p.dims.n[1] * p.pitch;
             s.ncols = p.nh;
-            auto kern = fast::y_hessian_tma<T, N, cfg::B, cfg::S, PRC_HESS_MINB>;
+            auto kern = fast::y_hessian_tma<T, N, cfg::B, cfg::S, cfg::MINB, cfg::PP>;
             const size_t smem = cfg::SMEM + 2 * N * sizeof(T);     // + the x1 and k_y tables
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             const int64_t ntiles = (int64_t)s.outer * ((s.ncols + cfg::B - 1) / cfg::B);

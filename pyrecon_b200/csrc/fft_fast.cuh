@@ -141,11 +141,49 @@ template <typename C, int N, int DIR, int P> struct Passes {
     }
 };
 
+// Same passes with the exchanges alternating between two buffers (s0 first) and no barrier after an
+// exchange's reads: the next write to a buffer comes one exchange later, behind that exchange's
+// barrier.  The caller orders its own accesses to s0 / s1 around the call: s0 must not be read by
+// anyone once the call starts, and neither buffer may be written after it before a barrier.
+template <typename C, int N, int R, int NS, class Addr>
+__device__ __forceinline__ void exchange_pp(C (&v)[8], int t, C* s, const Addr& addr) {
+    constexpr int T = N / 8, NB = 8 / R;
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        const int j = t + b * T;
+        const int k = j & (NS - 1);
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) s[addr(base + r * NS)] = v[b + r * NB];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = s[addr(t + i * T)];
+}
+
+template <typename C, int N, int DIR, int P> struct PassesPP {
+    template <class Addr>
+    static __device__ __forceinline__ void run(C (&v)[8], int t, C* s0, C* s1, const Addr& addr, const C* tw) {
+        constexpr int R = TwLayout<N>::radix(P);
+        constexpr int NS = ipow8(P);
+        pass_regs<C, N, R, NS, DIR>(v, t, tw + TwLayout<N>::offset(P));
+        if constexpr (P + 1 < Plan<N>::NPASS) {
+            exchange_pp<C, N, R, NS>(v, t, P % 2 == 0 ? s0 : s1, addr);
+            PassesPP<C, N, DIR, P + 1>::run(v, t, s0, s1, addr, tw);
+        }
+    }
+};
+
 // In: v[i] = x[t + i T].  Out: v[i] = X[t + i T] (unnormalised DFT, sign DIR).  tw: the pass
 // table filled by fill_pass_twiddles<C, N>.
 template <typename C, int N, int DIR, class Addr>
 __device__ __forceinline__ void fft_regs(C (&v)[8], int t, C* s, const Addr& addr, const C* tw) {
     Passes<C, N, DIR, 0>::run(v, t, s, addr, tw);
+}
+
+template <typename C, int N, int DIR, class Addr>
+__device__ __forceinline__ void fft_regs_pp(C (&v)[8], int t, C* s0, C* s1, const Addr& addr, const C* tw) {
+    PassesPP<C, N, DIR, 0>::run(v, t, s0, s1, addr, tw);
 }
 
 struct ColAddr {
@@ -300,38 +338,38 @@ template <typename T, int N, int KT> struct KLine {
                     u[i] = cscale(v[i], (o == 1 ? (T)0.5 * (kx - tx) : kx * kx) * kp[i].a);
                 }
             }
-            return;
-        }
+        } else {
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-            T re = 0, im = 0;
-            const int ix = t + i * TL;
-            const T kx = kval<T>(ix, dims.n[0], (T)op.fscale[0]);
-            const T tx = nyquist(ix, dims.n[0]) ? kx : -kx;
-            if constexpr (KT == KOP_GAUSS) {
-                re = kp[i].a;
-            } else if constexpr (KT == KOP_PP) {
-                // (i m(k) + conj(i m(k~))) / 2 with m = k_o / (k^2 (1 + beta mu^2))
-                const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
-                im = (T)0.5 * (ko * kp[i].a - to * kp[i].b) * norm;
-            } else if constexpr (KT == KOP_ITER_GLOBAL) {
-                const T kl = kx * l0 + ky * l1 + kz * l2, klt = tx * l0 + ty * l1 + tz * l2;
-                re = (T)0.5 * (kl * kl + klt * klt) * kp[i].a;
-            } else if constexpr (KT == KOP_ITER_LOCAL) {
-                const int ci = o < 3 ? 0 : (o < 5 ? 1 : 2);
-                const int cj = o < 3 ? o : (o < 5 ? o - 2 : 2);
-                const T ki = ci == 0 ? kx : (ci == 1 ? ky : kz), ti = ci == 0 ? tx : (ci == 1 ? ty : tz);
-                const T kj = cj == 0 ? kx : (cj == 1 ? ky : kz), tj = cj == 0 ? tx : (cj == 1 ? ty : tz);
-                re = (T)0.5 * (ki * kj + ti * tj) * kp[i].a;
-            } else if constexpr (KT == KOP_PSI) {
-                const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
-                im = (T)0.5 * (ko - to) * kp[i].a;
-            } else {
-                re = norm;
+            for (int i = 0; i < 8; i++) {
+                T re = 0, im = 0;
+                const int ix = t + i * TL;
+                const T kx = kval<T>(ix, dims.n[0], (T)op.fscale[0]);
+                const T tx = nyquist(ix, dims.n[0]) ? kx : -kx;
+                if constexpr (KT == KOP_GAUSS) {
+                    re = kp[i].a;
+                } else if constexpr (KT == KOP_PP) {
+                    // (i m(k) + conj(i m(k~))) / 2 with m = k_o / (k^2 (1 + beta mu^2))
+                    const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
+                    im = (T)0.5 * (ko * kp[i].a - to * kp[i].b) * norm;
+                } else if constexpr (KT == KOP_ITER_GLOBAL) {
+                    const T kl = kx * l0 + ky * l1 + kz * l2, klt = tx * l0 + ty * l1 + tz * l2;
+                    re = (T)0.5 * (kl * kl + klt * klt) * kp[i].a;
+                } else if constexpr (KT == KOP_ITER_LOCAL) {
+                    const int ci = o < 3 ? 0 : (o < 5 ? 1 : 2);
+                    const int cj = o < 3 ? o : (o < 5 ? o - 2 : 2);
+                    const T ki = ci == 0 ? kx : (ci == 1 ? ky : kz), ti = ci == 0 ? tx : (ci == 1 ? ty : tz);
+                    const T kj = cj == 0 ? kx : (cj == 1 ? ky : kz), tj = cj == 0 ? tx : (cj == 1 ? ty : tz);
+                    re = (T)0.5 * (ki * kj + ti * tj) * kp[i].a;
+                } else if constexpr (KT == KOP_PSI) {
+                    const T ko = o == 0 ? kx : (o == 1 ? ky : kz), to = o == 0 ? tx : (o == 1 ? ty : tz);
+                    im = (T)0.5 * (ko - to) * kp[i].a;
+                } else {
+                    re = norm;
+                }
+                // the multiplier is real or imaginary: one product per component
+                if constexpr (KT == KOP_PP || KT == KOP_PSI) u[i] = cmake<C>(-(im * v[i].y), im * v[i].x);
+                else u[i] = cmake<C>(re * v[i].x, re * v[i].y);
             }
-            // the multiplier is real or imaginary: one product per component
-            if constexpr (KT == KOP_PP || KT == KOP_PSI) u[i] = cmake<C>(-(im * v[i].y), im * v[i].x);
-            else u[i] = cmake<C>(re * v[i].x, re * v[i].y);
         }
     }
 

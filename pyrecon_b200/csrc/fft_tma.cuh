@@ -142,6 +142,15 @@ __global__ void __launch_bounds__(N / 8 * B) strided_tma(const __grid_constant__
 // LEAN: the forward spectrum is kept in the tile's stage (not in registers) and the per-point
 // multiplier terms are recomputed for every output, so two CTAs fit on an SM (FP32); the stage is
 // re-armed only after the tile's last output.
+// PRC_KSPACE_PP: the transforms of the k-space pass exchange through two scratch tiles in turn
+// (fft_regs_pp, one barrier per exchange), where the CTA's shared memory has room for both.
+#ifndef PRC_KSPACE_PP
+#define PRC_KSPACE_PP 1
+#endif
+template <typename T, int N, int B, int S, bool LEAN> struct KSpacePP {
+    static constexpr bool value = PRC_KSPACE_PP && !LEAN && TmaSmem<T, N, B, S, 2>::BYTES <= 227 * 1024;
+};
+
 template <typename T, int N, int B, int S, int KT, bool LEAN>
 __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 : PRC_KSPACE_MINB>::value))
     x_kspace_tma(const __grid_constant__ prc::tma::Maps maps, int nin, Specs<cplx_t<T>> out, Dims dims, int pitch,
@@ -151,8 +160,14 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 :
     constexpr int TL = N / 8;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* stages = (C*)smem_raw;
+    constexpr bool PP = KSpacePP<T, N, B, S, LEAN>::value;
+    // with an odd number of exchanges per transform, consecutive transforms would start on the buffer
+    // the previous one read last: a barrier separates them (as it does a transform without exchanges
+    // from the stage re-arm)
+    constexpr bool PP_SYNC = (Plan<N>::NPASS - 1) % 2 == 1 || Plan<N>::NPASS == 1;
     C* xbuf = stages + S * TS::ELEMS;
-    C* tw = xbuf + TS::ELEMS;
+    C* ybuf = xbuf + TS::ELEMS;                  // PP: the second scratch tile
+    C* tw = ybuf + (PP ? TS::ELEMS : 0);
     uint64_t* bars = (uint64_t*)(tw + N);
     const int tid = threadIdx.x, col = tid % B, t = tid / B;
     const ColAddr addr{B, col};
@@ -239,8 +254,14 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 :
             C v[8];
 #pragma unroll
             for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
-            __syncthreads();
-            fft_regs<C, N, -1>(v, t, sb, addr, tw);
+            if constexpr (PP) {
+                // the stage is free once every thread is past the first exchange's barrier
+                fft_regs_pp<C, N, -1>(v, t, xbuf, ybuf, addr, tw);
+                if constexpr (PP_SYNC) __syncthreads();
+            } else {
+                __syncthreads();
+                fft_regs<C, N, -1>(v, t, sb, addr, tw);
+            }
             refill();
             KLine<T, N, KT> kl;
             kl.setup(op, dims, t, iy, iz);
@@ -248,7 +269,12 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 :
             for (int o = 0; o < op.nper; o++) {
                 C u[8];
                 kl.apply(op, dims, t, o, v, u);
-                fft_regs<C, N, +1>(u, t, xbuf, addr, tw);
+                if constexpr (PP) {
+                    fft_regs_pp<C, N, +1>(u, t, xbuf, ybuf, addr, tw);
+                    if constexpr (PP_SYNC) __syncthreads();
+                } else {
+                    fft_regs<C, N, +1>(u, t, xbuf, addr, tw);
+                }
                 if (iz < nh) {
                     C* go = out.p[a.bi * op.nper + o] + off;
 #pragma unroll
@@ -404,7 +430,10 @@ struct HessGeom {
     const void* l02;
 };
 
-template <typename T, int N, int B, int S, int MINB>
+// PP: the transforms exchange through a scratch tile and the consumed stage in turn (fft_regs_pp), with
+// one barrier per exchange; a stage is then re-armed at the next unit's barrier, once every thread has
+// finished with it, so S - 1 units are in flight ahead of the one being transformed.
+template <typename T, int N, int B, int S, int MINB, bool PP>
 __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, MINB>::value)) y_hessian_tma(const __grid_constant__ prc::tma::Maps maps,
                                                            Specs<cplx_t<T>> out, Strided s, HessGeom h) {
     typedef cplx_t<T> C;
@@ -412,7 +441,8 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, MINB>::val
     constexpr int TL = N / 8;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* stages = (C*)smem_raw;
-    C* tw = stages + S * TS::ELEMS;
+    C* xscr = stages + S * TS::ELEMS;          // PP: the exchange scratch tile
+    C* tw = xscr + (PP ? TS::ELEMS : 0);
     uint64_t* bars = (uint64_t*)(tw + N);
     T* x1tab = (T*)(bars + S);     // x1 and k_y of every y index (2 N values after the barriers)
     T* kytab = x1tab + N;
@@ -469,10 +499,17 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, MINB>::val
             for (int j = 0; j < nterm; j++, u++) {
                 const int st = (int)(u % S);
                 const bool ok = prc::tma::wait(&bars[st], (uint32_t)((u / S) & 1));
-                if (__syncthreads_or(!ok)) {
+                const bool failed = __syncthreads_or(!ok);
+                if (PP && !failed && tid == 0 && u > 0) {
+                    // every thread is past unit u - 1: its stage takes unit u - 1 + S
+                    prc::tma::fence_proxy_async();
+                    issue(u - 1 + S);
+                }
+                if (failed) {
                     if (tid == 0) {
                         atomicOr(&prc::g_fault, prc::tma::FAULT_WAIT_TIMEOUT);
-                        for (int d = 0; d < S; d++) {
+                        // units u .. u + S - 1 (u + S - 2 under PP) were issued and may be in flight
+                        for (int d = 0; d < (PP ? S - 1 : S); d++) {
                             const int64_t uu = u + d;
                             if ((int64_t)blockIdx.x + (uu / 6) * gridDim.x >= ntiles) break;
                             prc::tma::wait(&bars[uu % S], (uint32_t)((uu / S) & 1));
@@ -511,11 +548,17 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, MINB>::val
 #pragma unroll
                     for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
                 }
-                __syncthreads();
-                fft_regs<C, N, +1>(v, t, sb, addr, tw);
-                if (tid == 0) {
-                    prc::tma::fence_proxy_async();
-                    issue(u + S);
+                if constexpr (PP) {
+                    // scratch first: the stage is written only by the second exchange, behind the first
+                    // exchange's barrier, when every thread has read its points from it
+                    fft_regs_pp<C, N, +1>(v, t, xscr, sb, addr, tw);
+                } else {
+                    __syncthreads();
+                    fft_regs<C, N, +1>(v, t, sb, addr, tw);
+                    if (tid == 0) {
+                        prc::tma::fence_proxy_async();
+                        issue(u + S);
+                    }
                 }
                 if (q == 1 && q01 != nullptr && iz < s.ncols) {
                     // D01 at the x and y Nyquist indices: q01[iz] (-1)^(x + y)
