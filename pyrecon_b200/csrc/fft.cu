@@ -922,7 +922,7 @@ template <typename T, int N> struct StridedTmaCfg {
     static constexpr int B = StridedTmaB<T, N>::value;
     static constexpr int THREADS = (N / 8) * B;
     static constexpr int S = StageCount<(int)(PRC_TMA_STAGE_KB * 1024 / fast::TileShape<T, N, B>::BYTES)>::value;
-    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, 0>::BYTES;
+    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, fast::StridedPP<T, N, B, S>::value ? 1 : 0>::BYTES;
 };
 
 template <typename T, int DIR> struct FastStridedTma {

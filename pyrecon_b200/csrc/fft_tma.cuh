@@ -73,15 +73,26 @@ template <typename T, int N, int B, int S, int EXTRA> struct TmaSmem {
     static constexpr size_t BYTES = TILES + TW + S * sizeof(uint64_t);
 };
 
+// PRC_STRIDED_PP: the strided passes exchange through a scratch tile, then the consumed stage
+// (fft_regs_pp), where shared memory has room for the scratch tile.
+#ifndef PRC_STRIDED_PP
+#define PRC_STRIDED_PP 1
+#endif
+template <typename T, int N, int B, int S> struct StridedPP {
+    static constexpr bool value = PRC_STRIDED_PP && TmaSmem<T, N, B, S, 1>::BYTES <= 227 * 1024;
+};
+
 template <typename T, int N, int B, int S, int DIR>
 __global__ void __launch_bounds__(N / 8 * B) strided_tma(const __grid_constant__ prc::tma::Maps maps,
                                                          Specs<cplx_t<T>> data, int nbatch, Strided s, int axis) {
     typedef cplx_t<T> C;
     typedef TileShape<T, N, B> TS;
     constexpr int TL = N / 8;
+    constexpr bool PP = StridedPP<T, N, B, S>::value;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* stages = (C*)smem_raw;
-    C* tw = stages + S * TS::ELEMS;
+    C* xscr = stages + S * TS::ELEMS;           // PP: the exchange scratch tile
+    C* tw = xscr + (PP ? TS::ELEMS : 0);
     uint64_t* bars = (uint64_t*)(tw + N);
     const int tid = threadIdx.x, col = tid % B, t = tid / B;
     const ColAddr addr{B, col};
@@ -121,8 +132,14 @@ __global__ void __launch_bounds__(N / 8 * B) strided_tma(const __grid_constant__
         C v[8];
 #pragma unroll
         for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
-        __syncthreads();
-        fft_regs<C, N, DIR>(v, t, sb, addr, tw);   // ends with a barrier when it exchanged through sb
+        if constexpr (PP) {
+            // the second exchange goes through the stage: a barrier after the last reads, before its re-arm
+            fft_regs_pp<C, N, DIR>(v, t, xscr, sb, addr, tw);
+            __syncthreads();
+        } else {
+            __syncthreads();
+            fft_regs<C, N, DIR>(v, t, sb, addr, tw);   // ends with a barrier when it exchanged through sb
+        }
         if (tid == 0) {
             const int64_t next = tile + (int64_t)S * gridDim.x;
             if (next < ntiles) {
@@ -290,12 +307,18 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 :
 // pitch), copied into stage u % S; a stage is re-armed with unit u + S once its rows have been read
 // into registers.  Units are consumed in the order z_c2r_body asks for them: inputs 0 .. nin - 1 of
 // each tile, tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// PRC_C2R_PP: the row transforms exchange through two row buffers in turn (fft_regs_pp); the barrier
+// before a stage is re-armed also orders each row's first exchange after the previous row's reads.
+#ifndef PRC_C2R_PP
+#define PRC_C2R_PP 1
+#endif
 template <typename T, int M, int ROWS, int S> struct TmaRows {
     typedef cplx_t<T> C;
     static constexpr int Q = (int)(32 / sizeof(C));
     static constexpr int PS = (M + 1 + Q - 1) / Q * Q;
     static constexpr int STAGE = ROWS * PS;
     C* stages;
+    C* buf2 = nullptr;       // PRC_C2R_PP: the second row buffer
     uint64_t* bars;
     const Specs<C>& in;
     int nin;
@@ -350,8 +373,10 @@ template <typename T, int M, int ROWS, int S> struct TmaRows {
             issue(next + S);
         }
         next++;
-        fft_regs<C, M, +1>(v, t, buf, addr, tw);
+        if constexpr (PRC_C2R_PP) fft_regs_pp<C, M, +1>(v, t, buf, buf2 + (buf - buf1), addr, tw);
+        else fft_regs<C, M, +1>(v, t, buf, addr, tw);
     }
+    C* buf1 = nullptr;       // PRC_C2R_PP: the first row buffer (buf2 mirrors its offsets)
 
     // End of a tile: if any thread's wait ran out, thread 0 waits (bounded) for the copies it issued
     // and has not seen land, and every thread leaves the kernel.
@@ -370,7 +395,8 @@ template <typename T, int M, int ROWS, int S> struct C2RTmaSmem {
     typedef cplx_t<T> C;
     static constexpr size_t STAGES = (size_t)S * TmaRows<T, M, ROWS, S>::STAGE * sizeof(C);
     static constexpr size_t BUF = (size_t)ROWS * row_stride(M) * sizeof(C);
-    static constexpr size_t BYTES = STAGES + BUF + (size_t)(2 * M + 1) * sizeof(C) + 8 + S * sizeof(uint64_t);
+    static constexpr size_t BYTES =
+        STAGES + (PRC_C2R_PP ? 2 : 1) * BUF + (size_t)(2 * M + 1) * sizeof(C) + 8 + S * sizeof(uint64_t);
 };
 
 template <typename T, int M, int ROWS, int ET, int S>
@@ -381,7 +407,8 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* stages = (C*)smem_raw;
     C* buf = stages + S * Rows::STAGE;
-    C* tw = buf + ROWS * row_stride(M);
+    C* buf2 = buf + ROWS * row_stride(M);        // PRC_C2R_PP: the second row buffer
+    C* tw = buf2 + (PRC_C2R_PP ? ROWS * row_stride(M) : 0);
     C* wk = tw + M;
     uint64_t* bars = (uint64_t*)(((uintptr_t)(wk + M + 1) + 7) & ~(uintptr_t)7);
     if (threadIdx.x == 0) {
@@ -396,6 +423,8 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
         return;
     }
     Rows src(stages, bars, in, nin, (int64_t)dims.n[0] * dims.n[1]);
+    src.buf1 = buf;
+    src.buf2 = buf2;
     src.start();
     z_c2r_body<T, M, ROWS, ET>(src, nin, dims, e, tw, wk, buf);
 }
