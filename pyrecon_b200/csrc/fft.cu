@@ -784,14 +784,10 @@ template <typename T, typename TIN> struct FastZR2C {
         static int run(RealsIn ri, Specs<cplx_t<T>> so, int nb, int64_t rows, int pitch, double bytes, cudaStream_t st) {
             typedef RowCfg<T, M> cfg;
             auto kern = fast::z_r2c<T, TIN, M, cfg::ROWS>;
-            // the ping-pong form holds a second set of row buffers
-            const size_t smem = cfg::SMEM + (fast::R2CPP<M>::value ? (size_t)cfg::ROWS * fast::row_stride(M) *
-                                                                          sizeof(cplx_t<T>)
-                                                                    : 0);
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg::SMEM);
             int64_t ntiles = ((rows + cfg::ROWS - 1) / cfg::ROWS) * nb;
             PRC_LAUNCH_B("fft_z_r2c", st, bytes,
-                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, smem, st>>>(ri, so, nb, rows, pitch));
+                         kern<<<fast_grid(ntiles, cfg::THREADS), cfg::THREADS, cfg::SMEM, st>>>(ri, so, nb, rows, pitch));
             PRC_CHECK_LAUNCH();
             return PRC_OK;
         }

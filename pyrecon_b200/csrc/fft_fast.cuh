@@ -448,30 +448,15 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE
 // ---------------------------------------------------------------------------------------------
 // z pass, forward r2c: rows of n2 = 2M reals, M-point FFT of the packed pairs, then unpack.
 // CTA = (M / 8) x ROWS threads.
-// PRC_R2C_PP (transforms with an even number of exchanges): two row buffers A, B; a row exchanges
-// through A, B, A, ..., B, publishes its spectrum in A behind the last exchange's barrier and unpacks
-// from it behind one more; the next row swaps the roles, so its first exchange (into B) and its second
-// (into A) each come behind a barrier that follows the last reads of that buffer.  Three barriers a
-// row instead of six.
 // ---------------------------------------------------------------------------------------------
-#ifndef PRC_R2C_PP
-#define PRC_R2C_PP 1
-#endif
-template <int M> struct R2CPP {
-    static constexpr int NEX = Plan<M>::NPASS - 1;
-    static constexpr bool value = PRC_R2C_PP && NEX >= 2 && NEX % 2 == 0;
-};
-
 template <typename T, typename TIN, int M, int ROWS>
 __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T>> out, int nbatch, int64_t rows, int pitch) {
     typedef cplx_t<T> C;
     constexpr int TL = M / 8, N2 = 2 * M, RS = row_stride(M);
-    constexpr bool PP = R2CPP<M>::value;
     extern __shared__ unsigned char smem_raw[];
     C* tw = (C*)smem_raw;                 // pass table of the M-point transform (M entries)
     C* wk = tw + M;                       // w_{n2}^k, k < M + 1, for the real-FFT unpack
     C* buf = wk + M + 1;                  // ROWS * RS
-    C* buf2 = buf + ROWS * RS;            // PP: the second row buffers
     fill_pass_twiddles<C, M>(tw);
     fill_roots(wk, M + 1, N2);
     __syncthreads();
@@ -479,8 +464,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
     const RowAddr addr{line * RS};
     const int64_t tiles_per = (rows + ROWS - 1) / ROWS;
     const int64_t ntiles = tiles_per * nbatch;
-    int64_t it = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int bi = (int)(tile / tiles_per);
         const int64_t row = (tile % tiles_per) * ROWS + line;
         const bool ok = row < rows;
@@ -498,25 +482,17 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
                 v[i] = cmake<C>((T)x.x, (T)x.y);
             }
         }
-        C* pub = buf;
-        if constexpr (PP) {
-            C* a = (it & 1) ? buf2 : buf;
-            C* b = (it & 1) ? buf : buf2;
-            fft_regs_pp<C, M, -1>(v, t, a, b, addr, tw);
-            pub = a;
-        } else {
-            fft_regs<C, M, -1>(v, t, buf, addr, tw);
-        }
+        fft_regs<C, M, -1>(v, t, buf, addr, tw);
         // unpack needs Z[M - k]: publish Z, then combine
 #pragma unroll
-        for (int i = 0; i < 8; i++) pub[addr(t + i * TL)] = v[i];
+        for (int i = 0; i < 8; i++) buf[addr(t + i * TL)] = v[i];
         __syncthreads();
         C* dst = out.p[bi] + row * pitch;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             const int k = t + i * TL;
             const C zk = v[i];
-            const C zc = cconj(pub[addr(k == 0 ? 0 : M - k)]);
+            const C zc = cconj(buf[addr(k == 0 ? 0 : M - k)]);
             const C e = cscale(cadd(zk, zc), (T)0.5);
             const C o = cmul_i(cscale(csub(zk, zc), (T)0.5), -1);
             const C x = cadd(e, cmul(wk[k], o));
@@ -526,7 +502,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
             const C z0 = v[0];
             dst[M] = cmake<C>(z0.x - z0.y, (T)0);
         }
-        if constexpr (!PP) __syncthreads();
+        __syncthreads();
     }
 }
 
