@@ -156,9 +156,6 @@ __global__ void __launch_bounds__(N / 8 * B) strided_tma(const __grid_constant__
     }
 }
 
-// LEAN: the forward spectrum is kept in the tile's stage (not in registers) and the per-point
-// multiplier terms are recomputed for every output, so two CTAs fit on an SM (FP32); the stage is
-// re-armed only after the tile's last output.
 // PRC_KSPACE_PP: the transforms of the k-space pass exchange through two scratch tiles in turn
 // (fft_regs_pp, one barrier per exchange), where the CTA's shared memory has room for both.
 #ifndef PRC_KSPACE_PP
@@ -168,6 +165,9 @@ template <typename T, int N, int B, int S, bool LEAN> struct KSpacePP {
     static constexpr bool value = PRC_KSPACE_PP && !LEAN && TmaSmem<T, N, B, S, 2>::BYTES <= 227 * 1024;
 };
 
+// LEAN: the forward spectrum is kept in the tile's stage (not in registers) and the per-point
+// multiplier terms are recomputed for every output, so two CTAs fit on an SM (FP32); the stage is
+// re-armed only after the tile's last output.
 template <typename T, int N, int B, int S, int KT, bool LEAN>
 __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 : PRC_KSPACE_MINB>::value))
     x_kspace_tma(const __grid_constant__ prc::tma::Maps maps, int nin, Specs<cplx_t<T>> out, Dims dims, int pitch,
@@ -318,7 +318,8 @@ template <typename T, int M, int ROWS, int S> struct TmaRows {
     static constexpr int PS = (M + 1 + Q - 1) / Q * Q;
     static constexpr int STAGE = ROWS * PS;
     C* stages;
-    C* buf2 = nullptr;       // PRC_C2R_PP: the second row buffer
+    C* buf1 = nullptr;       // PRC_C2R_PP: the row buffer the caller passes, and the second one
+    C* buf2 = nullptr;       // (same layout, so a row's offset in buf1 is its offset in buf2)
     uint64_t* bars;
     const Specs<C>& in;
     int nin;
@@ -376,7 +377,6 @@ template <typename T, int M, int ROWS, int S> struct TmaRows {
         if constexpr (PRC_C2R_PP) fft_regs_pp<C, M, +1>(v, t, buf, buf2 + (buf - buf1), addr, tw);
         else fft_regs<C, M, +1>(v, t, buf, addr, tw);
     }
-    C* buf1 = nullptr;       // PRC_C2R_PP: the first row buffer (buf2 mirrors its offsets)
 
     // End of a tile: if any thread's wait ran out, thread 0 waits (bounded) for the copies it issued
     // and has not seen land, and every thread leaves the kernel.
