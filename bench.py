@@ -13,9 +13,19 @@ own timing of a reconstruction goes from the constructor to both read_shifted_po
   the catalogues host->device and the shifted positions device->host.
 * roofline: the kernel with the largest device time in the timed region, its compulsory bytes
   (reported by the library per launch) / its event-timed duration, against MEASURED_PEAKS.json.
-* cpu_baseline / --impl reference: the reference's CPU path (its C kernels compiled from source
-  into oracle/_ref with OpenMP on all host cores, numpy glue, pocketfft with all cores) on a
-  1/8-scale sample of the workload (nmesh/2 per axis, 1/8 of the particles), scaled x8.
+* shift_err_mpc: max |shifted positions - those of the all-FP64 mode (dtype f8) of the same
+  reconstruction| over data and randoms, checked outside the timed region (the FP64 mode is pinned
+  to the FP64 oracle by the parity tests at nmesh 128-512).
+* baseline_metric: the metric's comparison with the plain GPU path: 64 batched periodic mocks and
+  500 Poisson-arriving requests through the request loop against the same requests run one at a time
+  (skipped with --no-multi or when N > 1).
+* --impl reference: the reference package itself (pip-installed unmodified into baseline/_ref, its C
+  kernels built from source with OpenMP on all host cores) running the full workload through its own
+  classes, fft_engine 'fftw' when pyfftw imports, else 'numpy'; 1 warm-up + 2 timed reconstructions
+  at most (each a few minutes on the CPU).
+* cpu_baseline (GPU arm): the reference's C kernels (oracle/_ref, OpenMP on all host cores) driven by
+  the oracle's restatement of its numpy glue with pocketfft on all cores, on a 1/8-scale sample of the
+  workload (nmesh/2 per axis, 1/8 of the particles), scaled x8.
 """
 import os
 import sys
@@ -72,15 +82,17 @@ MULTI_WORKLOADS = {
                                                                     'MultiGridReconstruction'],
                           nmesh=[128, 192, 256], ndata=(300_000, 2_000_000), randoms_factor=0, boxsize=1000.,
                           boxcenter=500., los='z', wrap=True, dtype='f4', slots=2, max_batch=8),
-    # BASELINE config: Poisson arrivals at 20 req/s, the three algorithms, nmesh in {128, 256, 384, 512},
-    # 0.5M-8M data with 4x randoms, 150 GB admission budget (100 requests instead of 500: same mix, a
-    # run that fits the bench's time)
-    'serving': dict(kind='serving', nrequests=100, rate=20., algorithms=['MultiGridReconstruction',
+    # BASELINE config: 500 requests with Poisson arrivals at 20 req/s, the three algorithms, nmesh in
+    # {128, 256, 384, 512}, 0.5M-8M data with 4x randoms, 150 GB admission budget
+    'serving': dict(kind='serving', nrequests=500, rate=20., algorithms=['MultiGridReconstruction',
                                                                         'IterativeFFTReconstruction',
                                                                         'PlaneParallelFFTReconstruction'],
                     nmesh=[128, 256, 384, 512], ndata=(500_000, 8_000_000), randoms_factor=4, boxsize=2000.,
                     boxcenter=2000., los=None, wrap=False, dtype='f4', slots=4, max_batch=8, hbm_budget=150e9),
 }
+
+for _name, _w in MULTI_WORKLOADS.items():
+    _w['name'] = _name
 
 
 def workload_name(w):
@@ -139,27 +151,101 @@ def reference_sample(w, seed=0):
     return dt, info
 
 
+REFERENCE_PACKAGE = os.path.join(ROOT, 'baseline', '_ref')
+
+
+def import_reference_package():
+    """(pyrecon, None) from the unmodified reference installed in baseline/_ref, or (None, why)."""
+    if not os.path.isfile(os.path.join(REFERENCE_PACKAGE, 'pyrecon', '__init__.py')):
+        return None, 'baseline/_ref holds no install of the reference (pip install --target baseline/_ref)'
+    if REFERENCE_PACKAGE not in sys.path:
+        sys.path.insert(0, REFERENCE_PACKAGE)
+    try:
+        import pyrecon
+    except Exception as exc:       # the reference's own import failing (missing C libraries, ...)
+        return None, 'the reference in baseline/_ref does not import: {}'.format(exc)
+    if not os.path.abspath(pyrecon.__file__).startswith(REFERENCE_PACKAGE):
+        return None, 'pyrecon imported from {}, not baseline/_ref'.format(pyrecon.__file__)
+    return pyrecon, None
+
+
+def reference_catalogs(w):
+    """The GPU arm's catalogues of rank 0 (same generators and seeds, drawn on the GPU when there is one),
+    as numpy arrays."""
+    import torch
+    if torch.cuda.is_available():
+        cats = make_catalogs(w, torch.device('cuda', 0), 0)
+        out = [None if t is None else t.cpu().numpy() for t in cats]
+        del cats
+        torch.cuda.empty_cache()
+        return out, 'the GPU arm\'s catalogues (rank 0 seeds)'
+    from pyrecon_b200 import mocks
+    data = mocks.lognormal_positions_numpy(w['ndata'], w['nmesh'], w['boxsize'], w['boxcenter'], seed=2003,
+                                           field_seed=1003, dtype=w['pos_dtype'])
+    randoms = mocks.uniform_positions_numpy(w['nrandoms'], w['boxsize'], w['boxcenter'], seed=3003,
+                                            dtype=w['pos_dtype'])
+    wd = wr = None
+    if w['weights'] is not None:
+        wd = mocks.weights_numpy(w['ndata'], *w['weights'], seed=4003, dtype=w['pos_dtype'])
+        wr = mocks.weights_numpy(w['nrandoms'], *w['weights'], seed=4004, dtype=w['pos_dtype'])
+    return [data, wd, randoms, wr], 'numpy draws of the same distributions (no GPU)'
+
+
 def run_reference_arm(args, w):
+    """The reference's own classes on the full workload, timed from the constructor to both
+    read_shifted_positions calls (catalogue generation excluded), on all host cores."""
     rank, _, world = dist_env()
     if rank != 0:
         return 0
-    times, info = [], None
-    budget = float(os.environ.get('PRC_REFERENCE_BUDGET_S', 150.))
+    pyrecon, why = import_reference_package()
+    if pyrecon is None:
+        print(json.dumps({'impl': 'reference', 'unavailable': why}), flush=True)
+        return 0
+    cores = os.cpu_count() or 1
+    try:
+        import pyfftw  # noqa: F401
+        engine = 'fftw'
+    except ImportError:
+        engine = 'numpy'
+    (data, wd, randoms, wr), source = reference_catalogs(w)
+    Cls = getattr(pyrecon, w['algorithm'])
+
+    def one():
+        t0 = time.perf_counter()
+        rec = Cls(f=0.8, bias=2., los=w['los'], nmesh=w['nmesh'], boxsize=w['boxsize'], boxcenter=w['boxcenter'],
+                  dtype=w['dtype'], fft_engine=engine, nthreads=cores)
+        rec.assign_data(data, wd)
+        rec.assign_randoms(randoms, wr)
+        rec.set_density_contrast(smoothing_radius=15., **w.get('density_kwargs', {}))
+        rec.run(**w['run_kwargs'])
+        rec.read_shifted_positions(data)
+        rec.read_shifted_positions(randoms)
+        return time.perf_counter() - t0
+
+    budget = float(os.environ.get('PRC_REFERENCE_BUDGET_S', 1500.))
+    nwarm, nsteps = min(args.warmup, 1), max(1, min(args.steps, 2))
     t_start = time.perf_counter()
-    for i in range(args.warmup + args.steps):
-        dt, info = reference_sample(w, seed=i)
-        if i >= args.warmup:
-            times.append(dt * info['scale'])
-        if time.perf_counter() - t_start > budget and len(times) >= 1:
+    warm = [one() for _ in range(nwarm)]
+    times = []
+    for _ in range(nsteps):
+        last = (times or warm or [0.])[-1]
+        if times and time.perf_counter() - t_start + last > budget:
             break
+        times.append(one())
     sec = statistics.median(times)
     value = 1. / sec
-    line = dict(metric=METRIC, value=value, unit='recons/s', n_gpus=args.gpus, steps=len(times), warmup=args.warmup,
-                ms_per_step=sec * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype=w['dtype'],
-                data='synthetic seeded lognormal data + uniform randoms',
-                config=dict(workload=workload_name(w)), impl='reference',
-                cpu_baseline=dict(value=value, unit='recons/s', cores=info['cores'], kind=info['kind'],
-                                  sample=info['sample']),
+    sample = ('the reference package {} (baseline/_ref, unmodified) through its {} on the full workload, '
+              'fft_engine={!r}{}, nthreads={} (OpenMP C kernels), {}; {} warm-up + {} timed reconstructions, '
+              'median').format(pyrecon.__version__, w['algorithm'], engine,
+                               '' if engine == 'fftw' else ' (pyfftw absent: single-threaded numpy FFTs)', cores,
+                               source, len(warm), len(times))
+    line = dict(metric=METRIC, value=value, unit='recons/s', n_gpus=args.gpus, steps=len(times), warmup=len(warm),
+                steps_requested=args.steps, warmup_requested=args.warmup, ms_per_step=sec * 1e3,
+                step_seconds=[round(t, 2) for t in times], warmup_seconds=[round(t, 2) for t in warm],
+                higher_is_better=True, scaling='weak', vs_baseline=None, dtype=w['dtype'],
+                data='synthetic seeded lognormal data + uniform randoms', config=dict(workload=workload_name(w)),
+                impl='reference', same_config=True,
+                cpu_baseline=dict(value=value, unit='recons/s', cores=cores, kind='reference', sample=sample),
                 e2e=dict(value=value, unit='recons/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
     return 0
@@ -178,12 +264,13 @@ class ClockSampler(object):
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, 'gpurun_out', 'clocks_rank{}.csv'.format(index))
+        self.path = None
 
     def __enter__(self):
+        import tempfile
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.fh = open(self.path, 'w')
+            fd, self.path = tempfile.mkstemp(prefix='prc_clocks_rank{}_'.format(self.index), suffix='.csv')
+            self.fh = os.fdopen(fd, 'w')
             self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.FIELDS,
                                           '--format=csv,noheader,nounits', '-lms', '200'], stdout=self.fh,
                                          stderr=subprocess.DEVNULL)
@@ -201,11 +288,15 @@ class ClockSampler(object):
             self.fh.close()
 
     def summary(self):
-        if self.proc is None or not os.path.isfile(self.path):
+        if self.proc is None or self.path is None or not os.path.isfile(self.path):
             return dict(sm_mhz=None, sm_max_mhz=None, reasons=['nvidia-smi unavailable'])
         sms, maxs, reasons = [], [], set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        for line in open(self.path):
+        with open(self.path) as fh:
+            lines = fh.readlines()
+        os.remove(self.path)
+        self.path = None
+        for line in lines:
             parts = [p.strip() for p in line.split(',')]
             if len(parts) < 9:
                 continue
@@ -333,8 +424,9 @@ def run_gpu_arm(args, w):
 
     data, wd, randoms, wr = make_catalogs(w, device, rank)
     step = lambda: reconstruct(w, device, data, wd, randoms, wr, check=False)
-    # correctness of the measured configuration: a checked run first (raises on bad inputs)
-    reconstruct(w, device, data, wd, randoms, wr, check=True)
+    # correctness of the measured configuration: a checked run first (raises on bad inputs), whose shifted
+    # positions are compared with the all-FP64 mode after the timed region
+    checked = reconstruct(w, device, data, wd, randoms, wr, check=True)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(device)
@@ -356,6 +448,18 @@ def run_gpu_arm(args, w):
     total_ms = max_over_ranks(total_ms)
     ms_per_step = total_ms / args.steps
     value = world * args.steps / (total_ms / 1e3)
+
+    # --- accuracy of the measured configuration: the all-FP64 mode on the same catalogues ---
+    shift_err = None
+    if w['dtype'] == 'f4' and not args.no_check:
+        d8 = lambda t: None if t is None else t.double()
+        ref = reconstruct(dict(w, dtype='f8'), device, d8(data), d8(wd), d8(randoms), d8(wr), check=False)
+        errs = [float((a.double() - b).abs().max()) for a, b in zip(checked, ref)]
+        shift_err = dict(max_abs=max(errs), data=errs[0], randoms=errs[1], unit='Mpc/h', tolerance=1e-3,
+                         vs='the all-FP64 mode (dtype f8) of the same reconstruction on the same catalogues; the '
+                            'FP64 mode is pinned to the FP64 oracle by the parity tests at nmesh 128-512')
+        del ref
+    del checked
 
     # --- end to end through the public API from pinned host memory ---
     e2e = None
@@ -389,6 +493,15 @@ def run_gpu_arm(args, w):
                     'scaled to this launch'.format(ratio),
                     bytes_per_launch=kbytes / nl, launch_ms=kms / nl, peak_source=peak_kind + ' (MEASURED_PEAKS.json hbm_gbs)')
 
+    # --- the metric's comparison with the plain GPU path: many requests through the request loop ---
+    baseline_metric = None
+    if world == 1 and not args.no_multi:
+        baseline_metric = {}
+        for name in ['batched_mocks', 'serving']:
+            m = multi_workload(args, MULTI_WORKLOADS[name], device, rank)
+            keep = ['served_vs_plain', 'served', 'plain', 'config', 'gpu_launches', 'clocks']
+            baseline_metric[name] = {k: m[k] for k in keep}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sec, info = reference_sample(w)
@@ -403,6 +516,7 @@ def run_gpu_arm(args, w):
                                 l2='inputs larger than L2 (positions {:.0f} MB)'.format(
                                     (data.numel() + randoms.numel()) * data.element_size() / 1e6)),
                     latency_ms=dict(p50=percentile(per_step, 50), p99=percentile(per_step, 99)),
+                    shift_err_mpc=shift_err, baseline_metric=baseline_metric,
                     e2e=e2e, roofline=roofline, cpu_baseline=cpu, gpu_launches=int(launches),
                     clocks=clocks.summary(), kernels=kernels)
         print(json.dumps(line), flush=True)
@@ -446,18 +560,26 @@ def multi_requests(w, device, seed=0):
 
 
 def run_multi_arm(args, w):
+    import torch
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    line = multi_workload(args, w, torch.device('cuda', local_rank), rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def multi_workload(args, w, device, rank):
     """Throughput and latency of a multi-request workload: the plain path (requests one after the other on one
     stream) and the request loop (continuous batching on `slots` streams; for 'serving', submitted at Poisson
     arrival times, where throughput is bounded by the arrival rate and the comparison is the latency against
     the plain path serving the same arrivals first come, first served).  Both warmed up by one pass over the
-    requests.  Wall clock with the device synchronised on both sides."""
+    requests.  Wall clock with the device synchronised on both sides.  Returns the JSON line."""
     import torch
     import numpy as np
     from pyrecon_b200 import _lib
     from pyrecon_b200.serving import ReconstructionServer, run_request
-    rank, local_rank, world = dist_env()
-    torch.cuda.set_device(local_rank)
-    device = torch.device('cuda', local_rank)
+    world = dist_env()[2]
     reqs = multi_requests(w, device, seed=rank)
     # warm-up of the plain path: every request once (kernels, multigrid graphs, allocator)
     for r in reqs:
@@ -513,11 +635,13 @@ def run_multi_arm(args, w):
     launches = _lib.launch_count() - launches0
     pct = lambda xs, q: 1e3 * sorted(xs)[min(len(xs) - 1, int(round(q / 100. * (len(xs) - 1))))]
     n = len(reqs)
-    if rank == 0:
+    del reqs
+    torch.cuda.empty_cache()
+    if True:
         line = dict(metric=METRIC, value=n / served_s, unit='recons/s', n_gpus=world, steps=1, warmup=1,
                     ms_per_step=served_s * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None,
                     dtype=w['dtype'], data='synthetic: seeded lognormal catalogues, one per nmesh, requests take prefixes',
-                    config=dict(workload=args.workload, requests=n, slots=w['slots'], max_batch=w.get('max_batch', 1),
+                    config=dict(workload=w['name'], requests=n, slots=w['slots'], max_batch=w.get('max_batch', 1),
                                 arrivals='poisson {:g}/s'.format(w['rate']) if w['kind'] == 'serving' else 'all at once',
                                 nmesh=w['nmesh'], algorithms=w['algorithms'], timing='wall clock, device synchronised'),
                     served=dict(recons_per_s=n / served_s, p50_ms=stats['p50_ms'], p99_ms=stats['p99_ms'],
@@ -528,8 +652,7 @@ def run_multi_arm(args, w):
                                top_kernels={k: round(v[1], 2) for k, v in top}),
                     served_vs_plain=(n / served_s) / (n / plain_s), gpu_launches=int(launches),
                     clocks=clocks.summary())
-        print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # Single-kernel timings through the C ABI (one launch per step, inputs above L2), for the per-kernel
@@ -615,6 +738,8 @@ def main(argv=None):
     ap.add_argument('--workload', default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(MULTI_WORKLOADS))
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-check', action='store_true', help='skip the FP64 comparison of the checked run')
+    ap.add_argument('--no-multi', action='store_true', help='skip the batched and served comparison with the plain path')
     ap.add_argument('--kernel', default=None, choices=sorted(KERNELS),
                     help='time one kernel through the C ABI instead of a workload')
     args = ap.parse_args(argv)

@@ -250,6 +250,12 @@ PRC_API prc_status_t prc_ifftp_read_f64(const double *psi4, const int32_t nmesh[
 #define PRC_FAULT_SMEM_ALIGN 2u
 PRC_API unsigned int prc_device_fault_flags(int reset);
 
+/* Test hook of the failure path (no counterpart in the reference): one CTA arms its transaction
+ * barrier for bytes that no copy delivers (none is issued, so nothing is ever in flight), waits at
+ * most limit_ns (0 < limit_ns <= 1 s) through the same bounded wait the FFT kernels use, sets
+ * PRC_FAULT_WAIT_TIMEOUT in the fault word and returns; out (device int) = 1 when the wait gave up. */
+PRC_API int prc_debug_wait_timeout(int64_t limit_ns, int* out, void* stream);
+
 /* ------------------------------------------------------------------------------------------
  * FFTs and the k-space steps (the numpy / pyfftw sites of pyrecon/mesh.py:974-1118 and the
  * algorithm modules).  Forward transforms are unnormalised; inverse ones divide by n0*n1*n2,

@@ -39,12 +39,17 @@ class OracleError(Exception):
 
 
 def build(reference_src=None):
-    """Compile the oracle C restatement and, when the reference sources are present, the reference kernels."""
+    """Compile the oracle C restatement and, given the reference's ``src/`` directory (argument, or the
+    environment variable PYRECON_REFERENCE_SRC), the reference kernels into oracle/_ref."""
     import subprocess
     subprocess.run(['make', '-s', '-C', HERE, 'all'], check=True)
-    src = reference_src or '/root/reference/src'
-    if os.path.isdir(src):
-        subprocess.run(['make', '-s', '-C', HERE, 'ref', 'REFERENCE_SRC={}'.format(src)], check=True)
+    src = reference_src or os.environ.get('PYRECON_REFERENCE_SRC')
+    if src is None:
+        print('oracle: reference kernels not built (no reference src/ given: set PYRECON_REFERENCE_SRC)')
+        return
+    if not os.path.isfile(os.path.join(src, 'mesh.c')):
+        raise OracleError('{} is not the reference\'s src/ directory (no mesh.c)'.format(src))
+    subprocess.run(['make', '-s', '-C', HERE, 'ref', 'REFERENCE_SRC={}'.format(src)], check=True)
 
 
 def reference_kernels_available():

@@ -20,7 +20,9 @@ DP = ctypes.POINTER(ctypes.c_double)   # optional 3-vector (NULL = local line of
 PRC_OK = 0
 PRC_FLAG_OUT_OF_BOX = 1
 PRC_FLAG_NONFINITE = 2
+PRC_ERR_ARG = 1
 PRC_ERR_TIMEOUT = 5
+PRC_FAULT_WAIT_TIMEOUT = 1
 FIELDS = {'disp': 0, 'rsd': 1, 'disp+rsd': 2}
 
 _lock = threading.Lock()
@@ -37,6 +39,7 @@ _SIGNATURES = {
     'prc_sum_f32': (c_int, [_p, c_i64, _p, _p, c_size, _p]),
     'prc_zeldovich_psi_workspace_bytes': (c_size, [I3, c_int]),
     'prc_device_fault_flags': (ctypes.c_uint, [c_int]),
+    'prc_debug_wait_timeout': (c_int, [c_i64, _p, _p]),
     'prc_assign_cic_workspace_bytes': (c_size, [I3, c_i64, c_int]),
     'prc_assign_cic': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size, _p]),
     'prc_assign_cic_order': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size,
@@ -100,6 +103,11 @@ class LibraryError(RuntimeError):
 
 
 def library_path():
+    """The in-tree library, or the build variant named by PRC_LIBRARY (a path, or a variant name such as
+    'nopp' for lib/libpyrecon_cuda_nopp.so)."""
+    alt = os.environ.get('PRC_LIBRARY')
+    if alt:
+        return alt if os.sep in alt else _build.library_path(alt)
     return _build.library_path()
 
 

@@ -5,6 +5,10 @@ Build libpyrecon_cuda.so in-tree (pyrecon_b200/lib/) with nvcc for sm_100a.
     python -m pyrecon_b200.build --force  # rebuild everything
 
 Objects go to pyrecon_b200/_build/; the shared library is what travels with the tree.
+
+Variants: the same library with some build-time knobs changed (VARIANTS), linked from a
+rebuilt fft.cu and the regular objects into lib/libpyrecon_cuda_<name>.so.  The tests load
+them in a subprocess (PRC_LIBRARY) to check that each variant computes the same bits.
 """
 import os
 import sys
@@ -28,8 +32,17 @@ FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-Xcompiler', 
          '--expt-relaxed-constexpr', '-I' + os.path.join(ROOT, 'include')]
 
 
-def library_path():
-    return os.path.join(LIBDIR, LIBNAME)
+# name -> extra nvcc flags for fft.cu.  'nopp': every TMA-fed FFT pass with two barriers per shared-memory
+# exchange instead of the ping-pong buffers (same arithmetic, same order).
+VARIANTS = {
+    'nopp': ['-DPRC_STRIDED_PP=0', '-DPRC_KSPACE_PP=0', '-DPRC_HESS_PP=0', '-DPRC_C2R_PP=0'],
+}
+
+
+def library_path(variant=None):
+    if variant is None:
+        return os.path.join(LIBDIR, LIBNAME)
+    return os.path.join(LIBDIR, 'libpyrecon_cuda_{}.so'.format(variant))
 
 
 def _stale(target, deps):
@@ -39,34 +52,50 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def _compile(src, extra=()):
-    obj = os.path.join(BUILD, os.path.splitext(src)[0] + '.o')
+def _compile(src, extra=(), obj=None):
+    obj = obj or os.path.join(BUILD, os.path.splitext(src)[0] + '.o')
     path = os.path.join(CSRC, src)
     cmd = [NVCC] + ARCH + FLAGS + list(extra) + ['-c', path, '-o', obj]
     subprocess.run(cmd, check=True)
     return obj
 
 
-def build(force=False, verbose=False, extra=()):
+def _link(lib, objs):
+    subprocess.run([NVCC] + ARCH + ['-shared', '-o', lib] + objs + ['-cudart', 'static'], check=True)
+
+
+def build(force=False, verbose=False, extra=(), variants=True):
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    todo = []
+    jobs = []          # (source, extra flags, object)
     objs = []
     for src in SOURCES:
         obj = os.path.join(BUILD, os.path.splitext(src)[0] + '.o')
         objs.append(obj)
         if force or _stale(obj, [os.path.join(CSRC, src)] + HEADERS):
-            todo.append(src)
-    if todo:
-        with concurrent.futures.ThreadPoolExecutor(max_workers=len(todo)) as ex:
-            for _ in ex.map(lambda s: _compile(s, extra), todo):
+            jobs.append((src, list(extra), obj))
+    variant_objs = {}
+    for name, flags in (VARIANTS.items() if variants else []):
+        obj = os.path.join(BUILD, 'fft_{}.o'.format(name))
+        variant_objs[name] = obj
+        if force or _stale(obj, [os.path.join(CSRC, 'fft.cu')] + HEADERS):
+            jobs.append(('fft.cu', list(extra) + flags, obj))
+    if jobs:
+        with concurrent.futures.ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+            for _ in ex.map(lambda j: _compile(j[0], j[1], j[2]), jobs):
                 pass
     lib = library_path()
-    if force or todo or _stale(lib, objs):
-        cmd = [NVCC] + ARCH + ['-shared', '-o', lib] + objs + ['-cudart', 'static']
-        subprocess.run(cmd, check=True)
+    if force or jobs or _stale(lib, objs):
+        _link(lib, objs)
         if verbose:
             print('built', lib)
+    for name, vobj in variant_objs.items():
+        vlib = library_path(name)
+        vobjs = [vobj if os.path.basename(o) == 'fft.o' else o for o in objs]
+        if force or _stale(vlib, vobjs):
+            _link(vlib, vobjs)
+            if verbose:
+                print('built', vlib)
     return lib
 
 

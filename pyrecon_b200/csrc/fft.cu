@@ -615,6 +615,27 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, in
 // Device fault word of the FFT kernels (bits prc::tma::FAULT_*), read by prc_device_fault_flags.
 __device__ unsigned int g_fault;
 
+// Failure path of the bounded waits, on purpose: thread 0 arms the CTA's transaction barrier for
+// `bytes` that no copy will ever deliver (no copy is issued, so nothing is in flight), every thread
+// waits on it for at most `limit_ns`, the wait runs out, the fault bit is set and the kernel returns
+// with the barrier invalidated.  `out[0]` = 1 when the wait gave up, 0 if it (impossibly) completed.
+__global__ void debug_wait_timeout(uint64_t limit_ns, uint32_t bytes, int* out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        tma::barrier_init(&bar, 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) tma::arrive_expect_tx(&bar, bytes);
+    const bool done = tma::wait_for(&bar, 0, limit_ns);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (!done) atomicOr(&g_fault, tma::FAULT_WAIT_TIMEOUT);
+        out[0] = done ? 0 : 1;
+        tma::barrier_inval(&bar);
+    }
+}
+
 #include "fft_fast.cuh"
 #include "fft_tma.cuh"
 
@@ -1549,6 +1570,14 @@ unsigned int prc_device_fault_flags(int reset) {
         cudaMemcpyToSymbol(g_fault, &zero, sizeof(zero));
     }
     return v;
+}
+
+int prc_debug_wait_timeout(int64_t limit_ns, int* out, void* stream) {
+    if (!out || limit_ns <= 0 || limit_ns > 1000000000ll) return PRC_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    PRC_LAUNCH("debug_wait_timeout", st, debug_wait_timeout<<<1, 32, 0, st>>>((uint64_t)limit_ns, 256u, out));
+    PRC_CHECK_LAUNCH();
+    return PRC_OK;
 }
 
 int prc_fft_supported(const int32_t nmesh[3]) {

@@ -59,13 +59,20 @@ __device__ __forceinline__ uint64_t globaltimer() {
     return t;
 }
 
-// Waits for the phase of `parity` to complete; false if it has not after WAIT_LIMIT_NS.
-__device__ __forceinline__ bool wait(uint64_t* bar, uint32_t parity) {
+// Waits for the phase of `parity` to complete; false if it has not after `limit_ns`.
+__device__ __forceinline__ bool wait_for(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
     if (try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
     while (!try_wait(bar, parity))
-        if (globaltimer() - t0 > WAIT_LIMIT_NS) return false;
+        if (globaltimer() - t0 > limit_ns) return false;
     return true;
+}
+
+// Waits for the phase of `parity` to complete; false if it has not after WAIT_LIMIT_NS.
+__device__ __forceinline__ bool wait(uint64_t* bar, uint32_t parity) { return wait_for(bar, parity, WAIT_LIMIT_NS); }
+
+__device__ __forceinline__ void barrier_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
 // Tiled 3D copy global -> shared (this CTA), completion counted in bytes on `bar`.

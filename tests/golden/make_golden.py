@@ -2,8 +2,8 @@
 Generate the golden fixtures in this directory by running the REFERENCE
 implementation (cosmodesi/pyrecon 1.0.0) on small seeded inputs.
 
-This script runs only where the reference source tree is available
-(default /root/reference, override with PYRECON_REFERENCE); it copies the
+This script runs only where the reference source tree is available (its
+path in the environment variable PYRECON_REFERENCE, required); it copies the
 tree to a temporary directory, builds its C kernels there with the system
 gcc (the reference's own src/Makefile), imports it and stores, per case,
 the inputs and every intermediate the drop-in exposes:
@@ -37,7 +37,10 @@ from pyrecon_b200 import mocks  # noqa: E402
 
 
 def import_reference(tmp):
-    src = os.environ.get('PYRECON_REFERENCE', '/root/reference')
+    src = os.environ.get('PYRECON_REFERENCE')
+    if not src or not os.path.isfile(os.path.join(src, 'pyrecon', 'recon.py')):
+        raise SystemExit('set PYRECON_REFERENCE to the root of the reference source tree (holding pyrecon/ and src/); '
+                         'got {!r}'.format(src))
     dst = os.path.join(tmp, 'reference')
     shutil.copytree(src, dst)
     subprocess.run(['make', '-s', '-C', os.path.join(dst, 'src'), 'CC=/usr/bin/gcc',

@@ -388,6 +388,39 @@ def test_no_device_faults_after_kernels():
     assert _lib.load().prc_device_fault_flags(0) == 0
 
 
+def test_bounded_wait_gives_up_and_is_reported():
+    """The failure path of the bounded barrier waits, without a GPU fault: a barrier armed for bytes that
+    no copy delivers (none is issued) makes the wait run out after 2 ms; the kernel sets the fault bit
+    and returns, the next read-out of a reconstruction raises ReconstructionError (clearing the word),
+    and the context stays usable: the read-out after it succeeds with the same result as before."""
+    import time
+    import pyrecon_b200
+    from pyrecon_b200 import _lib as L
+    t = torch()
+    assert L.load().prc_device_fault_flags(1) == 0
+    out = t.zeros(1, dtype=t.int32, device='cuda')
+    t0 = time.perf_counter()
+    L.call('prc_debug_wait_timeout', 2_000_000, L.ptr(out), stream())
+    t.cuda.synchronize()
+    assert time.perf_counter() - t0 < 5.
+    assert int(out.item()) == 1
+    assert L.load().prc_device_fault_flags(0) & L.PRC_FAULT_WAIT_TIMEOUT
+    assert L.load().prc_debug_wait_timeout(0, L.ptr(out), stream()) == L.PRC_ERR_ARG
+    pos = catalog(5000, [1000.] * 3, [2000.] * 3, seed=12)
+    rec = pyrecon_b200.IterativeFFTReconstruction(f=0.8, bias=2., nmesh=16, boxsize=1000., boxcenter=2000., dtype='f8')
+    rec.assign_data(pos)
+    rec.set_density_contrast(smoothing_radius=15.)
+    rec.run()
+    with pytest.raises(pyrecon_b200.ReconstructionError):
+        rec.read_shifted_positions(pos)
+    assert L.load().prc_device_fault_flags(0) == 0
+    first = rec.read_shifted_positions(pos)
+    L.call('prc_debug_wait_timeout', 1_000_000, L.ptr(out), stream())
+    with pytest.raises(pyrecon_b200.ReconstructionError):
+        rec.read_shifted_positions(pos)
+    np.testing.assert_array_equal(rec.read_shifted_positions(pos), first)
+
+
 def mg_solve(dtype, mixed, nmesh=(32, 32, 32), los=None, calls=1):
     """phi of prc_multigrid_* on a fixed random right-hand side, `calls` times on the same buffers."""
     L, t = lib(), torch()
