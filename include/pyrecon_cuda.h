@@ -70,8 +70,11 @@ PRC_API unsigned long long prc_launch_count(void);
 PRC_API void prc_profile_enable(int on);
 PRC_API int prc_profile_collect(char *buf, size_t cap);
 
-/* 1 if every axis of nmesh is handled by the FFT kernels (n = 2^a 3^b 5^c 7^d, n2 even,
- * n <= 1024), else 0. */
+/* 1 if every axis of nmesh is handled by the FFT kernels, else 0: any length 2 <= n <= 2048 (the
+ * reference's numpy / FFTW engines take any size, pyrecon/mesh.py:974-1118; a 2048^3 FP32 mesh is
+ * 34 GB, so a reconstruction's meshes reach the device memory before this limit).  Powers of two up to
+ * 1024 run the register-resident kernels, every other length (radices 2-8, any larger prime factor by
+ * direct summation, an odd last axis as a full-length transform) the shared-memory kernels. */
 PRC_API int prc_fft_supported(const int32_t nmesh[3]);
 
 /* ------------------------------------------------------------------------------------------

@@ -34,7 +34,8 @@ namespace prc {
 
 constexpr int FFT_THREADS = 256;
 constexpr int MAX_RADICES = 16;
-constexpr int MAX_FFT_N = 1024;
+constexpr int MAX_FFT_N = 2048;       // any length up to this on the shared-memory (generic) kernels
+constexpr int MAX_FAST_N = 1024;      // register-resident power-of-two kernels
 constexpr int MAX_BATCH = 6;
 
 struct Radices {
@@ -51,14 +52,16 @@ static bool factorize(int n, Radices* out) {
     while (m % 8 == 0 && m > 0) { rd.r[rd.count++] = 8; m /= 8; }
     if (m % 4 == 0) { rd.r[rd.count++] = 4; m /= 4; }
     if (m % 2 == 0) { rd.r[rd.count++] = 2; m /= 2; }
-    const int odd[3] = {3, 5, 7};
-    for (int i = 0; i < 3; i++)
-        while (m % odd[i] == 0) {
+    // odd primes in increasing order: 3, 5, 7 have their own butterflies, larger ones (11, 13, ...,
+    // up to a prime length itself) run the direct-summation pass
+    for (int f = 3; m > 1; f += 2) {
+        if (f * f > m) f = m;
+        while (m % f == 0) {
             if (rd.count >= MAX_RADICES) return false;
-            rd.r[rd.count++] = odd[i];
-            m /= odd[i];
+            rd.r[rd.count++] = f;
+            m /= f;
         }
-    if (m != 1) return false;
+    }
     *out = rd;
     return true;
 }
@@ -185,6 +188,33 @@ __device__ __forceinline__ void stockham_pass(const C* __restrict__ src, C* __re
     }
 }
 
+// One Stockham pass of any radix R (the primes above 7) by direct summation: a thread makes one output
+// m of one R-point sub-transform, y_m = sum_r x_r w_{Ns R}^{r k} w_R^{r m} = sum_r x_r w_n^{r E},
+// E = k twstep + m nb (input twiddle and DFT kernel in one table lookup, exponent kept mod n by
+// addition); O(R) operations per output.
+template <typename C, int DIR>
+__device__ __forceinline__ void stockham_pass_any(const C* __restrict__ src, C* __restrict__ dst, int n, int B, int bp,
+                                                  int Ns, int R, const C* __restrict__ tw, int tws) {
+    const int nb = n / R;
+    const int twstep = n / (Ns * R);
+    for (int q = threadIdx.x; q < n * B; q += blockDim.x) {
+        const int line = q % B, rest = q / B;
+        const int j = rest % nb, m = rest / nb;
+        const int k = j % Ns;
+        const int E = (k * twstep + m * nb) % n;
+        C acc = src[j * bp + line];
+        int ex = 0;
+        for (int r = 1; r < R; r++) {
+            ex += E;
+            if (ex >= n) ex -= n;
+            C w = tw[ex * tws];
+            if (DIR > 0) w = cconj(w);
+            acc = cadd(acc, cmul(src[(j + r * nb) * bp + line], w));
+        }
+        dst[((j - k) * R + k + m * Ns) * bp + line] = acc;
+    }
+}
+
 // Transforms B lines in place-ish: data in `a`, scratch `b`; returns the buffer with the result.
 // tw holds w_{n*tws}^m (so entry m*tws is w_n^m).
 template <typename C, int DIR>
@@ -198,7 +228,8 @@ __device__ C* fft_lines(C* a, C* b, int n, int B, int bp, const Radices& rd, con
             case 2: stockham_pass<C, DIR, 2>(a, b, n, B, bp, Ns, tw, tws); break;
             case 3: stockham_pass<C, DIR, 3>(a, b, n, B, bp, Ns, tw, tws); break;
             case 5: stockham_pass<C, DIR, 5>(a, b, n, B, bp, Ns, tw, tws); break;
-            default: stockham_pass<C, DIR, 7>(a, b, n, B, bp, Ns, tw, tws); break;
+            case 7: stockham_pass<C, DIR, 7>(a, b, n, B, bp, Ns, tw, tws); break;
+            default: stockham_pass_any<C, DIR>(a, b, n, B, bp, Ns, R, tw, tws); break;
         }
         __syncthreads();
         C* t = a;
@@ -226,17 +257,25 @@ struct RealsIn { const void* p[MAX_BATCH]; };
 
 // ---------------------------------------------------------------------------------------------
 // z pass, forward r2c.  Tile = B rows (lines along z) of one mesh of the batch.
+// Even n2: each row of n2 reals is read as n2/2 complex pairs (the packed real-FFT).  Odd n2: each row
+// is transformed as n2 complex values with zero imaginary parts and the first nh = (n2 + 1)/2
+// outputs are kept.  Buffers hold (k, line) at k * bp + line (bp = B + 1, or 1 for one row).
 // ---------------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int row_pitch(int B) { return B > 1 ? B + 1 : 1; }
+
 template <typename T, typename TIN>
 __global__ void __launch_bounds__(FFT_THREADS) fft_z_r2c(RealsIn in, Specs<cplx_t<T>> out, int nbatch, Dims dims,
                                                           int pitch, Radices rd, int B) {
     typedef cplx_t<T> C;
     extern __shared__ unsigned char smem_raw[];
-    const int n2 = dims.n[2], M = n2 / 2, nh = M + 1;
-    const int bp = B + 1;
+    const int n2 = dims.n[2], nh = n2 / 2 + 1;
+    const bool full = (n2 & 1) != 0;
+    const int M = full ? n2 : n2 / 2;              // transform length
+    const int L = full ? n2 : M + 1;               // buffer rows
+    const int bp = row_pitch(B);
     C* tw = (C*)smem_raw;                          // n2 entries
-    C* bufa = tw + n2;                             // (M + 1) * bp
-    C* bufb = bufa + (M + 1) * bp;
+    C* bufa = tw + n2;                             // L * bp
+    C* bufb = bufa + L * bp;
     fill_twiddles(tw, n2);
     __syncthreads();
     const int64_t rows = (int64_t)dims.n[0] * dims.n[1];
@@ -247,29 +286,39 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_z_r2c(RealsIn in, Specs<cplx_
         const int64_t row0 = (t % tiles_per) * B;
         const int nrow = (int)min((int64_t)B, rows - row0);
         const TIN* src = (const TIN*)in.p[bi] + row0 * n2;
-        // load rows as complex pairs (x[2m], x[2m+1])
-        for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
-            const int line = q / M, m = q % M;
-            C v = cmake<C>((T)0, (T)0);
-            if (line < nrow) {
-                const TIN* r = src + (int64_t)line * n2 + 2 * m;
-                v = cmake<C>((T)r[0], (T)r[1]);
+        if (full) {
+            for (int q = threadIdx.x; q < B * n2; q += blockDim.x) {
+                const int line = q / n2, m = q % n2;
+                bufa[m * bp + line] = cmake<C>(line < nrow ? (T)src[(int64_t)line * n2 + m] : (T)0, (T)0);
             }
-            bufa[m * bp + line] = v;
+        } else {
+            // load rows as complex pairs (x[2m], x[2m+1])
+            for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
+                const int line = q / M, m = q % M;
+                C v = cmake<C>((T)0, (T)0);
+                if (line < nrow) {
+                    const TIN* r = src + (int64_t)line * n2 + 2 * m;
+                    v = cmake<C>((T)r[0], (T)r[1]);
+                }
+                bufa[m * bp + line] = v;
+            }
         }
         __syncthreads();
-        C* z = fft_lines<C, -1>(bufa, bufb, M, B, bp, rd, tw, 2);
-        C* x = z == bufa ? bufb : bufa;
-        // unpack: X[k] = (Z[k] + conj Z[M-k]) / 2 - i w^k (Z[k] - conj Z[M-k]) / 2
-        for (int q = threadIdx.x; q < B * nh; q += blockDim.x) {
-            const int line = q % B, k = q / B;
-            const C zk = z[(k == M ? 0 : k) * bp + line];
-            const C zc = cconj(z[(k == 0 ? 0 : M - k) * bp + line]);
-            const C e = cscale(cadd(zk, zc), (T)0.5);
-            const C o = cmul_i(cscale(csub(zk, zc), (T)0.5), -1);   // -i (Zk - Zc*) / 2
-            x[k * bp + line] = cadd(e, cmul(tw[k == M ? M : k], o));
+        C* z = fft_lines<C, -1>(bufa, bufb, M, B, bp, rd, tw, full ? 1 : 2);
+        C* x = z;
+        if (!full) {
+            x = z == bufa ? bufb : bufa;
+            // unpack: X[k] = (Z[k] + conj Z[M-k]) / 2 - i w^k (Z[k] - conj Z[M-k]) / 2
+            for (int q = threadIdx.x; q < B * nh; q += blockDim.x) {
+                const int line = q % B, k = q / B;
+                const C zk = z[(k == M ? 0 : k) * bp + line];
+                const C zc = cconj(z[(k == 0 ? 0 : M - k) * bp + line]);
+                const C e = cscale(cadd(zk, zc), (T)0.5);
+                const C o = cmul_i(cscale(csub(zk, zc), (T)0.5), -1);   // -i (Zk - Zc*) / 2
+                x[k * bp + line] = cadd(e, cmul(tw[k == M ? M : k], o));
+            }
+            __syncthreads();
         }
-        __syncthreads();
         C* dst = out.p[bi] + row0 * pitch;
         for (int q = threadIdx.x; q < B * nh; q += blockDim.x) {
             const int line = q / nh, k = q % nh;
@@ -484,67 +533,98 @@ template <typename T> struct Epi {
     double offset[3], cell[3];   // node coordinates x_a = offset_a + cell_a * i (EPI_ITER_LOCAL)
 };
 
+// Epilogue of one cell (row, iz): vals[c * stride] is the inverse transform of input c there.
 template <typename T>
-__device__ __forceinline__ void epilogue_pair(const Epi<T>& e, int nin, const T* vals /* [nin][2] */, int64_t row,
-                                              int m, const Dims& dims, T out2[2]) {
-    const int n2 = dims.n[2];
-    for (int h = 0; h < 2; h++) {
-        const int64_t cell = row * n2 + 2 * m + h;
-        double res = 0.;
-        switch (e.type) {
-            case EPI_DENSITY: {
-                const double d = (double)vals[0 * 2 + h], r = (double)vals[1 * 2 + h];
-                const double sd = e.sums[0], sr = e.sums[1];
-                const double alpha = sd * 1. / sr;
-                const double threshold = e.ran_min * sr / e.size_randoms;
-                res = r > threshold ? (d - alpha * r) / (e.bias * alpha * r) : 0.;
-                break;
-            }
-            case EPI_DENSITY_NORANDOMS: {
-                const double mean = e.sums[0] / e.ncells;
-                res = ((double)vals[h] / mean - 1.) / e.bias;
-                break;
-            }
-            case EPI_ITER_GLOBAL: {
-                res = (double)e.delta[cell] - e.factor[0] * (double)vals[h];
-                break;
-            }
-            case EPI_ITER_LOCAL: {
-                const int iz = 2 * m + h;
-                const int ix = (int)(row / dims.n[1]), iy = (int)(row % dims.n[1]);
-                const double x[3] = {e.offset[0] + e.cell[0] * ix, e.offset[1] + e.cell[1] * iy,
-                                     e.offset[2] + e.cell[2] * iz};
-                const double x2 = (x[0] * x[0] + x[1] * x[1]) + x[2] * x[2];
-                const int pi[6] = {0, 0, 0, 1, 1, 2}, pj[6] = {0, 1, 2, 1, 2, 2};
-                double v = (double)e.delta[cell];
-                for (int c = 0; c < 6; c++)
-                    v -= e.factor[c] * ((x[pi[c]] * x[pj[c]] * (double)vals[c * 2 + h]) / x2);
-                res = v;
-                break;
-            }
-            default:
-                res = (double)vals[h];
+__device__ __forceinline__ T epilogue_value(const Epi<T>& e, const T* vals, int stride, int64_t row, int iz,
+                                            const Dims& dims) {
+    const int64_t cell = row * dims.n[2] + iz;
+    double res = 0.;
+    switch (e.type) {
+        case EPI_DENSITY: {
+            const double d = (double)vals[0], r = (double)vals[stride];
+            const double sd = e.sums[0], sr = e.sums[1];
+            const double alpha = sd * 1. / sr;
+            const double threshold = e.ran_min * sr / e.size_randoms;
+            res = r > threshold ? (d - alpha * r) / (e.bias * alpha * r) : 0.;
+            break;
         }
-        out2[h] = (T)res;
+        case EPI_DENSITY_NORANDOMS: {
+            const double mean = e.sums[0] / e.ncells;
+            res = ((double)vals[0] / mean - 1.) / e.bias;
+            break;
+        }
+        case EPI_ITER_GLOBAL: {
+            res = (double)e.delta[cell] - e.factor[0] * (double)vals[0];
+            break;
+        }
+        case EPI_ITER_LOCAL: {
+            const int ix = (int)(row / dims.n[1]), iy = (int)(row % dims.n[1]);
+            const double x[3] = {e.offset[0] + e.cell[0] * ix, e.offset[1] + e.cell[1] * iy,
+                                 e.offset[2] + e.cell[2] * iz};
+            const double x2 = (x[0] * x[0] + x[1] * x[1]) + x[2] * x[2];
+            const int pi[6] = {0, 0, 0, 1, 1, 2}, pj[6] = {0, 1, 2, 1, 2, 2};
+            double v = (double)e.delta[cell];
+            for (int c = 0; c < 6; c++)
+                v -= e.factor[c] * ((x[pi[c]] * x[pj[c]] * (double)vals[c * stride]) / x2);
+            res = v;
+            break;
+        }
+        case EPI_ITER_POLY: {
+            // inputs C, B, A of the quadratic in x2 formed by the Hessian y pass: the RSD term is
+            // ((C x2 + B) x2 + A) / |x|^2
+            const int ix = (int)(row / dims.n[1]), iy = (int)(row % dims.n[1]);
+            const double x0 = e.offset[0] + e.cell[0] * ix, x1 = e.offset[1] + e.cell[1] * iy;
+            const double xz = e.offset[2] + e.cell[2] * iz;
+            const double x2 = (x0 * x0 + x1 * x1) + xz * xz;
+            const double poly = ((double)vals[0] * xz + (double)vals[stride]) * xz + (double)vals[2 * stride];
+            res = (double)e.delta[cell] - poly / x2;
+            break;
+        }
+        default:
+            res = (double)vals[0];
+    }
+    return (T)res;
+}
+
+// Stores the inverse-transformed values of one cell: one output per input (EPI_STORE), the (N, 4)
+// interleaved displacement (EPI_STORE4) or the epilogue's single output.
+template <typename T>
+__device__ __forceinline__ void epilogue_store(const Epi<T>& e, int nin, const T* vals, int stride, int64_t row, int iz,
+                                               const Dims& dims) {
+    const int64_t cell = row * dims.n[2] + iz;
+    if (e.type == EPI_STORE) {
+        for (int i = 0; i < nin; i++) e.out[i][cell] = vals[i * stride];
+    } else if (e.type == EPI_STORE4) {
+        T* o = e.out[0] + cell * 4;
+        for (int i = 0; i < 3; i++) o[i] = vals[i * stride];
+        o[3] = 0;
+    } else {
+        e.out[0][cell] = epilogue_value(e, vals, stride, row, iz, dims);
     }
 }
 
+// Inverse z pass.  Even n2: the nh = n2/2 + 1 Hermitian-half values are packed into n2/2 complex
+// values whose inverse transform holds (x[2m], x[2m+1]).  Odd n2: the half is completed to all n2
+// values by Hermitian symmetry (X[n2 - k] = conj X[k]) and the real part of its n2-point inverse kept,
+// which is the reference's full complex inverse followed by .real.
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, int nin, Dims dims, int pitch,
                                                           Radices rd, int B, Epi<T> e) {
     typedef cplx_t<T> C;
     extern __shared__ unsigned char smem_raw[];
-    const int n2 = dims.n[2], M = n2 / 2, nh = M + 1;
-    const int bp = B + 1;
+    const int n2 = dims.n[2], nh = n2 / 2 + 1;
+    const bool full = (n2 & 1) != 0;
+    const int M = full ? n2 : n2 / 2;          // transform length
+    const int L = full ? n2 : nh;              // buffer rows
+    const int bp = row_pitch(B);
     C* tw = (C*)smem_raw;                    // n2
-    C* bufa = tw + n2;                       // nh * bp
-    C* bufb = bufa + nh * bp;                // nh * bp
-    C* acc = bufb + nh * bp;                 // nin * M * B (results kept for the epilogue)
+    C* bufa = tw + n2;                       // L * bp
+    C* bufb = bufa + L * bp;                 // L * bp
+    T* acc = (T*)(bufb + L * bp);            // nin * B * n2 reals kept for the epilogue, row-major per input
     fill_twiddles(tw, n2);
     __syncthreads();
     const int64_t rows = (int64_t)dims.n[0] * dims.n[1];
     const int64_t ntiles = (rows + B - 1) / B;
-    const bool multi_store = (e.type == EPI_STORE);
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t row0 = t * B;
         const int nrow = (int)min((int64_t)B, rows - row0);
@@ -555,58 +635,45 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_z_c2r(Specs<cplx_t<T>> in, in
                 bufa[k * bp + line] = line < nrow ? src[(int64_t)line * pitch + k] : cmake<C>(0, 0);
             }
             __syncthreads();
-            // pack: Z[k] = (X[k] + conj X[M-k]) + i w^-k (X[k] - conj X[M-k]), k < M
-            for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
-                const int line = q % B, k = q / B;
-                const C xk = bufa[k * bp + line];
-                const C xc = cconj(bufa[(M - k) * bp + line]);
-                const C ev = cadd(xk, xc);
-                const C od = cmul(cconj(tw[k]), csub(xk, xc));
-                bufb[k * bp + line] = cadd(ev, cmul_i(od, +1));
-            }
-            __syncthreads();
-            C* z = fft_lines<C, +1>(bufb, bufa, M, B, bp, rd, tw, 2);
-            // keep (x[2m], x[2m+1]) * scale for the epilogue, row-major per input
-            for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
-                const int line = q / M, m = q % M;
-                const C v = z[m * bp + line];
-                acc[((int64_t)i * B + line) * M + m] = cmake<C>((T)(v.x * e.scale), (T)(v.y * e.scale));
+            C* z;
+            if (full) {
+                for (int q = threadIdx.x; q < B * (n2 - nh); q += blockDim.x) {
+                    const int line = q % B, k = nh + q / B;
+                    bufa[k * bp + line] = cconj(bufa[(n2 - k) * bp + line]);
+                }
+                __syncthreads();
+                z = fft_lines<C, +1>(bufa, bufb, n2, B, bp, rd, tw, 1);
+                for (int q = threadIdx.x; q < B * n2; q += blockDim.x) {
+                    const int line = q / n2, m = q % n2;
+                    acc[((int64_t)i * B + line) * n2 + m] = (T)(z[m * bp + line].x * e.scale);
+                }
+            } else {
+                // pack: Z[k] = (X[k] + conj X[M-k]) + i w^-k (X[k] - conj X[M-k]), k < M
+                for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
+                    const int line = q % B, k = q / B;
+                    const C xk = bufa[k * bp + line];
+                    const C xc = cconj(bufa[(M - k) * bp + line]);
+                    const C ev = cadd(xk, xc);
+                    const C od = cmul(cconj(tw[k]), csub(xk, xc));
+                    bufb[k * bp + line] = cadd(ev, cmul_i(od, +1));
+                }
+                __syncthreads();
+                z = fft_lines<C, +1>(bufb, bufa, M, B, bp, rd, tw, 2);
+                // (x[2m], x[2m+1]) * scale
+                for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
+                    const int line = q / M, m = q % M;
+                    const C v = z[m * bp + line];
+                    T* a = acc + ((int64_t)i * B + line) * n2 + 2 * m;
+                    a[0] = (T)(v.x * e.scale);
+                    a[1] = (T)(v.y * e.scale);
+                }
             }
             __syncthreads();
         }
-        for (int q = threadIdx.x; q < B * M; q += blockDim.x) {
-            const int line = q / M, m = q % M;
+        for (int q = threadIdx.x; q < B * n2; q += blockDim.x) {
+            const int line = q / n2, iz = q % n2;
             if (line >= nrow) continue;
-            const int64_t row = row0 + line;
-            if (multi_store) {
-                for (int i = 0; i < nin; i++) {
-                    const C v = acc[((int64_t)i * B + line) * M + m];
-                    T* o = e.out[i] + row * n2 + 2 * m;
-                    o[0] = v.x;
-                    o[1] = v.y;
-                }
-            } else if (e.type == EPI_STORE4) {
-                T* o = e.out[0] + (row * n2 + 2 * m) * 4;
-                for (int i = 0; i < 3; i++) {
-                    const C v = acc[((int64_t)i * B + line) * M + m];
-                    o[i] = v.x;
-                    o[4 + i] = v.y;
-                }
-                o[3] = 0;
-                o[7] = 0;
-            } else {
-                T vals[2 * MAX_BATCH];
-                for (int i = 0; i < nin; i++) {
-                    const C v = acc[((int64_t)i * B + line) * M + m];
-                    vals[2 * i] = v.x;
-                    vals[2 * i + 1] = v.y;
-                }
-                T r2[2];
-                epilogue_pair(e, nin, vals, row, m, dims, r2);
-                T* o = e.out[0] + row * n2 + 2 * m;
-                o[0] = r2[0];
-                o[1] = r2[1];
-            }
+            epilogue_store(e, nin, acc + (int64_t)line * n2 + iz, B * n2, row0 + line, iz, dims);
         }
         __syncthreads();
     }
@@ -646,17 +713,20 @@ struct Plan3 {
     Dims dims;
     int nh;
     int pitch;            // row stride of the half spectra in complex elements (>= nh)
-    Radices rz, ry, rx;   // rz is for the n2/2-point complex transform
+    Radices rz, ry, rx;   // rz: the n2/2-point packed transform (even n2) or the n2-point one (odd n2)
 };
 
+// Any axis length in [2, MAX_FFT_N]: powers of two up to MAX_FAST_N run the register-resident kernels,
+// every other length (radices 8, 4, 2, 3, 5, 7 and any larger prime; an odd last axis unpacked) the
+// shared-memory kernels.
 static int make_plan(const int32_t nmesh[3], Plan3* p) {
     for (int d = 0; d < 3; d++)
         if (nmesh[d] < 2 || nmesh[d] > MAX_FFT_N) return PRC_ERR_UNSUPPORTED;
-    if (nmesh[2] % 2 != 0) return PRC_ERR_UNSUPPORTED;
     for (int d = 0; d < 3; d++) p->dims.n[d] = nmesh[d];
     p->nh = nmesh[2] / 2 + 1;
     p->pitch = p->nh;
-    if (!factorize(nmesh[2] / 2, &p->rz) || !factorize(nmesh[1], &p->ry) || !factorize(nmesh[0], &p->rx))
+    const int zlen = nmesh[2] % 2 ? nmesh[2] : nmesh[2] / 2;
+    if (!factorize(zlen, &p->rz) || !factorize(nmesh[1], &p->ry) || !factorize(nmesh[0], &p->rx))
         return PRC_ERR_UNSUPPORTED;
     return PRC_OK;
 }
@@ -685,7 +755,7 @@ static int fft_grid(int64_t ntiles, int ctas_per_sm) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, cap));
 }
 
-static bool fast_len(int n) { return n >= 8 && n <= MAX_FFT_N && (n & (n - 1)) == 0; }
+static bool fast_len(int n) { return n >= 8 && n <= MAX_FAST_N && (n & (n - 1)) == 0; }
 
 // PRC_FFT_GENERIC=1 in the environment routes every size through the mixed-radix kernels
 // (the tests use it to keep that path checked on power-of-two sizes too).
@@ -1123,7 +1193,7 @@ template <typename T> struct FFTLaunch {
 
     template <typename TIN>
     static int z_r2c(const Plan3& p, const void* const* in, C* const* out, int nb, cudaStream_t st) {
-        if (fast_len(p.dims.n[2] / 2) && !getenv_generic()) {
+        if (p.dims.n[2] % 2 == 0 && fast_len(p.dims.n[2] / 2) && !getenv_generic()) {
             RealsIn ri;
             Specs<C> so;
             for (int i = 0; i < nb; i++) {
@@ -1134,10 +1204,11 @@ template <typename T> struct FFTLaunch {
             double bytes = (double)nb * rows * (p.dims.n[2] * sizeof(TIN) + p.nh * CS);
             return dispatch_pow2<FastZR2C<T, TIN>::template K>(p.dims.n[2] / 2, ri, so, nb, rows, p.pitch, bytes, st);
         }
-        const int M = p.dims.n[2] / 2;
+        const int n2 = p.dims.n[2], L = n2 % 2 ? n2 : n2 / 2 + 1;
+        auto need = [&](int b) { return (size_t)(2 * L * row_pitch(b) + n2) * CS; };
         int B = 16;
-        while (B > 1 && (size_t)(2 * (M + 1) * (B + 1) + p.dims.n[2]) * CS > BUDGET) B >>= 1;
-        size_t smem = (size_t)(2 * (M + 1) * (B + 1) + p.dims.n[2]) * CS;
+        while (B > 1 && need(B) > BUDGET) B >>= 1;
+        const size_t smem = need(B);
         RealsIn ri;
         Specs<C> so;
         for (int i = 0; i < nb; i++) {
@@ -1242,7 +1313,7 @@ template <typename T> struct FFTLaunch {
 
     static int z_c2r(const Plan3& p, C* const* in, int nin, const Epi<T>& e, cudaStream_t st) {
         const int M = p.dims.n[2] / 2, nh = M + 1;
-        if (fast_len(M) && !getenv_generic()) {
+        if (p.dims.n[2] % 2 == 0 && fast_len(M) && !getenv_generic()) {
             Specs<C> si;
             for (int i = 0; i < nin; i++) si.p[i] = in[i];
             int64_t rows = (int64_t)p.dims.n[0] * p.dims.n[1];
@@ -1255,10 +1326,13 @@ template <typename T> struct FFTLaunch {
             }
             return dispatch_pow2<FastZC2R<T>::template K>(M, si, nin, p.dims, p.pitch, e, bytes, st);
         }
+        const int n2 = p.dims.n[2], L = n2 % 2 ? n2 : nh;
+        auto need = [&](int b) {
+            return (size_t)(2 * L * row_pitch(b) + n2) * CS + (size_t)nin * b * n2 * sizeof(T);
+        };
         int B = 16;
-        auto need = [&](int b) { return (size_t)(2 * nh * (b + 1) + nin * M * b + p.dims.n[2]) * CS; };
         while (B > 1 && need(B) > BUDGET) B >>= 1;
-        size_t smem = need(B);
+        const size_t smem = need(B);
         Specs<C> si;
         for (int i = 0; i < nin; i++) si.p[i] = in[i];
         cudaFuncSetAttribute(fft_z_c2r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1449,7 +1523,7 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
             const int pi[6] = {0, 0, 0, 1, 1, 2}, pj[6] = {0, 1, 2, 1, 2, 2};
             for (int c = 0; c < 6; c++) e.factor[c] = (1. + (pi[c] != pj[c])) * beta / (it == 0 ? (1. + beta) : 1.);
         }
-        if (!los && fast_len(p.dims.n[1]) && !getenv_generic() && tma_enabled()) {
+        if (!los && p.dims.n[2] % 2 == 0 && fast_len(p.dims.n[1]) && !getenv_generic() && tma_enabled()) {
             // x pass to the three spectra E, s_x E, k_x^2 E (S1..S3), inverse y forming the six
             // Hessian terms and combining them into the quadratic in x2 (A, B, C in S4..S6), then
             // the z pass over C, B, A

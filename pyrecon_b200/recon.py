@@ -63,8 +63,8 @@ class BaseReconstruction(BaseClass):
         self.set_los(los)
         _lib.load()
         if not _lib.load().prc_fft_supported(_lib.i3(self.info.nmesh)):
-            raise MeshError('nmesh {} is not supported by the CUDA FFT (each axis must be 2^a 3^b 5^c 7^d <= 1024, '
-                            'the last one even)'.format(self.info.nmesh))
+            raise MeshError('nmesh {} is not supported by the CUDA FFT (each axis must be between 2 and 2048)'.format(
+                self.info.nmesh))
         self.fft_engine = 'cuda'
         self.fft_wisdom = None
         self._ws = workspace if workspace is not None else _Workspace(self.device)

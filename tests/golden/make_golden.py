@@ -94,6 +94,22 @@ CASES = [
          density_kwargs=dict(method='real')),
     dict(name='ifft_f4_real', algorithm='iterative_fft', dtype='f4', los=None, nmesh=16, boxsize=800., boxcenter=1600.,
          density_kwargs=dict(method='real', nsigmas=3.)),
+    # mesh sizes with prime factors above 7 and odd last axes (any size the reference's FFT engines take)
+    dict(name='ifft_f8_prime', algorithm='iterative_fft', dtype='f8', los=None, nmesh=[13, 11, 9],
+         boxsize=[650., 550., 450.], boxcenter=[1600., 100., -200.]),
+    dict(name='ifft_f4_prime', algorithm='iterative_fft', dtype='f4', los=None, nmesh=[13, 11, 9],
+         boxsize=[650., 550., 450.], boxcenter=[1600., 100., -200.]),
+    dict(name='mg_f8_prime', algorithm='multigrid', dtype='f8', los=None, nmesh=[13, 11, 9],
+         boxsize=[650., 550., 450.], boxcenter=[1600., 100., -200.]),
+    dict(name='pp_f8_odd', algorithm='plane_parallel_fft', dtype='f8', los='z', nmesh=[15, 22, 21],
+         boxsize=[750., 1100., 1050.], boxcenter=[1600., 0., 300.]),
+    dict(name='ifftp_f8_prime', algorithm='iterative_fft_particle', dtype='f8', los=None, nmesh=[17, 12, 19],
+         boxsize=[850., 600., 950.], boxcenter=[1600., 100., -200.]),
+    # 125^3 (5^3: odd on every axis): inputs and shifts only (the meshes would make a 100 MB fixture)
+    dict(name='ifft_f8_n125', algorithm='iterative_fft', dtype='f8', los=None, nmesh=125, boxsize=1000.,
+         boxcenter=1600., light=True),
+    dict(name='mg_f8_n125', algorithm='multigrid', dtype='f8', los=None, nmesh=125, boxsize=1000., boxcenter=1600.,
+         light=True),
 ]
 
 NDATA, NRANDOMS = 1500, 4000
@@ -151,6 +167,9 @@ def run_case(pyrecon, case, seed):
         out['mesh_phi'] = np.array(recon.mesh_phi.value)
     else:
         out['mesh_psi'] = np.stack([np.array(p.value) for p in recon.mesh_psi])
+    if case.get('light', False):
+        for k in ['mesh_data', 'mesh_randoms', 'mesh_delta', 'mesh_phi', 'mesh_psi', 'keys_data']:
+            out.pop(k, None)
     out['shifts_disp'] = recon.read_shifts(data, field='disp')
     out['shifts_rsd'] = recon.read_shifts(data, field='rsd')
     out['shifted_data'] = recon.read_shifted_positions(data)

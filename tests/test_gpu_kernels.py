@@ -204,12 +204,38 @@ def test_fft_against_numpy(nmesh, dtype):
     assert maxrel(back.cpu().numpy(), x) < tol
 
 
-def test_fft_unsupported_sizes():
+def test_fft_supported_sizes():
     L = lib()
     assert L.load().prc_fft_supported(L.i3((16, 16, 16))) == 1
-    assert L.load().prc_fft_supported(L.i3((11, 16, 16))) == 0     # prime factor 11
-    assert L.load().prc_fft_supported(L.i3((16, 16, 15))) == 0     # odd last axis
-    assert L.load().prc_fft_supported(L.i3((2048, 16, 16))) == 0   # above 1024
+    assert L.load().prc_fft_supported(L.i3((11, 16, 16))) == 1     # prime factor 11
+    assert L.load().prc_fft_supported(L.i3((16, 16, 15))) == 1     # odd last axis
+    assert L.load().prc_fft_supported(L.i3((2048, 16, 16))) == 1   # above the register kernels' 1024
+    assert L.load().prc_fft_supported(L.i3((2049, 16, 16))) == 0   # above 2048
+    assert L.load().prc_fft_supported(L.i3((16, 1, 16))) == 0
+
+
+@pytest.mark.parametrize('nmesh', [(13, 11, 9), (17, 19, 23), (125, 125, 125), (1021, 4, 6), (6, 4, 1021),
+                                   (2048, 8, 8), (8, 6, 2048), (9, 2046, 5), (3, 2, 3), (22, 26, 34)])
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+def test_fft_any_size_against_numpy(nmesh, dtype):
+    """Every axis length the reference's FFT engines take (up to 2048): prime factors above 7 by direct
+    summation, odd last axes as full-length transforms, powers of two above 1024 on the shared-memory kernels."""
+    L = lib()
+    t = torch()
+    rng = np.random.default_rng(18)
+    x = rng.standard_normal(nmesh).astype(dtype)
+    ref = np.fft.rfftn(x.astype('f8'))
+    cdt = t.complex64 if dtype == 'f4' else t.complex128
+    spec = t.empty((nmesh[0], nmesh[1], nmesh[2] // 2 + 1), dtype=cdt, device='cuda')
+    nm = L.i3(nmesh)
+    dx = dev(x)
+    L.call('prc_rfft3d_' + L.suffix(dtype), L.ptr(dx), np.dtype(dtype).itemsize, L.ptr(spec), nm, stream())
+    tol = 5e-5 if dtype == 'f4' else 1e-12
+    got = spec.cpu().numpy()
+    assert np.abs(got - ref).max() / np.abs(ref).max() < tol
+    back = t.empty(nmesh, dtype=t.float32 if dtype == 'f4' else t.float64, device='cuda')
+    L.call('prc_irfft3d_' + L.suffix(dtype), L.ptr(spec), L.ptr(back), nm, stream())
+    assert maxrel(back.cpu().numpy(), x) < tol
 
 
 @pytest.mark.parametrize('los', [None, [0., 0., 1.], [0.3, -0.5, 0.8]])

@@ -21,12 +21,10 @@ F8_CASES = [c for c in golden_cases() if load_golden(c)['meta']['dtype'] == 'f8'
 def test_f8_matches_reference(name):
     g = load_golden(name)
     out, rec = run_gpu(g)
-    assert maxrel(out['mesh_data'], g['mesh_data']) < 1e-13
-    if 'mesh_randoms' in g:
-        assert maxrel(out['mesh_randoms'], g['mesh_randoms']) < 1e-13
-    assert maxrel(out['mesh_delta'], g['mesh_delta']) < 1e-10, name
-    key = 'mesh_phi' if 'mesh_phi' in g else 'mesh_psi'
-    assert maxrel(out[key], g[key]) < 1e-9, name
+    for key, tol in [('mesh_data', 1e-13), ('mesh_randoms', 1e-13), ('mesh_delta', 1e-10), ('mesh_phi', 1e-9),
+                     ('mesh_psi', 1e-9)]:
+        if key in g:        # the large-mesh fixtures keep inputs and shifts only
+            assert maxrel(out[key], g[key]) < tol, (name, key)
     for k in ['shifts_disp', 'shifts_rsd', 'shifted_data', 'shifted_randoms', 'shifts_data_disp', 'shifts_data_rsd',
               'shifted_data_str']:
         if k in g:
