@@ -41,7 +41,8 @@ def test_host_only_entry_points():
     assert _lib.status_string(2) == 'workspace too small'
     assert lib.prc_fft_supported(_lib.i3((512, 512, 512))) == 1
     assert lib.prc_fft_supported(_lib.i3((384, 192, 320))) == 1
-    assert lib.prc_fft_supported(_lib.i3((13, 16, 16))) == 0
+    assert lib.prc_fft_supported(_lib.i3((13, 16, 15))) == 1      # any size: prime factors, odd last axis
+    assert lib.prc_fft_supported(_lib.i3((2049, 16, 16))) == 0    # above 2048
     assert lib.prc_assign_cic_workspace_bytes(_lib.i3((512, 512, 512)), 25_000_000, 4) > 25_000_000 * 16
     assert lib.prc_iterative_fft_workspace_bytes(_lib.i3((512, 512, 512)), 4, 1) > 7 * 512 * 512 * 257 * 8
     assert lib.prc_multigrid_workspace_bytes(_lib.i3((64, 64, 64)), 4, 1) > 64 ** 3 * 8 * 2
