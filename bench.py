@@ -609,7 +609,7 @@ def multi_workload(args, w, device, rank):
         free_at = max(free_at, at) + dt
         fifo.append(free_at - at)
     launches0 = None
-    with ClockSampler(local_rank) as clocks:
+    with ClockSampler(device.index or 0) as clocks:
         server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=w.get('hbm_budget'),
                                       max_batch=w.get('max_batch', 1))
         # warm-up of the request loop: the whole request set once, all at once (each slot's scratch and
@@ -742,7 +742,15 @@ def main(argv=None):
     ap.add_argument('--no-multi', action='store_true', help='skip the batched and served comparison with the plain path')
     ap.add_argument('--kernel', default=None, choices=sorted(KERNELS),
                     help='time one kernel through the C ABI instead of a workload')
+    ap.add_argument('--tune', action='append', default=[], metavar='NAME:KEY=VALUE',
+                    help='set an entry of the run-time tuning table before running (repeatable)')
     args = ap.parse_args(argv)
+    if args.tune:
+        from pyrecon_b200 import _lib
+        for item in args.tune:
+            name, rest = item.split(':', 1)
+            key, value = rest.split('=', 1)
+            _lib.tune_set(name, int(key), int(value))
     if args.kernel is not None:
         return run_kernel_arm(args)
     if args.workload in MULTI_WORKLOADS:

@@ -253,6 +253,17 @@ PRC_API prc_status_t prc_ifftp_read_f64(const double *psi4, const int32_t nmesh[
 #define PRC_FAULT_SMEM_ALIGN 2u
 PRC_API unsigned int prc_device_fault_flags(int reset);
 
+/* Run-time tuning table (no counterpart in the reference; its nearest relative is the FFTW wisdom of
+ * pyrecon/mesh.py:1050-1081): integer knob `name` for key `key` (a mesh axis length), read by the
+ * launchers at launch time; value < 0 removes an entry, prc_tune_clear removes all.  Knobs:
+ *   "mg_jacobi" (FP32 sweeps), "mg_jacobi_f64" (FP64 sweeps), key = level n0: 0 = one damped-Jacobi
+ *   sweep per pass, s > 0 = two sweeps per pass (temporal blocking), each block marching through slabs
+ *   of s planes along x.
+ * pyrecon_b200.tuning times the choices on the device and stores them as JSON wisdom. */
+PRC_API int prc_tune_set(const char *name, int key, int value);
+PRC_API int prc_tune_get(const char *name, int key, int dflt);
+PRC_API void prc_tune_clear(void);
+
 /* Test hook of the failure path (no counterpart in the reference): one CTA arms its transaction
  * barrier for bytes that no copy delivers (none is issued, so nothing is ever in flight), waits at
  * most limit_ns (0 < limit_ns <= 1 s) through the same bounded wait the FFT kernels use, sets

@@ -40,6 +40,9 @@ _SIGNATURES = {
     'prc_zeldovich_psi_workspace_bytes': (c_size, [I3, c_int]),
     'prc_device_fault_flags': (ctypes.c_uint, [c_int]),
     'prc_debug_wait_timeout': (c_int, [c_i64, _p, _p]),
+    'prc_tune_set': (c_int, [ctypes.c_char_p, c_int, c_int]),
+    'prc_tune_get': (c_int, [ctypes.c_char_p, c_int, c_int]),
+    'prc_tune_clear': (None, []),
     'prc_assign_cic_workspace_bytes': (c_size, [I3, c_i64, c_int]),
     'prc_assign_cic': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size, _p]),
     'prc_assign_cic_order': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size,
@@ -167,6 +170,19 @@ def call(name, *args, error=None):
         exc = error or LibraryError
         raise exc('{} failed: {} (status {})'.format(name, status_string(status), status))
     return status
+
+
+def tune_set(name, key, value):
+    """Set knob `name` for key `key` (a mesh axis length) of the run-time tuning table; value < 0 removes it."""
+    call('prc_tune_set', name.encode(), int(key), int(value))
+
+
+def tune_get(name, key, default=-1):
+    return int(load().prc_tune_get(name.encode(), int(key), int(default)))
+
+
+def tune_clear():
+    load().prc_tune_clear()
 
 
 def launch_count():

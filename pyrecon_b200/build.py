@@ -22,7 +22,7 @@ CSRC = os.path.join(HERE, 'csrc')
 BUILD = os.path.join(HERE, '_build')
 LIBDIR = os.path.join(HERE, 'lib')
 LIBNAME = 'libpyrecon_cuda.so'
-SOURCES = ['cic.cu', 'fft.cu', 'multigrid.cu', 'misc.cu']
+SOURCES = ['cic.cu', 'fft.cu', 'multigrid.cu', 'misc.cu', 'tune.cu']
 HEADERS = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith('.cuh')) + \
     [os.path.join(ROOT, 'include', 'pyrecon_cuda.h')]
 

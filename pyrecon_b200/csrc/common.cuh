@@ -141,6 +141,10 @@ __device__ __forceinline__ typename promote<P, F>::type wrap_position(P p, const
 __host__ __forceinline__ int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
 int device_sm_count();
+// Run-time tuning table (tune.cu): knob `name` for key `key` (a mesh axis length), or `dflt` when unset;
+// the generation counter changes with every update.
+int tune_get(const char* name, int key, int dflt);
+unsigned tune_generation();
 
 // Adds n to the launch counter (kernels replayed inside a CUDA graph launch).
 void add_launches(unsigned long long n);

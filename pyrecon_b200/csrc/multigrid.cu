@@ -179,29 +179,54 @@ __device__ __forceinline__ bool quad_of(const int n[3], Quad& q) {
 //   W = sum_a p_a^2 (v+a + v-a) + 1/2 sum_{a<b} p_a p_b e_ab [+ sum_a p_a (v+a - v-a), local]
 //   S(v) = U + g W,   2 sum_a G_a = 2 (sum_a 1/h_a^2 + g P).
 // x and y are fixed for the thread, so the p_0, p_1 terms are computed once for its four cells.
-template <typename A, typename V, typename S, bool LOCAL>
-__device__ __forceinline__ void quad_terms(const V* __restrict__ v, const Stencil<S>& s, const Quad& q, A (&U)[4],
-                                           A (&W)[4], A (&qq)[4], A (&P)[4]) {
+// The nine columns a quad's operator reads: the centre and the four axis neighbours at z0 - 1 .. z0 + 4,
+// the four (x +- 1, y +- 1) edge columns at z0 .. z0 + 3.
+template <typename V> struct QuadCols {
+    V c[6], XP[6], XM[6], YP[6], YM[6], PP[4], MM[4], MP[4], PM[4];
+};
+
+template <typename V, typename S>
+__device__ __forceinline__ void quad_load(const V* __restrict__ v, const Stencil<S>& s, const Quad& q, QuadCols<V>& Q) {
     const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
     const int64_t sx = (int64_t)n1 * n2;
     const int64_t xp = (int64_t)wrap_up(q.x, n0) * sx, xm = (int64_t)wrap_dn(q.x, n0) * sx, x0 = (int64_t)q.x * sx;
     const int64_t yp = (int64_t)wrap_up(q.y, n1) * n2, ym = (int64_t)wrap_dn(q.y, n1) * n2, y0 = (int64_t)q.y * n2;
-    V c[6], XP[6], XM[6], YP[6], YM[6], PP[4], MM[4], MP[4], PM[4];
-    load6(v + x0 + y0, q.z0, n2, c);
-    load6(v + xp + y0, q.z0, n2, XP);
-    load6(v + xm + y0, q.z0, n2, XM);
-    load6(v + x0 + yp, q.z0, n2, YP);
-    load6(v + x0 + ym, q.z0, n2, YM);
-    load4(v + xp + yp + q.z0, PP);
-    load4(v + xm + ym + q.z0, MM);
-    load4(v + xm + yp + q.z0, MP);
-    load4(v + xp + ym + q.z0, PM);
+    load6(v + x0 + y0, q.z0, n2, Q.c);
+    load6(v + xp + y0, q.z0, n2, Q.XP);
+    load6(v + xm + y0, q.z0, n2, Q.XM);
+    load6(v + x0 + yp, q.z0, n2, Q.YP);
+    load6(v + x0 + ym, q.z0, n2, Q.YM);
+    load4(v + xp + yp + q.z0, Q.PP);
+    load4(v + xm + ym + q.z0, Q.MM);
+    load4(v + xm + yp + q.z0, Q.MP);
+    load4(v + xp + ym + q.z0, Q.PM);
+}
+
+// The operator at the four cells of a quad (x, y, z0 .. z0 + 3), rearranged so that a cell needs one
+// division.  With q = sum_a h_a^2 p_a^2 (so g = beta / q) and P = sum_a p_a^2:
+//   U = sum_a (v+a + v-a) / h_a^2
+//   W = sum_a p_a^2 (v+a + v-a) + 1/2 sum_{a<b} p_a p_b e_ab [+ sum_a p_a (v+a - v-a), local]
+//   S(v) = U + g W,   2 sum_a G_a = 2 (sum_a 1/h_a^2 + g P).
+// x and y are fixed for the thread, so the p_0, p_1 terms are computed once for its four cells.  Every
+// quad kernel (one sweep from global memory, two sweeps from shared memory) evaluates this function.
+template <typename A, typename V, typename S, bool LOCAL>
+__device__ __forceinline__ void quad_compute(const QuadCols<V>& Q, const Stencil<S>& s, int x, int y, int z0,
+                                             A (&U)[4], A (&W)[4], A (&qq)[4], A (&P)[4]) {
+    const V(&c)[6] = Q.c;
+    const V(&XP)[6] = Q.XP;
+    const V(&XM)[6] = Q.XM;
+    const V(&YP)[6] = Q.YP;
+    const V(&YM)[6] = Q.YM;
+    const V(&PP)[4] = Q.PP;
+    const V(&MM)[4] = Q.MM;
+    const V(&MP)[4] = Q.MP;
+    const V(&PM)[4] = Q.PM;
     const A ih0 = (A)s.ih2[0], ih1 = (A)s.ih2[1], ih2 = (A)s.ih2[2];
     A p0, p1, p2b;
     if (LOCAL) {
-        p0 = (A)q.x + (A)s.off[0];
-        p1 = (A)q.y + (A)s.off[1];
-        p2b = (A)q.z0 + (A)s.off[2];
+        p0 = (A)x + (A)s.off[0];
+        p1 = (A)y + (A)s.off[1];
+        p2b = (A)z0 + (A)s.off[2];
     } else {
         p0 = (A)s.losh[0];
         p1 = (A)s.losh[1];
@@ -232,9 +257,47 @@ __device__ __forceinline__ void quad_terms(const V* __restrict__ v, const Stenci
     }
 }
 
+
+template <typename A, typename V, typename S, bool LOCAL>
+__device__ __forceinline__ void quad_terms(const V* __restrict__ v, const Stencil<S>& s, const Quad& q, A (&U)[4],
+                                           A (&W)[4], A (&qq)[4], A (&P)[4]) {
+    QuadCols<V> Q;
+    quad_load(v, s, q, Q);
+    quad_compute<A, V, S, LOCAL>(Q, s, q.x, q.y, q.z0, U, W, qq, P);
+}
+
 template <typename T> __device__ __forceinline__ T quotient(T a, T b) {
     if constexpr (sizeof(T) == 4) return __fdividef(a, b);   // FP32 sweeps: fast reciprocal (2 ulp)
     else return a / b;
+}
+
+// quad_compute's terms where v is identically zero (the first sweep of a V-cycle started from zero).
+template <typename T, bool LOCAL>
+__device__ __forceinline__ void quad_zero_terms(const Stencil<T>& s, int x, int y, int z0, T (&U)[4], T (&W)[4],
+                                                T (&qq)[4], T (&P)[4], T (&vc)[4]) {
+    const T p0 = LOCAL ? (T)x + s.off[0] : s.losh[0], p1 = LOCAL ? (T)y + s.off[1] : s.losh[1];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const T p2 = LOCAL ? (T)(z0 + k) + s.off[2] : s.losh[2];
+        const T s2 = p2 * p2;
+        qq[k] = s.h2[0] * p0 * p0 + s.h2[1] * p1 * p1 + s.h2[2] * s2;
+        P[k] = p0 * p0 + p1 * p1 + s2;
+        U[k] = W[k] = vc[k] = (T)0;
+    }
+}
+
+// The damped-Jacobi update of a quad: jac = (q (f + U) + beta W) / (2 (q sum 1/h^2 + beta P)),
+// o = v + w (jac - v).
+template <typename T>
+__device__ __forceinline__ void quad_blend(const Stencil<T>& s, T w, const T (&fv)[4], const T (&vc)[4],
+                                           const T (&U)[4], const T (&W)[4], const T (&qq)[4], const T (&P)[4],
+                                           T (&o)[4]) {
+    const T sih = s.ih2[0] + s.ih2[1] + s.ih2[2];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const T jac = quotient<T>(qq[k] * (fv[k] + U[k]) + s.beta * W[k], (T)2 * (qq[k] * sih + s.beta * P[k]));
+        o[k] = vc[k] + w * (jac - vc[k]);
+    }
 }
 
 // Damped-Jacobi sweep of four cells per thread:
@@ -250,31 +313,177 @@ __global__ void __launch_bounds__(256) jacobi_sweep4(const T* __restrict__ v, co
     T fv[4], vc[4], U[4], W[4], qq[4], P[4];
     load4(f + q.c + q.z0, fv);
     if (zero_v) {
-        const T p0 = LOCAL ? (T)q.x + s.off[0] : s.losh[0], p1 = LOCAL ? (T)q.y + s.off[1] : s.losh[1];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const T p2 = LOCAL ? (T)(q.z0 + k) + s.off[2] : s.losh[2];
-            const T s2 = p2 * p2;
-            qq[k] = s.h2[0] * p0 * p0 + s.h2[1] * p1 * p1 + s.h2[2] * s2;
-            P[k] = p0 * p0 + p1 * p1 + s2;
-            U[k] = W[k] = vc[k] = (T)0;
-        }
+        quad_zero_terms<T, LOCAL>(s, q.x, q.y, q.z0, U, W, qq, P, vc);
     } else {
         quad_terms<T, T, T, LOCAL>(v, s, q, U, W, qq, P);
         load4(v + q.c + q.z0, vc);
     }
-    const T sih = s.ih2[0] + s.ih2[1] + s.ih2[2];
     T o[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const T jac = quotient<T>(qq[k] * (fv[k] + U[k]) + s.beta * W[k], (T)2 * (qq[k] * sih + s.beta * P[k]));
-        o[k] = vc[k] + w * (jac - vc[k]);
-    }
+    quad_blend(s, w, fv, vc, U, W, qq, P, o);
     if constexpr (sizeof(T) == 4) {
         *(float4*)(vout + q.c + q.z0) = make_float4(o[0], o[1], o[2], o[3]);
     } else {
         ((double2*)(vout + q.c + q.z0))[0] = make_double2(o[0], o[1]);
         ((double2*)(vout + q.c + q.z0))[1] = make_double2(o[2], o[3]);
+    }
+}
+
+// ---- two sweeps per pass (temporal blocking) ----
+// A block owns a tile of TY rows (y) x 4 TQ cells (z) and marches along x through a slab of planes.  At
+// plane step x it stages plane x + 1 of v (the tile grown by two rows and eight cells on each side;
+// planes x - 1 and x are already there), runs the first sweep at plane x over the tile grown by one
+// row and one quad on each side into a ring of three planes in shared memory, then the second sweep at
+// plane x - 1 over the tile from the ring's planes x - 2 .. x.  v and f are read from DRAM once and the
+// result written once per two sweeps (the halo of the first sweep is recomputed by the neighbouring
+// tiles).  Every quad goes through quad_compute / quad_blend, the arithmetic of jacobi_sweep4, so two
+// sweeps here equal two jacobi_sweep4 launches bit for bit.  Periodic in every axis: staged rows and
+// 4-cell chunks wrap (n2 % 4 == 0 keeps every chunk contiguous and aligned).
+template <typename T, int TY, int TQ> struct TbShape {
+    static constexpr int ZP = 4 * TQ + 16;         // row pitch: cells z0 - 8 .. z0 + 4 TQ + 8
+    static constexpr int R0 = TY + 4;              // rows of a staged v plane: y0 - 2 .. y0 + TY + 1
+    static constexpr int R1 = TY + 2;              // rows of a first-sweep plane: y0 - 1 .. y0 + TY
+    static constexpr int Q1 = TQ + 2;              // quads of a first-sweep row: z0 - 4 .. z0 + 4 TQ + 3
+    static constexpr int THREADS = TQ * TY;
+};
+
+__device__ __forceinline__ int wrap_mod(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+template <typename T>
+__device__ __forceinline__ void smem_quad6(const T* row, int i, T (&o)[6]) {   // cells i - 1 .. i + 4, i % 4 == 0
+    T m[4];
+    if constexpr (sizeof(T) == 4) {
+        const float4 a = *(const float4*)(row + i);
+        m[0] = a.x, m[1] = a.y, m[2] = a.z, m[3] = a.w;
+    } else {
+        const double2 a = *(const double2*)(row + i), b = *(const double2*)(row + i + 2);
+        m[0] = a.x, m[1] = a.y, m[2] = b.x, m[3] = b.y;
+    }
+    o[0] = row[i - 1], o[1] = m[0], o[2] = m[1], o[3] = m[2], o[4] = m[3], o[5] = row[i + 4];
+}
+template <typename T> __device__ __forceinline__ void smem_quad4(const T* row, int i, T (&o)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 a = *(const float4*)(row + i);
+        o[0] = a.x, o[1] = a.y, o[2] = a.z, o[3] = a.w;
+    } else {
+        const double2 a = *(const double2*)(row + i), b = *(const double2*)(row + i + 2);
+        o[0] = a.x, o[1] = a.y, o[2] = b.x, o[3] = b.y;
+    }
+}
+template <typename T> __device__ __forceinline__ void smem_store4(T* row, int i, const T (&o)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        *(float4*)(row + i) = make_float4(o[0], o[1], o[2], o[3]);
+    } else {
+        *(double2*)(row + i) = make_double2(o[0], o[1]);
+        *(double2*)(row + i + 2) = make_double2(o[2], o[3]);
+    }
+}
+
+// The columns of the quad at (row r, cell index i) of plane `mid`, its neighbours in planes `lo` (x - 1)
+// and `hi` (x + 1), all with row pitch ZP.
+template <typename T, int ZP>
+__device__ __forceinline__ void smem_cols(const T* lo, const T* mid, const T* hi, int r, int i, QuadCols<T>& Q) {
+    smem_quad6(mid + r * ZP, i, Q.c);
+    smem_quad6(hi + r * ZP, i, Q.XP);
+    smem_quad6(lo + r * ZP, i, Q.XM);
+    smem_quad6(mid + (r + 1) * ZP, i, Q.YP);
+    smem_quad6(mid + (r - 1) * ZP, i, Q.YM);
+    smem_quad4(hi + (r + 1) * ZP, i, Q.PP);
+    smem_quad4(lo + (r - 1) * ZP, i, Q.MM);
+    smem_quad4(lo + (r + 1) * ZP, i, Q.MP);
+    smem_quad4(hi + (r - 1) * ZP, i, Q.PM);
+}
+
+template <typename T, bool LOCAL, int TY, int TQ>
+__global__ void __launch_bounds__(TQ * TY, (sizeof(T) == 4 ? 6 : 4)) jacobi_sweep2_tb(const T* __restrict__ v, const T* __restrict__ f,
+                                                             T* __restrict__ vout, Stencil<T> s, T w, int zero_v,
+                                                             int slab, int nslab) {
+    typedef TbShape<T, TY, TQ> SH;
+    constexpr int ZP = SH::ZP;
+    constexpr int PL0 = SH::R0 * ZP, PL1 = SH::R1 * ZP;
+    __shared__ __align__(16) T v0s[3 * PL0];       // planes x - 1, x, x + 1 of v (ring)
+    __shared__ __align__(16) T v1s[3 * PL1];       // first-sweep planes x - 2, x - 1, x (ring)
+    const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
+    const int64_t N = (int64_t)n0 * n1 * n2;
+    const int prob = blockIdx.z / nslab;
+    const int x0 = (blockIdx.z % nslab) * slab, x1 = min(x0 + slab, n0);
+    v += prob * N, f += prob * N, vout += prob * N;
+    const int y0 = blockIdx.y * TY, z0 = blockIdx.x * (4 * TQ);
+    const int tid = threadIdx.x;
+    const int64_t sx = (int64_t)n1 * n2;
+
+    // stage plane x (periodic) of v into ring slot x mod 3
+    auto stage = [&](int x) {
+        T* dst = v0s + wrap_mod(x, 3) * PL0;
+        const int64_t xo = (int64_t)wrap_mod(x, n0) * sx;
+        constexpr int CH = ZP / 4;                 // 4-cell chunks per staged row
+        for (int q = tid; q < SH::R0 * CH; q += SH::THREADS) {
+            const int r = q / CH, ch = q % CH;
+            const int gy = wrap_mod(y0 - 2 + r, n1), gz = wrap_mod(z0 - 8 + 4 * ch, n2);
+            T m[4];
+            load4(v + xo + (int64_t)gy * n2 + gz, m);
+            smem_store4(dst + r * ZP, 4 * ch, m);
+        }
+    };
+    if (!zero_v) {
+        stage(x0 - 2);
+        stage(x0 - 1);
+    }
+    for (int x = x0 - 1; x <= x1; x++) {
+        if (!zero_v) stage(x + 1);
+        __syncthreads();
+        // first sweep at plane x over rows y0 - 1 .. y0 + TY, quads z0 - 4 .. z0 + 4 TQ
+        {
+            const int gx = wrap_mod(x, n0);
+            const T* lo = v0s + wrap_mod(x - 1, 3) * PL0;
+            const T* mid = v0s + wrap_mod(x, 3) * PL0;
+            const T* hi = v0s + wrap_mod(x + 1, 3) * PL0;
+            T* out = v1s + wrap_mod(x, 3) * PL1;
+            for (int q = tid; q < SH::R1 * SH::Q1; q += SH::THREADS) {
+                const int r = q / SH::Q1, k = q % SH::Q1;
+                const int gy = wrap_mod(y0 - 1 + r, n1), gz = wrap_mod(z0 - 4 + 4 * k, n2);
+                T fv[4], vc[4], U[4], W[4], qq[4], P[4], o[4];
+                load4(f + (int64_t)gx * sx + (int64_t)gy * n2 + gz, fv);
+                if (zero_v) {
+                    quad_zero_terms<T, LOCAL>(s, gx, gy, gz, U, W, qq, P, vc);
+                } else {
+                    QuadCols<T> Q;
+                    smem_cols<T, ZP>(lo, mid, hi, r + 1, 4 * k + 4, Q);
+                    quad_compute<T, T, T, LOCAL>(Q, s, gx, gy, gz, U, W, qq, P);
+                    smem_quad4(mid + (r + 1) * ZP, 4 * k + 4, vc);
+                }
+                quad_blend(s, w, fv, vc, U, W, qq, P, o);
+                smem_store4(out + r * ZP, 4 * k + 4, o);
+            }
+        }
+        __syncthreads();
+        // second sweep at plane x - 1 over the tile
+        const int xo = x - 1;
+        if (xo >= x0) {
+            const T* lo = v1s + wrap_mod(xo - 1, 3) * PL1;
+            const T* mid = v1s + wrap_mod(xo, 3) * PL1;
+            const T* hi = v1s + wrap_mod(xo + 1, 3) * PL1;
+            const int r = tid / TQ, k = tid % TQ;
+            const int gy = y0 + r, gz = z0 + 4 * k;
+            if (gy < n1 && gz < n2) {
+                const int64_t at = (int64_t)xo * sx + (int64_t)gy * n2 + gz;
+                T fv[4], vc[4], U[4], W[4], qq[4], P[4], o[4];
+                load4(f + at, fv);
+                QuadCols<T> Q;
+                smem_cols<T, ZP>(lo, mid, hi, r + 1, 4 * k + 8, Q);
+                quad_compute<T, T, T, LOCAL>(Q, s, xo, gy, gz, U, W, qq, P);
+                smem_quad4(mid + (r + 1) * ZP, 4 * k + 8, vc);
+                quad_blend(s, w, fv, vc, U, W, qq, P, o);
+                if constexpr (sizeof(T) == 4) {
+                    *(float4*)(vout + at) = make_float4(o[0], o[1], o[2], o[3]);
+                } else {
+                    ((double2*)(vout + at))[0] = make_double2(o[0], o[1]);
+                    ((double2*)(vout + at))[1] = make_double2(o[2], o[3]);
+                }
+            }
+        }
     }
 }
 
@@ -429,6 +638,17 @@ static bool quad_ok(const int n[3], const void* a, const void* b, const void* c)
     return n[2] % 4 == 0 && (((uintptr_t)a | (uintptr_t)b | (uintptr_t)c) & 15) == 0;
 }
 
+// Tile of the temporal-blocked sweeps: TB_TY rows x 4 TB_TQ cells.
+constexpr int TB_TY = 8, TB_TQ = 16;
+
+// Slab length of the temporal-blocked sweeps for a level with no tuning-table entry (0: one sweep per
+// pass).
+static int mg_tb_default(const int n[3], size_t tsize) {
+    (void)n;
+    (void)tsize;
+    return 0;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Level hierarchy and the FMG / V-cycle drivers
 // ---------------------------------------------------------------------------------------------
@@ -483,6 +703,8 @@ template <typename T> struct MGRunner {
 
     // niter sweeps ping-ponging between v and tmp; on return v points at the result and tmp at the
     // other buffer (the pointers are swapped instead of copying back).  zero_first: v known zero.
+    // Pairs of sweeps run as one temporal-blocked pass when the tuning table's "mg_jacobi" (FP32) or
+    // "mg_jacobi_f64" entry for the level (keyed by n0) is a slab length > 0 (mg_tb_default otherwise).
     int jacobi(int l, T*& v, const T* f, T*& tmp, int niter, bool zero_first) {
         Stencil<T> s = stencil(l);
         const int64_t N = L[l].size() * count;
@@ -490,7 +712,25 @@ template <typename T> struct MGRunner {
         if (niter == 0 && zero_first && cudaMemsetAsync(v, 0, N * sizeof(T), st) != cudaSuccess) return PRC_ERR_CUDA;
         const bool quad = quad_ok(L[l].n, v, f, tmp);
         const Grid3 gq = grid3_quad(L[l].n, count);
-        for (int it = 0; it < niter; it++) {
+        int it = 0;
+        const int slab =
+            quad ? tune_get(sizeof(T) == 4 ? "mg_jacobi" : "mg_jacobi_f64", L[l].n[0], mg_tb_default(L[l].n, sizeof(T)))
+                 : 0;
+        if (slab > 0) {
+            const int nslab = (L[l].n[0] + slab - 1) / slab;
+            const dim3 grid((L[l].n[2] + 4 * TB_TQ - 1) / (4 * TB_TQ), (L[l].n[1] + TB_TY - 1) / TB_TY, nslab * count);
+            if ((int64_t)nslab * count <= 65535) {
+                for (; it + 1 < niter; it += 2) {
+                    const bool z0 = zero_first && it == 0;
+                    PRC_LAUNCH_B("mg_jacobi2", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
+                                 (s.local ? jacobi_sweep2_tb<T, true, TB_TY, TB_TQ>
+                                          : jacobi_sweep2_tb<T, false, TB_TY, TB_TQ>)<<<grid, TB_TY * TB_TQ, 0, st>>>(
+                                     v, f, tmp, s, (T)P.damping, z0, slab, nslab));
+                    std::swap(v, tmp);
+                }
+            }
+        }
+        for (; it < niter; it++) {
             const bool z0 = zero_first && it == 0;
             if (quad)
                 PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
@@ -781,6 +1021,7 @@ std::string solve_key(int tsize, int mixed, const int32_t nmesh[3], const Params
     key_add(k, P.vn);
     key_add(k, ws);
     key_add(k, wsb);
+    key_add(k, tune_generation());   // kernel choices of the tuning table
     return k;
 }
 

@@ -43,9 +43,13 @@ class BaseReconstruction(BaseClass):
         """
         Parameters are the reference's (recon.py:66-120): growth rate ``f``, ``bias``, line of sight
         ``los`` (None / 'local' for a varying one, 'x' / 'y' / 'z' or a 3-vector), ``wrap`` and the
-        mesh keywords nmesh, boxsize, boxcenter, cellsize, positions, boxpad, dtype.  ``fft_engine``,
-        ``fft_wisdom``, ``save_fft_wisdom``, ``fft_plan`` and ``nthreads`` are accepted for
-        compatibility and ignored (the FFTs are this library's CUDA kernels).
+        mesh keywords nmesh, boxsize, boxcenter, cellsize, positions, boxpad, dtype.  ``fft_engine`` and
+        ``nthreads`` are accepted for compatibility and ignored (the FFTs are this library's CUDA kernels).
+        ``fft_wisdom``, ``save_fft_wisdom`` and ``fft_plan`` keep their meaning for this library's
+        autotuner (:mod:`pyrecon_b200.tuning`): ``fft_wisdom`` (a path or dict) is applied to the kernel
+        launchers' tuning table; with ``save_fft_wisdom`` (True for the default file name, or a path) that
+        file is loaded if it exists, the knobs it lacks for this mesh are timed on the device unless
+        ``fft_plan='estimate'``, and the result is saved there.
 
         Extra: ``device`` (CUDA device, default current), ``mixed_precision`` (dtype 'f4' multigrid
         with FP64 defect correction, default True), ``stream`` (torch.cuda.Stream to enqueue on),
@@ -66,7 +70,10 @@ class BaseReconstruction(BaseClass):
             raise MeshError('nmesh {} is not supported by the CUDA FFT (each axis must be between 2 and 2048)'.format(
                 self.info.nmesh))
         self.fft_engine = 'cuda'
-        self.fft_wisdom = None
+        from . import tuning
+        self.fft_wisdom = tuning.setup(self.info.nmesh, self.info.dtype, fft_wisdom=fft_wisdom,
+                                       save_fft_wisdom=save_fft_wisdom, fft_plan=fft_plan,
+                                       los=None if self.los is None else list(self.los), device=self.device)
         self._ws = workspace if workspace is not None else _Workspace(self.device)
         self._flags = _Flags(self.device)
         self._size_randoms = 0

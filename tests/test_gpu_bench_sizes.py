@@ -87,14 +87,15 @@ ALGOS = {'iterative_fft': 'IterativeFFTReconstruction', 'multigrid': 'MultiGridR
          'plane_parallel_fft': 'PlaneParallelFFTReconstruction'}
 
 
-def _catalogues(algorithm, nmesh):
-    """Seeded lognormal data and uniform randoms (a reduced count of the benchmark's catalogues:
-    the mesh-side kernels are the same at any particle count); multigrid takes FP64 positions and
-    weights U[0.5, 1.5] as in its benchmark, the FFT algorithms FP32 positions and unit weights."""
+def _catalogues(algorithm, nmesh, pos_dtype=None):
+    """Seeded lognormal data and uniform randoms (a reduced count of the benchmark's catalogues, with
+    randoms dense enough that no smoothed-randoms cell sits within rounding of the ran_min threshold,
+    where FP32 and FP64 would mask it differently); multigrid takes FP64 positions and weights
+    U[0.5, 1.5] as in its benchmark, the FFT algorithms FP32 positions and unit weights."""
     from pyrecon_b200 import mocks
     boxsize, boxcenter = 2000., 2000.
-    pos_dtype = 'f8' if algorithm == 'multigrid' else 'f4'
-    nd, nr = 400_000, 1_600_000
+    pos_dtype = pos_dtype or ('f8' if algorithm == 'multigrid' else 'f4')
+    nd, nr = (400_000, 1_600_000) if nmesh <= 256 else (2_000_000, 12_000_000)
     data = mocks.lognormal_positions_numpy(nd, nmesh, boxsize, boxcenter, seed=2100 + nmesh, field_seed=1100 + nmesh,
                                            dtype=pos_dtype)
     randoms = mocks.uniform_positions_numpy(nr, boxsize, boxcenter, seed=3100 + nmesh, dtype=pos_dtype)
@@ -112,13 +113,17 @@ def _los(algorithm):
 _ORACLE = {}
 
 
-def _oracle(algorithm, nmesh):
+def _oracle(algorithm, nmesh, pos_dtype=None):
     """FP64 oracle (the reference's C kernels compiled from source with OpenMP when built, else the C
-    restatement; pocketfft on all host cores) on the case's catalogues; cached per case."""
-    key = (algorithm, nmesh)
+    restatement; pocketfft on all host cores) on the case's catalogues, positions as the GPU run reads
+    them (rounded to `pos_dtype`); cached per case."""
+    rounded = 'f4' if 'f4' in (pos_dtype, 'f8' if algorithm == 'multigrid' else 'f4') else 'f8'
+    key = (algorithm, nmesh, rounded)
     if key not in _ORACLE:
         _ORACLE.clear()
         c = _catalogues(algorithm, nmesh)
+        if pos_dtype is not None:
+            c = dict(c, data=c['data'].astype(pos_dtype), randoms=c['randoms'].astype(pos_dtype))
         kernels = 'reference' if pipeline.reference_kernels_available() else 'oracle'
         rec = pipeline.OracleReconstruction(algorithm, f=0.8, bias=2., los=_los(algorithm), nmesh=nmesh,
                                             boxsize=c['boxsize'], boxcenter=c['boxcenter'], dtype='f8', kernels=kernels,
@@ -161,12 +166,13 @@ def _gpu(algorithm, nmesh, dtype, c, **kwargs):
 
 PIPELINES = [('iterative_fft', 128, 'f4'), ('iterative_fft', 256, 'f4'), ('iterative_fft', 256, 'f8'),
              ('multigrid', 256, 'f4'), ('multigrid', 256, 'f8'), ('plane_parallel_fft', 256, 'f4'),
-             ('plane_parallel_fft', 256, 'f8'), ('iterative_fft', 512, 'f4'), ('iterative_fft', 512, 'f8')]
+             ('plane_parallel_fft', 256, 'f8'), ('iterative_fft', 512, 'f4'), ('iterative_fft', 512, 'f8'),
+             ('multigrid', 512, 'f4')]
 
 
 @pytest.mark.parametrize('algorithm,nmesh,dtype', PIPELINES)
 def test_pipeline_against_fp64_oracle(algorithm, nmesh, dtype, record_property):
-    c, ref = _oracle(algorithm, nmesh)
+    c, ref = _oracle(algorithm, nmesh, pos_dtype=dtype)
     got = _gpu(algorithm, nmesh, dtype, c)
     errs = dict(delta=maxrel(got['delta'], ref['delta']), field=maxrel(got['field'], ref['field']),
                 shifted_data_mpc=maxabs(got['shifted_data'], ref['shifted_data']),

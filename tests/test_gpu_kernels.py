@@ -588,3 +588,56 @@ def test_density_contrast_original_matches_numpy(dtype, randoms):
     assert np.array_equal(out == 0, ref == 0)
     tol = 1e-12 if dtype == 'f8' else 1e-6
     assert maxrel(out, ref) < tol
+
+
+def _jacobi(dtype, nmesh, niter, los, slab, seed=41):
+    """prc_mg_jacobi_* with the tuning table's "mg_jacobi" entry for this n0 set to `slab` (0: one sweep
+    per pass, s > 0: two sweeps per pass in slabs of s planes)."""
+    L, t = lib(), torch()
+    rng = np.random.default_rng(seed)
+    v = dev(rng.standard_normal(nmesh).astype(dtype))
+    f = dev(rng.standard_normal(nmesh).astype(dtype))
+    scratch = t.empty_like(v)
+    knob = 'mg_jacobi' if dtype == 'f4' else 'mg_jacobi_f64'
+    L.tune_set(knob, nmesh[0], slab)
+    try:
+        L.call('prc_mg_jacobi_' + L.suffix(dtype), L.ptr(v), L.ptr(f), L.ptr(scratch), L.i3(nmesh),
+               L.d3([800., 600., 1000.]), L.d3([1600., 0., 300.]), 0.4, 0.4, niter, L.opt_d3(los), stream())
+        return v.cpu().numpy()
+    finally:
+        L.tune_set(knob, nmesh[0], -1)
+
+
+@pytest.mark.parametrize('nmesh', [(16, 12, 20), (24, 16, 32), (8, 8, 8), (64, 48, 40), (128, 64, 96), (96, 200, 68)])
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+@pytest.mark.parametrize('los', [None, [0.3, -0.5, 0.8]])
+def test_jacobi_two_sweeps_per_pass_bit_exact(nmesh, dtype, los):
+    """Temporal blocking (two damped-Jacobi sweeps per pass, shared-memory plane rings, x-marching slabs)
+    gives the bits of one sweep per pass: odd sweep counts, slabs longer and shorter than the mesh,
+    tiles cut by the mesh edge and tiles larger than the mesh."""
+    if los is not None:
+        los = list(np.asarray(los) / np.linalg.norm(los))
+    ref = _jacobi(dtype, nmesh, 5, los, 0)
+    for slab in [1, 3, 8, 64]:
+        got = _jacobi(dtype, nmesh, 5, los, slab)
+        assert np.array_equal(got, ref), (nmesh, dtype, slab, np.abs(got - ref).max())
+
+
+@pytest.mark.parametrize('dtype,mixed', [('f8', False), ('f4', True), ('f4', False)])
+def test_multigrid_solve_with_temporal_blocking_bit_exact(dtype, mixed):
+    """A whole solve (graph-captured) with two sweeps per pass on every level gives the bits of the solve
+    with one sweep per pass; the tuning change makes the solve capture a new graph."""
+    L = lib()
+    nmesh = (32, 32, 32)
+    knob = 'mg_jacobi' if dtype == 'f4' else 'mg_jacobi_f64'
+    for n in [32, 16, 8]:
+        L.tune_set(knob, n, 0)
+    try:
+        ref = mg_solve(dtype, mixed, nmesh=nmesh)[0]
+        for n in [32, 16, 8]:
+            L.tune_set(knob, n, 4)
+        got = mg_solve(dtype, mixed, nmesh=nmesh)[0]
+    finally:
+        for n in [32, 16, 8]:
+            L.tune_set(knob, n, -1)
+    assert np.array_equal(got, ref)
