@@ -110,9 +110,10 @@ PRC_API prc_status_t prc_assign_cic_order(double *mesh, double *column_sums, con
  * the library until the process exits).  Same arguments, results and flags as prc_assign_cic
  * (equal to it to FP64 rounding), but particles are painted in chunks of 2^18, each accumulated
  * into the mesh.  Meshes with more than 2^20 (x, y) columns, or n2 > 4096, are rejected with
- * PRC_ERR_UNSUPPORTED.  The first call on a device looks up the array's address (make it before
- * any stream capture).  Every call shares the array: calls that overlap on the GPU (other streams,
- * other host threads) race and must be serialised by the caller. */
+ * PRC_ERR_UNSUPPORTED.  The first call on a device (per driver context: each context holds its own
+ * copy of the array) looks up the array's address (make it before any stream capture).  Every call
+ * shares the array: calls that overlap on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller. */
 PRC_API prc_status_t prc_assign_cic_noalloc(double *mesh, double *column_sums, const int32_t nmesh[3],
                                             const double boxsize[3], const double boxcenter[3], int mesh_bytes,
                                             const void *positions, int pos_bytes, const void *weights,

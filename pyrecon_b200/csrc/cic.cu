@@ -13,6 +13,8 @@
 //                z = iz and z = iz + 1.  Same inputs -> same bits, run after run.
 #include "common.cuh"
 
+#include <cuda.h>
+
 #include <limits.h>
 
 #include <algorithm>
@@ -1098,18 +1100,38 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)17 << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch on the current device, looked up once per device.
+// The calling thread's current driver context (null when none is current yet: the runtime then uses
+// the device's primary context), fetched through the runtime so the library does not link libcuda.
+static void* current_context() {
+    typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+    static CtxGetCurrentFn fn = []() -> CtxGetCurrentFn {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return (CtxGetCurrentFn)f;
+    }();
+    CUcontext c = nullptr;
+    if (fn != nullptr && fn(&c) != CUDA_SUCCESS) c = nullptr;
+    return (void*)c;
+}
+
+// Device address of g_noalloc_scratch in the current context of the current device, looked up once per
+// (device, context): every context that loads the module holds its own copy of the array, so an address
+// is only valid in the context it was looked up in.
 static void* noalloc_scratch_address() {
     static std::mutex mu;
-    static std::map<int, void*> cache;
+    static std::map<std::pair<int, void*>, void*> cache;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    const std::pair<int, void*> key(dev, current_context());
     std::lock_guard<std::mutex> lock(mu);
-    auto it = cache.find(dev);
+    auto it = cache.find(key);
     if (it != cache.end()) return it->second;
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return nullptr;
-    cache[dev] = p;
+    cache[key] = p;
     return p;
 }
 

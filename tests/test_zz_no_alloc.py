@@ -72,3 +72,21 @@ def test_noalloc_paint_rejects_oversized_mesh():
     status = L.load().prc_assign_cic_noalloc(L.ptr(mesh), None, L.i3((2048, 1024, 8)), L.d3([1.] * 3), L.d3([0.] * 3),
                                              8, None, 8, None, 0, 0, 0, 0, L.ptr(flags), st)
     assert status == 4   # PRC_ERR_UNSUPPORTED: more than 2^20 (x, y) columns
+
+
+def test_noalloc_paint_at_the_stated_maximum():
+    """2^20 (x, y) columns in FP64, more particles than one chunk: the largest mesh the built-in scratch
+    serves gives the workspace paint's mesh; one more cell along z than 4096 is rejected."""
+    torch, L = _setup()
+    nmesh = (1024, 1024, 8)
+    pos, w = _catalog(600_000, 3, 'f8')
+    ref, ref_cols = _paint('prc_assign_cic', pos, w, nmesh, 8)
+    got, got_cols = _paint('prc_assign_cic_noalloc', pos, w, nmesh, 8)
+    assert float((got - ref).abs().max()) <= 1e-13 * float(ref.abs().max())
+    assert float((got_cols - ref_cols).abs().max()) <= 1e-12 * float(ref_cols.abs().max())
+    mesh = torch.zeros(1, dtype=torch.float64, device='cuda')
+    flags = torch.zeros(1, dtype=torch.int32, device='cuda')
+    st = L.stream_of(torch.device('cuda'))
+    status = L.load().prc_assign_cic_noalloc(L.ptr(mesh), None, L.i3((8, 8, 4104)), L.d3([1.] * 3), L.d3([0.] * 3),
+                                             8, None, 8, None, 0, 0, 0, 0, L.ptr(flags), st)
+    assert status == 4   # PRC_ERR_UNSUPPORTED: n2 above 4096
