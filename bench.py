@@ -494,6 +494,14 @@ def run_gpu_arm(args, w):
                     bytes_per_launch=kbytes / nl, launch_ms=kms / nl, peak_source=peak_kind + ' (MEASURED_PEAKS.json hbm_gbs)')
 
     # --- the metric's comparison with the plain GPU path: many requests through the request loop ---
+    # (the single-request workload's catalogues and cached scratch are released first)
+    pos_mb = (data.numel() + randoms.numel()) * data.element_size() / 1e6
+    del data, wd, randoms, wr, step
+    if e2e is not None:
+        del hd, hwd, hr, hwr, e2e_step
+    import gc
+    gc.collect()
+    torch.cuda.empty_cache()
     baseline_metric = None
     if world == 1 and not args.no_multi:
         baseline_metric = {}
@@ -513,8 +521,7 @@ def run_gpu_arm(args, w):
                     data='synthetic: seeded lognormal data (sigma_G=0.8, P(k)~k^-1.5 exp(-(8k)^2)) + uniform randoms',
                     config=dict(workload=workload_name(w), parallelism='replicas (one independent reconstruction per GPU)',
                                 precision='f4 mesh pipeline, FP64 CIC sums and normalisation',
-                                l2='inputs larger than L2 (positions {:.0f} MB)'.format(
-                                    (data.numel() + randoms.numel()) * data.element_size() / 1e6)),
+                                l2='inputs larger than L2 (positions {:.0f} MB)'.format(pos_mb)),
                     latency_ms=dict(p50=percentile(per_step, 50), p99=percentile(per_step, 99)),
                     shift_err_mpc=shift_err, baseline_metric=baseline_metric,
                     e2e=e2e, roofline=roofline, cpu_baseline=cpu, gpu_launches=int(launches),
@@ -575,6 +582,7 @@ def multi_workload(args, w, device, rank):
     arrival times, where throughput is bounded by the arrival rate and the comparison is the latency against
     the plain path serving the same arrivals first come, first served).  Both warmed up by one pass over the
     requests.  Wall clock with the device synchronised on both sides.  Returns the JSON line."""
+    import gc
     import torch
     import numpy as np
     from pyrecon_b200 import _lib
@@ -609,8 +617,16 @@ def multi_workload(args, w, device, rank):
         free_at = max(free_at, at) + dt
         fifo.append(free_at - at)
     launches0 = None
+    budget = w.get('hbm_budget')
+    if budget is not None:
+        # the admission budget cannot exceed what the device has free (the plain path's cached scratch is
+        # released first); the slots' resident scratch comes out of it too
+        gc.collect()
+        torch.cuda.empty_cache()
+        free, _ = torch.cuda.mem_get_info(device)
+        budget = min(budget, 0.8 * free)
     with ClockSampler(device.index or 0) as clocks:
-        server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=w.get('hbm_budget'),
+        server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=budget,
                                       max_batch=w.get('max_batch', 1))
         # warm-up of the request loop: the whole request set once, all at once (each slot's scratch and
         # multigrid graphs, the streams' allocator pools), as a long-running server would be
@@ -633,6 +649,9 @@ def multi_workload(args, w, device, rank):
         stats = server.stats()
         server.close()
     launches = _lib.launch_count() - launches0
+    del server
+    gc.collect()
+    torch.cuda.empty_cache()
     pct = lambda xs, q: 1e3 * sorted(xs)[min(len(xs) - 1, int(round(q / 100. * (len(xs) - 1))))]
     n = len(reqs)
     del reqs
@@ -642,6 +661,7 @@ def multi_workload(args, w, device, rank):
                     ms_per_step=served_s * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None,
                     dtype=w['dtype'], data='synthetic: seeded lognormal catalogues, one per nmesh, requests take prefixes',
                     config=dict(workload=w['name'], requests=n, slots=w['slots'], max_batch=w.get('max_batch', 1),
+                                hbm_budget_gb=None if budget is None else round(budget / 1e9, 1),
                                 arrivals='poisson {:g}/s'.format(w['rate']) if w['kind'] == 'serving' else 'all at once',
                                 nmesh=w['nmesh'], algorithms=w['algorithms'], timing='wall clock, device synchronised'),
                     served=dict(recons_per_s=n / served_s, p50_ms=stats['p50_ms'], p99_ms=stats['p99_ms'],

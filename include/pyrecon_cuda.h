@@ -416,6 +416,24 @@ PRC_API prc_status_t prc_multigrid_batch_f64(const double *const *delta, double 
                                              int jacobi_niterations, int vcycle_niterations, const double *los,
                                              void *workspace, size_t workspace_bytes, void *stream);
 
+/* The mixed-precision FP32 solve (prc_multigrid_f32 / prc_multigrid_batch_f32 with mixed_precision = 1)
+ * that also returns its FP64 iterate: phi (FP32, the mesh dtype) and phi64 (FP64; NULL entries, or a
+ * NULL array, skip it).  The reference stores phi in the mesh dtype (pyrecon/multigrid.py:115-133), so
+ * its FP32 finite-difference read-out inherits the FP32 rounding of phi (|phi| ~ 1e5 at 2000 Mpc/h and
+ * nmesh 256: ~1e-3 Mpc/h on the shifts); reading shifts from phi64 (prc_read_shifts_phi_f64 with the
+ * same positions) keeps the refinement's accuracy.  Same workspace as the mixed FP32 solve. */
+PRC_API prc_status_t prc_multigrid_mixed_f32(const float *delta, float *phi, double *phi64, const int32_t nmesh[3],
+                                             const double boxsize[3], const double boxcenter[3], double beta,
+                                             double damping, int jacobi_niterations, int vcycle_niterations,
+                                             const double *los, void *workspace, size_t workspace_bytes,
+                                             void *stream);
+PRC_API prc_status_t prc_multigrid_batch_mixed_f32(const float *const *delta, float *const *phi,
+                                                   double *const *phi64, int count, const int32_t nmesh[3],
+                                                   const double boxsize[3], const double boxcenter[3], double beta,
+                                                   double damping, int jacobi_niterations, int vcycle_niterations,
+                                                   const double *los, void *workspace, size_t workspace_bytes,
+                                                   void *stream);
+
 /* Components, one level (jacobi: src/multigrid.c:44-104, residual :107-164, prolong :167-209,
  * reduce :212-266).  jacobi runs `niterations` sweeps in place on v using `scratch` (one mesh). */
 PRC_API prc_status_t prc_mg_jacobi_f32(float *v, const float *f, float *scratch, const int32_t nmesh[3],

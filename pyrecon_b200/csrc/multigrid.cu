@@ -1111,8 +1111,8 @@ int run_plain_io(const T* const* delta, T* const* phi, int count, const int32_t 
     return PRC_OK;
 }
 
-int run_mixed_io(const float* const* delta, float* const* phi, int count, const int32_t nmesh[3], const Params& P,
-                 void* ws, const std::string& key, cudaStream_t st) {
+int run_mixed_io(const float* const* delta, float* const* phi, double* const* phi64, int count, const int32_t nmesh[3],
+                 const Params& P, void* ws, const std::string& key, cudaStream_t st) {
     MixedBufs m;
     mixed_layout(nmesh, (char*)ws, &m, count);
     const int64_t N = (int64_t)nmesh[0] * nmesh[1] * nmesh[2];
@@ -1121,9 +1121,13 @@ int run_mixed_io(const float* const* delta, float* const* phi, int count, const 
                      convert_kernel<float, double><<<grid_for(N), 256, 0, st>>>(delta[b], m.f64[0] + b * N, N));
     PRC_CHECK_LAUNCH();
     PRC_TRY(run_graph(key, st, [&](cudaStream_t s) { return solve_mixed(nmesh, P, ws, s, count); }));
-    for (int b = 0; b < count; b++)
+    for (int b = 0; b < count; b++) {
         PRC_LAUNCH_B("mg_convert", st, 12.0 * N,
                      convert_kernel<double, float><<<grid_for(N), 256, 0, st>>>(m.v64[0] + b * N, phi[b], N));
+        if (phi64 && phi64[b] &&
+            cudaMemcpyAsync(phi64[b], m.v64[0] + b * N, N * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return PRC_ERR_CUDA;
+    }
     PRC_CHECK_LAUNCH();
     return PRC_OK;
 }
@@ -1161,8 +1165,33 @@ prc_status_t prc_multigrid_batch_f32(const float* const* delta, float* const* ph
         return PRC_ERR_WORKSPACE;
     cudaStream_t st = (cudaStream_t)stream;
     const std::string key = solve_key(4, mixed_precision ? 1 : 0, nmesh, P, workspace, workspace_bytes, count);
-    if (mixed_precision) return run_mixed_io(delta, phi, count, nmesh, P, workspace, key, st);
+    if (mixed_precision) return run_mixed_io(delta, phi, nullptr, count, nmesh, P, workspace, key, st);
     return run_plain_io<float>(delta, phi, count, nmesh, P, workspace, key, st);
+}
+
+prc_status_t prc_multigrid_batch_mixed_f32(const float* const* delta, float* const* phi, double* const* phi64,
+                                           int count, const int32_t nmesh[3], const double boxsize[3],
+                                           const double boxcenter[3], double beta, double damping,
+                                           int jacobi_niterations, int vcycle_niterations, const double* los,
+                                           void* workspace, size_t workspace_bytes, void* stream) {
+    if (!delta || !phi || !batch_ok(nmesh, count)) return PRC_ERR_ARG;
+    for (int b = 0; b < count; b++)
+        if (!mg_args_ok(delta[b], phi[b], nmesh, boxsize, boxcenter, jacobi_niterations, vcycle_niterations))
+            return PRC_ERR_ARG;
+    Params P = make_params(boxsize, boxcenter, beta, damping, jacobi_niterations, vcycle_niterations, los);
+    if (!workspace || workspace_bytes < prc_multigrid_batch_workspace_bytes(nmesh, 4, 1, count))
+        return PRC_ERR_WORKSPACE;
+    const std::string key = solve_key(4, 1, nmesh, P, workspace, workspace_bytes, count);
+    return run_mixed_io(delta, phi, phi64, count, nmesh, P, workspace, key, (cudaStream_t)stream);
+}
+
+prc_status_t prc_multigrid_mixed_f32(const float* delta, float* phi, double* phi64, const int32_t nmesh[3],
+                                     const double boxsize[3], const double boxcenter[3], double beta, double damping,
+                                     int jacobi_niterations, int vcycle_niterations, const double* los,
+                                     void* workspace, size_t workspace_bytes, void* stream) {
+    return prc_multigrid_batch_mixed_f32(&delta, &phi, &phi64, 1, nmesh, boxsize, boxcenter, beta, damping,
+                                         jacobi_niterations, vcycle_niterations, los, workspace, workspace_bytes,
+                                         stream);
 }
 
 prc_status_t prc_multigrid_batch_f64(const double* const* delta, double* const* phi, int count,

@@ -72,12 +72,19 @@ class OriginalMultiGridReconstruction(BaseReconstruction):
             self.log_info('Computing displacement potential.')
             f32 = self.info.dtype.itemsize == 4
             ws = self._ws.get(lib.prc_multigrid_workspace_bytes(nm, self.info.dtype.itemsize, int(self.mixed_precision)))
-            args = [_lib.ptr(self.mesh_delta.value), _lib.ptr(phi.value), nm, bs, bc, float(self.beta),
-                    float(jacobi_damping_factor), int(jacobi_niterations), int(vcycle_niterations), self._los_arg()]
-            if f32:
-                args.append(int(self.mixed_precision))
-            _lib.call('prc_multigrid_' + _lib.suffix(self.info.dtype), *args, _lib.ptr(ws), ws.numel(),
-                      _lib.stream_of(self.device), error=MeshError)
+            tail = [nm, bs, bc, float(self.beta), float(jacobi_damping_factor), int(jacobi_niterations),
+                    int(vcycle_niterations), self._los_arg()]
+            self._phi64 = None
+            if f32 and self.mixed_precision:
+                # the FP64 iterate of the refinement is kept for the finite-difference read-out
+                self._phi64 = torch.empty(self.info.shape, dtype=torch.float64, device=self.device)
+                _lib.call('prc_multigrid_mixed_f32', _lib.ptr(self.mesh_delta.value), _lib.ptr(phi.value),
+                          _lib.ptr(self._phi64), *tail, _lib.ptr(ws), ws.numel(), _lib.stream_of(self.device),
+                          error=MeshError)
+            else:
+                args = [_lib.ptr(self.mesh_delta.value), _lib.ptr(phi.value)] + tail + ([0] if f32 else [])
+                _lib.call('prc_multigrid_' + _lib.suffix(self.info.dtype), *args, _lib.ptr(ws), ws.numel(),
+                          _lib.stream_of(self.device), error=MeshError)
             del self.mesh_delta
             self.mesh_phi = phi
 
@@ -86,7 +93,13 @@ class OriginalMultiGridReconstruction(BaseReconstruction):
             from .recon import ReconstructionError
             raise ReconstructionError('run() must be called before reading shifts')
         nm, bs, bc = self._geometry_args()
-        _lib.call('prc_read_shifts_phi_' + _lib.suffix(self.info.dtype), _lib.ptr(self.mesh_phi.value), nm, bs, bc,
+        phi64 = getattr(self, '_phi64', None)
+        if phi64 is not None:
+            # mixed precision: the gradient of the FP64 iterate (the FP32 mesh_phi would add its rounding)
+            name, mesh = 'prc_read_shifts_phi_f64', phi64
+        else:
+            name, mesh = 'prc_read_shifts_phi_' + _lib.suffix(self.info.dtype), self.mesh_phi.value
+        _lib.call(name, _lib.ptr(mesh), nm, bs, bc,
                   _lib.ptr(p.pos), p.pos_bytes, p.size, _lib.ptr(getattr(p, 'order', None)), float(self.f),
                   self._los_arg(), field, shifted, int(self.wrap),
                   _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device), error=MeshError)
@@ -131,19 +144,28 @@ def run_batch(recons, jacobi_damping_factor=0.4, jacobi_niterations=5, vcycle_ni
             phi.__dict__['value'] = torch.empty(r.info.shape, dtype=torch_dtype(r.info.dtype), device=r.device)
             phis.append(phi)
         ws = r0._ws.get(lib.prc_multigrid_batch_workspace_bytes(nm, item, int(r0.mixed_precision), count))
-        args = [_lib.pointer_array(deltas), _lib.pointer_array([p.value for p in phis]), count, nm, bs, bc,
-                float(r0.beta), float(jacobi_damping_factor), int(jacobi_niterations), int(vcycle_niterations),
-                r0._los_arg()]
-        if item == 4:
-            args.append(int(r0.mixed_precision))
-        _lib.call('prc_multigrid_batch_' + _lib.suffix(r0.info.dtype), *args, _lib.ptr(ws), ws.numel(),
-                  _lib.stream_of(r0.device), error=MeshError)
-        for r, st, phi in zip(recons, streams, phis):
+        tail = [count, nm, bs, bc, float(r0.beta), float(jacobi_damping_factor), int(jacobi_niterations),
+                int(vcycle_niterations), r0._los_arg()]
+        mixed = item == 4 and r0.mixed_precision
+        phis64 = [torch.empty(r.info.shape, dtype=torch.float64, device=r.device) for r in recons] if mixed else None
+        if mixed:
+            _lib.call('prc_multigrid_batch_mixed_f32', _lib.pointer_array(deltas),
+                      _lib.pointer_array([p.value for p in phis]), _lib.pointer_array(phis64), *tail, _lib.ptr(ws),
+                      ws.numel(), _lib.stream_of(r0.device), error=MeshError)
+        else:
+            args = [_lib.pointer_array(deltas), _lib.pointer_array([p.value for p in phis])] + tail + \
+                ([0] if item == 4 else [])
+            _lib.call('prc_multigrid_batch_' + _lib.suffix(r0.info.dtype), *args, _lib.ptr(ws), ws.numel(),
+                      _lib.stream_of(r0.device), error=MeshError)
+        for i, (r, st, phi) in enumerate(zip(recons, streams, phis)):
             if st != st0:
                 st.wait_stream(st0)         # later work on that reconstruction's stream sees its phi
                 phi.value.record_stream(st)
+                if mixed:
+                    phis64[i].record_stream(st)
             del r.mesh_delta
             r.mesh_phi = phi
+            r._phi64 = phis64[i] if mixed else None
 
 
 class MultiGridReconstruction(OriginalMultiGridReconstruction):

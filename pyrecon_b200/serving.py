@@ -72,6 +72,8 @@ def estimate_device_bytes(request):
     total += n * item                                                                     # delta
     if issubclass(cls, OriginalMultiGridReconstruction):
         total += lib.prc_multigrid_workspace_bytes(nm, item, 1) + n * item                # hierarchy, phi
+        if item == 4:
+            total += 8 * n                                                                # FP64 phi (mixed)
     elif request.algorithm == 'IterativeFFTReconstruction':
         total += lib.prc_iterative_fft_workspace_bytes(nm, item, int(kw.get('los') is None)) + 4 * n * item
     else:

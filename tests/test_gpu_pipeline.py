@@ -41,7 +41,9 @@ def test_f4_within_1e3_of_f8_oracle(name):
             g[k] = g[k].astype('f4')
     ref = run_oracle(g, dtype='f8')
     out, rec = run_gpu(g, dtype='f4')
-    assert maxrel(out['mesh_data'], ref['mesh_data']) < 1e-5   # float index coordinates, as the reference's f4
+    # float index coordinates, as the reference's f4: a CIC fraction is off by up to ~n 2^-24
+    tol = max(1e-5, 3. * max(np.broadcast_to(g['meta']['nmesh'], 3)) * 2. ** -24)
+    assert maxrel(out['mesh_data'], ref['mesh_data']) < tol
     for k in ['shifted_data', 'shifted_randoms', 'shifted_data_str']:
         if k in ref:
             assert out[k].dtype == np.float32
