@@ -13,7 +13,8 @@ keywords of ``run``), ``delta`` (set_density_contrast keywords, selection_functi
 randoms), ``cosmology`` (f, bias, Omega_m for rdz conversions), ``mesh`` (nmesh, dtype, boxsize,
 cellsize, boxpad, wrap...).
 
-Catalogue formats, by extension: FITS (.fits, needs fitsio), HDF5 (.hdf5, .h5, ..., needs h5py),
+Catalogue formats, by extension: FITS (.fits: fitsio when installed, else the built-in binary-table
+reader / writer of :mod:`pyrecon_b200.fits`), HDF5 (.hdf5, .h5, ..., needs h5py),
 numpy (.npz: one array per column, .npy: a structured array) and Arrow (.parquet, .feather, needs
 pyarrow).  Redshift <-> comoving distance (Mpc/h) of a flat LambdaCDM model with Omega_m: astropy's
 when it is installed, else the same integral computed here.
@@ -65,7 +66,11 @@ def read_columns(fn, columns, hdf5_prefix=''):
     """The requested columns of a catalogue file, as a dict of numpy arrays."""
     fmt = _format_of(fn)
     if fmt == 'fits':
-        import fitsio
+        try:
+            import fitsio
+        except ImportError:        # the built-in binary-table reader
+            from . import fits
+            return fits.read(fn, columns=columns)
         tmp = fitsio.read(fn, columns=columns)
         return {col: tmp[col] for col in columns}
     if fmt == 'hdf5':
@@ -97,11 +102,16 @@ def write_columns(fn, catalog, hdf5_prefix=''):
     fmt = _format_of(fn)
     columns = list(catalog.keys())
     if fmt == 'fits':
-        import fitsio
         array = np.empty(len(catalog[columns[0]]), dtype=[(c, catalog[c].dtype, catalog[c].shape[1:]) for c in columns])
         for c in columns:
             array[c] = catalog[c]
-        fitsio.write(fn, array, clobber=True)
+        try:
+            import fitsio
+        except ImportError:        # the built-in binary-table writer
+            from . import fits
+            fits.write(fn, array)
+        else:
+            fitsio.write(fn, array, clobber=True)
     elif fmt == 'hdf5':
         import h5py
         with h5py.File(fn, 'w') as file:

@@ -27,7 +27,7 @@ def test_config_defaults_file_and_errors(tmp_path):
         cli.run(nodata)
 
 
-@pytest.mark.parametrize('ext', ['.npz', '.npy', '.parquet', '.feather'])
+@pytest.mark.parametrize('ext', ['.npz', '.npy', '.parquet', '.feather', '.fits'])
 def test_catalogue_io_roundtrip(tmp_path, ext):
     rng = np.random.default_rng(0)
     catalog = {'Position': rng.normal(size=(50, 3)), 'RA': rng.uniform(0, 360, 50).astype('f4'),
@@ -62,26 +62,28 @@ def test_mask_and_weight_expressions():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('convention', ['RecSym', 'RecIso', 'RSD'])
-def test_cli_run_equals_api(tmp_path, convention):
-    """A configuration run (xyz catalogues in .npz, mask and weight expressions, randoms selection function)
-    writes the shifted positions the API gives for the same inputs."""
+@pytest.mark.parametrize('convention,ext', [('RecSym', '.npz'), ('RecIso', '.npz'), ('RSD', '.npz'),
+                                            ('RecSym', '.fits')])
+def test_cli_run_equals_api(tmp_path, convention, ext):
+    """A configuration run (xyz catalogues in .npz or FITS, mask and weight expressions, randoms selection
+    function) writes the shifted positions the API gives for the same inputs."""
     import pyrecon_b200
     from pyrecon_b200 import mocks
     data = mocks.lognormal_positions_numpy(20000, 32, 1000., 2000., seed=1, field_seed=2)
     randoms = mocks.uniform_positions_numpy(60000, 1000., 2000., seed=3)
     w = np.random.default_rng(4).uniform(0.5, 1.5, len(data))
-    cli.write_columns(str(tmp_path / 'data.npz'), {'Position': data, 'W': w})
-    cli.write_columns(str(tmp_path / 'randoms.npz'), {'Position': randoms})
-    config = cli.load_config(None, input={'dir': str(tmp_path), 'data_fn': 'data.npz', 'randoms_fn': 'randoms.npz',
+    cli.write_columns(str(tmp_path / ('data' + ext)), {'Position': data, 'W': w})
+    cli.write_columns(str(tmp_path / ('randoms' + ext)), {'Position': randoms})
+    config = cli.load_config(None, input={'dir': str(tmp_path), 'data_fn': 'data' + ext, 'randoms_fn': 'randoms' + ext,
                                           'xyz': 'Position', 'weights_data': '${W}', 'mask_data': '${W} > 0.6'},
-                             output={'dir': str(tmp_path), 'data_fn': 'out_data.npz', 'randoms_fn': 'out_randoms.npz',
-                                     'xyz_rec': 'Position_rec', 'columns_data': ['W']},
+                             output={'dir': str(tmp_path), 'data_fn': 'out_data' + ext,
+                                     'randoms_fn': 'out_randoms' + ext, 'xyz_rec': 'Position_rec',
+                                     'columns_data': ['W']},
                              algorithm={'name': 'MultiGridReconstruction', 'convention': convention},
                              cosmology={'f': 0.8, 'bias': 2.}, mesh={'nmesh': 32, 'boxpad': 1.5, 'dtype': 'f8'})
     cli.run(config)
-    out_d = cli.read_columns(str(tmp_path / 'out_data.npz'), ['Position_rec', 'W'])
-    out_r = cli.read_columns(str(tmp_path / 'out_randoms.npz'), ['Position_rec'])
+    out_d = cli.read_columns(str(tmp_path / ('out_data' + ext)), ['Position_rec', 'W'])
+    out_r = cli.read_columns(str(tmp_path / ('out_randoms' + ext)), ['Position_rec'])
     keep = w > 0.6
     rec = pyrecon_b200.MultiGridReconstruction(f=0.8, bias=2., nmesh=32, boxpad=1.5, dtype='f8', positions=randoms)
     rec.assign_data(data[keep], w[keep])
