@@ -343,21 +343,25 @@ def reconstruct(w, device, data, wd, randoms, wr, check):
     return out_d, out_r
 
 
-# ncu DRAM-traffic summary of the small case of the iterative FFT workload (profiles/): per kernel, DRAM bytes
-# per launch over the algorithmic bytes of the same launches
-TRAFFIC_PROFILE = os.path.join(ROOT, 'profiles', 'traffic_iterative_fft_256.md')
+# ncu DRAM-traffic summaries (profiles/): per kernel, DRAM bytes per launch over the algorithmic bytes of the
+# same launches; the nmesh-512 capture of the FFT passes first, the nmesh-256 capture of the whole pipeline
+# (particle kernels included) for the rest
+TRAFFIC_PROFILES = [os.path.join(ROOT, 'profiles', 'traffic_iterative_fft_512.md'),
+                    os.path.join(ROOT, 'profiles', 'traffic_iterative_fft_256.md')]
 
 
 def traffic_ratio(kernel):
-    try:
-        with open(TRAFFIC_PROFILE) as fh:
-            for line in fh:
-                cells = [c.strip() for c in line.strip().strip('|').split('|')]
-                if len(cells) == 5 and cells[0] == kernel:
-                    return float(cells[4])
-    except (OSError, ValueError):
-        return None
-    return None
+    """(ratio, profile file name) of the first summary with a row for `kernel`, or (None, None)."""
+    for path in TRAFFIC_PROFILES:
+        try:
+            with open(path) as fh:
+                for line in fh:
+                    cells = [c.strip() for c in line.strip().strip('|').split('|')]
+                    if len(cells) >= 5 and cells[0] == kernel:
+                        return float(cells[4]), os.path.basename(path)
+        except (OSError, ValueError):
+            continue
+    return None, None
 
 
 def load_peaks():
@@ -483,14 +487,13 @@ def run_gpu_arm(args, w):
     achieved = (kbytes / 1e9) / (kms / 1e3) if kms > 0 else 0.
     kernels = {k: dict(launches=v[0], ms=round(v[1], 3), share=round(v[1] / max(sum(x[1] for x in prof.values()), 1e-9), 4),
                        gbs=round((v[2] / 1e9) / (v[1] / 1e3), 1) if v[1] > 0 else None) for k, v in prof.items()}
-    ratio = traffic_ratio(name) if w['algorithm'] == 'IterativeFFTReconstruction' else None
+    ratio, tsrc = traffic_ratio(name) if w['algorithm'] == 'IterativeFFTReconstruction' else (None, None)
     traffic = None if ratio is None else ratio * kbytes / nl
     roofline = dict(bound='hbm', kernel=name, achieved=round(achieved, 1), peak=peak, unit='GB/s',
                     frac=round(achieved / peak, 4), traffic=traffic,
                     traffic_source=None if ratio is None else
-                    'ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at nmesh 256 '
-                    '(profiles/traffic_iterative_fft_256.md), ratio {:.3f} to the algorithmic bytes, '
-                    'scaled to this launch'.format(ratio),
+                    'ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel '
+                    '(profiles/{}), ratio {:.3f} to its algorithmic bytes, applied to this launch'.format(tsrc, ratio),
                     bytes_per_launch=kbytes / nl, launch_ms=kms / nl, peak_source=peak_kind + ' (MEASURED_PEAKS.json hbm_gbs)')
 
     # --- the metric's comparison with the plain GPU path: many requests through the request loop ---
@@ -624,7 +627,7 @@ def multi_workload(args, w, device, rank):
         gc.collect()
         torch.cuda.empty_cache()
         free, _ = torch.cuda.mem_get_info(device)
-        budget = min(budget, 0.8 * free)
+        budget = min(budget, 0.75 * free)
     with ClockSampler(device.index or 0) as clocks:
         server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=budget,
                                       max_batch=w.get('max_batch', 1))

@@ -160,6 +160,10 @@ class ReconstructionServer(object):
         # device scratch resident per slot: reused by every request the slot runs
         self._workspaces = [_Workspace(self.device) for _ in range(slots)]
         self._free_streams = list(range(slots))
+        # device memory each slot's stream keeps: torch's caching allocator pools freed blocks per stream,
+        # so a slot holds (at least) the largest job it has run; admission counts these, not only the
+        # jobs in flight
+        self._resident = [0.] * slots
         self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=slots)
         self._cv = threading.Condition()
         self._queue = collections.deque()
@@ -190,20 +194,37 @@ class ReconstructionServer(object):
             self._cv.notify_all()
         return fut
 
+    def _pick_slot(self, need):
+        """A free slot whose stream can take a job of `need` bytes within the budget (preferring one that
+        already holds that much), and the budget left for the job beyond `need`; (None, 0) if none fits."""
+        total = sum(self._resident)
+        best = None
+        for s in self._free_streams:
+            grown = max(self._resident[s], need)
+            left = self.hbm_budget - (total - self._resident[s] + grown)
+            if left < 0:
+                continue
+            # fewest bytes added to the resident total, then the smallest resident slot
+            score = (grown - self._resident[s], self._resident[s])
+            if best is None or score < best[0]:
+                best = (score, s, left + (grown - need))
+        return (None, 0.) if best is None else (best[1], best[2])
+
     def _loop(self):
         while True:
             with self._cv:
                 while True:
-                    if self._queue and self._free_streams and self._in_use + self._queue[0][1] <= self.hbm_budget:
-                        break
+                    if self._queue and self._free_streams:
+                        slot, room = self._pick_slot(self._queue[0][1])
+                        if slot is not None:
+                            break
                     if self._closed and not self._queue:
                         return
                     self._cv.wait()
                 job = [self._queue.popleft()]
                 key = job[0][3]
                 if key is not None:
-                    # queued requests of the same batch key join, while the budget allows
-                    room = self.hbm_budget - self._in_use - job[0][1]
+                    # queued requests of the same batch key join, while the slot's budget allows
                     for item in list(self._queue):
                         if len(job) >= self.max_batch:
                             break
@@ -216,8 +237,9 @@ class ReconstructionServer(object):
                     job = job[:n]
                     for item in job[1:]:
                         self._queue.remove(item)
-                slot = self._free_streams.pop()
+                self._free_streams.remove(slot)
                 need = sum(item[1] for item in job)
+                self._resident[slot] = max(self._resident[slot], need)
                 self._in_use += need
                 self._active += len(job)
                 self.peak_active = max(self.peak_active, self._active)

@@ -195,3 +195,18 @@ def test_memory_monitor_and_mkdir(tmp_path, capsys):
         mem('step')
     out = capsys.readouterr().out
     assert '[step] using' in out and 'increase of' in out
+
+
+def test_serving_admission_counts_resident_slot_memory():
+    """The request loop's admission: each slot's stream keeps (at least) the largest job it ran, so a job
+    goes to a free slot only if every slot's resident memory, that slot grown to the job, fits the budget;
+    a slot that already holds enough is preferred (it adds nothing)."""
+    import types
+    from pyrecon_b200.serving import ReconstructionServer
+    srv = types.SimpleNamespace(hbm_budget=100., _resident=[60., 0., 0.], _free_streams=[0, 1, 2])
+    assert ReconstructionServer._pick_slot(srv, 30.) == (0, 70.)      # slot 0 holds 60 >= 30; may grow to 100
+    srv._free_streams = [1, 2]                                        # slot 0 busy with its 60
+    assert ReconstructionServer._pick_slot(srv, 50.) == (None, 0.)    # 60 + 50 > 100
+    assert ReconstructionServer._pick_slot(srv, 40.) == (1, 0.)
+    srv._resident = [60., 10., 30.]
+    assert ReconstructionServer._pick_slot(srv, 20.) == (2, 10.)      # slot 2 holds 30: nothing added
