@@ -620,14 +620,12 @@ def multi_workload(args, w, device, rank):
         free_at = max(free_at, at) + dt
         fifo.append(free_at - at)
     launches0 = None
-    budget = w.get('hbm_budget')
-    if budget is not None:
-        # the admission budget cannot exceed what the device has free (the plain path's cached scratch is
-        # released first); the slots' resident scratch comes out of it too
-        gc.collect()
-        torch.cuda.empty_cache()
-        free, _ = torch.cuda.mem_get_info(device)
-        budget = min(budget, 0.75 * free)
+    # the admission budget cannot exceed what the device has free once the plain path's cached scratch is
+    # released (torch's allocator keeps freed blocks per stream, and the slots run on their own streams)
+    gc.collect()
+    torch.cuda.empty_cache()
+    free, _ = torch.cuda.mem_get_info(device)
+    budget = min(w.get('hbm_budget') or float('inf'), 0.75 * free)
     with ClockSampler(device.index or 0) as clocks:
         server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=budget,
                                       max_batch=w.get('max_batch', 1))
@@ -664,7 +662,7 @@ def multi_workload(args, w, device, rank):
                     ms_per_step=served_s * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None,
                     dtype=w['dtype'], data='synthetic: seeded lognormal catalogues, one per nmesh, requests take prefixes',
                     config=dict(workload=w['name'], requests=n, slots=w['slots'], max_batch=w.get('max_batch', 1),
-                                hbm_budget_gb=None if budget is None else round(budget / 1e9, 1),
+                                hbm_budget_gb=round(budget / 1e9, 1),
                                 arrivals='poisson {:g}/s'.format(w['rate']) if w['kind'] == 'serving' else 'all at once',
                                 nmesh=w['nmesh'], algorithms=w['algorithms'], timing='wall clock, device synchronised'),
                     served=dict(recons_per_s=n / served_s, p50_ms=stats['p50_ms'], p99_ms=stats['p99_ms'],

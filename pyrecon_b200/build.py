@@ -36,6 +36,8 @@ FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-Xcompiler', 
 # exchange instead of the ping-pong buffers (same arithmetic, same order).
 VARIANTS = {
     'nopp': ['-DPRC_STRIDED_PP=0', '-DPRC_KSPACE_PP=0', '-DPRC_HESS_PP=0', '-DPRC_C2R_PP=0'],
+    # every radix-8 twiddle read from the pass table (7 loads per butterfly instead of 3 and 4 products)
+    'twload': ['-DPRC_TW_RECUR=0'],
 }
 
 

@@ -85,6 +85,13 @@ template <typename C, int DIR, int R> __device__ __forceinline__ void dftR(C* u)
     else dft2<C, DIR>(u);
 }
 
+// PRC_TW_RECUR=1: a radix-8 butterfly reads w, w^2 and w^4 from the pass table and forms w^3, w^5, w^6,
+// w^7 as products (at most two roundings deep), so it issues 3 shared-memory loads instead of 7; the
+// passes are bound by shared-memory instruction traffic (exchanges and twiddles), not by arithmetic.
+#ifndef PRC_TW_RECUR
+#define PRC_TW_RECUR 1
+#endif
+
 // One radix-R pass on the thread's 8 points (8 / R butterflies); tw = this pass's table.
 template <typename C, int N, int R, int NS, int DIR>
 __device__ __forceinline__ void pass_regs(C (&v)[8], int t, const C* __restrict__ tw) {
@@ -97,11 +104,29 @@ __device__ __forceinline__ void pass_regs(C (&v)[8], int t, const C* __restrict_
         if constexpr (NS > 1) {
             const int k = (t + b * T) & (NS - 1);
             const C* row = tw + k * (R - 1);
+            if constexpr (R == 8 && PRC_TW_RECUR) {
+                C w[8];
+                w[1] = row[0];
+                w[2] = row[1];
+                w[4] = row[3];
+                if (DIR > 0) {
+                    w[1] = cconj(w[1]);
+                    w[2] = cconj(w[2]);
+                    w[4] = cconj(w[4]);
+                }
+                w[3] = cmul(w[1], w[2]);
+                w[5] = cmul(w[1], w[4]);
+                w[6] = cmul(w[2], w[4]);
+                w[7] = cmul(w[3], w[4]);
 #pragma unroll
-            for (int r = 1; r < R; r++) {
-                C w = row[r - 1];
-                if (DIR > 0) w = cconj(w);
-                u[r] = cmul(u[r], w);
+                for (int r = 1; r < 8; r++) u[r] = cmul(u[r], w[r]);
+            } else {
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    C w = row[r - 1];
+                    if (DIR > 0) w = cconj(w);
+                    u[r] = cmul(u[r], w);
+                }
             }
         }
         dftR<C, DIR, R>(u);
