@@ -565,7 +565,7 @@ def multi_requests(w, device, seed=0):
                                           randoms=None if randoms is None else randoms[:w['randoms_factor'] * nd],
                                           f=0.8, bias=2., los=los, nmesh=n, boxsize=w['boxsize'],
                                           boxcenter=w['boxcenter'], wrap=w['wrap'], dtype=w['dtype'],
-                                          density_kwargs=dict(smoothing_radius=15.)))
+                                          density_kwargs=dict(smoothing_radius=15.), keep_output=False))
     return reqs
 
 

@@ -36,8 +36,12 @@ class ReconstructionRequest(object):
     keywords of set_density_contrast and of run."""
 
     def __init__(self, algorithm, data, data_weights=None, randoms=None, randoms_weights=None,
-                 density_kwargs=None, run_kwargs=None, **kwargs):
+                 density_kwargs=None, run_kwargs=None, keep_output=True, **kwargs):
         self.algorithm = algorithm
+        # keep_output=False: the shifted positions are computed and then dropped (the future's result
+        # holds their shapes only), so a long stream of requests on device catalogues does not pile up
+        # outputs in device memory
+        self.keep_output = bool(keep_output)
         self.data, self.data_weights = data, data_weights
         self.randoms, self.randoms_weights = randoms, randoms_weights
         self.density_kwargs = dict(density_kwargs or {})
@@ -95,10 +99,13 @@ def prepare_request(request, device=None, stream=None, workspace=None):
 
 
 def finish_request(request, rec):
-    """The shifted positions of a request whose reconstruction has run."""
+    """The shifted positions of a request whose reconstruction has run (their shapes only when the
+    request does not keep its output)."""
     out = {'shifted_data': rec.read_shifted_positions(request.data)}
     if request.randoms is not None:
         out['shifted_randoms'] = rec.read_shifted_positions(request.randoms)
+    if not request.keep_output:
+        out = {k: tuple(v.shape) for k, v in out.items()}
     return out
 
 
