@@ -103,6 +103,17 @@ PRC_API prc_status_t prc_assign_cic_order(double *mesh, double *column_sums, con
                                   int32_t *flags, void *workspace, size_t workspace_bytes, void *stream,
                                   uint32_t *order);
 
+/* prc_assign_cic_order that also writes the positions themselves in that order (sorted_positions:
+ * npos x 3 of the positions' dtype, particle order[i] at row i), so that a read-out of the same positions
+ * in cell order (prc_read_shifts_* with order and sorted_positions) streams them instead of gathering
+ * through the permutation.  Extends assign_cic (src/mesh.c:26-63) the same way prc_assign_cic_order does. */
+PRC_API prc_status_t prc_assign_cic_sorted(double *mesh, double *column_sums, const int32_t nmesh[3],
+                                   const double boxsize[3], const double boxcenter[3], int mesh_bytes,
+                                   const void *positions, int pos_bytes, const void *weights,
+                                   int weight_bytes, int64_t npos, int wrap, int accumulate,
+                                   int32_t *flags, void *workspace, size_t workspace_bytes, void *stream,
+                                   uint32_t *order, void *sorted_positions);
+
 /* Allocation-free variant of prc_assign_cic, with no counterpart in the reference.  For callers
  * that cannot allocate device memory (no allocator of their own, or code running where a
  * cudaMalloc is not allowed): it takes no workspace and calls no cudaMalloc / cudaFree; its
@@ -165,28 +176,29 @@ PRC_API prc_status_t prc_read_finite_difference_cic_f64(const double *mesh, cons
  * out is (npos, 3) in `out_bytes` precision.  `order` (may be NULL) is a permutation of 0..npos-1
  * in which to visit the particles, e.g. the cell order prc_assign_cic_order returned when these
  * positions were painted: neighbouring threads then gather neighbouring cells.  Results do not
- * depend on it. */
+ * depend on it.  sorted_positions (optional, with order): the same positions in that order, as
+ * prc_assign_cic_sorted wrote them; they are read from there (a stream) instead of positions[order[k]]. */
 PRC_API prc_status_t prc_read_shifts_psi_f32(const float *psi_x, const float *psi_y, const float *psi_z, int psi_stride,
                                      const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
                                      int64_t npos, const uint32_t *order, double f, const double *los, int field,
-                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream, const void *sorted_positions);
 PRC_API prc_status_t prc_read_shifts_psi_f64(const double *psi_x, const double *psi_y, const double *psi_z,
                                      int psi_stride, const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
                                      int64_t npos, const uint32_t *order, double f, const double *los, int field,
-                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream, const void *sorted_positions);
 
 /* Same for the multigrid potential: finite-difference CIC gradient of phi, RSD direction from
  * the UNWRAPPED positions (pyrecon/multigrid.py:137-158). */
 PRC_API prc_status_t prc_read_shifts_phi_f32(const float *phi, const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
                                      int64_t npos, const uint32_t *order, double f, const double *los, int field,
-                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream, const void *sorted_positions);
 PRC_API prc_status_t prc_read_shifts_phi_f64(const double *phi, const int32_t nmesh[3], const double boxsize[3],
                                      const double boxcenter[3], const void *positions, int pos_bytes,
                                      int64_t npos, const uint32_t *order, double f, const double *los, int field,
-                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream);
+                                     int shifted, int wrap, void *out, int out_bytes, int32_t *flags, void *stream, const void *sorted_positions);
 
 /* Sum of a float mesh accumulated in float64 (deterministic, as prc_sum_f64); replaces np.sum of the
  * smoothed meshes in IterativeFFTParticleReconstruction.set_density_contrast

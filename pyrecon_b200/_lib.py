@@ -47,6 +47,8 @@ _SIGNATURES = {
     'prc_assign_cic': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size, _p]),
     'prc_assign_cic_order': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size,
                                      _p, _p]),
+    'prc_assign_cic_sorted': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p, c_size,
+                                      _p, _p, _p]),
     'prc_cic_cell_order': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, c_i64, c_int, _p, _p, c_size, _p]),
     'prc_assign_cic_noalloc': (c_int, [_p, _p, I3, D3, D3, c_int, _p, c_int, _p, c_int, c_i64, c_int, c_int, _p, _p]),
     'prc_sum_workspace_bytes': (c_size, [c_i64]),
@@ -64,9 +66,9 @@ for _s in ['f32', 'f64']:
         'prc_read_cic_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, c_int, _p, _p, _p]),
         'prc_read_finite_difference_cic_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, c_int, _p, _p, _p]),
         'prc_read_shifts_psi_' + _s: (c_int, [_p, _p, _p, c_int, I3, D3, D3, _p, c_int, c_i64, _p, c_double, DP,
-                                              c_int, c_int, c_int, _p, c_int, _p, _p]),
+                                              c_int, c_int, c_int, _p, c_int, _p, _p, _p]),
         'prc_read_shifts_phi_' + _s: (c_int, [_p, I3, D3, D3, _p, c_int, c_i64, _p, c_double, DP, c_int, c_int, c_int,
-                                              _p, c_int, _p, _p]),
+                                              _p, c_int, _p, _p, _p]),
         'prc_delta_from_meshes_' + _s: (c_int, [_p, _p, c_int, _p, I3, c_double, c_double, c_double, _p, _p]),
         'prc_zeldovich_psi_' + _s: (c_int, [_p, I3, D3, _p, _p, _p, c_int, _p, c_size, _p]),
         'prc_ifftp_update_' + _s: (c_int, [_p, I3, D3, D3, _p, _p, c_int, c_i64, c_double, c_double, c_int, DP, c_int,

@@ -387,10 +387,13 @@ __global__ void __launch_bounds__(256) paint_keys(const P* __restrict__ pos, con
 // offsets are taken after the modulo as src/mesh.c:45-47 does.
 template <typename F> struct alignas(4 * sizeof(F)) Payload { F t[3]; F w; };
 
+// sorted_pos (optional): the positions themselves in the same order (pos of particle order[i] at i), so a
+// later read-out in cell order streams them instead of gathering through the permutation.
 template <typename P, typename F, typename W>
 __global__ void __launch_bounds__(256) paint_payload(const P* __restrict__ pos, const W* __restrict__ weights, int64_t n,
                                                      BoxGeom g, int wrap, const uint32_t* __restrict__ order,
-                                                     Payload<F>* __restrict__ out, const int32_t* __restrict__ flags) {
+                                                     Payload<F>* __restrict__ out, P* __restrict__ sorted_pos,
+                                                     const int32_t* __restrict__ flags) {
     if (*flags) return;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         int64_t id = order[i];
@@ -402,6 +405,10 @@ __global__ void __launch_bounds__(256) paint_payload(const P* __restrict__ pos, 
         for (int d = 0; d < 3; d++) pl.t[d] = rn_sub(q[d], (F)base_cell(q[d], g.n[d]));
         pl.w = weights != nullptr ? (F)weights[id] : (F)1;
         out[i] = pl;
+        if (sorted_pos != nullptr) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) sorted_pos[3 * i + d] = pos[3 * id + d];
+        }
     }
 }
 
@@ -680,7 +687,8 @@ __global__ void __launch_bounds__(256) read_shifts_kernel(const F* __restrict__ 
                                                           const P* __restrict__ pos, int64_t n, double f,
                                                           int global_los, double l0, double l1, double l2, int field,
                                                           int shifted, int wrap, O* __restrict__ out, int32_t* flags,
-                                                          const uint32_t* __restrict__ order) {
+                                                          const uint32_t* __restrict__ order,
+                                                          const P* __restrict__ sorted_pos) {
     typedef typename promote<P, F>::type T;
     const F twocell[3] = {tc0, tc1, tc2};
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -690,12 +698,15 @@ __global__ void __launch_bounds__(256) read_shifts_kernel(const F* __restrict__ 
         int bad = 0;
         if (k < n) {
             // particles visited in `order` (cell-sorted, from the paint): neighbouring threads gather
-            // neighbouring cells; each particle's result only depends on its own position
+            // neighbouring cells; each particle's result only depends on its own position, read from the
+            // paint's cell-ordered copy when there is one (a stream, not a gather)
             const int64_t i = order != nullptr ? (int64_t)order[k] : k;
+            const P* src = sorted_pos != nullptr ? sorted_pos : pos;
+            const int64_t at = sorted_pos != nullptr ? k : i;
             F q[3] = {0, 0, 0};
             P s[3];
-            const P p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
-            const bool ok = particle_index<P, F>(pos, i, g, wrap, q, &bad);
+            const P p[3] = {src[3 * at], src[3 * at + 1], src[3 * at + 2]};
+            const bool ok = particle_index<P, F>(src, at, g, wrap, q, &bad);
             const Cic<F> c = cic_setup(q, g.n);
             if (PHI) {
                 F d[3] = {(F)NAN, (F)NAN, (F)NAN};
@@ -1017,7 +1028,8 @@ int paint_sort(const P* pos, const W* w, int64_t n, const BoxGeom& g, int wrap, 
 
 template <typename P, typename F, typename W>
 int paint_run(double* mesh, double* colsums, const BoxGeom& g, const P* pos, const W* w, int64_t n, int wrap,
-              int accumulate, int32_t* flags, const PaintWs& ws, cudaStream_t st, uint32_t* order_out = nullptr) {
+              int accumulate, int32_t* flags, const PaintWs& ws, cudaStream_t st, uint32_t* order_out = nullptr,
+              P* sorted_out = nullptr) {
     uint32_t *keys = nullptr, *order = nullptr;
     if (n > 0) PRC_TRY((paint_sort<P, F, W>(pos, w, n, g, wrap, ws, flags, &keys, &order, st)));
     if (n > 0 && order_out != nullptr &&
@@ -1025,7 +1037,10 @@ int paint_run(double* mesh, double* colsums, const BoxGeom& g, const P* pos, con
         return PRC_ERR_CUDA;
     Payload<F>* pl = (Payload<F>*)ws.payload;
     if (n > 0) {
-        PRC_LAUNCH_B("paint_payload", st, (double)n * (4 + 3 * sizeof(P) + (w ? sizeof(W) : 0) + sizeof(Payload<F>)), paint_payload<P, F, W><<<particle_grid(n), 256, 0, st>>>(pos, w, n, g, wrap, order, pl, flags));
+        PRC_LAUNCH_B("paint_payload", st,
+                     (double)n * (4 + 3 * sizeof(P) * (sorted_out ? 2 : 1) + (w ? sizeof(W) : 0) + sizeof(Payload<F>)),
+                     paint_payload<P, F, W><<<particle_grid(n), 256, 0, st>>>(pos, w, n, g, wrap, order, pl, sorted_out,
+                                                                             flags));
         PRC_CHECK_LAUNCH();
     } else {
         keys = ws.k0;
@@ -1045,18 +1060,21 @@ int paint_run(double* mesh, double* colsums, const BoxGeom& g, const P* pos, con
 
 template <typename P, typename F>
 int paint_dispatch_w(double* mesh, double* colsums, const BoxGeom& g, const void* pos, const void* w, int wb, int64_t n,
-                     int wrap, int acc, int32_t* flags, const PaintWs& ws, cudaStream_t st, uint32_t* order_out) {
+                     int wrap, int acc, int32_t* flags, const PaintWs& ws, cudaStream_t st, uint32_t* order_out,
+                     void* sorted_out) {
+    P* so = (P*)sorted_out;
     if (w == nullptr)
-        return paint_run<P, F, F>(mesh, colsums, g, (const P*)pos, (const F*)nullptr, n, wrap, acc, flags, ws, st, order_out);
+        return paint_run<P, F, F>(mesh, colsums, g, (const P*)pos, (const F*)nullptr, n, wrap, acc, flags, ws, st, order_out, so);
     if (wb == 4)
-        return paint_run<P, F, float>(mesh, colsums, g, (const P*)pos, (const float*)w, n, wrap, acc, flags, ws, st, order_out);
-    return paint_run<P, F, double>(mesh, colsums, g, (const P*)pos, (const double*)w, n, wrap, acc, flags, ws, st, order_out);
+        return paint_run<P, F, float>(mesh, colsums, g, (const P*)pos, (const float*)w, n, wrap, acc, flags, ws, st, order_out, so);
+    return paint_run<P, F, double>(mesh, colsums, g, (const P*)pos, (const double*)w, n, wrap, acc, flags, ws, st, order_out, so);
 }
 
 template <typename P, typename F>
 int read_shifts_launch(const F* m0, const F* m1, const F* m2, int stride, bool phi, const BoxGeom& g, const void* pos,
                        int64_t n, const uint32_t* order, double f, const double* los, int field, int shifted, int wrap,
-                       void* out, int ob, int32_t* flags, cudaStream_t st) {
+                       void* out, int ob, int32_t* flags, cudaStream_t st, const void* sorted_pos) {
+    if (sorted_pos != nullptr && order == nullptr) return PRC_ERR_ARG;
     const bool il = !phi && stride == 4;
     if (il && (m1 != m0 + 1 || m2 != m0 + 2 || ((uintptr_t)m0 % (4 * sizeof(F))) != 0)) return PRC_ERR_ARG;
     if (!phi && !il && stride != 1) return PRC_ERR_ARG;
@@ -1075,7 +1093,8 @@ int read_shifts_launch(const F* m0, const F* m1, const F* m2, int stride, bool p
                  read_shifts_kernel<P, F, O, PH, IL><<<grid, 256, 0, st>>>(m0, m1, m2, g, tc[0], tc[1], tc[2],     \
                                                                          (const P*)pos, n, f, los != nullptr, l[0], \
                                                                          l[1], l[2], field, shifted, wrap,          \
-                                                                         (O*)out, flags, order))
+                                                                         (O*)out, flags, order,             \
+                                                                         (const P*)sorted_pos))
     if (phi) {
         if (ob == 4) LAUNCH(float, true, false); else LAUNCH(double, true, false);
     } else if (il) {
@@ -1206,7 +1225,7 @@ static prc_status_t assign_cic_impl(double* mesh, double* column_sums, const int
                                     const double boxcenter[3], int mesh_bytes, const void* positions, int pos_bytes,
                                     const void* weights, int weight_bytes, int64_t npos, int wrap, int accumulate,
                                     int32_t* flags, void* workspace, size_t workspace_bytes, void* stream,
-                                    uint32_t* order_out) {
+                                    uint32_t* order_out, void* sorted_out = nullptr) {
     if (!mesh || !valid_nmesh(nmesh) || !boxsize || !boxcenter || !flags || npos < 0) return PRC_ERR_ARG;
     if (npos >= ((int64_t)1 << 32) || (npos > 0 && !positions)) return PRC_ERR_ARG;
     if ((mesh_bytes != 4 && mesh_bytes != 8) || (pos_bytes != 4 && pos_bytes != 8)) return PRC_ERR_ARG;
@@ -1219,12 +1238,12 @@ static prc_status_t assign_cic_impl(double* mesh, double* column_sums, const int
     BoxGeom g = make_geom(nmesh, boxsize, boxcenter);
     if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return PRC_ERR_CUDA;
     if (pos_bytes == 4 && mesh_bytes == 4)
-        return paint_dispatch_w<float, float>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st, order_out);
+        return paint_dispatch_w<float, float>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st, order_out, sorted_out);
     if (pos_bytes == 4 && mesh_bytes == 8)
-        return paint_dispatch_w<float, double>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st, order_out);
+        return paint_dispatch_w<float, double>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st, order_out, sorted_out);
     if (pos_bytes == 8 && mesh_bytes == 4)
-        return paint_dispatch_w<double, float>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st, order_out);
-    return paint_dispatch_w<double, double>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st, order_out);
+        return paint_dispatch_w<double, float>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st, order_out, sorted_out);
+    return paint_dispatch_w<double, double>(mesh, column_sums, g, positions, weights, weight_bytes, npos, wrap, accumulate, flags, ws, st, order_out, sorted_out);
 }
 
 prc_status_t prc_assign_cic(double* mesh, double* column_sums, const int32_t nmesh[3], const double boxsize[3],
@@ -1243,6 +1262,17 @@ prc_status_t prc_assign_cic_order(double* mesh, double* column_sums, const int32
     if (!order && npos > 0) return PRC_ERR_ARG;
     return assign_cic_impl(mesh, column_sums, nmesh, boxsize, boxcenter, mesh_bytes, positions, pos_bytes, weights,
                            weight_bytes, npos, wrap, accumulate, flags, workspace, workspace_bytes, stream, order);
+}
+
+prc_status_t prc_assign_cic_sorted(double* mesh, double* column_sums, const int32_t nmesh[3], const double boxsize[3],
+                                   const double boxcenter[3], int mesh_bytes, const void* positions, int pos_bytes,
+                                   const void* weights, int weight_bytes, int64_t npos, int wrap, int accumulate,
+                                   int32_t* flags, void* workspace, size_t workspace_bytes, void* stream,
+                                   uint32_t* order, void* sorted_positions) {
+    if ((!order || !sorted_positions) && npos > 0) return PRC_ERR_ARG;
+    return assign_cic_impl(mesh, column_sums, nmesh, boxsize, boxcenter, mesh_bytes, positions, pos_bytes, weights,
+                           weight_bytes, npos, wrap, accumulate, flags, workspace, workspace_bytes, stream, order,
+                           sorted_positions);
 }
 
 prc_status_t prc_cic_cell_order(uint32_t* keys_sorted, uint32_t* order, const int32_t nmesh[3], const double boxsize[3],
@@ -1361,34 +1391,34 @@ READ_FD_IMPL(prc_read_finite_difference_cic_f64, double)
         BoxGeom g = make_geom(nmesh, boxsize, boxcenter);                                                          \
         if (pos_bytes == 4)                                                                                        \
             return read_shifts_launch<float, F>(M0, M1, M2, STRIDE, PHI, g, positions, npos, order, f, los, field,  \
-                                                shifted, wrap, out, out_bytes, flags, st);                        \
+                                                shifted, wrap, out, out_bytes, flags, st, sorted_positions);      \
         return read_shifts_launch<double, F>(M0, M1, M2, STRIDE, PHI, g, positions, npos, order, f, los, field,   \
-                                             shifted, wrap, out, out_bytes, flags, st);                           \
+                                             shifted, wrap, out, out_bytes, flags, st, sorted_positions);         \
     }
 
 READ_SHIFTS_IMPL(prc_read_shifts_psi_f32, float, false,
                  (const float* psi_x, const float* psi_y, const float* psi_z, int psi_stride, const int32_t nmesh[3],
                   const double boxsize[3], const double boxcenter[3], const void* positions, int pos_bytes,
                   int64_t npos, const uint32_t* order, double f, const double* los, int field, int shifted, int wrap, void* out,
-                  int out_bytes, int32_t* flags, void* stream),
+                  int out_bytes, int32_t* flags, void* stream, const void* sorted_positions),
                  psi_x, psi_y, psi_z, psi_stride)
 READ_SHIFTS_IMPL(prc_read_shifts_psi_f64, double, false,
                  (const double* psi_x, const double* psi_y, const double* psi_z, int psi_stride, const int32_t nmesh[3],
                   const double boxsize[3], const double boxcenter[3], const void* positions, int pos_bytes,
                   int64_t npos, const uint32_t* order, double f, const double* los, int field, int shifted, int wrap, void* out,
-                  int out_bytes, int32_t* flags, void* stream),
+                  int out_bytes, int32_t* flags, void* stream, const void* sorted_positions),
                  psi_x, psi_y, psi_z, psi_stride)
 READ_SHIFTS_IMPL(prc_read_shifts_phi_f32, float, true,
                  (const float* phi, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
                   const void* positions, int pos_bytes, int64_t npos, const uint32_t* order, double f,
                   const double* los, int field, int shifted, int wrap, void* out, int out_bytes, int32_t* flags,
-                  void* stream),
+                  void* stream, const void* sorted_positions),
                  phi, phi, phi, 1)
 READ_SHIFTS_IMPL(prc_read_shifts_phi_f64, double, true,
                  (const double* phi, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
                   const void* positions, int pos_bytes, int64_t npos, const uint32_t* order, double f,
                   const double* los, int field, int shifted, int wrap, void* out, int out_bytes, int32_t* flags,
-                  void* stream),
+                  void* stream, const void* sorted_positions),
                  phi, phi, phi, 1)
 
 

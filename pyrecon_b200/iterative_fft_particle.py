@@ -21,6 +21,9 @@ class OriginalIterativeFFTParticleReconstruction(FFTShiftsMixin, BaseReconstruct
     reconstructed real-space positions.
     """
 
+    # its read-outs gather through prc_ifftp_read (cell order only): no sorted copy of the catalogues
+    _sorted_positions = False
+
     def assign_data(self, positions, weights=None, check=True):
         """Paint data and keep positions and weights for :meth:`run` (iterative_fft_particle.py:16-33)."""
         import torch
@@ -35,7 +38,7 @@ class OriginalIterativeFFTParticleReconstruction(FFTShiftsMixin, BaseReconstruct
             else:
                 self._positions_data = torch.cat([self._positions_data, p.pos.to(self._positions_data.dtype)], dim=0)
                 self._weights_data = torch.cat([self._weights_data, w.to(self._weights_data.dtype)], dim=0)
-            order = self._new_order(positions)
+            order, _ = self._new_order(positions)
             self.mesh_data.assign_cic(p.pos, weights=w, wrap=self.wrap, check=check, order_out=order)
             self._keep_order(positions, order)
 

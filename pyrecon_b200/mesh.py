@@ -518,10 +518,11 @@ class RealMesh(BaseMesh):
         low, high = self.boxcenter - self.boxsize / 2., self.boxcenter + self.boxsize / 2.
         return low, high
 
-    def assign_cic(self, positions, weights=None, wrap=False, check=True, order_out=None):
+    def assign_cic(self, positions, weights=None, wrap=False, check=True, order_out=None, sorted_out=None):
         """Paint positions with CIC, accumulating (mesh.py:529-568); FP64 sums, deterministic.
         ``order_out``: optional int32 device tensor of len(positions) that receives the particles'
-        indices in the (cell-sorted) order the paint summed them."""
+        indices in the (cell-sorted) order the paint summed them; ``sorted_out`` (with ``order_out``):
+        optional device tensor shaped like the positions that receives them in that order."""
         torch = _torch()
         p = Particles(positions, self.device, weights=weights, weight_dtype=self.dtype)
         accumulate = True
@@ -534,7 +535,7 @@ class RealMesh(BaseMesh):
             else:
                 accumulate = False
         paint(self.info, self._accum, self._colsums, p, wrap, accumulate, self._workspace(), self._flags(), check=check,
-              order_out=order_out)
+              order_out=order_out, sorted_out=sorted_out)
         if self.dtype.itemsize == 8:
             self.__dict__['value'] = self._accum
         else:
@@ -672,7 +673,8 @@ class ComplexMesh(BaseMesh):
         return RealMesh(out, info=self.info, device=self.device, attrs=self.attrs)
 
 
-def paint(info, accum, colsums, particles, wrap, accumulate, workspace, flags, check=True, order_out=None):
+def paint(info, accum, colsums, particles, wrap, accumulate, workspace, flags, check=True, order_out=None,
+          sorted_out=None):
     """Deterministic CIC paint of ``particles`` into the FP64 ``accum`` mesh (C ABI prc_assign_cic)."""
     nm, bs, bc = info.c_geometry()
     lib = _lib.load()
@@ -681,7 +683,9 @@ def paint(info, accum, colsums, particles, wrap, accumulate, workspace, flags, c
     args = [_lib.ptr(accum), _lib.ptr(colsums), nm, bs, bc, info.dtype.itemsize, _lib.ptr(particles.pos),
             particles.pos_bytes, _lib.ptr(w), 0 if w is None else w.element_size(), particles.size, int(bool(wrap)),
             int(bool(accumulate)), flags.ptr, _lib.ptr(ws), ws.numel(), _lib.stream_of(accum.device)]
-    if order_out is not None:
+    if order_out is not None and sorted_out is not None:
+        _lib.call('prc_assign_cic_sorted', *args, _lib.ptr(order_out), _lib.ptr(sorted_out), error=MeshError)
+    elif order_out is not None:
         _lib.call('prc_assign_cic_order', *args, _lib.ptr(order_out), error=MeshError)
     else:
         _lib.call('prc_assign_cic', *args, error=MeshError)

@@ -102,7 +102,8 @@ class OriginalMultiGridReconstruction(BaseReconstruction):
         _lib.call(name, _lib.ptr(mesh), nm, bs, bc,
                   _lib.ptr(p.pos), p.pos_bytes, p.size, _lib.ptr(getattr(p, 'order', None)), float(self.f),
                   self._los_arg(), field, shifted, int(self.wrap),
-                  _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device), error=MeshError)
+                  _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device),
+                  _lib.ptr(getattr(p, 'sorted', None)), error=MeshError)
 
 
 def run_batch(recons, jacobi_damping_factor=0.4, jacobi_niterations=5, vcycle_niterations=6):

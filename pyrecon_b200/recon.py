@@ -32,6 +32,8 @@ class BaseReconstruction(BaseClass):
     """Base template reconstruction class (pyrecon/recon.py:15-325).  Algorithms implement :meth:`run`."""
 
     _needs_fft_mesh = True
+    # keep the cell-ordered copy of painted device catalogues for the read-out (prc_assign_cic_sorted)
+    _sorted_positions = True
 
     @staticmethod
     def _select_nmesh(nmesh):
@@ -138,24 +140,28 @@ class BaseReconstruction(BaseClass):
         """Paint data (accumulates over calls, e.g. slab by slab).  ``check=False`` defers the
         box / NaN check (no host synchronisation)."""
         with self._stream_ctx():
-            order = self._new_order(positions)
-            self.mesh_data.assign_cic(positions, weights=weights, wrap=self.wrap, check=check, order_out=order)
-            self._keep_order(positions, order)
+            order, spos = self._new_order(positions)
+            self.mesh_data.assign_cic(positions, weights=weights, wrap=self.wrap, check=check, order_out=order,
+                                      sorted_out=spos)
+            self._keep_order(positions, order, spos)
 
     def assign_randoms(self, positions, weights=None, check=True):
         """Same as :meth:`assign_data`, for randoms."""
         if not self.mesh_randoms.is_set:
             self._size_randoms = 0
         with self._stream_ctx():
-            order = self._new_order(positions)
-            self.mesh_randoms.assign_cic(positions, weights=weights, wrap=self.wrap, check=check, order_out=order)
-            self._keep_order(positions, order)
+            order, spos = self._new_order(positions)
+            self.mesh_randoms.assign_cic(positions, weights=weights, wrap=self.wrap, check=check, order_out=order,
+                                         sorted_out=spos)
+            self._keep_order(positions, order, spos)
         self._size_randoms += len(positions)
 
     # Device-resident catalogues keep the cell order their paint used: a later read-out of the same
     # tensor visits the particles in that order, so the gathers of neighbouring threads hit
     # neighbouring cells.  Any permutation gives the same results; the key (address, length) only
-    # picks which one.
+    # picks which one.  The paint also keeps the positions in that order, which the read-out streams
+    # instead of gathering them through the permutation, as long as the tensor has not been modified
+    # in place since (its version counter is unchanged).
 
     @staticmethod
     def _order_key(positions):
@@ -167,18 +173,30 @@ class BaseReconstruction(BaseClass):
     def _new_order(self, positions):
         import torch
         if self._order_key(positions) is None or len(positions) == 0:
-            return None
-        return torch.empty(len(positions), dtype=torch.int32, device=self.device)
+            return None, None
+        order = torch.empty(len(positions), dtype=torch.int32, device=self.device)
+        spos = None
+        if self._sorted_positions and positions.shape[-1] == 3 and positions.dtype in (torch.float32, torch.float64):
+            spos = torch.empty(positions.shape, dtype=positions.dtype, device=self.device)
+        return order, spos
 
-    def _keep_order(self, positions, order):
+    def _keep_order(self, positions, order, spos=None):
         if order is not None:
             if not hasattr(self, '_orders'):
                 self._orders = {}
-            self._orders[self._order_key(positions)] = order
+            self._orders[self._order_key(positions)] = (order, spos, positions._version)
 
     def _order_for(self, positions):
         key = self._order_key(positions)
-        return None if key is None else getattr(self, '_orders', {}).get(key)
+        kept = None if key is None else getattr(self, '_orders', {}).get(key)
+        return None if kept is None else kept[0]
+
+    def _sorted_for(self, positions):
+        key = self._order_key(positions)
+        kept = None if key is None else getattr(self, '_orders', {}).get(key)
+        if kept is None or kept[1] is None or positions._version != kept[2]:
+            return None
+        return kept[1]
 
     @property
     def has_randoms(self):
@@ -284,6 +302,7 @@ class BaseReconstruction(BaseClass):
         with self._stream_ctx():
             p = Particles(positions, self.device)
             p.order = self._order_for(positions)
+            p.sorted = self._sorted_for(positions) if p.order is not None else None
             pbytes = p.pos_bytes
             obytes = max(pbytes, self.info.dtype.itemsize) if (shifted and self.wrap) else pbytes
             out = torch.empty((p.size, 3), dtype=torch_dtype('f4' if obytes == 4 else 'f8'), device=self.device)
@@ -404,4 +423,5 @@ class FFTShiftsMixin(object):
         _lib.call('prc_read_shifts_psi_' + _lib.suffix(self.info.dtype), *self._psi_pointers(self._psi4), 4, nm, bs,
                   bc, _lib.ptr(p.pos), p.pos_bytes, p.size, _lib.ptr(getattr(p, 'order', None)), float(self.f),
                   self._los_arg(), field, shifted,
-                  int(self.wrap), _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device), error=MeshError)
+                  int(self.wrap), _lib.ptr(out), obytes, self._flags.ptr, _lib.stream_of(self.device),
+                  _lib.ptr(getattr(p, 'sorted', None)), error=MeshError)

@@ -96,10 +96,13 @@ def test_chunked_host_readout_equals_device_readout(kind):
     assert np.array_equal(disp, out['shifts_disp'])
 
 
-@pytest.mark.parametrize('name', ['ifft_f4_local', 'mg_f8_local', 'ifftp_f8_local', 'ifftp_f4_local'])
+@pytest.mark.parametrize('name', ['ifft_f4_local', 'mg_f8_local', 'ifftp_f8_local', 'ifftp_f4_local', 'pp_f8_box_wrap',
+                                  'mg_f8_box_wrap', 'mg_f4_local'])
 def test_readout_in_paint_order_equals_plain_readout(name):
-    """Device catalogues are read out in the cell order of their paint; a copy of the same positions
-    (no order remembered) gives the same bits."""
+    """Device catalogues are read out in the cell order of their paint, from the cell-ordered copy of the
+    positions the paint kept; a copy of the same positions (no order remembered) gives the same bits,
+    and so does the read-out after the catalogue was modified in place (the kept copy is then stale and
+    not used)."""
     import torch
     import pyrecon_b200
     from _util import ALGOS
@@ -117,11 +120,17 @@ def test_readout_in_paint_order_equals_plain_readout(name):
     rec.set_density_contrast(smoothing_radius=m['smoothing_radius'])
     rec.run()
     assert rec._order_for(data) is not None
+    assert (rec._sorted_for(data) is not None) == (m['algorithm'] != 'iterative_fft_particle')
     for cat in [data] + ([randoms] if randoms is not None else []):
         ordered = rec.read_shifted_positions(cat)
         plain = rec.read_shifted_positions(cat.clone())
         assert torch.equal(ordered, plain)
         assert torch.equal(rec.read_shifts(cat, field='rsd'), rec.read_shifts(cat.clone(), field='rsd'))
+    # an in-place change of the catalogue: the order is still used (any order gives the same bits), the
+    # kept cell-ordered positions are not
+    data[:10] = data[10:20].clone()
+    assert rec._sorted_for(data) is None and rec._order_for(data) is not None
+    assert torch.equal(rec.read_shifted_positions(data), rec.read_shifted_positions(data.clone()))
 
 
 def test_sky_conversions_on_device():
