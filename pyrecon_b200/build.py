@@ -32,12 +32,14 @@ FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-Xcompiler', 
          '--expt-relaxed-constexpr', '-I' + os.path.join(ROOT, 'include')]
 
 
-# name -> extra nvcc flags for fft.cu.  'nopp': every TMA-fed FFT pass with two barriers per shared-memory
-# exchange instead of the ping-pong buffers (same arithmetic, same order).
+# name -> (source rebuilt, extra nvcc flags).  'nopp': every TMA-fed FFT pass with two barriers per
+# shared-memory exchange instead of the ping-pong buffers (same arithmetic, same order).
 VARIANTS = {
-    'nopp': ['-DPRC_STRIDED_PP=0', '-DPRC_KSPACE_PP=0', '-DPRC_HESS_PP=0', '-DPRC_C2R_PP=0'],
+    'nopp': ('fft.cu', ['-DPRC_STRIDED_PP=0', '-DPRC_KSPACE_PP=0', '-DPRC_HESS_PP=0', '-DPRC_C2R_PP=0']),
     # every radix-8 twiddle read from the pass table (7 loads per butterfly instead of 3 and 4 products)
-    'twload': ['-DPRC_TW_RECUR=0'],
+    'twload': ('fft.cu', ['-DPRC_TW_RECUR=0']),
+    # the CIC read-out left to the register allocator (no minimum of blocks per SM)
+    'readfree': ('cic.cu', ['-DPRC_READ_MINB=1']),
 }
 
 
@@ -77,11 +79,11 @@ def build(force=False, verbose=False, extra=(), variants=True):
         if force or _stale(obj, [os.path.join(CSRC, src)] + HEADERS):
             jobs.append((src, list(extra), obj))
     variant_objs = {}
-    for name, flags in (VARIANTS.items() if variants else []):
-        obj = os.path.join(BUILD, 'fft_{}.o'.format(name))
-        variant_objs[name] = obj
-        if force or _stale(obj, [os.path.join(CSRC, 'fft.cu')] + HEADERS):
-            jobs.append(('fft.cu', list(extra) + flags, obj))
+    for name, (src, flags) in (VARIANTS.items() if variants else []):
+        obj = os.path.join(BUILD, '{}_{}.o'.format(os.path.splitext(src)[0], name))
+        variant_objs[name] = (src, obj)
+        if force or _stale(obj, [os.path.join(CSRC, src)] + HEADERS):
+            jobs.append((src, list(extra) + flags, obj))
     if jobs:
         with concurrent.futures.ThreadPoolExecutor(max_workers=len(jobs)) as ex:
             for _ in ex.map(lambda j: _compile(j[0], j[1], j[2]), jobs):
@@ -91,9 +93,10 @@ def build(force=False, verbose=False, extra=(), variants=True):
         _link(lib, objs)
         if verbose:
             print('built', lib)
-    for name, vobj in variant_objs.items():
+    for name, (src, vobj) in variant_objs.items():
         vlib = library_path(name)
-        vobjs = [vobj if os.path.basename(o) == 'fft.o' else o for o in objs]
+        base = os.path.splitext(src)[0] + '.o'
+        vobjs = [vobj if os.path.basename(o) == base else o for o in objs]
         if force or _stale(vlib, vobjs):
             _link(vlib, vobjs)
             if verbose:

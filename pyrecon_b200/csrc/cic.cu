@@ -681,8 +681,15 @@ __global__ void __launch_bounds__(256) read_fd_kernel(const F* __restrict__ mesh
 // displacement read in F then cast to P (the shifts array has the positions' dtype); RSD in
 // R = promoted type of (shifts, los); result cast back to P; positions - shifts in P, then
 // wrapped in T = promote(P, F) when `wrap`; the output type O is chosen by the caller.
+// PRC_READ_MINB: blocks per SM asked of the register allocator for the CIC shift read-out (its gathers
+// are latency-bound: ncu shows long-scoreboard stalls first at 50 % occupancy); the finite-difference
+// read-out (48 loads a particle) is left to the allocator.
+#ifndef PRC_READ_MINB
+#define PRC_READ_MINB 5
+#endif
+
 template <typename P, typename F, typename O, bool PHI, bool IL>
-__global__ void __launch_bounds__(256) read_shifts_kernel(const F* __restrict__ m0, const F* __restrict__ m1,
+__global__ void __launch_bounds__(256, (PHI ? 1 : PRC_READ_MINB)) read_shifts_kernel(const F* __restrict__ m0, const F* __restrict__ m1,
                                                           const F* __restrict__ m2, BoxGeom g, F tc0, F tc1, F tc2,
                                                           const P* __restrict__ pos, int64_t n, double f,
                                                           int global_los, double l0, double l1, double l2, int field,
