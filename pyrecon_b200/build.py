@@ -38,8 +38,6 @@ VARIANTS = {
     'nopp': ('fft.cu', ['-DPRC_STRIDED_PP=0', '-DPRC_KSPACE_PP=0', '-DPRC_HESS_PP=0', '-DPRC_C2R_PP=0']),
     # every radix-8 twiddle read from the pass table (7 loads per butterfly instead of 3 and 4 products)
     'twload': ('fft.cu', ['-DPRC_TW_RECUR=0']),
-    # the CIC read-out left to the register allocator (no minimum of blocks per SM)
-    'readfree': ('cic.cu', ['-DPRC_READ_MINB=1']),
 }
 
 

@@ -682,10 +682,11 @@ __global__ void __launch_bounds__(256) read_fd_kernel(const F* __restrict__ mesh
 // R = promoted type of (shifts, los); result cast back to P; positions - shifts in P, then
 // wrapped in T = promote(P, F) when `wrap`; the output type O is chosen by the caller.
 // PRC_READ_MINB: blocks per SM asked of the register allocator for the CIC shift read-out (its gathers
-// are latency-bound: ncu shows long-scoreboard stalls first at 50 % occupancy); the finite-difference
-// read-out (48 loads a particle) is left to the allocator.
+// are latency-bound: ncu shows long-scoreboard stalls first at 50 % occupancy).  Measured: 5 blocks (48
+// registers, a few spilled) made it slower (1.90 against 1.77 ms per nmesh-512 reconstruction), so the
+// default leaves the allocator free; the finite-difference read-out (48 loads a particle) always is.
 #ifndef PRC_READ_MINB
-#define PRC_READ_MINB 5
+#define PRC_READ_MINB 1
 #endif
 
 template <typename P, typename F, typename O, bool PHI, bool IL>

@@ -146,6 +146,34 @@ int device_sm_count();
 int tune_get(const char* name, int key, int dflt);
 unsigned tune_generation();
 
+// Programmatic dependent launch.  A kernel launched by launch_pdl may be scheduled while its predecessor
+// on the stream (or in a captured graph) is still finishing: its blocks call pdl_wait() before reading
+// anything the predecessor wrote (the wait returns once the predecessor grid has completed and its
+// memory is visible; at once when there is no programmatic predecessor), and pdl_trigger() to let
+// their own successor be scheduled as soon as every block of this grid has started.  No spin of ours:
+// the ordering is the hardware's.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// PRC_PDL=0 in the environment launches these kernels without the attribute (plain stream order).
+bool pdl_enabled();
+
+template <typename... K, typename... A>
+inline cudaError_t launch_pdl(void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<K>(args)...);
+}
+
 // Adds n to the launch counter (kernels replayed inside a CUDA graph launch).
 void add_launches(unsigned long long n);
 // Launches and compulsory bytes recorded by this thread's captures since the last call (reset).

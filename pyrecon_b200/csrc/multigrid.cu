@@ -122,6 +122,8 @@ __device__ __forceinline__ int64_t batch_offset(const int n[3]) {
 template <typename T, typename FT>
 __global__ void __launch_bounds__(256) jacobi_sweep(const T* __restrict__ v, const FT* __restrict__ f,
                                                     T* __restrict__ vout, Stencil<T> s, T w, int zero_v) {
+    pdl_trigger();
+    pdl_wait();
     int x, y, z;
     if (!cell3(s.n, x, y, z)) return;
     const int64_t bo = batch_offset(s.n);
@@ -306,6 +308,8 @@ __device__ __forceinline__ void quad_blend(const Stencil<T>& s, T w, const T (&f
 template <typename T, bool LOCAL>
 __global__ void __launch_bounds__(256) jacobi_sweep4(const T* __restrict__ v, const T* __restrict__ f,
                                                      T* __restrict__ vout, Stencil<T> s, T w, int zero_v) {
+    pdl_trigger();
+    pdl_wait();
     Quad q;
     if (!quad_of(s.n, q)) return;
     const int64_t bo = batch_offset(s.n);
@@ -400,6 +404,8 @@ template <typename T, bool LOCAL, int TY, int TQ>
 __global__ void __launch_bounds__(TQ * TY, (sizeof(T) == 4 ? 6 : 4)) jacobi_sweep2_tb(const T* __restrict__ v, const T* __restrict__ f,
                                                              T* __restrict__ vout, Stencil<T> s, T w, int zero_v,
                                                              int slab, int nslab) {
+    pdl_trigger();
+    pdl_wait();
     typedef TbShape<T, TY, TQ> SH;
     constexpr int ZP = SH::ZP;
     constexpr int PL0 = SH::R0 * ZP, PL1 = SH::R1 * ZP;
@@ -491,6 +497,8 @@ __global__ void __launch_bounds__(TQ * TY, (sizeof(T) == 4 ? 6 : 4)) jacobi_swee
 template <typename A, typename V, typename FT, typename R, typename S, bool LOCAL>
 __global__ void __launch_bounds__(256) residual_kernel4(const V* __restrict__ v, const FT* __restrict__ f,
                                                         R* __restrict__ r, Stencil<S> s) {
+    pdl_trigger();
+    pdl_wait();
     Quad q;
     if (!quad_of(s.n, q)) return;
     const int64_t bo = batch_offset(s.n);
@@ -514,6 +522,8 @@ __global__ void __launch_bounds__(256) residual_kernel4(const V* __restrict__ v,
 template <typename A, typename V, typename FT, typename R, typename S>
 __global__ void __launch_bounds__(256) residual_kernel(const V* __restrict__ v, const FT* __restrict__ f,
                                                        R* __restrict__ r, Stencil<S> s) {
+    pdl_trigger();
+    pdl_wait();
     int x, y, z;
     if (!cell3(s.n, x, y, z)) return;
     const int64_t bo = batch_offset(s.n);
@@ -529,6 +539,8 @@ __global__ void __launch_bounds__(256) residual_kernel(const V* __restrict__ v, 
 // 27-point full weighting, coarse cell (x, y, z) centred on fine (2x, 2y, 2z).
 template <typename A, typename TI, typename TO>
 __global__ void __launch_bounds__(256) reduce_kernel(const TI* __restrict__ fine, TO* __restrict__ coarse, Dims nf) {
+    pdl_trigger();
+    pdl_wait();
     const int nc[3] = {nf.n[0] / 2, nf.n[1] / 2, nf.n[2] / 2};
     {
         int x, y, z;
@@ -560,6 +572,8 @@ __global__ void __launch_bounds__(256) reduce_kernel(const TI* __restrict__ fine
 // else fine = value.
 template <typename A, typename TI, typename TO, bool ADD>
 __global__ void __launch_bounds__(256) prolong_kernel(const TI* __restrict__ coarse, TO* __restrict__ fine, Dims nc) {
+    pdl_trigger();
+    pdl_wait();
     const int nf1 = 2 * nc.n[1], nf2 = 2 * nc.n[2];
     {
         int x, y, z;
@@ -595,12 +609,16 @@ __global__ void __launch_bounds__(256) prolong_kernel(const TI* __restrict__ coa
 
 template <typename TI, typename TO>
 __global__ void convert_kernel(const TI* __restrict__ in, TO* __restrict__ out, int64_t n) {
+    pdl_trigger();
+    pdl_wait();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = (TO)in[i];
 }
 
 template <typename TA, typename TB>
 __global__ void add_kernel(TA* __restrict__ acc, const TB* __restrict__ x, int64_t n) {
+    pdl_trigger();
+    pdl_wait();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         acc[i] = acc[i] + (TA)x[i];
 }
@@ -723,9 +741,8 @@ template <typename T> struct MGRunner {
                 for (; it + 1 < niter; it += 2) {
                     const bool z0 = zero_first && it == 0;
                     PRC_LAUNCH_B("mg_jacobi2", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
-                                 (s.local ? jacobi_sweep2_tb<T, true, TB_TY, TB_TQ>
-                                          : jacobi_sweep2_tb<T, false, TB_TY, TB_TQ>)<<<grid, TB_TY * TB_TQ, 0, st>>>(
-                                     v, f, tmp, s, (T)P.damping, z0, slab, nslab));
+                                 launch_pdl((s.local ? jacobi_sweep2_tb<T, true, TB_TY, TB_TQ>
+                                          : jacobi_sweep2_tb<T, false, TB_TY, TB_TQ>), grid, TB_TY * TB_TQ, 0, st, v, f, tmp, s, (T)P.damping, z0, slab, nslab));
                     std::swap(v, tmp);
                 }
             }
@@ -734,11 +751,10 @@ template <typename T> struct MGRunner {
             const bool z0 = zero_first && it == 0;
             if (quad)
                 PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
-                             (s.local ? jacobi_sweep4<T, true> : jacobi_sweep4<T, false>)<<<gq.grid, gq.block, 0, st>>>(
-                                 v, f, tmp, s, (T)P.damping, z0));
+                             launch_pdl((s.local ? jacobi_sweep4<T, true> : jacobi_sweep4<T, false>), gq.grid, gq.block, 0, st, v, f, tmp, s, (T)P.damping, z0));
             else
                 PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
-                             jacobi_sweep<T, T><<<g.grid, g.block, 0, st>>>(v, f, tmp, s, (T)P.damping, z0));
+                             launch_pdl(jacobi_sweep<T, T>, g.grid, g.block, 0, st, v, f, tmp, s, (T)P.damping, z0));
             std::swap(v, tmp);
         }
         PRC_CHECK_LAUNCH();
@@ -755,20 +771,19 @@ template <typename T> struct MGRunner {
             if (quad_ok(L[l].n, v, f, B[l].r)) {
                 const Grid3 gq = grid3_quad(L[l].n, count);
                 PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T),
-                             (s.local ? residual_kernel4<T, T, T, T, T, true> : residual_kernel4<T, T, T, T, T, false>)
-                                 <<<gq.grid, gq.block, 0, st>>>(v, f, B[l].r, s));
+                             launch_pdl((s.local ? residual_kernel4<T, T, T, T, T, true> : residual_kernel4<T, T, T, T, T, false>), gq.grid, gq.block, 0, st, v, f, B[l].r, s));
             } else {
                 PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T),
-                             residual_kernel<T, T, T, T, T><<<g.grid, g.block, 0, st>>>(v, f, B[l].r, s));
+                             launch_pdl(residual_kernel<T, T, T, T, T>, g.grid, g.block, 0, st, v, f, B[l].r, s));
             }
             Dims nf = {{L[l].n[0], L[l].n[1], L[l].n[2]}};
             PRC_LAUNCH_B("mg_reduce", st, (double)(N + L[l + 1].size() * count) * sizeof(T),
-                         reduce_kernel<T, T, T><<<gc.grid, gc.block, 0, st>>>(B[l].r, B[l + 1].f, nf));
+                         launch_pdl(reduce_kernel<T, T, T>, gc.grid, gc.block, 0, st, B[l].r, B[l + 1].f, nf));
             PRC_CHECK_LAUNCH();
             PRC_TRY(vcycle(l + 1, B[l + 1].v, B[l + 1].f, true));
             Dims nc = {{L[l + 1].n[0], L[l + 1].n[1], L[l + 1].n[2]}};
             PRC_LAUNCH_B("mg_prolong_add", st, (double)(2 * N + L[l + 1].size() * count) * sizeof(T),
-                         prolong_kernel<T, T, T, true><<<gc.grid, gc.block, 0, st>>>(B[l + 1].v, v, nc));
+                         launch_pdl(prolong_kernel<T, T, T, true>, gc.grid, gc.block, 0, st, B[l + 1].v, v, nc));
             PRC_CHECK_LAUNCH();
         }
         return jacobi(l, v, f, B[l].tmp, P.jn, false);
@@ -786,7 +801,7 @@ template <typename T> static int fmg_plain(MGRunner<T>& R, const T* f0, T* v0) {
         Dims nf = {{R.L[l].n[0], R.L[l].n[1], R.L[l].n[2]}};
         const Grid3 gc = grid3_coarse(R.L[l].n, cnt);
         PRC_LAUNCH_B("mg_reduce", st, (double)(R.L[l].size() + R.L[l + 1].size()) * cnt * sizeof(T),
-                     reduce_kernel<T, T, T><<<gc.grid, gc.block, 0, st>>>(R.B[l].f, R.B[l + 1].f, nf));
+                     launch_pdl(reduce_kernel<T, T, T>, gc.grid, gc.block, 0, st, R.B[l].f, R.B[l + 1].f, nf));
     }
     PRC_CHECK_LAUNCH();
     // the FMG solution of level l >= 1 lives in B[l].v; level 0 starts in v0 and may end in
@@ -800,7 +815,7 @@ template <typename T> static int fmg_plain(MGRunner<T>& R, const T* f0, T* v0) {
             Dims nc = {{R.L[l + 1].n[0], R.L[l + 1].n[1], R.L[l + 1].n[2]}};
             const Grid3 gc = grid3(R.L[l + 1].n, cnt);
             PRC_LAUNCH_B("mg_prolong", st, (double)(R.L[l].size() + R.L[l + 1].size()) * cnt * sizeof(T),
-                         prolong_kernel<T, T, T, false><<<gc.grid, gc.block, 0, st>>>(R.B[l + 1].v, v, nc));
+                         launch_pdl(prolong_kernel<T, T, T, false>, gc.grid, gc.block, 0, st, R.B[l + 1].v, v, nc));
             PRC_CHECK_LAUNCH();
         }
         for (int it = 0; it < R.P.vn; it++) PRC_TRY(R.vcycle(l, v, R.B[l].f, l == nl - 1 && it == 0));
@@ -927,7 +942,7 @@ int solve_mixed(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t 
         Dims nf = {{m.L[l].n[0], m.L[l].n[1], m.L[l].n[2]}};
         const Grid3 gc = grid3_coarse(m.L[l].n, count);
         PRC_LAUNCH_B("mg_reduce", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()) * count,
-                     reduce_kernel<double, double, double><<<gc.grid, gc.block, 0, st>>>(m.f64[l], m.f64[l + 1], nf));
+                     launch_pdl(reduce_kernel<double, double, double>, gc.grid, gc.block, 0, st, m.f64[l], m.f64[l + 1], nf));
     }
     PRC_CHECK_LAUNCH();
     for (int l = nl - 1; l >= 0; l--) {
@@ -939,7 +954,7 @@ int solve_mixed(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t 
             Dims nc = {{m.L[l + 1].n[0], m.L[l + 1].n[1], m.L[l + 1].n[2]}};
             const Grid3 gc = grid3(m.L[l + 1].n, count);
             PRC_LAUNCH_B("mg_prolong", st, 8.0 * (m.L[l].size() + m.L[l + 1].size()) * count,
-                         prolong_kernel<double, double, double, false><<<gc.grid, gc.block, 0, st>>>(m.v64[l + 1],
+                         launch_pdl(prolong_kernel<double, double, double, false>, gc.grid, gc.block, 0, st, m.v64[l + 1],
                                                                                                   m.v64[l], nc));
         }
         Stencil<double> s64 = make_stencil<double>(m.L[l].n, P.boxsize, P.boxcenter, P.beta,
@@ -949,18 +964,16 @@ int solve_mixed(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t 
             if (quad_ok(m.L[l].n, m.v64[l], m.f64[l], R.B[l].f)) {
                 const Grid3 gq = grid3_quad(m.L[l].n, count);
                 PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N,
-                             (s64.local ? residual_kernel4<double, double, double, float, double, true>
-                                        : residual_kernel4<double, double, double, float, double, false>)
-                                 <<<gq.grid, gq.block, 0, st>>>(m.v64[l], m.f64[l], R.B[l].f, s64));
+                             launch_pdl((s64.local ? residual_kernel4<double, double, double, float, double, true>
+                                        : residual_kernel4<double, double, double, float, double, false>), gq.grid, gq.block, 0, st, m.v64[l], m.f64[l], R.B[l].f, s64));
             } else {
                 PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N,
-                             residual_kernel<double, double, double, float, double><<<g.grid, g.block, 0, st>>>(
-                                 m.v64[l], m.f64[l], R.B[l].f, s64));
+                             launch_pdl(residual_kernel<double, double, double, float, double>, g.grid, g.block, 0, st, m.v64[l], m.f64[l], R.B[l].f, s64));
             }
             PRC_CHECK_LAUNCH();
             PRC_TRY(R.vcycle(l, R.B[l].v, R.B[l].f, true));
             PRC_LAUNCH_B("mg_correct_fp64", st, 20.0 * N,
-                         add_kernel<double, float><<<grid_for(N), 256, 0, st>>>(m.v64[l], R.B[l].v, N));
+                         launch_pdl(add_kernel<double, float>, grid_for(N), 256, 0, st, m.v64[l], R.B[l].v, N));
             PRC_CHECK_LAUNCH();
         }
     }

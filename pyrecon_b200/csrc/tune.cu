@@ -6,6 +6,7 @@
 #include "common.cuh"
 
 #include <map>
+#include <stdlib.h>
 #include <mutex>
 #include <string>
 #include <utility>
@@ -27,6 +28,14 @@ int tune_get(const char* name, int key, int dflt) {
 unsigned tune_generation() {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     return g_tune_generation;
+}
+
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* v = getenv("PRC_PDL");
+        return !(v != nullptr && v[0] == '0');
+    }();
+    return on;
 }
 
 }  // namespace prc
