@@ -1048,7 +1048,8 @@ template <typename T, int N> struct KSpaceTmaCfg {
     static constexpr int B = KSpaceCfg<T, N>::B;
     static constexpr int THREADS = KSpaceCfg<T, N>::THREADS;
     static constexpr int S = 2;
-    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, fast::KSpacePP<T, N, B, S, LEAN>::value ? 2 : 1>::BYTES;
+    static constexpr bool PP = fast::KSpacePP<T, N, B, S, LEAN>::value;
+    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, PP ? 2 : 1, PP ? fast::PadFirst<T, B>::value : 0>::BYTES;
 };
 
 template <typename T> struct FastXTma {
@@ -1111,11 +1112,12 @@ template <typename T, int N> struct HessTmaCfg {
     static constexpr int B = (N / 8) * B0 <= 1024 ? B0 : 1024 / (N / 8);
     static constexpr int THREADS = (N / 8) * B;
     static constexpr int MINB = THREADS * PRC_HESS_MINB <= 1024 ? PRC_HESS_MINB : 1;
+    static constexpr int PADX = fast::PadFirst<T, B>::value;
     static constexpr bool PP =
-        PRC_HESS_PP != 0 && fast::TmaSmem<T, N, B, PRC_HESS_PP_S, 1>::BYTES + 2 * N * sizeof(T) <= 227 * 1024;
+        PRC_HESS_PP != 0 && fast::TmaSmem<T, N, B, PRC_HESS_PP_S, 1, PADX>::BYTES + 2 * N * sizeof(T) <= 227 * 1024;
     static constexpr int S = PP ? PRC_HESS_PP_S
                                 : StageCount<(int)(PRC_TMA_STAGE_KB * 1024 / fast::TileShape<T, N, B>::BYTES)>::value;
-    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, PP ? 1 : 0>::BYTES;
+    static constexpr size_t SMEM = fast::TmaSmem<T, N, B, S, PP ? 1 : 0, PP ? PADX : 0>::BYTES;
 };
 
 template <typename T> struct FastHessTma {

@@ -187,14 +187,16 @@ __device__ __forceinline__ void exchange_pp(C (&v)[8], int t, C* s, const Addr& 
 }
 
 template <typename C, int N, int DIR, int P> struct PassesPP {
-    template <class Addr>
-    static __device__ __forceinline__ void run(C (&v)[8], int t, C* s0, C* s1, const Addr& addr, const C* tw) {
+    template <class Addr0, class Addr1>
+    static __device__ __forceinline__ void run(C (&v)[8], int t, C* s0, const Addr0& addr0, C* s1, const Addr1& addr1,
+                                               const C* tw) {
         constexpr int R = TwLayout<N>::radix(P);
         constexpr int NS = ipow8(P);
         pass_regs<C, N, R, NS, DIR>(v, t, tw + TwLayout<N>::offset(P));
         if constexpr (P + 1 < Plan<N>::NPASS) {
-            exchange_pp<C, N, R, NS>(v, t, P % 2 == 0 ? s0 : s1, addr);
-            PassesPP<C, N, DIR, P + 1>::run(v, t, s0, s1, addr, tw);
+            if constexpr (P % 2 == 0) exchange_pp<C, N, R, NS>(v, t, s0, addr0);
+            else exchange_pp<C, N, R, NS>(v, t, s1, addr1);
+            PassesPP<C, N, DIR, P + 1>::run(v, t, s0, addr0, s1, addr1, tw);
         }
     }
 };
@@ -208,12 +210,29 @@ __device__ __forceinline__ void fft_regs(C (&v)[8], int t, C* s, const Addr& add
 
 template <typename C, int N, int DIR, class Addr>
 __device__ __forceinline__ void fft_regs_pp(C (&v)[8], int t, C* s0, C* s1, const Addr& addr, const C* tw) {
-    PassesPP<C, N, DIR, 0>::run(v, t, s0, s1, addr, tw);
+    PassesPP<C, N, DIR, 0>::run(v, t, s0, addr, s1, addr, tw);
+}
+
+// The same with a separate layout for s0, the buffer of the first (and every even) exchange.
+template <typename C, int N, int DIR, class Addr0, class Addr1>
+__device__ __forceinline__ void fft_regs_pp(C (&v)[8], int t, C* s0, const Addr0& addr0, C* s1, const Addr1& addr1,
+                                            const C* tw) {
+    PassesPP<C, N, DIR, 0>::run(v, t, s0, addr0, s1, addr1, tw);
 }
 
 struct ColAddr {
     int B, col;
     __device__ __forceinline__ int operator()(int k) const { return k * B + col; }
+};
+
+// ColAddr with one row of padding after every 8 rows, for the exchange buffer of the first Stockham pass
+// of a tile with B = 8 FP32 columns: that pass writes the rows 8 t + r of the four lines t a warp holds,
+// which in the dense layout all start on the same bank (a row is 16 banks wide), two-way conflicting;
+// padded, they alternate between the two halves of the banks.  Reads of consecutive rows stay
+// conflict-free.  The buffer holds (N + N / 8) B values.
+struct PadAddr {
+    int B, col;
+    __device__ __forceinline__ int operator()(int k) const { return (k + (k >> 3)) * B + col; }
 };
 
 struct RowAddr {

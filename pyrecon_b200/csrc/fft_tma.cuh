@@ -66,11 +66,18 @@ __device__ __forceinline__ void drain(uint64_t* bars, int64_t j, int64_t ntiles)
 }
 
 // Shared memory of S stages (+ `extra` tile buffers) and the pass twiddles, then the barriers.
-template <typename T, int N, int B, int S, int EXTRA> struct TmaSmem {
+// PADX: the first of the EXTRA tiles is a padded first-exchange buffer (PadAddr, N / 8 more rows).
+template <typename T, int N, int B, int S, int EXTRA, int PADX = 0> struct TmaSmem {
     typedef TileShape<T, N, B> TS;
-    static constexpr size_t TILES = (size_t)(S + EXTRA) * TS::ELEMS * sizeof(cplx_t<T>);
+    static constexpr size_t TILES = ((size_t)(S + EXTRA) * TS::ELEMS + (size_t)PADX * (N / 8) * B) * sizeof(cplx_t<T>);
     static constexpr size_t TW = (size_t)N * sizeof(cplx_t<T>);
     static constexpr size_t BYTES = TILES + TW + S * sizeof(uint64_t);
+};
+
+// The first exchange of a tile of B columns is padded where a row is half the banks wide (B * complex =
+// 64 bytes, FP32 with B = 8): see PadAddr.
+template <typename T, int B> struct PadFirst {
+    static constexpr int value = B * sizeof(cplx_t<T>) == 64 ? 1 : 0;
 };
 
 // PRC_STRIDED_PP: the strided passes exchange through a scratch tile, then the consumed stage
@@ -162,7 +169,8 @@ __global__ void __launch_bounds__(N / 8 * B) strided_tma(const __grid_constant__
 #define PRC_KSPACE_PP 1
 #endif
 template <typename T, int N, int B, int S, bool LEAN> struct KSpacePP {
-    static constexpr bool value = PRC_KSPACE_PP && !LEAN && TmaSmem<T, N, B, S, 2>::BYTES <= 227 * 1024;
+    static constexpr bool value =
+        PRC_KSPACE_PP && !LEAN && TmaSmem<T, N, B, S, 2, PadFirst<T, B>::value>::BYTES <= 227 * 1024;
 };
 
 // LEAN: the forward spectrum is kept in the tile's stage (not in registers) and the per-point
@@ -182,12 +190,14 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 :
     // the previous one read last: a barrier separates them (as it does a transform without exchanges
     // from the stage re-arm)
     constexpr bool PP_SYNC = (Plan<N>::NPASS - 1) % 2 == 1 || Plan<N>::NPASS == 1;
+    constexpr int PADX = PP ? PadFirst<T, B>::value : 0;   // PP: xbuf, the first exchange's, padded
     C* xbuf = stages + S * TS::ELEMS;
-    C* ybuf = xbuf + TS::ELEMS;                  // PP: the second scratch tile
+    C* ybuf = xbuf + TS::ELEMS + PADX * (N / 8) * B;   // PP: the second scratch tile
     C* tw = ybuf + (PP ? TS::ELEMS : 0);
     uint64_t* bars = (uint64_t*)(tw + N);
     const int tid = threadIdx.x, col = tid % B, t = tid / B;
     const ColAddr addr{B, col};
+    const PadAddr paddr{B, col};
     if (tid == 0) {
         for (int i = 0; i < S; i++) prc::tma::barrier_init(&bars[i], 1);
         prc::tma::fence_barrier_init();
@@ -273,7 +283,8 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 :
             for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
             if constexpr (PP) {
                 // the stage is free once every thread is past the first exchange's barrier
-                fft_regs_pp<C, N, -1>(v, t, xbuf, ybuf, addr, tw);
+                if constexpr (PADX) fft_regs_pp<C, N, -1>(v, t, xbuf, paddr, ybuf, addr, tw);
+                else fft_regs_pp<C, N, -1>(v, t, xbuf, ybuf, addr, tw);
                 if constexpr (PP_SYNC) __syncthreads();
             } else {
                 __syncthreads();
@@ -287,7 +298,8 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, LEAN ? 2 :
                 C u[8];
                 kl.apply(op, dims, t, o, v, u);
                 if constexpr (PP) {
-                    fft_regs_pp<C, N, +1>(u, t, xbuf, ybuf, addr, tw);
+                    if constexpr (PADX) fft_regs_pp<C, N, +1>(u, t, xbuf, paddr, ybuf, addr, tw);
+                    else fft_regs_pp<C, N, +1>(u, t, xbuf, ybuf, addr, tw);
                     if constexpr (PP_SYNC) __syncthreads();
                 } else {
                     fft_regs<C, N, +1>(u, t, xbuf, addr, tw);
@@ -470,13 +482,15 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, MINB>::val
     constexpr int TL = N / 8;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* stages = (C*)smem_raw;
+    constexpr int PADX = PP ? PadFirst<T, B>::value : 0;   // PP: the scratch tile (first exchange) padded
     C* xscr = stages + S * TS::ELEMS;          // PP: the exchange scratch tile
-    C* tw = xscr + (PP ? TS::ELEMS : 0);
+    C* tw = xscr + (PP ? TS::ELEMS + PADX * (N / 8) * B : 0);
     uint64_t* bars = (uint64_t*)(tw + N);
     T* x1tab = (T*)(bars + S);     // x1 and k_y of every y index (2 N values after the barriers)
     T* kytab = x1tab + N;
     const int tid = threadIdx.x, col = tid % B, t = tid / B;
     const ColAddr addr{B, col};
+    const PadAddr paddr{B, col};
     if (tid == 0) {
         for (int i = 0; i < S; i++) prc::tma::barrier_init(&bars[i], 1);
         prc::tma::fence_barrier_init();
@@ -580,7 +594,8 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, MINB>::val
                 if constexpr (PP) {
                     // scratch first: the stage is written only by the second exchange, behind the first
                     // exchange's barrier, when every thread has read its points from it
-                    fft_regs_pp<C, N, +1>(v, t, xscr, sb, addr, tw);
+                    if constexpr (PADX) fft_regs_pp<C, N, +1>(v, t, xscr, paddr, sb, addr, tw);
+                    else fft_regs_pp<C, N, +1>(v, t, xscr, sb, addr, tw);
                 } else {
                     __syncthreads();
                     fft_regs<C, N, +1>(v, t, sb, addr, tw);
