@@ -1112,7 +1112,7 @@ template <typename T, int N> struct HessTmaCfg {
     static constexpr int B = (N / 8) * B0 <= 1024 ? B0 : 1024 / (N / 8);
     static constexpr int THREADS = (N / 8) * B;
     static constexpr int MINB = THREADS * PRC_HESS_MINB <= 1024 ? PRC_HESS_MINB : 1;
-    static constexpr int PADX = fast::PadFirst<T, B>::value;
+    static constexpr int PADX = 0;     // see y_hessian_tma
     static constexpr bool PP =
         PRC_HESS_PP != 0 && fast::TmaSmem<T, N, B, PRC_HESS_PP_S, 1, PADX>::BYTES + 2 * N * sizeof(T) <= 227 * 1024;
     static constexpr int S = PP ? PRC_HESS_PP_S
