@@ -9,8 +9,9 @@
 //   4. columns:  start offset of every (ix, iy) column in the sorted array;
 //   5. pull:     one warp per OUTPUT column (X, Y) sums, in a fixed order, the contributions of
 //                the four base columns (X-cx, Y-cy) in FP64 shared memory: per 32-particle chunk
-//                a segmented warp scan over equal iz, then two conflict-free phases add to
-//                z = iz and z = iz + 1.  Same inputs -> same bits, run after run.
+//                the k-th particles of the runs of equal iz add in round k (distinct cells per
+//                round), the z = iz terms before the z = iz + 1 terms, so every cell sums its
+//                particles in sorted order.  Same inputs -> same bits, run after run.
 #include "common.cuh"
 
 #include <cuda.h>
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_add(uint32_t* __restrict__ 
 }
 
 // Stable scatter of one tile: each warp ranks its contiguous 512-item slice chunk by chunk
-// (__match_any_sync groups equal digits; lanes keep input order), warps are then offset by the
+// (ballots group equal digits; lanes keep input order), warps are then offset by the
 // counts of the warps before them.  The tile is first reordered by digit in shared memory, so the
 // writes to the output run over consecutive addresses of each digit's range (coalesced) instead of
 // scattering single items; the tile's base in each digit's range comes from the scanned histogram.
@@ -165,8 +166,17 @@ __global__ void __launch_bounds__(THREADS, 3) downsweep(const uint32_t* __restri
         for (int c = 0; c < SLICE; c += 32) {
             int k = warp * SLICE + c + lane;
             bool ok = k < valid;
-            uint32_t d = ok ? (s_key[k] >> shift) & mask : 0xffffffffu;
-            uint32_t peers = __match_any_sync(0xffffffffu, d);
+            uint32_t d = ok ? (s_key[k] >> shift) & mask : 0u;
+            // lanes with the same digit (the set __match_any_sync returns), from one vote per digit bit and
+            // one for validity: short-latency votes instead of the match instruction
+            const uint32_t okm = __ballot_sync(0xffffffffu, ok);
+            uint32_t peers = ok ? okm : ~okm;
+#pragma unroll
+            for (int b = 0; b < MAXBITS; b++) {
+                const bool bit = (d >> b) & 1u;
+                const uint32_t v = __ballot_sync(0xffffffffu, bit);
+                peers &= bit ? v : ~v;
+            }
             uint32_t before = ok ? cnt[d] : 0u;
             __syncwarp();
             if (ok) {
@@ -472,23 +482,23 @@ __global__ void __launch_bounds__(PULL_WARPS * 32) paint_pull(const uint32_t* __
                     a = (double)rn_mul(rn_mul(wxy, rn_sub((F)1, pl.t[2])), pl.w);
                     b = (double)rn_mul(rn_mul(wxy, pl.t[2]), pl.w);
                 }
-                // segmented inclusive scan over runs of equal iz (keys are sorted within a column)
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const double ua = __shfl_up_sync(0xffffffffu, a, o);
-                    const double ub = __shfl_up_sync(0xffffffffu, b, o);
-                    const int uz = __shfl_up_sync(0xffffffffu, iz, o);
-                    if (lane >= o && uz == iz) {
-                        a += ua;
-                        b += ub;
-                    }
+                // runs of equal iz (keys are sorted within a column): the r-th particle of every run adds
+                // in round r, so the lanes of a round write distinct cells and every cell sums its
+                // particles in their sorted order; a's (cell iz) and b's (cell iz + 1) in separate phases
+                const int pz = __shfl_up_sync(0xffffffffu, iz, 1);
+                const uint32_t heads = __ballot_sync(0xffffffffu, ok && (lane == 0 || pz != iz));
+                const uint32_t upto = heads & ((2u << lane) - 1u);       // lane 31: every head
+                const int rank = ok ? lane - (31 - __clz(upto)) : 0;
+                const int rmax = __reduce_max_sync(0xffffffffu, (unsigned)rank);
+                const int iz1 = iz + 1 == n2 ? 0 : iz + 1;
+                for (int r = 0; r <= rmax; r++) {
+                    if (ok && rank == r) col[iz] += a;
+                    __syncwarp();
                 }
-                const int nz = __shfl_down_sync(0xffffffffu, iz, 1);
-                const bool tail = ok && (lane == 31 || nz != iz);
-                if (tail) col[iz] += a;
-                __syncwarp();
-                if (tail) col[iz + 1 == n2 ? 0 : iz + 1] += b;
-                __syncwarp();
+                for (int r = 0; r <= rmax; r++) {
+                    if (ok && rank == r) col[iz1] += b;
+                    __syncwarp();
+                }
             }
         }
         double* dst = mesh + c * (int64_t)n2;
