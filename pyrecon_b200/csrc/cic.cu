@@ -317,10 +317,8 @@ template <typename P, typename F> __device__ __forceinline__ bool in_box(P p, co
 // Index-space coordinates (mesh dtype F) of particle i, after the optional wrap; flags
 // out-of-box / non-finite.  Returns false when the particle is invalid.
 template <typename P, typename F>
-__device__ __forceinline__ bool particle_index(const P* __restrict__ pos, int64_t i, const BoxGeom& g, int wrap,
-                                               F q[3], int* bad) {
+__device__ __forceinline__ bool particle_index_of(const P (&p)[3], const BoxGeom& g, int wrap, F q[3], int* bad) {
     typedef typename promote<P, F>::type T;
-    P p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
     if (wrap) {
         T w[3];
 #pragma unroll
@@ -345,6 +343,13 @@ __device__ __forceinline__ bool particle_index(const P* __restrict__ pos, int64_
         for (int d = 0; d < 3; d++) q[d] = index_coord<P, F>(p[d], g, d);
     }
     return true;
+}
+
+template <typename P, typename F>
+__device__ __forceinline__ bool particle_index(const P* __restrict__ pos, int64_t i, const BoxGeom& g, int wrap,
+                                               F q[3], int* bad) {
+    const P p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    return particle_index_of<P, F>(p, g, wrap, q, bad);
 }
 
 // Base cell: C (int) truncation, then modulo n (src/mesh.c:35-37); kept in [0, n) for any input.
@@ -692,9 +697,10 @@ __global__ void __launch_bounds__(256) read_fd_kernel(const F* __restrict__ mesh
 // R = promoted type of (shifts, los); result cast back to P; positions - shifts in P, then
 // wrapped in T = promote(P, F) when `wrap`; the output type O is chosen by the caller.
 // PRC_READ_MINB: blocks per SM asked of the register allocator for the CIC shift read-out (its gathers
-// are latency-bound: ncu shows long-scoreboard stalls first at 50 % occupancy).  Measured: 5 blocks (48
-// registers, a few spilled) made it slower (1.90 against 1.77 ms per nmesh-512 reconstruction), so the
-// default leaves the allocator free; the finite-difference read-out (48 loads a particle) always is.
+// are latency-bound: ncu shows long-scoreboard stalls first).  Measured per nmesh-512 reconstruction,
+// with the next round's position loaded ahead: 1.73 ms free (100 registers, 2 blocks), 1.72 ms at 3
+// blocks (80), 1.84 ms at 4 (64), and 5 blocks (48, a few spilled) slower still, so the default leaves
+// the allocator free; the finite-difference read-out (48 loads a particle) always is.
 #ifndef PRC_READ_MINB
 #define PRC_READ_MINB 1
 #endif
@@ -711,20 +717,31 @@ __global__ void __launch_bounds__(256, (PHI ? 1 : PRC_READ_MINB)) read_shifts_ke
     const F twocell[3] = {tc0, tc1, tc2};
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t nround = (n + stride - 1) / stride;
-    for (int64_t r = 0; r < nround; r++) {
-        const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + r * stride;
+    // particles visited in `order` (cell-sorted, from the paint): neighbouring threads gather neighbouring
+    // cells; each particle's result only depends on its own position, read from the paint's cell-ordered
+    // copy when there is one (a stream, not a gather).  The next round's position (and output index) is
+    // loaded one round ahead, so a round waits on memory only for its mesh gathers.
+    const P* src = sorted_pos != nullptr ? sorted_pos : pos;
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t inext = 0;
+    P pnext[3] = {(P)0, (P)0, (P)0};
+    auto fetch = [&](int64_t kk) {
+        inext = order != nullptr ? (int64_t)order[kk] : kk;
+        const int64_t at = sorted_pos != nullptr ? kk : inext;
+        pnext[0] = src[3 * at];
+        pnext[1] = src[3 * at + 1];
+        pnext[2] = src[3 * at + 2];
+    };
+    if (k < n) fetch(k);
+    for (int64_t r = 0; r < nround; r++, k += stride) {
         int bad = 0;
+        const int64_t i = inext;
+        const P p[3] = {pnext[0], pnext[1], pnext[2]};
+        if (k + stride < n) fetch(k + stride);
         if (k < n) {
-            // particles visited in `order` (cell-sorted, from the paint): neighbouring threads gather
-            // neighbouring cells; each particle's result only depends on its own position, read from the
-            // paint's cell-ordered copy when there is one (a stream, not a gather)
-            const int64_t i = order != nullptr ? (int64_t)order[k] : k;
-            const P* src = sorted_pos != nullptr ? sorted_pos : pos;
-            const int64_t at = sorted_pos != nullptr ? k : i;
             F q[3] = {0, 0, 0};
             P s[3];
-            const P p[3] = {src[3 * at], src[3 * at + 1], src[3 * at + 2]};
-            const bool ok = particle_index<P, F>(src, at, g, wrap, q, &bad);
+            const bool ok = particle_index_of<P, F>(p, g, wrap, q, &bad);
             const Cic<F> c = cic_setup(q, g.n);
             if (PHI) {
                 F d[3] = {(F)NAN, (F)NAN, (F)NAN};
