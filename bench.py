@@ -470,7 +470,10 @@ def run_gpu_arm(args, w):
     if not args.no_e2e:
         pin = lambda t: None if t is None else t.cpu().pin_memory()
         hd, hwd, hr, hwr = pin(data), pin(wd), pin(randoms), pin(wr)
+        # positions cross twice: to the device for the paint, and again (in chunks, overlapped with the
+        # kernel and the copy back) for the read-out of the host catalogues
         h2d = sum(t.numel() * t.element_size() for t in [hd, hwd, hr, hwr] if t is not None)
+        h2d += (hd.numel() + hr.numel()) * hd.element_size()
         d2h = (hd.numel() + hr.numel()) * hd.element_size()
         e2e_step = lambda: reconstruct(w, device, hd, hwd, hr, hwr, check=False)
         e2e_step()

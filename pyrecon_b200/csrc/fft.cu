@@ -519,8 +519,10 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_x_fused(Specs<cplx_t<T>> in, 
 // ---------------------------------------------------------------------------------------------
 // z pass, inverse c2r, with real-space epilogues
 // ---------------------------------------------------------------------------------------------
+// EPI_ITER_POLY_R2C: EPI_ITER_POLY whose real row is not stored but transformed forward at once (the
+// next iteration's r2c z pass, same arithmetic) into the spectrum rows at `spec`.
 enum EpiType { EPI_STORE = 0, EPI_DENSITY = 1, EPI_DENSITY_NORANDOMS = 2, EPI_ITER_GLOBAL = 3, EPI_ITER_LOCAL = 4,
-               EPI_STORE4 = 5, EPI_ITER_POLY = 6 };
+               EPI_STORE4 = 5, EPI_ITER_POLY = 6, EPI_ITER_POLY_R2C = 7 };
 
 template <typename T> struct Epi {
     int type;
@@ -531,6 +533,8 @@ template <typename T> struct Epi {
     double bias, ran_min, size_randoms, ncells;
     double factor[6];      // RSD-removal factors (EPI_ITER_*)
     double offset[3], cell[3];   // node coordinates x_a = offset_a + cell_a * i (EPI_ITER_LOCAL)
+    void* spec;            // EPI_ITER_POLY_R2C: the z-transformed rows (complex T, spec_pitch values a row)
+    int spec_pitch;
 };
 
 // Epilogue of one cell (row, iz): vals[c * stride] is the inverse transform of input c there.
@@ -895,6 +899,7 @@ template <typename T> struct FastZC2R {
                 case EPI_ITER_LOCAL: return go<EPI_ITER_LOCAL>(si, nin, dims, pitch, e, bytes, st);
                 case EPI_STORE4: return go<EPI_STORE4>(si, nin, dims, pitch, e, bytes, st);
                 case EPI_ITER_POLY: return go<EPI_ITER_POLY>(si, nin, dims, pitch, e, bytes, st);
+                case EPI_ITER_POLY_R2C: return go<EPI_ITER_POLY_R2C>(si, nin, dims, pitch, e, bytes, st);
                 default: return go<EPI_STORE>(si, nin, dims, pitch, e, bytes, st);
             }
         }
@@ -1169,6 +1174,7 @@ template <typename T> struct FastZC2RTma {
                 case EPI_ITER_LOCAL: return go<EPI_ITER_LOCAL>(p, si, nin, e, bytes, st);
                 case EPI_STORE4: return go<EPI_STORE4>(p, si, nin, e, bytes, st);
                 case EPI_ITER_POLY: return go<EPI_ITER_POLY>(p, si, nin, e, bytes, st);
+                case EPI_ITER_POLY_R2C: return go<EPI_ITER_POLY_R2C>(p, si, nin, e, bytes, st);
                 default: return go<EPI_STORE>(p, si, nin, e, bytes, st);
             }
         }
@@ -1322,12 +1328,15 @@ template <typename T> struct FFTLaunch {
             double bytes = (double)nin * rows * nh * CS +
                            (double)rows * p.dims.n[2] * sizeof(T) *
                                (e.type == EPI_STORE ? nin : (e.type == EPI_STORE4 ? 4 : (e.delta ? 2 : 1)));
+            if (e.type == EPI_ITER_POLY_R2C)   // the spectrum rows written instead of the real rows
+                bytes += (double)rows * (nh * CS - (double)p.dims.n[2] * sizeof(T));
             if (tma_enabled()) {
                 const int r = dispatch_pow2<FastZC2RTma<T>::template K>(M, p, si, nin, e, bytes, st);
                 if (r != TMA_UNAVAILABLE) return r;
             }
             return dispatch_pow2<FastZC2R<T>::template K>(M, si, nin, p.dims, p.pitch, e, bytes, st);
         }
+        if (e.type == EPI_ITER_POLY_R2C) return PRC_ERR_ARG;   // register z kernels only
         const int n2 = p.dims.n[2], L = n2 % 2 ? n2 : nh;
         auto need = [&](int b) {
             return (size_t)(2 * L * row_pitch(b) + n2) * CS + (size_t)nin * b * n2 * sizeof(T);
@@ -1512,9 +1521,22 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
         e.offset[a] = sizeof(T) == 4 ? (double)(float)((float)bc - (float)bs / 2.f) : bc - bs / 2.;
         e.cell[a] = bs / (double)p.dims.n[a];
     }
+    // The Hessian iteration's inverse z pass can hand its rows straight to the next forward z transform
+    // (EPI_ITER_POLY_R2C), when both z passes are the register kernels; then S[0] already holds the
+    // z-transformed rows and only the y transform is left (knob fft_fuse_z, 0 = store and reload).
+    const bool fuse_z = p.dims.n[2] % 2 == 0 && fast_len(p.dims.n[2] / 2) && !getenv_generic() &&
+                        tune_get("fft_fuse_z", 0, 1) != 0;
+    bool z_done = false;   // S[0] holds the z transform of the next forward input
+    auto forward = [&](const void* in) -> int {
+        if (z_done) {
+            z_done = false;
+            return FFTLaunch<T>::template strided<-1>(p, 1, S, 1, st);
+        }
+        const void* ins[1] = {in};
+        return forward_zy<T, T>(p, ins, S, 1, st);
+    };
     for (int it = 0; it < niter; it++) {
-        const void* ins[1] = {it == 0 ? (const void*)delta : (const void*)dreal};
-        PRC_TRY((forward_zy<T, T>(p, ins, S, 1, st)));
+        PRC_TRY(forward(it == 0 ? (const void*)delta : (const void*)dreal));
         double base = beta;
         if (it == 0) base /= (1. + beta);
         if (los) {
@@ -1555,9 +1577,12 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
                 PRC_TRY(r);
                 PRC_TRY(dispatch_pow2<FastHessTma<T>::template K>(p.dims.n[1], p, S + 1, outs, h, st, false));
                 Epi<T> ep = e;
-                ep.type = EPI_ITER_POLY;
+                ep.type = fuse_z ? EPI_ITER_POLY_R2C : EPI_ITER_POLY;
+                ep.spec = S[0];
+                ep.spec_pitch = p.pitch;
                 cplx_t<T>* cba[3] = {S[6], S[5], S[4]};
                 PRC_TRY(FFTLaunch<T>::z_c2r(p, cba, 3, ep, st));
+                z_done = fuse_z;
                 continue;
             }
         }
@@ -1567,8 +1592,7 @@ static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsiz
         PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, S + 1, nout, st));
         PRC_TRY(FFTLaunch<T>::z_c2r(p, S + 1, nout, e, st));
     }
-    const void* ins[1] = {niter > 0 ? (const void*)dreal : (const void*)delta};
-    PRC_TRY((forward_zy<T, T>(p, ins, S, 1, st)));
+    PRC_TRY(forward(niter > 0 ? (const void*)dreal : (const void*)delta));
     op.type = KOP_PSI;
     op.nper = 3;
     PRC_TRY(FFTLaunch<T>::x_fused(p, S, 1, S + 1, op, st));

@@ -493,6 +493,69 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE
 // z pass, forward r2c: rows of n2 = 2M reals, M-point FFT of the packed pairs, then unpack.
 // CTA = (M / 8) x ROWS threads.
 // ---------------------------------------------------------------------------------------------
+// Forward real transform of one row held as packed pairs, v[i] = (x[2k], x[2k+1]) for k = t + i TL:
+// the M-point transform Z, then X[k] = (Z[k] + conj Z[M-k]) / 2 - i w^k (Z[k] - conj Z[M-k]) / 2 for
+// k < M and X[M] = Re Z[0] - Im Z[0], stored at dst when ok.  buf (the row's exchange buffer, addr) is
+// written from the start: the caller's earlier reads of it must be behind a barrier.  Ends with a barrier.
+template <typename T, int M, class Addr>
+__device__ __forceinline__ void row_r2c(cplx_t<T> (&v)[8], bool ok, int t, cplx_t<T>* buf, const Addr& addr,
+                                        const cplx_t<T>* tw, const cplx_t<T>* wk, cplx_t<T>* dst) {
+    typedef cplx_t<T> C;
+    constexpr int TL = M / 8;
+    fft_regs<C, M, -1>(v, t, buf, addr, tw);
+    // unpack needs Z[M - k]: publish Z, then combine
+#pragma unroll
+    for (int i = 0; i < 8; i++) buf[addr(t + i * TL)] = v[i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int k = t + i * TL;
+        const C zk = v[i];
+        const C zc = cconj(buf[addr(k == 0 ? 0 : M - k)]);
+        const C e = cscale(cadd(zk, zc), (T)0.5);
+        const C o = cmul_i(cscale(csub(zk, zc), (T)0.5), -1);
+        const C x = cadd(e, cmul(wk[k], o));
+        if (ok) dst[k] = x;
+    }
+    if (t == 0 && ok) {
+        const C z0 = v[0];
+        dst[M] = cmake<C>(z0.x - z0.y, (T)0);
+    }
+    __syncthreads();
+}
+
+// row_r2c with the transform's exchanges alternating between s0 and s1 (fft_regs_pp) and Z published in
+// the buffer the last exchange did not use, which every thread has finished reading by that exchange's
+// barrier: a barrier per exchange plus one.  On entry s0 must be free (not read by anyone after the
+// caller's last barrier) and s1 free once the first exchange's barrier is reached; on return the
+// partner reads of Z are not fenced: the caller puts a barrier before the next write to either buffer.
+template <typename T, int M, class Addr>
+__device__ __forceinline__ void row_r2c_pp(cplx_t<T> (&v)[8], bool ok, int t, cplx_t<T>* s0, cplx_t<T>* s1,
+                                           const Addr& addr, const cplx_t<T>* tw, const cplx_t<T>* wk,
+                                           cplx_t<T>* dst) {
+    typedef cplx_t<T> C;
+    constexpr int TL = M / 8, NX = Plan<M>::NPASS - 1;   // exchanges: s0, s1, s0, ...
+    fft_regs_pp<C, M, -1>(v, t, s0, s1, addr, tw);
+    C* zb = NX == 0 ? s0 : ((NX - 1) % 2 == 0 ? s1 : s0);
+#pragma unroll
+    for (int i = 0; i < 8; i++) zb[addr(t + i * TL)] = v[i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int k = t + i * TL;
+        const C zk = v[i];
+        const C zc = cconj(zb[addr(k == 0 ? 0 : M - k)]);
+        const C e = cscale(cadd(zk, zc), (T)0.5);
+        const C o = cmul_i(cscale(csub(zk, zc), (T)0.5), -1);
+        const C x = cadd(e, cmul(wk[k], o));
+        if (ok) dst[k] = x;
+    }
+    if (t == 0 && ok) {
+        const C z0 = v[0];
+        dst[M] = cmake<C>(z0.x - z0.y, (T)0);
+    }
+}
+
 template <typename T, typename TIN, int M, int ROWS>
 __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T>> out, int nbatch, int64_t rows, int pitch) {
     typedef cplx_t<T> C;
@@ -526,27 +589,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
                 v[i] = cmake<C>((T)x.x, (T)x.y);
             }
         }
-        fft_regs<C, M, -1>(v, t, buf, addr, tw);
-        // unpack needs Z[M - k]: publish Z, then combine
-#pragma unroll
-        for (int i = 0; i < 8; i++) buf[addr(t + i * TL)] = v[i];
-        __syncthreads();
-        C* dst = out.p[bi] + row * pitch;
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int k = t + i * TL;
-            const C zk = v[i];
-            const C zc = cconj(buf[addr(k == 0 ? 0 : M - k)]);
-            const C e = cscale(cadd(zk, zc), (T)0.5);
-            const C o = cmul_i(cscale(csub(zk, zc), (T)0.5), -1);
-            const C x = cadd(e, cmul(wk[k], o));
-            if (ok) dst[k] = x;
-        }
-        if (t == 0 && ok) {
-            const C z0 = v[0];
-            dst[M] = cmake<C>(z0.x - z0.y, (T)0);
-        }
-        __syncthreads();
+        row_r2c<T, M>(v, ok, t, buf, addr, tw, wk, out.p[bi] + (ok ? row : 0) * pitch);
     }
 }
 
@@ -566,7 +609,9 @@ __device__ __forceinline__ double select6(const double (&f)[6], int c) {
 template <int ET> struct EpiInputs {
     static constexpr int NMAX =
         ET == EPI_ITER_LOCAL ? 6
-                             : (ET == EPI_DENSITY ? 2 : ((ET == EPI_STORE || ET == EPI_STORE4 || ET == EPI_ITER_POLY) ? 3 : 1));
+                             : (ET == EPI_DENSITY ? 2
+                                                  : ((ET == EPI_STORE || ET == EPI_STORE4 || ET == EPI_ITER_POLY ||
+                                                      ET == EPI_ITER_POLY_R2C) ? 3 : 1));
 };
 
 // Inverse z transform of one row: returns v[i] = (x[2k], x[2k+1]), k = t + i TL, unscaled.
@@ -597,6 +642,7 @@ __device__ __forceinline__ void row_c2r(const cplx_t<T>* __restrict__ src, bool 
 // Input rows read straight from global memory into the row buffer (register kernels).
 template <typename T, int M> struct GlobalRows {
     typedef cplx_t<T> C;
+    static constexpr bool PP = false;   // one exchange buffer (row_c2r uses fft_regs)
     const Specs<C>& in;
     int pitch;
     __device__ __forceinline__ void row(int c, int64_t row, bool ok, int t, C* buf, const RowAddr& addr, const C* tw,
@@ -683,9 +729,11 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
                     out0[t + i * TL] = cmake<C>((T)o0, (T)o1);
                 }
             }
-        } else if constexpr (ET == EPI_ITER_POLY) {
+        } else if constexpr (ET == EPI_ITER_POLY || ET == EPI_ITER_POLY_R2C) {
             // RSD removal from the quadratic in x2 formed by the Hessian y pass: inputs C, B, A, so
             // sum_ij f_ij x_i x_j d_ij = (C x2 + B) x2 + A, evaluated by Horner as the rows arrive.
+            // EPI_ITER_POLY_R2C: the new real row goes straight into the next iteration's forward z
+            // transform (row_r2c, the arithmetic of the r2c pass) instead of to memory.
             const T x0 = (T)(e.offset[0] + e.cell[0] * ix), x1 = (T)(e.offset[1] + e.cell[1] * iy);
             const T oz = (T)e.offset[2], cz = (T)e.cell[2];
             // the original density contrast is fetched first, so its latency hides behind the transforms
@@ -708,21 +756,37 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
                     }
                 }
             }
-            if (ok) {
+            C z[8];
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const C d0 = dv[i];
-                    T o[2];
+            for (int i = 0; i < 8; i++) {
+                const C d0 = dv[i];
+                T o[2];
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const T xz = oz + cz * (T)(2 * (t + i * TL) + h);
-                        const T x2 = (x0 * x0 + x1 * x1) + xz * xz;
-                        // FP32: fast reciprocal (2 ulp, far inside the FP32 mode's tolerance); FP64: exact
-                        const T ix2 = sizeof(T) == 4 ? (T)__fdividef(1.f, (float)x2) : (T)1 / x2;
-                        o[h] = (h ? d0.y : d0.x) - r[i][h] * ix2;
-                    }
-                    out0[t + i * TL] = cmake<C>(o[0], o[1]);
+                for (int h = 0; h < 2; h++) {
+                    const T xz = oz + cz * (T)(2 * (t + i * TL) + h);
+                    const T x2 = (x0 * x0 + x1 * x1) + xz * xz;
+                    // FP32: fast reciprocal (2 ulp, far inside the FP32 mode's tolerance); FP64: exact
+                    const T ix2 = sizeof(T) == 4 ? (T)__fdividef(1.f, (float)x2) : (T)1 / x2;
+                    o[h] = (h ? d0.y : d0.x) - r[i][h] * ix2;
                 }
+                z[i] = ok ? cmake<C>(o[0], o[1]) : cmake<C>(0, 0);
+            }
+            if constexpr (ET == EPI_ITER_POLY_R2C) {
+                C* dst = (C*)e.spec + (ok ? row : 0) * e.spec_pitch;
+                if constexpr (Src::PP) {
+                    // the inverse transforms exchanged through buf, buf2, buf, ...: the first buffer
+                    // the forward one writes must not be the one their last exchange read
+                    constexpr int NX = Plan<M>::NPASS - 1;
+                    if constexpr (NX == 0 || (NX - 1) % 2 == 0) __syncthreads();
+                    row_r2c_pp<T, M>(z, ok, t, buf, src.buf2, addr, tw, wk, dst);
+                    __syncthreads();
+                } else {
+                    __syncthreads();   // every thread is past its reads of the exchange buffer
+                    row_r2c<T, M>(z, ok, t, buf, addr, tw, wk, dst);
+                }
+            } else if (ok) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) out0[t + i * TL] = z[i];
             }
         } else {
             // RSD removal: delta_real = delta - sum_c factor_c w_c(x) IFFT_c, accumulated in registers;

@@ -329,6 +329,7 @@ template <typename T, int M, int ROWS, int S> struct TmaRows {
     static constexpr int Q = (int)(32 / sizeof(C));
     static constexpr int PS = (M + 1 + Q - 1) / Q * Q;
     static constexpr int STAGE = ROWS * PS;
+    static constexpr bool PP = PRC_C2R_PP;   // the row transforms alternate between buf1 and buf2
     C* stages;
     C* buf1 = nullptr;       // PRC_C2R_PP: the row buffer the caller passes, and the second one
     C* buf2 = nullptr;       // (same layout, so a row's offset in buf1 is its offset in buf2)

@@ -13,6 +13,8 @@ host-to-device copies asynchronous) or CUDA tensors; results come back in the sa
 container.  ``dtype='f4'`` runs the FP32 pipeline with FP64 cloud-in-cell sums, FP64
 normalisation and (multigrid) FP64 defect correction; ``dtype='f8'`` runs everything in FP64.
 """
+import weakref
+
 import numpy as np
 
 from . import _lib
@@ -160,8 +162,9 @@ class BaseReconstruction(BaseClass):
     # tensor visits the particles in that order, so the gathers of neighbouring threads hit
     # neighbouring cells.  Any permutation gives the same results; the key (address, length) only
     # picks which one.  The paint also keeps the positions in that order, which the read-out streams
-    # instead of gathering them through the permutation, as long as the tensor has not been modified
-    # in place since (its version counter is unchanged).
+    # instead of gathering them through the permutation, only for the very tensor object that was
+    # painted (a weak reference: a new tensor that the allocator places at the same address is not
+    # it) and as long as it has not been modified in place since (its version counter is unchanged).
 
     @staticmethod
     def _order_key(positions):
@@ -184,7 +187,7 @@ class BaseReconstruction(BaseClass):
         if order is not None:
             if not hasattr(self, '_orders'):
                 self._orders = {}
-            self._orders[self._order_key(positions)] = (order, spos, positions._version)
+            self._orders[self._order_key(positions)] = (order, spos, positions._version, weakref.ref(positions))
 
     def _order_for(self, positions):
         key = self._order_key(positions)
@@ -194,7 +197,7 @@ class BaseReconstruction(BaseClass):
     def _sorted_for(self, positions):
         key = self._order_key(positions)
         kept = None if key is None else getattr(self, '_orders', {}).get(key)
-        if kept is None or kept[1] is None or positions._version != kept[2]:
+        if kept is None or kept[1] is None or kept[3]() is not positions or positions._version != kept[2]:
             return None
         return kept[1]
 

@@ -227,3 +227,35 @@ def test_library_variant_same_bits(variant, tmp_path):
         a, b = np.load(path), np.load(ref)
         for k in b.files:
             assert np.array_equal(a[k], b[k]), (kind, k)
+
+
+def _iterative_psi(nmesh, dtype, fuse):
+    """psi of prc_iterative_fft (local line of sight, 3 iterations) with the inverse z pass handing its
+    rows to the next forward z transform (fuse) or storing and reloading them."""
+    import torch
+    from pyrecon_b200 import _lib as L
+    item = np.dtype(dtype).itemsize
+    x = np.random.default_rng(11).standard_normal(nmesh, dtype='f8').astype(dtype)
+    delta = torch.from_numpy(x).cuda()
+    psi4 = torch.empty(tuple(nmesh) + (4,), dtype=delta.dtype, device='cuda')
+    nm = L.i3(nmesh)
+    ws = torch.empty(L.load().prc_iterative_fft_workspace_bytes(nm, item, 1), dtype=torch.uint8, device='cuda')
+    psis = [L.c_void_p(psi4.data_ptr() + a * item) for a in range(3)]
+    L.tune_set('fft_fuse_z', 0, int(fuse))
+    try:
+        L.call('prc_iterative_fft_' + L.suffix(dtype), L.ptr(delta), nm, L.d3([1000., 1200., 900.]),
+               L.d3([0., 100., 2000.]), 0.4, None, 3, *psis, 4, L.ptr(ws), ws.numel(), L.stream_of(torch.device('cuda')))
+        torch.cuda.synchronize()
+    finally:
+        L.tune_set('fft_fuse_z', 0, -1)
+    assert L.load().prc_device_fault_flags(1) == 0
+    return psi4.cpu().numpy()
+
+
+@pytest.mark.parametrize('nmesh', [(256, 256, 256), (64, 32, 128), (32, 64, 16)])
+@pytest.mark.parametrize('dtype', ['f4', 'f8'])
+def test_fused_z_passes_same_bits(nmesh, dtype):
+    """The local-line-of-sight iteration's inverse z pass transforms its new density rows forward at once
+    (the next iteration's r2c z pass, the same arithmetic), instead of storing them and reading them back:
+    the displacements are the same bits."""
+    assert np.array_equal(_iterative_psi(nmesh, dtype, True), _iterative_psi(nmesh, dtype, False))

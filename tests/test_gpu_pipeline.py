@@ -131,6 +131,16 @@ def test_readout_in_paint_order_equals_plain_readout(name):
     data[:10] = data[10:20].clone()
     assert rec._sorted_for(data) is None and rec._order_for(data) is not None
     assert torch.equal(rec.read_shifted_positions(data), rec.read_shifted_positions(data.clone()))
+    # the painted tensor freed and another catalogue of the same length created in its place (same
+    # address from the caching allocator, version counter 0 again): the kept positions are not its own
+    shape, ptr = tuple(data.shape), data.data_ptr()
+    other = np.ascontiguousarray(np.flip(g['data'], axis=0))
+    del data, ordered, plain, cat
+    torch.cuda.synchronize()
+    fresh = torch.from_numpy(other).cuda()
+    if fresh.data_ptr() == ptr and tuple(fresh.shape) == shape:
+        assert rec._sorted_for(fresh) is None
+    assert torch.equal(rec.read_shifted_positions(fresh), rec.read_shifted_positions(fresh.clone()))
 
 
 def test_sky_conversions_on_device():
