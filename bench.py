@@ -83,12 +83,14 @@ MULTI_WORKLOADS = {
                           nmesh=[128, 192, 256], ndata=(300_000, 2_000_000), randoms_factor=0, boxsize=1000.,
                           boxcenter=500., los='z', wrap=True, dtype='f4', slots=2, max_batch=8),
     # BASELINE config: 500 requests with Poisson arrivals at 20 req/s, the three algorithms, nmesh in
-    # {128, 256, 384, 512}, 0.5M-8M data with 4x randoms, 150 GB admission budget
+    # {128, 256, 384, 512}, 0.5M-8M data with 4x randoms, 150 GB admission budget.  Two slots: measured
+    # p50 / p99 19.5-19.9 / 162-171 ms with 2, 21.3 / 174 with 1, 20.1 / 201 with 4 (the device is ~43 %
+    # busy at this rate; more concurrent requests stretch the long ones)
     'serving': dict(kind='serving', nrequests=500, rate=20., algorithms=['MultiGridReconstruction',
                                                                         'IterativeFFTReconstruction',
                                                                         'PlaneParallelFFTReconstruction'],
                     nmesh=[128, 256, 384, 512], ndata=(500_000, 8_000_000), randoms_factor=4, boxsize=2000.,
-                    boxcenter=2000., los=None, wrap=False, dtype='f4', slots=4, max_batch=8, hbm_budget=150e9),
+                    boxcenter=2000., los=None, wrap=False, dtype='f4', slots=2, max_batch=8, hbm_budget=150e9),
 }
 
 for _name, _w in MULTI_WORKLOADS.items():
