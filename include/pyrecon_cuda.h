@@ -47,6 +47,7 @@ typedef int prc_status_t;
 
 #define PRC_FLAG_OUT_OF_BOX 1  /* a position outside [boxcenter - boxsize/2, boxcenter + boxsize/2] */
 #define PRC_FLAG_NONFINITE 2   /* a NaN/inf position or weight */
+#define PRC_FLAG_DEVICE_WAIT 4 /* a bounded wait between the CTAs of a kernel gave up (the paint's sort) */
 
 #define PRC_FIELD_DISP 0       /* Zeldovich displacement only */
 #define PRC_FIELD_RSD 1        /* RSD displacement f (s.l) l only */

@@ -20,6 +20,7 @@ DP = ctypes.POINTER(ctypes.c_double)   # optional 3-vector (NULL = local line of
 PRC_OK = 0
 PRC_FLAG_OUT_OF_BOX = 1
 PRC_FLAG_NONFINITE = 2
+PRC_FLAG_DEVICE_WAIT = 4
 PRC_ERR_ARG = 1
 PRC_ERR_TIMEOUT = 5
 PRC_FAULT_WAIT_TIMEOUT = 1

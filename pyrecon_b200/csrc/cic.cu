@@ -243,22 +243,262 @@ __global__ void __launch_bounds__(THREADS, 3) downsweep(const uint32_t* __restri
 
 inline size_t downsweep_smem(int radix) { return (size_t)(3 * TILE + WARPS * radix + 2 * radix) * sizeof(uint32_t); }
 
+// ---- one sweep per digit (decoupled look-back) ----
+// The digit histograms of every pass come from one read of the keys; then each pass is one kernel whose
+// CTAs take tiles in the order they start (a tile counter), rank a tile as the downsweep does, publish
+// the tile's count of every digit, and find the tile's output offset for a digit by looking back over
+// the tiles before it: a predecessor that has published its inclusive prefix ends the walk, one that has
+// only published its count adds it and the walk goes on.  Status words: 2 flag bits (count / prefix)
+// over a 30-bit value, so a sort of up to 2^30 - 1 items; larger ones take the reduce-then-scan passes.
+// A predecessor always runs (it took its tile earlier) and publishes its counts before it looks back
+// itself, so every wait ends; it is bounded all the same (WAIT_LIMIT_NS): one that runs out raises
+// PRC_FLAG_DEVICE_WAIT in the caller's flags, which the kernels downstream honour.
+constexpr uint32_t LB_VALUE = (1u << 30) - 1;
+constexpr uint32_t LB_COUNT = 1u << 30, LB_PREFIX = 2u << 30;
+constexpr int MAXPASS = 4;
+constexpr uint64_t WAIT_LIMIT_NS = 200ull * 1000 * 1000;
+
+// The look-back exchanges only the status words themselves (a count is the whole message, in the same
+// word as its flag), so relaxed loads and stores at GPU scope suffice: no fence, and several loads can
+// be in flight at once.
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+constexpr int LB_WINDOW = 8;    // predecessors read at once by a look-back step (per digit)
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Digit counts of every pass (dbits-bit digits, npass of them) over all keys, added into hist[p * radix + d].
+__global__ void __launch_bounds__(THREADS) digit_histograms(const uint32_t* __restrict__ keys, int64_t n, int dbits,
+                                                            int npass, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t cnt[MAXPASS * MAXRADIX];
+    const int radix = 1 << dbits;
+    const uint32_t mask = (uint32_t)radix - 1;
+    for (int i = threadIdx.x; i < npass * radix; i += THREADS) cnt[i] = 0u;
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * THREADS) {
+        const uint32_t k = keys[i];
+        for (int p = 0; p < npass; p++) atomicAdd(&cnt[p * radix + ((k >> (p * dbits)) & mask)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < npass * radix; i += THREADS)
+        if (cnt[i]) atomicAdd(&hist[i], cnt[i]);
+}
+
+// One pass of the sort: the ranking and the shared-memory reorder of downsweep, the tile's offset in each
+// digit's range from the look-back.  hist: this pass's digit counts; lookback (ntiles * radix) and
+// *tile_counter zeroed before the launch.
+__global__ void __launch_bounds__(THREADS, 3) onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                    uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n,
+                                                    int shift, int radix, int ntiles, const uint32_t* __restrict__ hist,
+                                                    uint32_t* lookback, uint32_t* tile_counter, int32_t* flags) {
+    extern __shared__ uint32_t smem[];
+    uint32_t* s_key = smem;                       // TILE
+    uint32_t* s_val = s_key + TILE;               // TILE
+    uint32_t* s_rank = s_val + TILE;              // TILE: rank in the warp's digit group, then local index
+    uint32_t* s_cnt = s_rank + TILE;              // WARPS * radix
+    uint32_t* s_loc = s_cnt + WARPS * radix;      // radix: first local index of each digit
+    uint32_t* s_glob = s_loc + radix;             // radix: the tile's first output index of each digit
+    uint32_t* s_base = s_glob + radix;            // radix: first output index of each digit (all tiles)
+    __shared__ uint32_t s_warp[32];
+    __shared__ int s_tile;
+    const uint32_t mask = (uint32_t)radix - 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    constexpr int SLICE = TILE / WARPS;
+    {
+        const uint32_t g0 = 2 * threadIdx.x < radix ? hist[2 * threadIdx.x] : 0u;
+        const uint32_t g1 = 2 * threadIdx.x + 1 < radix ? hist[2 * threadIdx.x + 1] : 0u;
+        const uint32_t ex = block_exclusive_scan(g0 + g1, s_warp, nullptr);
+        if (2 * threadIdx.x < radix) s_base[2 * threadIdx.x] = ex;
+        if (2 * threadIdx.x + 1 < radix) s_base[2 * threadIdx.x + 1] = ex + g0;
+    }
+    bool gave_up = false;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (int)atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile >= ntiles) break;
+        int64_t base = (int64_t)tile * TILE;
+        int valid = (int)min((int64_t)TILE, n - base);
+        for (int k = threadIdx.x; k < TILE; k += THREADS) {
+            if (k < valid) {
+                s_key[k] = kin[base + k];
+                s_val[k] = vin[base + k];
+            }
+        }
+        for (int k = threadIdx.x; k < WARPS * radix; k += THREADS) s_cnt[k] = 0u;
+        for (int d = threadIdx.x; d < radix; d += THREADS) s_glob[d] = 0u;
+        __syncthreads();
+        // the tile's digit counts (in s_glob until the look-back), published before the ranking so the tiles
+        // after this one can look back past it early
+        for (int k = threadIdx.x; k < valid; k += THREADS) atomicAdd(&s_glob[(s_key[k] >> shift) & mask], 1u);
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int d = 2 * threadIdx.x + j;
+            if (d < radix) st_relaxed(lookback + (int64_t)tile * radix + d, (tile == 0 ? LB_PREFIX : LB_COUNT) | s_glob[d]);
+        }
+        uint32_t* cnt = s_cnt + warp * radix;
+        for (int c = 0; c < SLICE; c += 32) {
+            int k = warp * SLICE + c + lane;
+            bool ok = k < valid;
+            uint32_t d = ok ? (s_key[k] >> shift) & mask : 0u;
+            const uint32_t okm = __ballot_sync(0xffffffffu, ok);
+            uint32_t peers = ok ? okm : ~okm;
+#pragma unroll
+            for (int b = 0; b < MAXBITS; b++) {
+                const bool bit = (d >> b) & 1u;
+                const uint32_t v = __ballot_sync(0xffffffffu, bit);
+                peers &= bit ? v : ~v;
+            }
+            uint32_t before = ok ? cnt[d] : 0u;
+            __syncwarp();
+            if (ok) {
+                s_rank[k] = before + __popc(peers & lt);
+                if ((peers & lt) == 0u) cnt[d] = before + __popc(peers);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        uint32_t tot[2] = {0u, 0u};
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int d = 2 * threadIdx.x + j;
+            if (d < radix) {
+                uint32_t run = 0u;
+                for (int w = 0; w < WARPS; w++) {
+                    uint32_t c = s_cnt[w * radix + d];
+                    s_cnt[w * radix + d] = run;
+                    run += c;
+                }
+                tot[j] = run;
+            }
+        }
+        {
+            // each digit's offset in the output: walk back over the predecessors LB_WINDOW at a time (both
+            // digits' words read together), adding counts up to the first inclusive prefix; a word not yet
+            // published stops the walk there and it is read again (bounded)
+            int t[2] = {tile - 1, tile - 1};
+            uint32_t excl[2] = {0u, 0u};
+            bool done[2] = {tile == 0 || 2 * (int)threadIdx.x >= radix, tile == 0 || 2 * (int)threadIdx.x + 1 >= radix};
+            uint64_t t0 = 0;
+            while (!(done[0] && done[1])) {
+                uint32_t w[2][LB_WINDOW];
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int i = 0; i < LB_WINDOW; i++)
+                        w[j][i] = !done[j] && t[j] - i >= 0
+                                      ? ld_relaxed(lookback + (int64_t)(t[j] - i) * radix + 2 * threadIdx.x + j)
+                                      : LB_PREFIX;
+                bool stalled = false;
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    if (done[j]) continue;
+                    int used = 0;
+                    bool fin = false;
+#pragma unroll
+                    for (int i = 0; i < LB_WINDOW; i++) {
+                        if (fin || used < i) continue;                 // stopped earlier in the window
+                        if ((w[j][i] & ~LB_VALUE) == 0u) continue;     // not published: the walk waits here
+                        excl[j] += w[j][i] & LB_VALUE;
+                        used = i + 1;
+                        fin = (w[j][i] & LB_PREFIX) != 0u;
+                    }
+                    t[j] -= used;
+                    done[j] = fin;
+                    if (!fin && used < LB_WINDOW) stalled = true;
+                }
+                if (stalled) {
+                    const uint64_t now = global_ns();
+                    if (t0 == 0) t0 = now;
+                    else if (now - t0 > WAIT_LIMIT_NS) {
+                        gave_up = true;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const int d = 2 * threadIdx.x + j;
+                if (d < radix) {
+                    if (tile > 0) st_relaxed(lookback + (int64_t)tile * radix + d, LB_PREFIX | (excl[j] + tot[j]));
+                    s_glob[d] = s_base[d] + excl[j];
+                }
+            }
+        }
+        const uint32_t ex = block_exclusive_scan(tot[0] + tot[1], s_warp, nullptr);
+        if (2 * threadIdx.x < radix) s_loc[2 * threadIdx.x] = ex;
+        if (2 * threadIdx.x + 1 < radix) s_loc[2 * threadIdx.x + 1] = ex + tot[0];
+        __syncthreads();
+        uint32_t rk[ITEMS], rv[ITEMS], ri[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const int k = j * THREADS + threadIdx.x;
+            if (k < valid) {
+                const uint32_t key = s_key[k];
+                const uint32_t d = (key >> shift) & mask;
+                rk[j] = key;
+                rv[j] = s_val[k];
+                ri[j] = s_loc[d] + s_cnt[(k / SLICE) * radix + d] + s_rank[k];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const int k = j * THREADS + threadIdx.x;
+            if (k < valid) {
+                s_key[ri[j]] = rk[j];
+                s_val[ri[j]] = rv[j];
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < valid; k += THREADS) {
+            const uint32_t key = s_key[k];
+            const uint32_t d = (key >> shift) & mask;
+            const uint32_t pos = s_glob[d] + ((uint32_t)k - s_loc[d]);
+            kout[pos] = key;
+            vout[pos] = s_val[k];
+        }
+        __syncthreads();
+    }
+    if (gave_up) atomicOr(flags, PRC_FLAG_DEVICE_WAIT);
+}
+
+inline size_t onesweep_smem(int radix) { return downsweep_smem(radix) + (size_t)radix * sizeof(uint32_t); }
+
 inline int num_tiles(int64_t n) { return (int)((n + TILE - 1) / TILE); }
 
 inline int64_t scan_count(int64_t n, int radix) { return (int64_t)num_tiles(n) * radix; }
 
 inline int scan_blocks(int64_t count) { return (int)((count + SCAN_TILE - 1) / SCAN_TILE); }
 
-// Bytes of scratch for sorting n items with the largest digit (histogram + scan tile sums).
+// Bytes of scratch for sorting n items with the largest digit: the reduce-then-scan passes' tile
+// histograms and scan tile sums, or the one-sweep passes' digit counts, tile counters and look-back
+// words (the larger of the two).
 inline size_t scratch_bytes(int64_t n) {
     int64_t c = scan_count(n, MAXRADIX);
-    return (size_t)(c + scan_blocks(c) + 64) * sizeof(uint32_t);
+    const int64_t rts = c + scan_blocks(c) + 64;
+    const int64_t one = (int64_t)MAXPASS * MAXRADIX + 64 + c;
+    return (size_t)std::max(rts, one) * sizeof(uint32_t);
 }
 
 // Sorts (k0, v0) by the low `bits` bits of the key.  Ping-pongs with (k1, v1); returns through
-// *kres / *vres which pair holds the result.
+// *kres / *vres which pair holds the result.  One kernel per digit (onesweep) up to 2^30 - 1 items
+// (run-time knob sort_onesweep = 0: the reduce-then-scan passes, the same result), else per digit a
+// histogram pass, a scan and a scatter pass.  flags: the caller's status word (PRC_FLAG_DEVICE_WAIT).
 int sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, int64_t n, int bits, uint32_t* scratch,
-               uint32_t** kres, uint32_t** vres, cudaStream_t st) {
+               uint32_t** kres, uint32_t** vres, int32_t* flags, cudaStream_t st) {
     *kres = k0;
     *vres = v0;
     if (n <= 1 || bits <= 0) return PRC_OK;
@@ -267,16 +507,44 @@ int sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, int64_t n
     int radix = 1 << dbits;
     int ntiles = num_tiles(n);
     int64_t count = (int64_t)ntiles * radix;
+    int sms = device_sm_count();
+    uint32_t *ka = k0, *va = v0, *kb = k1, *vb = v1;
+    if (n <= (int64_t)LB_VALUE && npass <= MAXPASS && tune_get("sort_onesweep", 0, 1) != 0) {
+        static bool attr_set1 = false;
+        if (!attr_set1) {
+            cudaFuncSetAttribute(onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)onesweep_smem(MAXRADIX));
+            attr_set1 = true;
+        }
+        uint32_t* hist = scratch;                                   // MAXPASS * MAXRADIX
+        uint32_t* counters = scratch + MAXPASS * MAXRADIX;          // MAXPASS (64 words)
+        uint32_t* lookback = counters + 64;                         // ntiles * radix
+        if (cudaMemsetAsync(scratch, 0, (MAXPASS * MAXRADIX + 64) * sizeof(uint32_t), st) != cudaSuccess)
+            return PRC_ERR_CUDA;
+        const int hgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + THREADS - 1) / THREADS, (int64_t)sms * 4));
+        PRC_LAUNCH_B("sort_histograms", st, 4.0 * n, digit_histograms<<<hgrid, THREADS, 0, st>>>(ka, n, dbits, npass, hist));
+        const int grid = min(ntiles, sms * 3);
+        for (int p = 0; p < npass; p++) {
+            if (cudaMemsetAsync(lookback, 0, (size_t)count * sizeof(uint32_t), st) != cudaSuccess) return PRC_ERR_CUDA;
+            PRC_LAUNCH_B("sort_onesweep", st, 16.0 * n + 4.0 * radix,
+                         onesweep<<<grid, THREADS, onesweep_smem(radix), st>>>(ka, va, kb, vb, n, p * dbits, radix, ntiles,
+                                                                              hist + p * radix, lookback, counters + p, flags));
+            PRC_CHECK_LAUNCH();
+            uint32_t* t;
+            t = ka; ka = kb; kb = t;
+            t = va; va = vb; vb = t;
+        }
+        *kres = ka;
+        *vres = va;
+        return PRC_OK;
+    }
     uint32_t* hist = scratch;
     uint32_t* tsums = scratch + count;
-    int sms = device_sm_count();
     int grid = min(ntiles, sms * 8);
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(downsweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)downsweep_smem(MAXRADIX));
         attr_set = true;
     }
-    uint32_t *ka = k0, *va = v0, *kb = k1, *vb = v1;
     for (int p = 0; p < npass; p++) {
         int shift = p * dbits;
         PRC_LAUNCH_B("sort_upsweep", st, 4.0 * n + 4.0 * count, upsweep<<<grid, THREADS, 0, st>>>(ka, n, shift, radix, ntiles, hist));
@@ -1058,7 +1326,7 @@ int paint_sort(const P* pos, const W* w, int64_t n, const BoxGeom& g, int wrap, 
     PRC_LAUNCH_B("paint_keys", st, (double)n * (3 * sizeof(P) + (w ? sizeof(W) : 0) + 8), paint_keys<P, F, W><<<particle_grid(n), 256, 0, st>>>(pos, w, n, g, wrap, ws.k0, ws.v0, flags));
     PRC_CHECK_LAUNCH();
     int32_t nm[3] = {g.n[0], g.n[1], g.n[2]};
-    return rsort::sort_pairs(ws.k0, ws.v0, ws.k1, ws.v1, n, key_bits(nm), ws.scratch, keys, order, st);
+    return rsort::sort_pairs(ws.k0, ws.v0, ws.k1, ws.v1, n, key_bits(nm), ws.scratch, keys, order, flags, st);
 }
 
 template <typename P, typename F, typename W>

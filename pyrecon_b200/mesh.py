@@ -278,6 +278,8 @@ class _Flags(object):
             raise MeshError('{} not in box range {} - {}'.format(what, low, high))
         if v & _lib.PRC_FLAG_NONFINITE:
             raise MeshError('Some positions or weights are NaN/inf')
+        if v & _lib.PRC_FLAG_DEVICE_WAIT:
+            raise MeshError('a bounded wait on the device gave up (sort look-back); the mesh was not painted')
 
 
 class BaseMesh(BaseClass):

@@ -70,6 +70,46 @@ def test_cell_order_bit_exact(nmesh, npos, pos_dtype, mesh_dtype, wrap):
     np.testing.assert_array_equal(o.cpu().numpy().view(np.uint32).astype('i8'), order)
 
 
+def _cell_order(pos, geom, wrap=False):
+    L = lib()
+    t = torch()
+    npos = len(pos)
+    k = t.empty(npos, dtype=t.int32, device='cuda')
+    o = t.empty(npos, dtype=t.int32, device='cuda')
+    fl = flags()
+    nm, bs, bc = L.i3(geom.nmesh), L.d3(geom.boxsize), L.d3(geom.boxcenter)
+    w = ws(L.load().prc_assign_cic_workspace_bytes(nm, npos, geom.dtype.itemsize))
+    dpos = dev(pos)
+    L.call('prc_cic_cell_order', L.ptr(k), L.ptr(o), nm, bs, bc, geom.dtype.itemsize, L.ptr(dpos),
+           pos.dtype.itemsize, npos, int(wrap), L.ptr(fl), L.ptr(w), w.numel(), stream())
+    assert int(fl.item()) == 0
+    return k.cpu().numpy(), o.cpu().numpy()
+
+
+@pytest.mark.parametrize('nmesh,npos', [
+    ((8, 8, 8), 200000),           # few digits: long runs, every tile waits on the same digits
+    ((512, 512, 512), 20_000_000), # the bench's randoms: 4883 tiles, three passes
+    ((64, 48, 40), 4096),          # exactly one tile
+    ((16, 12, 20), 4097),          # one item in the second tile
+    ((100, 90, 80), 1),
+])
+def test_sort_one_sweep_equals_reduce_then_scan(nmesh, npos):
+    """The paint's sort with one kernel per digit (tiles find their offsets by looking back over the tiles
+    before them) gives the keys and the order of the reduce-then-scan passes (histogram, scan, scatter)."""
+    L = lib()
+    boxsize, boxcenter = np.array([1000., 900., 800.]), np.array([100., -200., 3000.])
+    pos = catalog(npos, boxsize, boxcenter, seed=3, dtype='f4')
+    geom = pipeline.Geometry(nmesh, boxsize, boxcenter, dtype='f4')
+    one = _cell_order(pos, geom)
+    L.tune_set('sort_onesweep', 0, 0)
+    try:
+        rts = _cell_order(pos, geom)
+    finally:
+        L.tune_set('sort_onesweep', 0, -1)
+    np.testing.assert_array_equal(one[0], rts[0])
+    np.testing.assert_array_equal(one[1], rts[1])
+
+
 def gpu_paint(pos, weights, geom, wrap=False, accumulate_into=None):
     L = lib()
     t = torch()
