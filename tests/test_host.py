@@ -210,3 +210,20 @@ def test_serving_admission_counts_resident_slot_memory():
     assert ReconstructionServer._pick_slot(srv, 40.) == (1, 0.)
     srv._resident = [60., 10., 30.]
     assert ReconstructionServer._pick_slot(srv, 20.) == (2, 10.)      # slot 2 holds 30: nothing added
+
+
+def test_flag_words_map_to_mesh_errors():
+    """Every PRC_FLAG_* bit the kernels can raise (box, NaN/inf, a bounded device wait that gave up) turns
+    into MeshError on the host; the header and the binding agree on the values."""
+    from pyrecon_b200 import _lib, MeshError
+    from pyrecon_b200.mesh import _Flags
+    text = open(os.path.join(ROOT, 'include', 'pyrecon_cuda.h')).read()
+    for name in ['PRC_FLAG_OUT_OF_BOX', 'PRC_FLAG_NONFINITE', 'PRC_FLAG_DEVICE_WAIT']:
+        value = int(re.search(r'#define {}\s+(\d+)'.format(name), text).group(1))
+        assert getattr(_lib, name) == value
+        fl = _Flags('cpu')
+        fl.t[0] = value
+        with pytest.raises(MeshError):
+            fl.raise_if_set(0., 1.)
+    fl = _Flags('cpu')
+    fl.raise_if_set(0., 1.)
