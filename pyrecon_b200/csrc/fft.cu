@@ -720,9 +720,9 @@ struct Plan3 {
     Radices rz, ry, rx;   // rz: the n2/2-point packed transform (even n2) or the n2-point one (odd n2)
 };
 
-// Any axis length in [2, MAX_FFT_N]: powers of two up to MAX_FAST_N run the register-resident kernels,
-// every other length (radices 8, 4, 2, 3, 5, 7 and any larger prime; an odd last axis unpacked) the
-// shared-memory kernels.
+// Any axis length in [2, MAX_FFT_N]: powers of two up to MAX_FAST_N and 96, 192, 384 run the
+// register-resident kernels (fast_len), every other length (radices 8, 4, 2, 3, 5, 7 and any larger
+// prime; an odd last axis unpacked) the shared-memory kernels.
 static int make_plan(const int32_t nmesh[3], Plan3* p) {
     for (int d = 0; d < 3; d++)
         if (nmesh[d] < 2 || nmesh[d] > MAX_FFT_N) return PRC_ERR_UNSUPPORTED;
@@ -759,7 +759,11 @@ static int fft_grid(int64_t ntiles, int ctas_per_sm) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, cap));
 }
 
-static bool fast_len(int n) { return n >= 8 && n <= MAX_FAST_N && (n & (n - 1)) == 0; }
+// Lengths of the register-resident kernels: powers of two from 8 to MAX_FAST_N, and 96, 192, 384 (three
+// times a power of two: three sub-transforms and a radix-3 step, fft_fast.cuh).
+static bool fast_len(int n) {
+    return (n >= 8 && n <= MAX_FAST_N && (n & (n - 1)) == 0) || n == 96 || n == 192 || n == 384;
+}
 
 // PRC_FFT_GENERIC=1 in the environment routes every size through the mixed-radix kernels
 // (the tests use it to keep that path checked on power-of-two sizes too).
@@ -772,9 +776,12 @@ static bool getenv_generic() {
     return cached == 1;
 }
 
-// Compile-time dispatch of a runtime power-of-two length onto F<N>::run(args...).
+// Compile-time dispatch of a runtime length (fast_len) onto F<N>::run(args...).
 template <template <int> class F, typename... A> static int dispatch_pow2(int n, A... a) {
     switch (n) {
+        case 96: return F<96>::run(a...);
+        case 192: return F<192>::run(a...);
+        case 384: return F<384>::run(a...);
         case 8: return F<8>::run(a...);
         case 16: return F<16>::run(a...);
         case 32: return F<32>::run(a...);

@@ -51,7 +51,23 @@ template <int N> struct TwLayout {
     static constexpr int SIZE = N - 1;
 };
 
+// tw[m] = w_n^m = exp(-2 pi i m / n) for m < count.
+template <typename C> __device__ void fill_roots(C* tw, int count, int n) {
+    typedef decltype(C().x) T;
+    for (int m = threadIdx.x; m < count; m += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * (double)m / (double)n, &sn, &cs);
+        tw[m] = cmake<C>((T)cs, (T)sn);
+    }
+}
+
+// Twiddle table of an N-point transform (fft_regs).  Powers of two: the pass table (N - 1 entries).  N = 3 M:
+// the pass table of the M-point sub-transforms, then w_N^k for k < M at tw + M (2 M <= N entries).
 template <typename C, int N> __device__ void fill_pass_twiddles(C* tw) {
+    if constexpr (N % 3 == 0) {
+        fill_pass_twiddles<C, N / 3>(tw);
+        fill_roots(tw + N / 3, N / 3, N);
+    } else {
     typedef decltype(C().x) T;
     for (int idx = threadIdx.x; idx < TwLayout<N>::SIZE; idx += blockDim.x) {
         int off = 0, ns = 1, R = 8;
@@ -67,17 +83,9 @@ template <typename C, int N> __device__ void fill_pass_twiddles(C* tw) {
         sincospi(-2.0 * (double)m / (double)N, &sn, &cs);
         tw[idx] = cmake<C>((T)cs, (T)sn);
     }
-}
-
-// tw[m] = w_n^m = exp(-2 pi i m / n) for m < count.
-template <typename C> __device__ void fill_roots(C* tw, int count, int n) {
-    typedef decltype(C().x) T;
-    for (int m = threadIdx.x; m < count; m += blockDim.x) {
-        double sn, cs;
-        sincospi(-2.0 * (double)m / (double)n, &sn, &cs);
-        tw[m] = cmake<C>((T)cs, (T)sn);
     }
 }
+
 
 template <typename C, int DIR, int R> __device__ __forceinline__ void dftR(C* u) {
     if constexpr (R == 8) dft8<C, DIR>(u);
@@ -201,23 +209,121 @@ template <typename C, int N, int DIR, int P> struct PassesPP {
     }
 };
 
-// In: v[i] = x[t + i T].  Out: v[i] = X[t + i T] (unnormalised DFT, sign DIR).  tw: the pass
-// table filled by fill_pass_twiddles<C, N>.
+// ---- lines of N = 3 M points (M a power of two) ----
+// The transform is three M-point transforms of the points decimated by 3 (sub-line r holds x[3 m + r] at
+// position m) followed by one radix-3 step, X[k + j M] = sum_r w_N^(r k) w_3^(r j) X_r[k]: an exchange
+// that decimates, the sub-transforms (threads t = r M/8 + t' work on sub-line r, in its own region
+// r M .. r M + M - 1 of the exchange buffer), an exchange that makes X_0..2[k] readable by the thread of
+// each output, and the radix-3 step in registers.  Points in and out stay t + i T, T = N / 8.
+template <int N> struct Shape {
+    static constexpr bool R3 = N % 3 == 0;
+    static constexpr int M = R3 ? N / 3 : N;                          // the power-of-two part
+    static constexpr int NX = Plan<M>::NPASS - 1 + (R3 ? 2 : 0);      // shared-memory exchanges of a transform
+};
+
+template <class Addr> struct SubAddr {
+    Addr a;
+    int off;
+    __device__ __forceinline__ int operator()(int k) const { return a(off + k); }
+};
+
+// Output p of the radix-3 step from the sub-transforms in s (sub-line r at r M): with b = w^k X_1[k],
+// c = w^(2k) X_2[k], X[k] = a + b + c, X[k + M] = a - (b + c) / 2 + i s (b - c), X[k + 2M] = a - (b + c) / 2
+// - i s (b - c), s = DIR sqrt(3) / 2.
+template <typename C, int N, int DIR, class Addr>
+__device__ __forceinline__ C combine3(const C* s, const Addr& addr, const C* tw, int p) {
+    typedef decltype(C().x) T;
+    constexpr int M = N / 3;
+    const int k = p & (M - 1), j = p / M;
+    C w1 = tw[M + k];
+    if (DIR > 0) w1 = cconj(w1);
+    const C w2 = cmul(w1, w1);
+    const C a = s[addr(k)];
+    const C b = cmul(s[addr(M + k)], w1);
+    const C c = cmul(s[addr(2 * M + k)], w2);
+    const C sum = cadd(b, c), dif = csub(b, c);
+    const C h = csub(a, cscale(sum, (T)0.5));
+    const T sg = (T)(DIR * 0.86602540378443864676);
+    const C rot = cmake<C>(-sg * dif.y, sg * dif.x);
+    return j == 0 ? cadd(a, sum) : (j == 1 ? cadd(h, rot) : csub(h, rot));
+}
+
+template <typename C, int N, int DIR, class Addr>
+__device__ __forceinline__ void fft_regs3(C (&v)[8], int t, C* s, const Addr& addr, const C* tw) {
+    constexpr int M = N / 3, T = N / 8, TM = M / 8;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int p = t + i * T;
+        s[addr((p % 3) * M + p / 3)] = v[i];
+    }
+    __syncthreads();
+    const int r = t / TM, tm = t - r * TM;
+    const SubAddr<Addr> sa{addr, r * M};
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = s[sa(tm + i * TM)];
+    __syncthreads();
+    Passes<C, M, DIR, 0>::run(v, tm, s, sa, tw);
+#pragma unroll
+    for (int i = 0; i < 8; i++) s[sa(tm + i * TM)] = v[i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = combine3<C, N, DIR>(s, addr, tw, t + i * T);
+    __syncthreads();
+}
+
+// The same with the exchanges alternating between s0 and s1 (the fft_regs_pp contract): decimation in s0,
+// the sub-transforms' exchanges from s1 on, the radix-3 exchange in the buffer the last one did not use.
+template <typename C, int N, int DIR, class Addr0, class Addr1>
+__device__ __forceinline__ void fft_regs3_pp(C (&v)[8], int t, C* s0, const Addr0& addr0, C* s1, const Addr1& addr1,
+                                             const C* tw) {
+    constexpr int M = N / 3, T = N / 8, TM = M / 8, NXM = Plan<M>::NPASS - 1;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int p = t + i * T;
+        s0[addr0((p % 3) * M + p / 3)] = v[i];
+    }
+    __syncthreads();
+    const int r = t / TM, tm = t - r * TM;
+    const SubAddr<Addr0> sa0{addr0, r * M};
+    const SubAddr<Addr1> sa1{addr1, r * M};
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = s0[sa0(tm + i * TM)];
+    PassesPP<C, M, DIR, 0>::run(v, tm, s1, sa1, s0, sa0, tw);
+    if constexpr ((NXM + 1) % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) s0[sa0(tm + i * TM)] = v[i];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = combine3<C, N, DIR>(s0, addr0, tw, t + i * T);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; i++) s1[sa1(tm + i * TM)] = v[i];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = combine3<C, N, DIR>(s1, addr1, tw, t + i * T);
+    }
+}
+
+// In: v[i] = x[t + i T].  Out: v[i] = X[t + i T] (unnormalised DFT, sign DIR).  tw: the table filled by
+// fill_pass_twiddles<C, N>.  N a power of two, or 3 times one.
 template <typename C, int N, int DIR, class Addr>
 __device__ __forceinline__ void fft_regs(C (&v)[8], int t, C* s, const Addr& addr, const C* tw) {
-    Passes<C, N, DIR, 0>::run(v, t, s, addr, tw);
+    if constexpr (N % 3 == 0) fft_regs3<C, N, DIR>(v, t, s, addr, tw);
+    else Passes<C, N, DIR, 0>::run(v, t, s, addr, tw);
 }
 
 template <typename C, int N, int DIR, class Addr>
 __device__ __forceinline__ void fft_regs_pp(C (&v)[8], int t, C* s0, C* s1, const Addr& addr, const C* tw) {
-    PassesPP<C, N, DIR, 0>::run(v, t, s0, addr, s1, addr, tw);
+    if constexpr (N % 3 == 0) fft_regs3_pp<C, N, DIR>(v, t, s0, addr, s1, addr, tw);
+    else PassesPP<C, N, DIR, 0>::run(v, t, s0, addr, s1, addr, tw);
 }
 
 // The same with a separate layout for s0, the buffer of the first (and every even) exchange.
 template <typename C, int N, int DIR, class Addr0, class Addr1>
 __device__ __forceinline__ void fft_regs_pp(C (&v)[8], int t, C* s0, const Addr0& addr0, C* s1, const Addr1& addr1,
                                             const C* tw) {
-    PassesPP<C, N, DIR, 0>::run(v, t, s0, addr0, s1, addr1, tw);
+    if constexpr (N % 3 == 0) fft_regs3_pp<C, N, DIR>(v, t, s0, addr0, s1, addr1, tw);
+    else PassesPP<C, N, DIR, 0>::run(v, t, s0, addr0, s1, addr1, tw);
 }
 
 struct ColAddr {
@@ -534,7 +640,7 @@ __device__ __forceinline__ void row_r2c_pp(cplx_t<T> (&v)[8], bool ok, int t, cp
                                            const Addr& addr, const cplx_t<T>* tw, const cplx_t<T>* wk,
                                            cplx_t<T>* dst) {
     typedef cplx_t<T> C;
-    constexpr int TL = M / 8, NX = Plan<M>::NPASS - 1;   // exchanges: s0, s1, s0, ...
+    constexpr int TL = M / 8, NX = Shape<M>::NX;   // exchanges: s0, s1, s0, ...
     fft_regs_pp<C, M, -1>(v, t, s0, s1, addr, tw);
     C* zb = NX == 0 ? s0 : ((NX - 1) % 2 == 0 ? s1 : s0);
 #pragma unroll
@@ -776,7 +882,7 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
                 if constexpr (Src::PP) {
                     // the inverse transforms exchanged through buf, buf2, buf, ...: the first buffer
                     // the forward one writes must not be the one their last exchange read
-                    constexpr int NX = Plan<M>::NPASS - 1;
+                    constexpr int NX = Shape<M>::NX;
                     if constexpr (NX == 0 || (NX - 1) % 2 == 0) __syncthreads();
                     row_r2c_pp<T, M>(z, ok, t, buf, src.buf2, addr, tw, wk, dst);
                     __syncthreads();

@@ -19,7 +19,8 @@ namespace fast {
 template <typename T, int N, int B> struct TileShape {
     typedef cplx_t<T> C;
     static constexpr int U = (int)(sizeof(C) / 8);    // 8-byte map elements per complex value
-    static constexpr int BOXL = N < 256 ? N : 256;    // points per copy (a box extent is at most 256)
+    // points per copy: a box extent is at most 256 and divides N (384 = 2 x 192)
+    static constexpr int BOXL = N <= 256 ? N : (N % 256 == 0 ? 256 : N / 2);
     static constexpr int NCHUNK = N / BOXL;
     static constexpr int ELEMS = N * B;
     static constexpr uint32_t BYTES = (uint32_t)(ELEMS * sizeof(C));
@@ -198,7 +199,7 @@ __global__ void __launch_bounds__(N / 8 * B, (LEAN ? MinBlocks<T, N / 8 * B, 2>:
     // with an odd number of exchanges per transform, consecutive transforms would start on the buffer
     // the previous one read last: a barrier separates them (as it does a transform without exchanges
     // from the stage re-arm)
-    constexpr bool PP_SYNC = (Plan<N>::NPASS - 1) % 2 == 1 || Plan<N>::NPASS == 1;
+    constexpr bool PP_SYNC = Shape<N>::NX % 2 == 1 || Shape<N>::NX == 0;
     constexpr int PADX = PP ? PadFirst<T, B>::value : 0;   // PP: xbuf, the first exchange's, padded
     C* xbuf = stages + S * TS::ELEMS;
     C* ybuf = xbuf + TS::ELEMS + PADX * (N / 8) * B;   // PP: the second scratch tile
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(N / 8 * B, (LEAN ? MinBlocks<T, N / 8 * B, 2>:
                 for (int i = 0; i < 8; i++) v[i] = sb[(t + i * TL) * B + col];
                 __syncthreads();
                 fft_regs<C, N, -1>(v, t, sb, addr, tw);
-                if constexpr (Plan<N>::NPASS == 1) __syncthreads();
+                if constexpr (Shape<N>::NX == 0) __syncthreads();
 #pragma unroll
                 for (int i = 0; i < 8; i++) sb[(t + i * TL) * B + col] = v[i];
             }

@@ -49,8 +49,9 @@ def _fft_roundtrip(nmesh, dtype, seed=8):
     return e_spec, e_back
 
 
+# 96, 192 and 384 run the register kernels' radix-3 form (three sub-transforms and a radix-3 step)
 FFT_SIZES = [(128, 128, 128), (192, 192, 192), (256, 256, 256), (384, 384, 384), (512, 512, 512), (512, 256, 128),
-             (128, 512, 256)]
+             (128, 512, 256), (96, 96, 96), (96, 384, 192), (384, 192, 96)]
 
 
 @pytest.mark.parametrize('nmesh', FFT_SIZES)
@@ -75,7 +76,8 @@ def _subprocess(code, **env):
 def test_fft_bench_sizes_without_tma():
     """The register-prefetch strided passes (PRC_FFT_TMA=0) at the bench sizes."""
     _subprocess("import test_gpu_bench_sizes as T; "
-                "[T.test_fft_bench_sizes(n, d) for n in [(256, 256, 256), (512, 256, 128)] for d in ['f4', 'f8']]",
+                "[T.test_fft_bench_sizes(n, d) for n in [(256, 256, 256), (512, 256, 128), (384, 192, 96)] "
+                "for d in ['f4', 'f8']]",
                 PRC_FFT_TMA='0')
 
 
@@ -167,7 +169,8 @@ def _gpu(algorithm, nmesh, dtype, c, **kwargs):
 PIPELINES = [('iterative_fft', 128, 'f4'), ('iterative_fft', 256, 'f4'), ('iterative_fft', 256, 'f8'),
              ('multigrid', 256, 'f4'), ('multigrid', 256, 'f8'), ('plane_parallel_fft', 256, 'f4'),
              ('plane_parallel_fft', 256, 'f8'), ('iterative_fft', 512, 'f4'), ('iterative_fft', 512, 'f8'),
-             ('multigrid', 512, 'f4')]
+             ('multigrid', 512, 'f4'), ('iterative_fft', 192, 'f8'), ('iterative_fft', 192, 'f4'),
+             ('plane_parallel_fft', 192, 'f4'), ('iterative_fft', 384, 'f4')]
 
 
 @pytest.mark.parametrize('algorithm,nmesh,dtype', PIPELINES)
@@ -252,7 +255,7 @@ def _iterative_psi(nmesh, dtype, fuse):
     return psi4.cpu().numpy()
 
 
-@pytest.mark.parametrize('nmesh', [(256, 256, 256), (64, 32, 128), (32, 64, 16)])
+@pytest.mark.parametrize('nmesh', [(256, 256, 256), (64, 32, 128), (32, 64, 16), (96, 192, 384)])
 @pytest.mark.parametrize('dtype', ['f4', 'f8'])
 def test_fused_z_passes_same_bits(nmesh, dtype):
     """The local-line-of-sight iteration's inverse z pass transforms its new density rows forward at once
