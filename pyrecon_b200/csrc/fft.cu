@@ -1123,7 +1123,9 @@ template <typename T, int N> struct HessTmaCfg {
                                               : (sizeof(T) == 4 ? PRC_HESS_B : PRC_HESS_B / 2);
     static constexpr int B = (N / 8) * B0 <= 1024 ? B0 : 1024 / (N / 8);
     static constexpr int THREADS = (N / 8) * B;
-    static constexpr int MINB = THREADS * PRC_HESS_MINB <= 1024 ? PRC_HESS_MINB : 1;
+    // PRC_HESS_MINB blocks, and at least 16 warps per SM for short lines (192 threads at 192 points)
+    static constexpr int MINB0 = THREADS * PRC_HESS_MINB >= 512 ? PRC_HESS_MINB : (511 + THREADS) / THREADS;
+    static constexpr int MINB = THREADS * MINB0 <= 1024 ? MINB0 : 1;
     static constexpr int PADX = 0;     // see y_hessian_tma
     static constexpr bool PP =
         PRC_HESS_PP != 0 && fast::TmaSmem<T, N, B, PRC_HESS_PP_S, 1, PADX>::BYTES + 2 * N * sizeof(T) <= 227 * 1024;

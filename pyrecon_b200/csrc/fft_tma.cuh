@@ -178,16 +178,22 @@ template <typename T, int N, int B, int S, bool LEAN> struct KSpacePP {
 // multiplier terms are recomputed for every output, so two CTAs fit on an SM (FP32); the stage is
 // re-armed only after the tile's last output.
 // Blocks per SM asked of the register allocator: at least 16 warps per SM in FP32 (a tile of B columns of
-// a short line has few threads: 256 at 256 points, 128 at 128), so at most 128 registers a thread; tiles
-// of less than a warp (lines of 8 or 16 points) are left free.
-template <typename T, int THREADS> struct KSpaceMinBlocks {
-    static constexpr int value = MinBlocks<T, THREADS,
-                                           (PRC_KSPACE_MINB > 1 ? PRC_KSPACE_MINB
-                                                                : (THREADS >= 512 || THREADS < 32 ? 1 : 512 / THREADS))>::value;
+// a short line has few threads: 256 at 256 points, 128 at 128, 384 at 384), so at most 128 registers a
+// thread (85 for 384 threads); tiles of less than a warp (lines of 8 or 16 points) are left free.
+// CEIL = false (lines of 3 2^k points, whose radix-3 step needs more registers): 512 / THREADS rounded
+// down; rounded up, the 384-point pass (80 registers, ~100 bytes spilled) measured 2.91 against 2.66 ms
+// per nmesh-384 reconstruction.
+template <typename T, int THREADS, bool CEIL = true> struct KSpaceMinBlocks {
+    static constexpr int value =
+        MinBlocks<T, THREADS,
+                  (PRC_KSPACE_MINB > 1 ? PRC_KSPACE_MINB
+                                       : (THREADS >= 512 || THREADS < 32 ? 1
+                                                                         : (CEIL ? (511 + THREADS) / THREADS : 512 / THREADS)))>::value;
 };
 
 template <typename T, int N, int B, int S, int KT, bool LEAN>
-__global__ void __launch_bounds__(N / 8 * B, (LEAN ? MinBlocks<T, N / 8 * B, 2>::value : KSpaceMinBlocks<T, N / 8 * B>::value))
+__global__ void __launch_bounds__(N / 8 * B, (LEAN ? MinBlocks<T, N / 8 * B, 2>::value
+                                                  : KSpaceMinBlocks<T, N / 8 * B, N % 3 != 0>::value))
     x_kspace_tma(const __grid_constant__ prc::tma::Maps maps, int nin, Specs<cplx_t<T>> out, Dims dims, int pitch,
                  KOp op) {
     typedef cplx_t<T> C;
