@@ -633,7 +633,7 @@ def multi_workload(args, w, device, rank):
     budget = min(w.get('hbm_budget') or float('inf'), 0.75 * free)
     with ClockSampler(device.index or 0) as clocks:
         server = ReconstructionServer(device=device, slots=w['slots'], hbm_budget=budget,
-                                      max_batch=w.get('max_batch', 1))
+                                      max_batch=w.get('max_batch', 1), batch_algorithms=w.get('batch_algorithms'))
         # warm-up of the request loop: the whole request set once, all at once (each slot's scratch and
         # multigrid graphs, the streams' allocator pools), as a long-running server would be
         for f in [server.submit(r) for r in reqs]:
@@ -687,7 +687,10 @@ KERNELS = {
     'mg_jacobi': ('f4', 512),          # damped-Jacobi sweeps (two per step), local line of sight, FP32
     'mg_jacobi_256': ('f4', 256),
     'mg_jacobi_f64': ('f8', 384),
+    'mg_jacobi_axis': ('f4', 512),     # line of sight along z: the 7-point form of the operator
+    'mg_jacobi_axis_256': ('f4', 256),
     'mg_residual': ('f4', 512),
+    'mg_residual_axis': ('f4', 512),
     'smooth_real': ('f4', 256),        # truncated real-space Gaussian, radius 15 Mpc/h on 7.8 Mpc/h cells
     'iterative_fft': ('f4', 512),      # the FFT pipeline of IterativeFFTReconstruction.run on a mesh (3 iterations,
                                        # local line of sight), no particles: the FFT passes alone, ~6.5 GB on the device
@@ -710,6 +713,7 @@ def run_kernel_arm(args):
     nm, bs, bc = _lib.i3((n, n, n)), _lib.d3([2000.] * 3), _lib.d3([2000.] * 3)
     st = _lib.stream_of(device)
     N = n ** 3
+    los = _lib.d3([0., 0., 1.]) if 'axis' in args.kernel else None
     if args.kernel == 'iterative_fft':
         del f
         psi4 = torch.empty((n, n, n, 4), device=device, dtype=tdt)
@@ -721,10 +725,10 @@ def run_kernel_arm(args):
     elif args.kernel.startswith('mg_jacobi'):
         # two sweeps per step (v -> out -> v), so the result lands back in v without a copy
         name, nbytes = 'prc_mg_jacobi_' + _lib.suffix(dtype), 2 * 3 * N * item
-        call = lambda: _lib.call(name, _lib.ptr(v), _lib.ptr(f), _lib.ptr(out), nm, bs, bc, 0.4, 0.4, 2, None, st)
-    elif args.kernel == 'mg_residual':
+        call = lambda: _lib.call(name, _lib.ptr(v), _lib.ptr(f), _lib.ptr(out), nm, bs, bc, 0.4, 0.4, 2, los, st)
+    elif args.kernel.startswith('mg_residual'):
         name, nbytes = 'prc_mg_residual_' + _lib.suffix(dtype), 3 * N * item
-        call = lambda: _lib.call(name, _lib.ptr(v), _lib.ptr(f), _lib.ptr(out), nm, bs, bc, 0.4, None, st)
+        call = lambda: _lib.call(name, _lib.ptr(v), _lib.ptr(f), _lib.ptr(out), nm, bs, bc, 0.4, los, st)
     else:
         box = np.array([15. / 2000.] * 3, dtype=dtype)
         ws = torch.empty(_lib.load().prc_smooth_gaussian_real_workspace_bytes(nm, _lib.d3(box), 2.5, item),

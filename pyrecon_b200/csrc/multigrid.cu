@@ -53,6 +53,24 @@ static Stencil<T> make_stencil(const int n[3], const double boxsize[3], const do
     return s;
 }
 
+// Operator forms of the quad kernels (template argument MODE).  MG_LOCAL: p = position / h, 19 points
+// with the first-derivative term.  MG_GLOBAL: p = los / h, 19 points.  MG_AXIS0..2: a line of sight
+// along one axis, where every edge coefficient p_a p_b and all but one p_a^2 are exactly zero, so the
+// operator reads 7 points; the terms it leaves out are exact zeros in the 19-point form, so the two agree
+// up to the compiler's contraction of the kept terms into multiply-adds (run-time knob mg_axis_stencil = 0
+// keeps the 19-point form for comparison).
+enum { MG_GLOBAL = 0, MG_LOCAL = 1, MG_AXIS0 = 2, MG_AXIS1 = 3, MG_AXIS2 = 4 };
+
+template <typename T> static int mg_mode(const Stencil<T>& s) {
+    if (s.local) return MG_LOCAL;
+    int zeros = 0, axis = 0;
+    for (int d = 0; d < 3; d++) {
+        if (s.losh[d] == (T)0) zeros++;
+        else axis = d;
+    }
+    return zeros == 2 && tune_get("mg_axis_stencil", 0, 1) != 0 ? MG_AXIS0 + axis : MG_GLOBAL;
+}
+
 template <typename T, typename S>
 __device__ __forceinline__ void coeffs(const Stencil<S>& s, int x, int y, int z, T p[3], T& g, T G[3]) {
     if (s.local) {
@@ -187,13 +205,31 @@ template <typename V> struct QuadCols {
     V c[6], XP[6], XM[6], YP[6], YM[6], PP[4], MM[4], MP[4], PM[4];
 };
 
-template <typename V, typename S>
+// Axis modes read the centre column at z0 - 1 .. z0 + 4 and the four axis neighbours at z0 .. z0 + 3
+// (entries 1..4 of their arrays), nothing else.
+template <int MODE, typename V, typename S>
 __device__ __forceinline__ void quad_load(const V* __restrict__ v, const Stencil<S>& s, const Quad& q, QuadCols<V>& Q) {
     const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
     const int64_t sx = (int64_t)n1 * n2;
     const int64_t xp = (int64_t)wrap_up(q.x, n0) * sx, xm = (int64_t)wrap_dn(q.x, n0) * sx, x0 = (int64_t)q.x * sx;
     const int64_t yp = (int64_t)wrap_up(q.y, n1) * n2, ym = (int64_t)wrap_dn(q.y, n1) * n2, y0 = (int64_t)q.y * n2;
     load6(v + x0 + y0, q.z0, n2, Q.c);
+    if constexpr (MODE >= MG_AXIS0) {
+        V t[4];
+        load4(v + xp + y0 + q.z0, t);
+#pragma unroll
+        for (int k = 0; k < 4; k++) Q.XP[k + 1] = t[k];
+        load4(v + xm + y0 + q.z0, t);
+#pragma unroll
+        for (int k = 0; k < 4; k++) Q.XM[k + 1] = t[k];
+        load4(v + x0 + yp + q.z0, t);
+#pragma unroll
+        for (int k = 0; k < 4; k++) Q.YP[k + 1] = t[k];
+        load4(v + x0 + ym + q.z0, t);
+#pragma unroll
+        for (int k = 0; k < 4; k++) Q.YM[k + 1] = t[k];
+        return;
+    }
     load6(v + xp + y0, q.z0, n2, Q.XP);
     load6(v + xm + y0, q.z0, n2, Q.XM);
     load6(v + x0 + yp, q.z0, n2, Q.YP);
@@ -211,9 +247,10 @@ __device__ __forceinline__ void quad_load(const V* __restrict__ v, const Stencil
 //   S(v) = U + g W,   2 sum_a G_a = 2 (sum_a 1/h_a^2 + g P).
 // x and y are fixed for the thread, so the p_0, p_1 terms are computed once for its four cells.  Every
 // quad kernel (one sweep from global memory, two sweeps from shared memory) evaluates this function.
-template <typename A, typename V, typename S, bool LOCAL>
+template <typename A, typename V, typename S, int MODE>
 __device__ __forceinline__ void quad_compute(const QuadCols<V>& Q, const Stencil<S>& s, int x, int y, int z0,
                                              A (&U)[4], A (&W)[4], A (&qq)[4], A (&P)[4]) {
+    constexpr bool LOCAL = MODE == MG_LOCAL;
     const V(&c)[6] = Q.c;
     const V(&XP)[6] = Q.XP;
     const V(&XM)[6] = Q.XM;
@@ -243,6 +280,15 @@ __device__ __forceinline__ void quad_compute(const QuadCols<V>& Q, const Stencil
         const A s2 = p2 * p2;
         const A xpv = (A)XP[k + 1], xmv = (A)XM[k + 1], ypv = (A)YP[k + 1], ymv = (A)YM[k + 1];
         const A zpv = (A)c[k + 2], zmv = (A)c[k];
+        if constexpr (MODE >= MG_AXIS0) {
+            U[k] = ih0 * (xpv + xmv) + ih1 * (ypv + ymv) + ih2 * (zpv + zmv);
+            if constexpr (MODE == MG_AXIS0) W[k] = s0 * (xpv + xmv);
+            else if constexpr (MODE == MG_AXIS1) W[k] = s1 * (ypv + ymv);
+            else W[k] = s2 * (zpv + zmv);
+            qq[k] = q01 + (A)s.h2[2] * s2;
+            P[k] = P01 + s2;
+            continue;
+        }
         const A exy = ((A)PP[k] + (A)MM[k]) - ((A)MP[k] + (A)PM[k]);
         const A exz = ((A)XP[k + 2] + (A)XM[k]) - ((A)XM[k + 2] + (A)XP[k]);
         const A eyz = ((A)YP[k + 2] + (A)YM[k]) - ((A)YM[k + 2] + (A)YP[k]);
@@ -260,12 +306,12 @@ __device__ __forceinline__ void quad_compute(const QuadCols<V>& Q, const Stencil
 }
 
 
-template <typename A, typename V, typename S, bool LOCAL>
+template <typename A, typename V, typename S, int MODE>
 __device__ __forceinline__ void quad_terms(const V* __restrict__ v, const Stencil<S>& s, const Quad& q, A (&U)[4],
                                            A (&W)[4], A (&qq)[4], A (&P)[4]) {
     QuadCols<V> Q;
-    quad_load(v, s, q, Q);
-    quad_compute<A, V, S, LOCAL>(Q, s, q.x, q.y, q.z0, U, W, qq, P);
+    quad_load<MODE>(v, s, q, Q);
+    quad_compute<A, V, S, MODE>(Q, s, q.x, q.y, q.z0, U, W, qq, P);
 }
 
 template <typename T> __device__ __forceinline__ T quotient(T a, T b) {
@@ -305,7 +351,7 @@ __device__ __forceinline__ void quad_blend(const Stencil<T>& s, T w, const T (&f
 // Damped-Jacobi sweep of four cells per thread:
 //   jac = (f + S) / (2 sum G) = (q (f + U) + beta W) / (2 (q sum 1/h^2 + beta P)),
 //   vout = v + w (jac - v).
-template <typename T, bool LOCAL>
+template <typename T, int MODE>
 __global__ void __launch_bounds__(256) jacobi_sweep4(const T* __restrict__ v, const T* __restrict__ f,
                                                      T* __restrict__ vout, Stencil<T> s, T w, int zero_v) {
     pdl_trigger();
@@ -317,9 +363,9 @@ __global__ void __launch_bounds__(256) jacobi_sweep4(const T* __restrict__ v, co
     T fv[4], vc[4], U[4], W[4], qq[4], P[4];
     load4(f + q.c + q.z0, fv);
     if (zero_v) {
-        quad_zero_terms<T, LOCAL>(s, q.x, q.y, q.z0, U, W, qq, P, vc);
+        quad_zero_terms<T, MODE == MG_LOCAL>(s, q.x, q.y, q.z0, U, W, qq, P, vc);
     } else {
-        quad_terms<T, T, T, LOCAL>(v, s, q, U, W, qq, P);
+        quad_terms<T, T, T, MODE>(v, s, q, U, W, qq, P);
         load4(v + q.c + q.z0, vc);
     }
     T o[4];
@@ -494,7 +540,7 @@ __global__ void __launch_bounds__(TQ * TY, (sizeof(T) == 4 ? 6 : 4)) jacobi_swee
 }
 
 // r = f - A v = (f + U - 2 v sum 1/h^2) + g (W - 2 P v), g = beta / q, evaluated in type A.
-template <typename A, typename V, typename FT, typename R, typename S, bool LOCAL>
+template <typename A, typename V, typename FT, typename R, typename S, int MODE>
 __global__ void __launch_bounds__(256) residual_kernel4(const V* __restrict__ v, const FT* __restrict__ f,
                                                         R* __restrict__ r, Stencil<S> s) {
     pdl_trigger();
@@ -504,7 +550,7 @@ __global__ void __launch_bounds__(256) residual_kernel4(const V* __restrict__ v,
     const int64_t bo = batch_offset(s.n);
     v += bo, f += bo, r += bo;
     A U[4], W[4], qq[4], P[4];
-    quad_terms<A, V, S, LOCAL>(v, s, q, U, W, qq, P);
+    quad_terms<A, V, S, MODE>(v, s, q, U, W, qq, P);
     V vc[4];
     FT fv[4];
     load4(v + q.c + q.z0, vc);
@@ -534,6 +580,27 @@ __global__ void __launch_bounds__(256) residual_kernel(const V* __restrict__ v, 
     const A nb = neighbour_sum<A>(v, s.n, x, y, z, p, g, G, s.local);
     const A av = (A)2 * (G[0] + G[1] + G[2]) * (A)v[i] - nb;
     r[i] = (R)((A)f[i] - av);
+}
+
+// The quad kernels' instance for an operator form (mg_mode).
+template <typename T> static decltype(&jacobi_sweep4<T, MG_GLOBAL>) sweep4_kernel(int mode) {
+    switch (mode) {
+    case MG_LOCAL: return jacobi_sweep4<T, MG_LOCAL>;
+    case MG_AXIS0: return jacobi_sweep4<T, MG_AXIS0>;
+    case MG_AXIS1: return jacobi_sweep4<T, MG_AXIS1>;
+    case MG_AXIS2: return jacobi_sweep4<T, MG_AXIS2>;
+    default: return jacobi_sweep4<T, MG_GLOBAL>;
+    }
+}
+template <typename A, typename V, typename FT, typename R, typename S>
+static decltype(&residual_kernel4<A, V, FT, R, S, MG_GLOBAL>) residual4_kernel(int mode) {
+    switch (mode) {
+    case MG_LOCAL: return residual_kernel4<A, V, FT, R, S, MG_LOCAL>;
+    case MG_AXIS0: return residual_kernel4<A, V, FT, R, S, MG_AXIS0>;
+    case MG_AXIS1: return residual_kernel4<A, V, FT, R, S, MG_AXIS1>;
+    case MG_AXIS2: return residual_kernel4<A, V, FT, R, S, MG_AXIS2>;
+    default: return residual_kernel4<A, V, FT, R, S, MG_GLOBAL>;
+    }
 }
 
 // 27-point full weighting, coarse cell (x, y, z) centred on fine (2x, 2y, 2z).
@@ -751,7 +818,7 @@ template <typename T> struct MGRunner {
             const bool z0 = zero_first && it == 0;
             if (quad)
                 PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
-                             launch_pdl((s.local ? jacobi_sweep4<T, true> : jacobi_sweep4<T, false>), gq.grid, gq.block, 0, st, v, f, tmp, s, (T)P.damping, z0));
+                             launch_pdl(sweep4_kernel<T>(mg_mode(s)), gq.grid, gq.block, 0, st, v, f, tmp, s, (T)P.damping, z0));
             else
                 PRC_LAUNCH_B("mg_jacobi", st, (double)N * sizeof(T) * (z0 ? 2 : 3),
                              launch_pdl(jacobi_sweep<T, T>, g.grid, g.block, 0, st, v, f, tmp, s, (T)P.damping, z0));
@@ -771,7 +838,7 @@ template <typename T> struct MGRunner {
             if (quad_ok(L[l].n, v, f, B[l].r)) {
                 const Grid3 gq = grid3_quad(L[l].n, count);
                 PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T),
-                             launch_pdl((s.local ? residual_kernel4<T, T, T, T, T, true> : residual_kernel4<T, T, T, T, T, false>), gq.grid, gq.block, 0, st, v, f, B[l].r, s));
+                             launch_pdl(residual4_kernel<T, T, T, T, T>(mg_mode(s)), gq.grid, gq.block, 0, st, v, f, B[l].r, s));
             } else {
                 PRC_LAUNCH_B("mg_residual", st, 3.0 * N * sizeof(T),
                              launch_pdl(residual_kernel<T, T, T, T, T>, g.grid, g.block, 0, st, v, f, B[l].r, s));
@@ -964,8 +1031,7 @@ int solve_mixed(const int32_t nmesh[3], const Params& P, void* ws, cudaStream_t 
             if (quad_ok(m.L[l].n, m.v64[l], m.f64[l], R.B[l].f)) {
                 const Grid3 gq = grid3_quad(m.L[l].n, count);
                 PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N,
-                             launch_pdl((s64.local ? residual_kernel4<double, double, double, float, double, true>
-                                        : residual_kernel4<double, double, double, float, double, false>), gq.grid, gq.block, 0, st, m.v64[l], m.f64[l], R.B[l].f, s64));
+                             launch_pdl(residual4_kernel<double, double, double, float, double>(mg_mode(s64)), gq.grid, gq.block, 0, st, m.v64[l], m.f64[l], R.B[l].f, s64));
             } else {
                 PRC_LAUNCH_B("mg_residual_fp64", st, 20.0 * N,
                              launch_pdl(residual_kernel<double, double, double, float, double>, g.grid, g.block, 0, st, m.v64[l], m.f64[l], R.B[l].f, s64));
@@ -1262,7 +1328,7 @@ prc_status_t prc_multigrid_f64(const double* delta, double* phi, const int32_t n
         const double bytes = 3.0 * sizeof(T) * n[0] * n[1] * n[2];                                                   \
         if (quad_ok(n, v, f, r))                                                                                     \
             PRC_LAUNCH_B("mg_residual", (cudaStream_t)stream, bytes,                                                 \
-                         (s.local ? residual_kernel4<T, T, T, T, T, true> : residual_kernel4<T, T, T, T, T, false>)  \
+                         residual4_kernel<T, T, T, T, T>(mg_mode(s))                                              \
                              <<<grid3_quad(n).grid, grid3_quad(n).block, 0, (cudaStream_t)stream>>>(v, f, r, s));     \
         else                                                                                                         \
             PRC_LAUNCH_B("mg_residual", (cudaStream_t)stream, bytes,                                                 \
