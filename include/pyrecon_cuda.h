@@ -376,6 +376,23 @@ PRC_API prc_status_t prc_plane_parallel_fft_f64(const double *delta, const int32
                                         double *psi_z, int psi_stride, void *workspace, size_t workspace_bytes,
                                         void *stream);
 
+/* `count` PlaneParallelFFTReconstruction.run (pyrecon/plane_parallel_fft.py:41-55) of catalogues in the
+ * same box with the same beta and line of sight: the meshes share the launches of each FFT pass, two at
+ * a time (one launch over the tiles of both).  delta, psi_x, psi_y, psi_z are host arrays of `count`
+ * device pointers (psi_stride as above); the workspace does not grow past two meshes' worth; results
+ * equal `count` separate calls. */
+PRC_API size_t prc_plane_parallel_batch_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int count);
+PRC_API prc_status_t prc_plane_parallel_fft_batch_f32(const float *const *delta, float *const *psi_x,
+                                              float *const *psi_y, float *const *psi_z, int count,
+                                              const int32_t nmesh[3], const double boxsize[3], double beta,
+                                              const double los[3], int psi_stride, void *workspace,
+                                              size_t workspace_bytes, void *stream);
+PRC_API prc_status_t prc_plane_parallel_fft_batch_f64(const double *const *delta, double *const *psi_x,
+                                              double *const *psi_y, double *const *psi_z, int count,
+                                              const int32_t nmesh[3], const double boxsize[3], double beta,
+                                              const double los[3], int psi_stride, void *workspace,
+                                              size_t workspace_bytes, void *stream);
+
 /* IterativeFFTReconstruction.run (pyrecon/iterative_fft.py:12-82), niterations of the
  * Burden et al. 2015 field-level iteration then psi_a = IFFT(i k_a delta_k / k^2).
  * los = NULL selects the local line of sight. */

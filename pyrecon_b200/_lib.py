@@ -93,6 +93,10 @@ for _s in ['f32', 'f64']:
 _SIGNATURES['prc_multigrid_f32'] = (c_int, [_p, _p, I3, D3, D3, c_double, c_double, c_int, c_int, DP, c_int, _p, c_size, _p])
 _SIGNATURES['prc_multigrid_f64'] = (c_int, [_p, _p, I3, D3, D3, c_double, c_double, c_int, c_int, DP, _p, c_size, _p])
 _SIGNATURES['prc_multigrid_batch_workspace_bytes'] = (c_size, [I3, c_int, c_int, c_int])
+_SIGNATURES['prc_plane_parallel_batch_workspace_bytes'] = (c_size, [I3, c_int, c_int])
+for _s in ('f32', 'f64'):
+    _SIGNATURES['prc_plane_parallel_fft_batch_' + _s] = (c_int, [_p, _p, _p, _p, c_int, I3, D3, c_double, D3, c_int, _p,
+                                                                 c_size, _p])
 _SIGNATURES['prc_multigrid_mixed_f32'] = (c_int, [_p, _p, _p, I3, D3, D3, c_double, c_double, c_int, c_int, DP, _p,
                                                   c_size, _p])
 _SIGNATURES['prc_multigrid_batch_mixed_f32'] = (c_int, [_p, _p, _p, c_int, I3, D3, D3, c_double, c_double, c_int,

@@ -1496,6 +1496,54 @@ static int pp_impl(const T* delta, const int32_t nmesh[3], const double boxsize[
     return FFTLaunch<T>::z_c2r(p, S + 1, 3, e, st);
 }
 
+// Several plane-parallel reconstructions of the same mesh, box and parameters: the meshes go through the
+// passes in groups of PP_GROUP, each pass one launch over the (mesh, tile) pairs of its group (the three
+// outputs of every mesh fill the pointer tables of the inverse passes); the inverse z pass, whose
+// epilogue writes one displacement mesh, runs per mesh.  Each tile is computed as in pp_impl, so the
+// results are those of separate calls.
+constexpr int PP_GROUP = MAX_BATCH / 3;
+
+template <typename T>
+static int pp_batch_impl(const T* const* deltas, T* const* px, T* const* py, T* const* pz, int count,
+                         const int32_t nmesh[3], const double boxsize[3], double beta, const double los[3],
+                         int psi_stride, void* ws, size_t wsb, cudaStream_t st) {
+    Plan3 p;
+    PRC_TRY(make_plan(nmesh, &p));
+    pad_pitch<T>(&p);
+    const size_t sb = spec_bytes<T>(p);
+    const int G = std::min(count, PP_GROUP);
+    if (!ws || wsb < (size_t)4 * G * sb) return PRC_ERR_WORKSPACE;
+    for (int i = 0; i < count; i++) {
+        Epi<T> e;
+        if (!deltas[i]) return PRC_ERR_ARG;
+        PRC_TRY(psi_epilogue(px[i], py[i], pz[i], psi_stride, &e));
+    }
+    KOp op;
+    fill_kop_geometry(&op, p, boxsize, sizeof(T));
+    op.type = KOP_PP;
+    op.nper = 3;
+    op.beta = beta;
+    for (int a = 0; a < 3; a++) op.los[a] = sizeof(T) == 4 ? (double)(float)los[a] : los[a];
+    cplx_t<T>* F[PP_GROUP];
+    cplx_t<T>* O[3 * PP_GROUP];
+    for (int i = 0; i < G; i++) F[i] = (cplx_t<T>*)((char*)ws + i * sb);
+    for (int i = 0; i < 3 * G; i++) O[i] = (cplx_t<T>*)((char*)ws + (G + i) * sb);
+    for (int b = 0; b < count; b += G) {
+        const int g = std::min(G, count - b);
+        const void* ins[PP_GROUP];
+        for (int i = 0; i < g; i++) ins[i] = deltas[b + i];
+        PRC_TRY((forward_zy<T, T>(p, ins, F, g, st)));
+        PRC_TRY(FFTLaunch<T>::x_fused(p, F, g, O, op, st));
+        PRC_TRY(FFTLaunch<T>::template strided<+1>(p, 1, O, 3 * g, st));
+        for (int i = 0; i < g; i++) {
+            Epi<T> e;
+            PRC_TRY(psi_epilogue(px[b + i], py[b + i], pz[b + i], psi_stride, &e));
+            PRC_TRY(FFTLaunch<T>::z_c2r(p, O + 3 * i, 3, e, st));
+        }
+    }
+    return PRC_OK;
+}
+
 template <typename T>
 static int iter_impl(const T* delta, const int32_t nmesh[3], const double boxsize[3], const double boxcenter[3],
                      double beta, const double* los, int niter, T* px, T* py, T* pz, int psi_stride, void* ws,
@@ -1774,6 +1822,28 @@ prc_status_t prc_plane_parallel_fft_f64(const double* delta, const int32_t nmesh
     if (!delta || !geom_ok(nmesh, boxsize) || !los || !psi_x || !psi_y || !psi_z) return PRC_ERR_ARG;
     return pp_impl<double>(delta, nmesh, boxsize, beta, los, psi_x, psi_y, psi_z, psi_stride, workspace, workspace_bytes,
                            (cudaStream_t)stream);
+}
+
+size_t prc_plane_parallel_batch_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int count) {
+    if (count < 1) return 0;
+    return prc_fft_workspace_bytes(nmesh, mesh_bytes, 4 * std::min(count, PP_GROUP));
+}
+
+prc_status_t prc_plane_parallel_fft_batch_f32(const float* const* delta, float* const* psi_x, float* const* psi_y,
+                                              float* const* psi_z, int count, const int32_t nmesh[3],
+                                              const double boxsize[3], double beta, const double los[3],
+                                              int psi_stride, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!delta || !psi_x || !psi_y || !psi_z || count < 1 || !geom_ok(nmesh, boxsize) || !los) return PRC_ERR_ARG;
+    return pp_batch_impl<float>(delta, psi_x, psi_y, psi_z, count, nmesh, boxsize, beta, los, psi_stride, workspace,
+                                workspace_bytes, (cudaStream_t)stream);
+}
+prc_status_t prc_plane_parallel_fft_batch_f64(const double* const* delta, double* const* psi_x, double* const* psi_y,
+                                              double* const* psi_z, int count, const int32_t nmesh[3],
+                                              const double boxsize[3], double beta, const double los[3],
+                                              int psi_stride, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!delta || !psi_x || !psi_y || !psi_z || count < 1 || !geom_ok(nmesh, boxsize) || !los) return PRC_ERR_ARG;
+    return pp_batch_impl<double>(delta, psi_x, psi_y, psi_z, count, nmesh, boxsize, beta, los, psi_stride, workspace,
+                                 workspace_bytes, (cudaStream_t)stream);
 }
 
 size_t prc_iterative_fft_workspace_bytes(const int32_t nmesh[3], int mesh_bytes, int local_los) {

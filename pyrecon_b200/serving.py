@@ -13,11 +13,12 @@ scratch) is free and their estimated device memory fits in what the budget has l
 request runs the plain
 pipeline (constructor, assign_data, assign_randoms, set_density_contrast, run,
 read_shifted_positions) on its own stream from a worker thread, so the kernels of the requests
-in flight overlap on the device while requests keep arriving.  Queued multigrid requests of the same
-mesh and settings are admitted together (up to max_batch) and their solves run as one batched solve,
-every kernel of the multigrid schedule covering all of them in one launch.  A request's result does
-not depend on what else is running: every kernel is deterministic, requests share no device buffers
-and a batched solve gives each problem the bits of its own solve.
+in flight overlap on the device while requests keep arriving.  Queued multigrid or plane-parallel
+requests of the same mesh and settings are admitted together (up to max_batch) and run as one batched
+run: every kernel of the multigrid schedule covers all the solves in one launch, every plane-parallel FFT
+pass two meshes at a time.  A request's result does not depend on what else is running: every kernel is
+deterministic, requests share no device buffers and a batched run gives each problem the bits of its own
+run.
 """
 import threading
 import time
@@ -119,13 +120,15 @@ def run_request(request, device=None, stream=None, workspace=None):
 
 
 def batch_key(request):
-    """Requests with the same key can share one batched multigrid solve (same algorithm, mesh, line of
-    sight, cosmology, precision and solver settings; the catalogues may differ); None: not batchable."""
+    """Requests with the same key can share one batched run: a multigrid solve or the plane-parallel FFT
+    passes (same algorithm, mesh, line of sight, cosmology, precision and solver settings; the catalogues
+    may differ); None: not batchable."""
     import pyrecon_b200
     from .multigrid import OriginalMultiGridReconstruction
+    from .plane_parallel_fft import PlaneParallelFFTReconstruction
     cls = getattr(pyrecon_b200, request.algorithm)
     kw = request.kwargs
-    if not issubclass(cls, OriginalMultiGridReconstruction) or 'positions' in kw:
+    if not issubclass(cls, (OriginalMultiGridReconstruction, PlaneParallelFFTReconstruction)) or 'positions' in kw:
         return None
     if not all(k in kw for k in ('nmesh', 'boxsize', 'boxcenter')) and not ('cellsize' in kw and 'boxsize' in kw):
         return None
@@ -135,11 +138,15 @@ def batch_key(request):
 
 
 def run_batch_requests(requests, device=None, stream=None, workspace=None):
-    """Several batchable requests (same batch_key) on one stream: each is prepared, the multigrid solves
-    run as one batched solve, then each is read out; returns their outputs in order."""
-    from .multigrid import run_batch
+    """Several batchable requests (same batch_key) on one stream: each is prepared, their runs go as one
+    batched run (multigrid solve or plane-parallel FFT passes), then each is read out; returns their outputs
+    in order."""
+    from . import multigrid, plane_parallel_fft
     recs = [prepare_request(r, device=device, stream=stream, workspace=workspace) for r in requests]
-    run_batch(recs, **requests[0].run_kwargs)
+    if isinstance(recs[0], plane_parallel_fft.PlaneParallelFFTReconstruction):
+        plane_parallel_fft.run_batch(recs)
+    else:
+        multigrid.run_batch(recs, **requests[0].run_kwargs)
     return [finish_request(r, rec) for r, rec in zip(requests, recs)]
 
 
@@ -150,10 +157,11 @@ class ReconstructionServer(object):
     requests in flight may hold together (default: 90% of the free memory at start).  max_batch:
     queued multigrid requests with the same mesh and settings (batch_key) are taken together as one
     job of up to this many, whose solves run as one batched solve (a power of two, so the slot's
-    captured solves are reused); 1 disables.
+    captured solves are reused); 1 disables.  batch_algorithms: the algorithm classes whose requests are
+    batched (default: the multigrid and plane-parallel ones).
     """
 
-    def __init__(self, device=None, slots=8, hbm_budget=None, max_batch=8):
+    def __init__(self, device=None, slots=8, hbm_budget=None, max_batch=8, batch_algorithms=None):
         import torch
         self.device = _device_of(device)
         _lib.load()
@@ -162,6 +170,7 @@ class ReconstructionServer(object):
             hbm_budget = 0.9 * free
         self.hbm_budget = float(hbm_budget)
         self.max_batch = max(1, int(max_batch))
+        self.batch_algorithms = None if batch_algorithms is None else set(batch_algorithms)
         from .mesh import _Workspace
         self._streams = [torch.cuda.Stream(self.device) for _ in range(slots)]
         # device scratch resident per slot: reused by every request the slot runs
@@ -197,7 +206,8 @@ class ReconstructionServer(object):
             request.submitted = time.perf_counter()
             if self._first_submit is None:
                 self._first_submit = request.submitted
-            self._queue.append((request, need, fut, batch_key(request) if self.max_batch > 1 else None))
+            batched = self.max_batch > 1 and (self.batch_algorithms is None or request.algorithm in self.batch_algorithms)
+            self._queue.append((request, need, fut, batch_key(request) if batched else None))
             self._cv.notify_all()
         return fut
 

@@ -71,6 +71,35 @@ def test_repeatable_bitwise():
         assert np.array_equal(a[k], b[k]), k
 
 
+@pytest.mark.parametrize('dtype,nmesh', [('f4', (48, 32, 64)), ('f8', (32, 32, 32)), ('f4', (192, 192, 192))])
+def test_plane_parallel_run_batch_equals_separate_runs(dtype, nmesh):
+    """plane_parallel_fft.run_batch: three reconstructions (a pair sharing the FFT passes, then one) give
+    the displacements and shifted positions of three separate runs, bit for bit."""
+    import pyrecon_b200
+    from pyrecon_b200 import mocks
+    from pyrecon_b200.plane_parallel_fft import run_batch
+    cats = [mocks.lognormal_positions_numpy(20000 + 4000 * i, 32, 1000., 500., seed=130 + i, field_seed=140 + i)
+            for i in range(3)]
+
+    def prepared(data):
+        rec = pyrecon_b200.PlaneParallelFFTReconstruction(f=0.8, bias=2., los='y', nmesh=nmesh, boxsize=1000.,
+                                                           boxcenter=500., wrap=True, dtype=dtype)
+        rec.assign_data(data.astype(dtype))
+        rec.set_density_contrast(smoothing_radius=15.)
+        return rec
+
+    alone = []
+    for data in cats:
+        rec = prepared(data)
+        rec.run()
+        alone.append((rec._psi4.cpu().numpy(), rec.read_shifted_positions(data.astype(dtype))))
+    recs = [prepared(data) for data in cats]
+    run_batch(recs)
+    for rec, data, (psi, shifted) in zip(recs, cats, alone):
+        assert np.array_equal(rec._psi4.cpu().numpy(), psi)
+        assert np.array_equal(rec.read_shifted_positions(data.astype(dtype)), shifted)
+
+
 @pytest.mark.parametrize('kind', ['numpy', 'pinned', 'pageable'])
 def test_chunked_host_readout_equals_device_readout(kind):
     """Host positions read out in overlapping chunks (copy in / kernel / copy out on separate

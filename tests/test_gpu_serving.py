@@ -70,15 +70,18 @@ def test_admission_keeps_requests_within_the_budget():
             server.submit(big)
 
 
-def test_batched_multigrid_requests_equal_requests_alone():
-    """Queued multigrid requests of the same mesh and settings run as one job with a batched solve;
-    each result has the bits of the same request run alone."""
+@pytest.mark.parametrize('algorithm,dtype', [('MultiGridReconstruction', 'f4'), ('PlaneParallelFFTReconstruction', 'f4'),
+                                             ('PlaneParallelFFTReconstruction', 'f8')])
+def test_batched_requests_equal_requests_alone(algorithm, dtype):
+    """Queued multigrid or plane-parallel requests of the same mesh and settings run as one job with a
+    batched run (one solve, or FFT passes shared by pairs of meshes); each result has the bits of the
+    same request run alone."""
     from pyrecon_b200.serving import ReconstructionRequest, ReconstructionServer, run_request, batch_key
     reqs = []
     for i in range(5):
         data = mocks.lognormal_positions_numpy(10000 + 3000 * i, 32, 1000., 500., seed=100 + i, field_seed=110 + i)
-        reqs.append(ReconstructionRequest('MultiGridReconstruction', data=data, f=0.8, bias=2., los='z', nmesh=32,
-                                          boxsize=1000., boxcenter=500., wrap=True, dtype='f4',
+        reqs.append(ReconstructionRequest(algorithm, data=data, f=0.8, bias=2., los='z', nmesh=32,
+                                          boxsize=1000., boxcenter=500., wrap=True, dtype=dtype,
                                           density_kwargs=dict(smoothing_radius=15.)))
     assert len(set(batch_key(r) for r in reqs)) == 1
     alone = [run_request(r) for r in reqs]
