@@ -81,7 +81,7 @@ MULTI_WORKLOADS = {
     'batched_mocks': dict(kind='batched', nrequests=64, algorithms=['PlaneParallelFFTReconstruction',
                                                                     'MultiGridReconstruction'],
                           nmesh=[128, 192, 256], ndata=(300_000, 2_000_000), randoms_factor=0, boxsize=1000.,
-                          boxcenter=500., los='z', wrap=True, dtype='f4', slots=2, max_batch=8),
+                          boxcenter=500., los='z', wrap=True, dtype='f4', slots=2, max_batch=8, passes=5),
     # BASELINE config: 500 requests with Poisson arrivals at 20 req/s, the three algorithms, nmesh in
     # {128, 256, 384, 512}, 0.5M-8M data with 4x randoms, 150 GB admission budget.  Two slots: measured
     # p50 / p99 19.5-19.9 / 162-171 ms with 2, 21.3 / 174 with 1, 20.1 / 201 with 4 (the device is ~43 %
@@ -601,18 +601,24 @@ def multi_workload(args, w, device, rank):
     for r in reqs:
         run_request(r, device=device)
     torch.cuda.synchronize(device)
-    # plain path (kernel times recorded: how busy the device is when requests run one at a time)
-    lat_plain = []
-    _lib.profile_enable(True)
-    t0 = time.perf_counter()
-    for r in reqs:
-        t = time.perf_counter()
-        run_request(r, device=device)
-        torch.cuda.synchronize(device)
-        lat_plain.append(time.perf_counter() - t)
-    plain_s = time.perf_counter() - t0
-    prof = _lib.profile_collect()
-    _lib.profile_enable(False)
+    # plain path (kernel times recorded: how busy the device is when requests run one at a time).  A
+    # workload whose requests all arrive at once is timed `passes` times (one pass takes a fraction of a
+    # second and varies by 10-20 % run to run): the median pass, its latencies and kernel times are kept.
+    passes = int(w.get('passes', 1)) if w['kind'] != 'serving' else 1
+    runs = []
+    for _ in range(passes):
+        lat = []
+        _lib.profile_enable(True)
+        t0 = time.perf_counter()
+        for r in reqs:
+            t = time.perf_counter()
+            run_request(r, device=device)
+            torch.cuda.synchronize(device)
+            lat.append(time.perf_counter() - t)
+        runs.append((time.perf_counter() - t0, lat, _lib.profile_collect()))
+        _lib.profile_enable(False)
+    plain_all = sorted(x[0] for x in runs)
+    plain_s, lat_plain, prof = sorted(runs, key=lambda x: x[0])[len(runs) // 2]
     plain_kernel_ms = sum(v[1] for v in prof.values())
     top = sorted(prof.items(), key=lambda kv: -kv[1][1])[:6]
     # request loop
@@ -638,23 +644,25 @@ def multi_workload(args, w, device, rank):
         # multigrid graphs, the streams' allocator pools), as a long-running server would be
         for f in [server.submit(r) for r in reqs]:
             f.result()
-        server.reset_stats()
-        launches0 = _lib.launch_count()
-        torch.cuda.synchronize(device)
-        start = time.perf_counter()
-        futures = []
-        for r, at in zip(reqs, arrivals):
-            delay = start + at - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            futures.append(server.submit(r))
-        for f in futures:
-            f.result()
-        torch.cuda.synchronize(device)
-        served_s = time.perf_counter() - start
-        stats = server.stats()
+        served_runs = []
+        for _ in range(passes):
+            server.reset_stats()
+            launches0 = _lib.launch_count()
+            torch.cuda.synchronize(device)
+            start = time.perf_counter()
+            futures = []
+            for r, at in zip(reqs, arrivals):
+                delay = start + at - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                futures.append(server.submit(r))
+            for f in futures:
+                f.result()
+            torch.cuda.synchronize(device)
+            served_runs.append((time.perf_counter() - start, server.stats(), _lib.launch_count() - launches0))
         server.close()
-    launches = _lib.launch_count() - launches0
+    served_all = sorted(x[0] for x in served_runs)
+    served_s, stats, launches = sorted(served_runs, key=lambda x: x[0])[len(served_runs) // 2]
     del server
     gc.collect()
     torch.cuda.empty_cache()
@@ -669,12 +677,15 @@ def multi_workload(args, w, device, rank):
                     config=dict(workload=w['name'], requests=n, slots=w['slots'], max_batch=w.get('max_batch', 1),
                                 hbm_budget_gb=round(budget / 1e9, 1),
                                 arrivals='poisson {:g}/s'.format(w['rate']) if w['kind'] == 'serving' else 'all at once',
-                                nmesh=w['nmesh'], algorithms=w['algorithms'], timing='wall clock, device synchronised'),
+                                nmesh=w['nmesh'], algorithms=w['algorithms'],
+                                timing='wall clock, device synchronised; median of {} timed pass(es)'.format(passes)),
                     served=dict(recons_per_s=n / served_s, p50_ms=stats['p50_ms'], p99_ms=stats['p99_ms'],
-                                peak_in_flight=stats['peak_active']),
+                                peak_in_flight=stats['peak_active'],
+                                passes_recons_per_s=[round(n / x, 1) for x in served_all]),
                     plain=dict(recons_per_s=n / plain_s, p50_ms=pct(lat_plain, 50), p99_ms=pct(lat_plain, 99),
                                fifo_p50_ms=pct(fifo, 50), fifo_p99_ms=pct(fifo, 99),
                                kernel_ms=plain_kernel_ms, wall_ms=plain_s * 1e3,
+                               passes_recons_per_s=[round(n / x, 1) for x in plain_all],
                                top_kernels={k: round(v[1], 2) for k, v in top}),
                     served_vs_plain=(n / served_s) / (n / plain_s), gpu_launches=int(launches),
                     clocks=clocks.summary())
