@@ -98,8 +98,9 @@ __device__ __forceinline__ A stencil_terms(A vxp, A vxm, A vyp, A vym, A vzp, A 
     return s;
 }
 
-// The neighbour terms of S(v) at one cell, accumulated in type A from a mesh of type V.
-template <typename A, typename V>
+// The neighbour terms of S(v) at one cell, accumulated in type A from a mesh of type V (read-only global
+// memory, or shared memory when SMEM).
+template <typename A, typename V, bool SMEM = false>
 __device__ __forceinline__ A neighbour_sum(const V* __restrict__ v, const int n[3], int x, int y, int z, const A p[3],
                                            A g, const A G[3], int local) {
     const int xp = wrap_up(x, n[0]), xm = wrap_dn(x, n[0]);
@@ -108,7 +109,7 @@ __device__ __forceinline__ A neighbour_sum(const V* __restrict__ v, const int n[
     const int64_t sx = (int64_t)n[1] * n[2], sy = n[2];
     const int64_t X0 = x * sx, Xp = xp * sx, Xm = xm * sx;
     const int64_t Y0 = y * sy, Yp = yp * sy, Ym = ym * sy;
-#define L(a, b, c) ((A)__ldg(v + (a) + (b) + (c)))
+#define L(a, b, c) ((A)(SMEM ? v[(a) + (b) + (c)] : __ldg(v + (a) + (b) + (c))))
     const A vxp = L(Xp, Y0, z), vxm = L(Xm, Y0, z);
     const A vyp = L(X0, Yp, z), vym = L(X0, Ym, z);
     const A vzp = L(X0, Y0, zp), vzm = L(X0, Y0, zm);
@@ -734,6 +735,169 @@ static int mg_tb_default(const int n[3], size_t tsize) {
     return 0;
 }
 
+// ---- the V-cycle of the smallest levels in one block per problem ----
+// Below a few thousand cells a level costs more in launches than in work: a V-cycle visit of the levels
+// under 16^3 is ~40 kernels of a few microseconds each.  vcycle_small runs the V-cycle of levels
+// l0 .. l0 + nl - 1 (MGRunner::vcycle's pre-sweeps, residual, restriction, prolongation and post-sweeps,
+// with the one-cell expressions of jacobi_sweep, residual_kernel, reduce_kernel and prolong_kernel) in one
+// block, each level's v, f and scratch in shared memory, a block barrier between steps.  The problems of
+// a batch are one block each.
+constexpr int MG_SMALL_LEVELS = 8;
+constexpr int MG_SMALL_THREADS = 512;
+// Default top level of vcycle_small: 8^3.  Measured per 256^3 local-line-of-sight solve, 10.40 ms with every
+// step its own graph node, 10.05 ms from 8^3 down, 11.98 ms from 16^3 down (one block then does ~93k cell
+// updates per visit on one SM, slower than the ~40 launches it replaces).
+constexpr int MG_SMALL_DEFAULT_CELLS = 512;
+constexpr size_t MG_SMALL_MAX_SMEM = 200 * 1024;
+
+template <typename T> struct SmallVCycle {
+    int nl;
+    Stencil<T> s[MG_SMALL_LEVELS];
+    int off[MG_SMALL_LEVELS];    // level l's arrays v, f, scratch (cells(l) values each) start at off[l]
+    T w;
+    int jn;
+    int zero_v;                  // the top level's v starts at zero (not read)
+};
+
+__device__ __forceinline__ int cells_of(const int n[3]) { return n[0] * n[1] * n[2]; }
+
+__device__ __forceinline__ void cell_xyz(int i, const int n[3], int& x, int& y, int& z) {
+    z = i % n[2];
+    y = (i / n[2]) % n[1];
+    x = i / (n[1] * n[2]);
+}
+
+template <typename T>
+__device__ void small_sweeps(const Stencil<T>& s, T*& v, const T* f, T*& tmp, T w, int niter, bool zero) {
+    const int N = cells_of(s.n);
+    if (niter == 0 && zero)
+        for (int i = threadIdx.x; i < N; i += blockDim.x) v[i] = (T)0;
+    for (int it = 0; it < niter; it++) {
+        const bool z0 = zero && it == 0;
+        for (int i = threadIdx.x; i < N; i += blockDim.x) {
+            int x, y, z;
+            cell_xyz(i, s.n, x, y, z);
+            T p[3], g, G[3];
+            coeffs<T>(s, x, y, z, p, g, G);
+            T jac = f[i];
+            T vc = (T)0;
+            if (!z0) {
+                jac += neighbour_sum<T, T, true>(v, s.n, x, y, z, p, g, G, s.local);
+                vc = v[i];
+            }
+            jac /= (T)2 * (G[0] + G[1] + G[2]);
+            tmp[i] = ((T)1 - w) * vc + w * jac;
+        }
+        T* t = v;
+        v = tmp;
+        tmp = t;
+        __syncthreads();
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MG_SMALL_THREADS) vcycle_small(const T* __restrict__ fg, T* __restrict__ vg,
+                                                                 SmallVCycle<T> P) {
+    pdl_trigger();
+    pdl_wait();
+    extern __shared__ __align__(16) unsigned char mg_smem[];
+    T* sm = (T*)mg_smem;
+    const int N0 = cells_of(P.s[0].n);
+    fg += (int64_t)blockIdx.x * N0;
+    vg += (int64_t)blockIdx.x * N0;
+    T *v[MG_SMALL_LEVELS], *f[MG_SMALL_LEVELS], *t[MG_SMALL_LEVELS];
+    for (int l = 0; l < P.nl; l++) {
+        const int N = cells_of(P.s[l].n);
+        v[l] = sm + P.off[l];
+        f[l] = v[l] + N;
+        t[l] = f[l] + N;
+    }
+    for (int i = threadIdx.x; i < N0; i += blockDim.x) {
+        f[0][i] = fg[i];
+        if (!P.zero_v) v[0][i] = vg[i];
+    }
+    __syncthreads();
+    // down: pre-sweeps, then the residual restricted to the next level's right-hand side
+    for (int l = 0; l < P.nl; l++) {
+        const Stencil<T>& s = P.s[l];
+        small_sweeps(s, v[l], f[l], t[l], P.w, P.jn, l > 0 || P.zero_v);
+        if (l + 1 == P.nl) break;
+        const int N = cells_of(s.n);
+        for (int i = threadIdx.x; i < N; i += blockDim.x) {
+            int x, y, z;
+            cell_xyz(i, s.n, x, y, z);
+            T p[3], g, G[3];
+            coeffs<T>(s, x, y, z, p, g, G);
+            const T nb = neighbour_sum<T, T, true>(v[l], s.n, x, y, z, p, g, G, s.local);
+            const T av = (T)2 * (G[0] + G[1] + G[2]) * v[l][i] - nb;
+            t[l][i] = f[l][i] - av;
+        }
+        __syncthreads();
+        const int* nf = s.n;
+        const int* nc = P.s[l + 1].n;
+        const int Nc = cells_of(nc);
+        for (int i = threadIdx.x; i < Nc; i += blockDim.x) {
+            int x, y, z;
+            cell_xyz(i, nc, x, y, z);
+            const int X[3] = {wrap_dn(2 * x, nf[0]), 2 * x, wrap_up(2 * x, nf[0])};
+            const int Y[3] = {wrap_dn(2 * y, nf[1]), 2 * y, wrap_up(2 * y, nf[1])};
+            const int Z[3] = {wrap_dn(2 * z, nf[2]), 2 * z, wrap_up(2 * z, nf[2])};
+            T acc = 0;
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++) {
+                    const T* row = t[l] + (X[a] * nf[1] + Y[b]) * nf[2];
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        const int side = (a != 1) + (b != 1) + (c != 1);
+                        acc += (T)(8 >> side) * row[Z[c]];
+                    }
+                }
+            f[l + 1][i] = acc / (T)64;
+        }
+        __syncthreads();
+    }
+    // up: the coarse correction prolonged and added, then post-sweeps
+    for (int l = P.nl - 1; l >= 0; l--) {
+        if (l + 1 < P.nl) {
+            const int* nc = P.s[l + 1].n;
+            const int Nc = cells_of(nc);
+            const int nf1 = 2 * nc[1], nf2 = 2 * nc[2];
+            for (int i = threadIdx.x; i < Nc; i += blockDim.x) {
+                int x, y, z;
+                cell_xyz(i, nc, x, y, z);
+                const int xs[2] = {x, wrap_up(x, nc[0])}, ys[2] = {y, wrap_up(y, nc[1])}, zs[2] = {z, wrap_up(z, nc[2])};
+                T c[2][2][2];
+#pragma unroll
+                for (int a = 0; a < 2; a++)
+#pragma unroll
+                    for (int b = 0; b < 2; b++)
+#pragma unroll
+                        for (int d = 0; d < 2; d++) c[a][b][d] = v[l + 1][(xs[a] * nc[1] + ys[b]) * nc[2] + zs[d]];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int ex = (e >> 2) & 1, ey = (e >> 1) & 1, ez = e & 1;
+                    T sum = 0;
+#pragma unroll
+                    for (int a = 0; a <= ex; a++)
+#pragma unroll
+                        for (int b = 0; b <= ey; b++)
+#pragma unroll
+                            for (int d = 0; d <= ez; d++) sum += c[a][b][d];
+                    sum /= (T)((1 + ex) * (1 + ey) * (1 + ez));
+                    T* dst = v[l] + ((2 * x + ex) * nf1 + (2 * y + ey)) * nf2 + (2 * z + ez);
+                    *dst = *dst + sum;
+                }
+            }
+            __syncthreads();
+        }
+        small_sweeps(P.s[l], v[l], f[l], t[l], P.w, P.jn, false);
+    }
+    for (int i = threadIdx.x; i < N0; i += blockDim.x) vg[i] = v[0][i];
+}
+
 // ---------------------------------------------------------------------------------------------
 // Level hierarchy and the FMG / V-cycle drivers
 // ---------------------------------------------------------------------------------------------
@@ -828,8 +992,41 @@ template <typename T> struct MGRunner {
         return PRC_OK;
     }
 
+    // The V-cycle from level l down as one vcycle_small launch, when level l has at most "mg_small_cells"
+    // cells (run-time knob, key 0; 0 runs every step as its own kernel) and its levels fit in shared memory.
+    int small_vcycle(int l, T* v, const T* f, bool v_zero, bool* done) {
+        *done = false;
+        const int limit = tune_get("mg_small_cells", 0, MG_SMALL_DEFAULT_CELLS);
+        const int nl = (int)L.size() - l;
+        if (limit <= 0 || L[l].size() > limit || nl > MG_SMALL_LEVELS) return PRC_OK;
+        SmallVCycle<T> sv;
+        size_t off = 0;
+        sv.nl = nl;
+        for (int j = 0; j < nl; j++) {
+            sv.s[j] = stencil(l + j);
+            sv.off[j] = (int)off;
+            off = (off + 3 * (size_t)L[l + j].size() + 3) & ~(size_t)3;
+        }
+        const size_t smem = off * sizeof(T);
+        if (smem > MG_SMALL_MAX_SMEM) return PRC_OK;
+        sv.w = (T)P.damping;
+        sv.jn = P.jn;
+        sv.zero_v = v_zero ? 1 : 0;
+        if (smem > 48 * 1024 &&
+            cudaFuncSetAttribute(vcycle_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return PRC_ERR_CUDA;
+        PRC_LAUNCH_B("mg_vcycle_small", st, (double)L[l].size() * count * sizeof(T) * (v_zero ? 2 : 3),
+                     launch_pdl(vcycle_small<T>, dim3(count), dim3(MG_SMALL_THREADS), smem, st, f, v, sv));
+        PRC_CHECK_LAUNCH();
+        *done = true;
+        return PRC_OK;
+    }
+
     // Recursive V-cycle on level l: v (B[l].v, or the caller's level-0 pointer) with right-hand side f.
     int vcycle(int l, T*& v, const T* f, bool v_zero) {
+        bool small = false;
+        PRC_TRY(small_vcycle(l, v, f, v_zero, &small));
+        if (small) return PRC_OK;
         PRC_TRY(jacobi(l, v, f, B[l].tmp, P.jn, v_zero));
         if (l + 1 < (int)L.size()) {
             Stencil<T> s = stencil(l);

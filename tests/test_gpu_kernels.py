@@ -573,6 +573,30 @@ def test_multigrid_axis_stencil_same_bits(dtype, mixed, axis):
     assert maxrel(fast, full) < (2e-6 if dtype == 'f4' else 1e-13)
 
 
+@pytest.mark.parametrize('dtype,mixed', [('f8', False), ('f4', True)])
+@pytest.mark.parametrize('los,nmesh', [(None, (32, 32, 32)), ([0., 0., 1.], (64, 32, 48)), ([0.3, -0.5, 0.8], (24, 24, 24)),
+                                       (None, (48, 48, 48))])
+def test_multigrid_small_levels_in_one_block(dtype, mixed, los, nmesh):
+    """The V-cycles of the levels of at most 16^3 cells run as one block per visit (vcycle_small, shared
+    memory); the solve agrees with every step launched as its own kernel (mg_small_cells = 0) to rounding."""
+    L = lib()
+    if los is not None:
+        los = list(np.asarray(los) / np.linalg.norm(los))
+    n0 = L.launch_count()
+    fused = mg_solve(dtype, mixed, nmesh=nmesh, los=los)[0]
+    fused_launches = L.launch_count() - n0
+    L.tune_set('mg_small_cells', 0, 0)
+    try:
+        n0 = L.launch_count()
+        steps = mg_solve(dtype, mixed, nmesh=nmesh, los=los)[0]
+        step_launches = L.launch_count() - n0
+    finally:
+        L.tune_set('mg_small_cells', 0, -1)
+    assert np.isfinite(fused).all()
+    assert fused_launches < step_launches
+    assert maxrel(fused, steps) < (1e-5 if dtype == 'f4' else 1e-12)
+
+
 def _smooth_real_gpu(value, radius_box, nsigmas, dtype):
     L = lib()
     t = torch()
