@@ -38,6 +38,8 @@ VARIANTS = {
     'nopp': ('fft.cu', ['-DPRC_STRIDED_PP=0', '-DPRC_KSPACE_PP=0', '-DPRC_HESS_PP=0', '-DPRC_C2R_PP=0']),
     # every radix-8 twiddle read from the pass table (7 loads per butterfly instead of 3 and 4 products)
     'twload': ('fft.cu', ['-DPRC_TW_RECUR=0']),
+    # the z passes' row transforms with block barriers instead of warp barriers (same arithmetic, same order)
+    'rowblock': ('fft.cu', ['-DPRC_ROW_WARP_SYNC=0']),
 }
 
 

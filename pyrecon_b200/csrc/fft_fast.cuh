@@ -143,8 +143,25 @@ __device__ __forceinline__ void pass_regs(C (&v)[8], int t, const C* __restrict_
     }
 }
 
+// The barrier of an exchange: the block's, or the warp's (WS) when every line the exchange buffer serves
+// lies within one warp (rows of at most 32 threads in whole warps: RowWarp).
+template <bool WS> __device__ __forceinline__ void xsync() {
+    if constexpr (WS) __syncwarp();
+    else __syncthreads();
+}
+
+// PRC_ROW_WARP_SYNC=1: the z passes of power-of-two rows of at most 256 complex points (one warp or less a
+// row, rows in whole warps) synchronise their row-private exchanges per warp instead of per block.
+#ifndef PRC_ROW_WARP_SYNC
+#define PRC_ROW_WARP_SYNC 1
+#endif
+template <int M, int ROWS> struct RowWarp {
+    static constexpr bool value =
+        PRC_ROW_WARP_SYNC && (M & (M - 1)) == 0 && M / 8 <= 32 && (M / 8 * ROWS) % 32 == 0;
+};
+
 // Write the pass outputs to their Stockham destinations, then read back points t + i T.
-template <typename C, int N, int R, int NS, class Addr>
+template <typename C, int N, int R, int NS, class Addr, bool WS = false>
 __device__ __forceinline__ void exchange(C (&v)[8], int t, C* s, const Addr& addr) {
     constexpr int T = N / 8, NB = 8 / R;
 #pragma unroll
@@ -155,21 +172,21 @@ __device__ __forceinline__ void exchange(C (&v)[8], int t, C* s, const Addr& add
 #pragma unroll
         for (int r = 0; r < R; r++) s[addr(base + r * NS)] = v[b + r * NB];
     }
-    __syncthreads();
+    xsync<WS>();
 #pragma unroll
     for (int i = 0; i < 8; i++) v[i] = s[addr(t + i * T)];
-    __syncthreads();
+    xsync<WS>();
 }
 
-template <typename C, int N, int DIR, int P> struct Passes {
+template <typename C, int N, int DIR, int P, bool WS = false> struct Passes {
     template <class Addr>
     static __device__ __forceinline__ void run(C (&v)[8], int t, C* s, const Addr& addr, const C* tw) {
         constexpr int R = TwLayout<N>::radix(P);
         constexpr int NS = ipow8(P);
         pass_regs<C, N, R, NS, DIR>(v, t, tw + TwLayout<N>::offset(P));
         if constexpr (P + 1 < Plan<N>::NPASS) {
-            exchange<C, N, R, NS>(v, t, s, addr);
-            Passes<C, N, DIR, P + 1>::run(v, t, s, addr, tw);
+            exchange<C, N, R, NS, Addr, WS>(v, t, s, addr);
+            Passes<C, N, DIR, P + 1, WS>::run(v, t, s, addr, tw);
         }
     }
 };
@@ -178,7 +195,7 @@ template <typename C, int N, int DIR, int P> struct Passes {
 // exchange's reads: the next write to a buffer comes one exchange later, behind that exchange's
 // barrier.  The caller orders its own accesses to s0 / s1 around the call: s0 must not be read by
 // anyone once the call starts, and neither buffer may be written after it before a barrier.
-template <typename C, int N, int R, int NS, class Addr>
+template <typename C, int N, int R, int NS, class Addr, bool WS = false>
 __device__ __forceinline__ void exchange_pp(C (&v)[8], int t, C* s, const Addr& addr) {
     constexpr int T = N / 8, NB = 8 / R;
 #pragma unroll
@@ -189,12 +206,12 @@ __device__ __forceinline__ void exchange_pp(C (&v)[8], int t, C* s, const Addr& 
 #pragma unroll
         for (int r = 0; r < R; r++) s[addr(base + r * NS)] = v[b + r * NB];
     }
-    __syncthreads();
+    xsync<WS>();
 #pragma unroll
     for (int i = 0; i < 8; i++) v[i] = s[addr(t + i * T)];
 }
 
-template <typename C, int N, int DIR, int P> struct PassesPP {
+template <typename C, int N, int DIR, int P, bool WS = false> struct PassesPP {
     template <class Addr0, class Addr1>
     static __device__ __forceinline__ void run(C (&v)[8], int t, C* s0, const Addr0& addr0, C* s1, const Addr1& addr1,
                                                const C* tw) {
@@ -202,9 +219,9 @@ template <typename C, int N, int DIR, int P> struct PassesPP {
         constexpr int NS = ipow8(P);
         pass_regs<C, N, R, NS, DIR>(v, t, tw + TwLayout<N>::offset(P));
         if constexpr (P + 1 < Plan<N>::NPASS) {
-            if constexpr (P % 2 == 0) exchange_pp<C, N, R, NS>(v, t, s0, addr0);
-            else exchange_pp<C, N, R, NS>(v, t, s1, addr1);
-            PassesPP<C, N, DIR, P + 1>::run(v, t, s0, addr0, s1, addr1, tw);
+            if constexpr (P % 2 == 0) exchange_pp<C, N, R, NS, Addr0, WS>(v, t, s0, addr0);
+            else exchange_pp<C, N, R, NS, Addr1, WS>(v, t, s1, addr1);
+            PassesPP<C, N, DIR, P + 1, WS>::run(v, t, s0, addr0, s1, addr1, tw);
         }
     }
 };
@@ -306,16 +323,19 @@ __device__ __forceinline__ void fft_regs3_pp(C (&v)[8], int t, C* s0, const Addr
 
 // In: v[i] = x[t + i T].  Out: v[i] = X[t + i T] (unnormalised DFT, sign DIR).  tw: the table filled by
 // fill_pass_twiddles<C, N>.  N a power of two, or 3 times one.
-template <typename C, int N, int DIR, class Addr>
+// WS: warp barriers (RowWarp; powers of two only).
+template <typename C, int N, int DIR, bool WS = false, class Addr>
 __device__ __forceinline__ void fft_regs(C (&v)[8], int t, C* s, const Addr& addr, const C* tw) {
+    static_assert(!WS || N % 3 != 0, "warp barriers need power-of-two lines");
     if constexpr (N % 3 == 0) fft_regs3<C, N, DIR>(v, t, s, addr, tw);
-    else Passes<C, N, DIR, 0>::run(v, t, s, addr, tw);
+    else Passes<C, N, DIR, 0, WS>::run(v, t, s, addr, tw);
 }
 
-template <typename C, int N, int DIR, class Addr>
+template <typename C, int N, int DIR, bool WS = false, class Addr>
 __device__ __forceinline__ void fft_regs_pp(C (&v)[8], int t, C* s0, C* s1, const Addr& addr, const C* tw) {
+    static_assert(!WS || N % 3 != 0, "warp barriers need power-of-two lines");
     if constexpr (N % 3 == 0) fft_regs3_pp<C, N, DIR>(v, t, s0, addr, s1, addr, tw);
-    else PassesPP<C, N, DIR, 0>::run(v, t, s0, addr, s1, addr, tw);
+    else PassesPP<C, N, DIR, 0, WS>::run(v, t, s0, addr, s1, addr, tw);
 }
 
 // The same with a separate layout for s0, the buffer of the first (and every even) exchange.
@@ -603,16 +623,16 @@ __global__ void __launch_bounds__(N / 8 * B, (MinBlocks<T, N / 8 * B, PRC_KSPACE
 // the M-point transform Z, then X[k] = (Z[k] + conj Z[M-k]) / 2 - i w^k (Z[k] - conj Z[M-k]) / 2 for
 // k < M and X[M] = Re Z[0] - Im Z[0], stored at dst when ok.  buf (the row's exchange buffer, addr) is
 // written from the start: the caller's earlier reads of it must be behind a barrier.  Ends with a barrier.
-template <typename T, int M, class Addr>
+template <typename T, int M, bool WS = false, class Addr>
 __device__ __forceinline__ void row_r2c(cplx_t<T> (&v)[8], bool ok, int t, cplx_t<T>* buf, const Addr& addr,
                                         const cplx_t<T>* tw, const cplx_t<T>* wk, cplx_t<T>* dst) {
     typedef cplx_t<T> C;
     constexpr int TL = M / 8;
-    fft_regs<C, M, -1>(v, t, buf, addr, tw);
+    fft_regs<C, M, -1, WS>(v, t, buf, addr, tw);
     // unpack needs Z[M - k]: publish Z, then combine
 #pragma unroll
     for (int i = 0; i < 8; i++) buf[addr(t + i * TL)] = v[i];
-    __syncthreads();
+    xsync<WS>();
 #pragma unroll
     for (int i = 0; i < 8; i++) {
         const int k = t + i * TL;
@@ -627,7 +647,7 @@ __device__ __forceinline__ void row_r2c(cplx_t<T> (&v)[8], bool ok, int t, cplx_
         const C z0 = v[0];
         dst[M] = cmake<C>(z0.x - z0.y, (T)0);
     }
-    __syncthreads();
+    xsync<WS>();
 }
 
 // row_r2c with the transform's exchanges alternating between s0 and s1 (fft_regs_pp) and Z published in
@@ -635,17 +655,17 @@ __device__ __forceinline__ void row_r2c(cplx_t<T> (&v)[8], bool ok, int t, cplx_
 // barrier: a barrier per exchange plus one.  On entry s0 must be free (not read by anyone after the
 // caller's last barrier) and s1 free once the first exchange's barrier is reached; on return the
 // partner reads of Z are not fenced: the caller puts a barrier before the next write to either buffer.
-template <typename T, int M, class Addr>
+template <typename T, int M, bool WS = false, class Addr>
 __device__ __forceinline__ void row_r2c_pp(cplx_t<T> (&v)[8], bool ok, int t, cplx_t<T>* s0, cplx_t<T>* s1,
                                            const Addr& addr, const cplx_t<T>* tw, const cplx_t<T>* wk,
                                            cplx_t<T>* dst) {
     typedef cplx_t<T> C;
     constexpr int TL = M / 8, NX = Shape<M>::NX;   // exchanges: s0, s1, s0, ...
-    fft_regs_pp<C, M, -1>(v, t, s0, s1, addr, tw);
+    fft_regs_pp<C, M, -1, WS>(v, t, s0, s1, addr, tw);
     C* zb = NX == 0 ? s0 : ((NX - 1) % 2 == 0 ? s1 : s0);
 #pragma unroll
     for (int i = 0; i < 8; i++) zb[addr(t + i * TL)] = v[i];
-    __syncthreads();
+    xsync<WS>();
 #pragma unroll
     for (int i = 0; i < 8; i++) {
         const int k = t + i * TL;
@@ -695,7 +715,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS) z_r2c(RealsIn in, Specs<cplx_t<T
                 v[i] = cmake<C>((T)x.x, (T)x.y);
             }
         }
-        row_r2c<T, M>(v, ok, t, buf, addr, tw, wk, out.p[bi] + (ok ? row : 0) * pitch);
+        row_r2c<T, M, RowWarp<M, ROWS>::value>(v, ok, t, buf, addr, tw, wk, out.p[bi] + (ok ? row : 0) * pitch);
     }
 }
 
@@ -721,7 +741,7 @@ template <int ET> struct EpiInputs {
 };
 
 // Inverse z transform of one row: returns v[i] = (x[2k], x[2k+1]), k = t + i TL, unscaled.
-template <typename T, int M, class Addr>
+template <typename T, int M, bool WS = false, class Addr>
 __device__ __forceinline__ void row_c2r(const cplx_t<T>* __restrict__ src, bool ok, int t, cplx_t<T>* buf,
                                         const Addr& addr, const cplx_t<T>* tw, const cplx_t<T>* wk,
                                         cplx_t<T> (&v)[8]) {
@@ -731,7 +751,7 @@ __device__ __forceinline__ void row_c2r(const cplx_t<T>* __restrict__ src, bool 
 #pragma unroll
     for (int i = 0; i < 8; i++) buf[addr(t + i * TL)] = ok ? src[t + i * TL] : cmake<C>(0, 0);
     if (t == 0) buf[addr(M)] = ok ? src[M] : cmake<C>(0, 0);
-    __syncthreads();
+    xsync<WS>();
 #pragma unroll
     for (int i = 0; i < 8; i++) {
         const int k = t + i * TL;
@@ -741,8 +761,8 @@ __device__ __forceinline__ void row_c2r(const cplx_t<T>* __restrict__ src, bool 
         const C od = cmul(cconj(wk[k]), csub(xk, xc));
         v[i] = cadd(ev, cmul_i(od, +1));
     }
-    __syncthreads();
-    fft_regs<C, M, +1>(v, t, buf, addr, tw);
+    xsync<WS>();
+    fft_regs<C, M, +1, WS>(v, t, buf, addr, tw);
 }
 
 // Input rows read straight from global memory into the row buffer (register kernels).
@@ -751,9 +771,10 @@ template <typename T, int M> struct GlobalRows {
     static constexpr bool PP = false;   // one exchange buffer (row_c2r uses fft_regs)
     const Specs<C>& in;
     int pitch;
+    template <bool WS>
     __device__ __forceinline__ void row(int c, int64_t row, bool ok, int t, C* buf, const RowAddr& addr, const C* tw,
                                         const C* wk, C (&v)[8]) {
-        row_c2r<T, M>(select6(in, c) + row * pitch, ok, t, buf, addr, tw, wk, v);
+        row_c2r<T, M, WS>(select6(in, c) + row * pitch, ok, t, buf, addr, tw, wk, v);
     }
     __device__ __forceinline__ bool stop() { return false; }
 };
@@ -767,6 +788,7 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
     typedef cplx_t<T> C;
     constexpr int TL = M / 8, N2 = 2 * M, RS = row_stride(M);
     constexpr int NMAX = EpiInputs<ET>::NMAX;
+    constexpr bool WS = RowWarp<M, ROWS>::value;   // row-private exchanges synchronised per warp
     const int line = threadIdx.x / TL, t = threadIdx.x % TL;
     const RowAddr addr{line * RS};
     const int64_t rows = (int64_t)dims.n[0] * dims.n[1];
@@ -782,7 +804,7 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
             for (int c = 0; c < NMAX; c++) {
                 if (c < nin) {
                     C v[8];
-                    src.row(c, row, ok, t, buf, addr, tw, wk, v);
+                    src.template row<WS>(c, row, ok, t, buf, addr, tw, wk, v);
                     C* o = (C*)(e.out[c] + (ok ? row : 0) * N2);
                     if (ok) {
 #pragma unroll
@@ -793,9 +815,9 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
         } else if constexpr (ET == EPI_STORE4) {
             // three inputs -> one interleaved (x, y, z, 0) quadruple per cell
             C v0[8], v1[8], v2[8];
-            src.row(0, row, ok, t, buf, addr, tw, wk, v0);
-            src.row(1, row, ok, t, buf, addr, tw, wk, v1);
-            src.row(2, row, ok, t, buf, addr, tw, wk, v2);
+            src.template row<WS>(0, row, ok, t, buf, addr, tw, wk, v0);
+            src.template row<WS>(1, row, ok, t, buf, addr, tw, wk, v1);
+            src.template row<WS>(2, row, ok, t, buf, addr, tw, wk, v2);
             if (ok) {
                 typedef typename vec4_of<T>::type V4;
                 V4* o = (V4*)(e.out[0] + row * N2 * 4);
@@ -808,8 +830,8 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
             }
         } else if constexpr (ET == EPI_DENSITY) {
             C d[8], r[8];
-            src.row(0, row, ok, t, buf, addr, tw, wk, d);
-            src.row(1, row, ok, t, buf, addr, tw, wk, r);
+            src.template row<WS>(0, row, ok, t, buf, addr, tw, wk, d);
+            src.template row<WS>(1, row, ok, t, buf, addr, tw, wk, r);
             const double sd = e.sums[0], sr = e.sums[1];
             const double alpha = sd * 1. / sr;
             const double threshold = e.ran_min * sr / e.size_randoms;
@@ -825,7 +847,7 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
             }
         } else if constexpr (ET == EPI_DENSITY_NORANDOMS) {
             C d[8];
-            src.row(0, row, ok, t, buf, addr, tw, wk, d);
+            src.template row<WS>(0, row, ok, t, buf, addr, tw, wk, d);
             const double mean = e.sums[0] / e.ncells;
             if (ok) {
 #pragma unroll
@@ -851,7 +873,7 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
 #pragma unroll 1
             for (int c = 0; c < 3; c++) {
                 C v[8];
-                src.row(c, row, ok, t, buf, addr, tw, wk, v);
+                src.template row<WS>(c, row, ok, t, buf, addr, tw, wk, v);
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
 #pragma unroll
@@ -883,12 +905,12 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
                     // the inverse transforms exchanged through buf, buf2, buf, ...: the first buffer
                     // the forward one writes must not be the one their last exchange read
                     constexpr int NX = Shape<M>::NX;
-                    if constexpr (NX == 0 || (NX - 1) % 2 == 0) __syncthreads();
-                    row_r2c_pp<T, M>(z, ok, t, buf, src.buf2, addr, tw, wk, dst);
-                    __syncthreads();
+                    if constexpr (NX == 0 || (NX - 1) % 2 == 0) xsync<WS>();
+                    row_r2c_pp<T, M, WS>(z, ok, t, buf, src.buf2, addr, tw, wk, dst);
+                    xsync<WS>();
                 } else {
-                    __syncthreads();   // every thread is past its reads of the exchange buffer
-                    row_r2c<T, M>(z, ok, t, buf, addr, tw, wk, dst);
+                    xsync<WS>();   // every thread of the row is past its reads of the exchange buffer
+                    row_r2c<T, M, WS>(z, ok, t, buf, addr, tw, wk, dst);
                 }
             } else if (ok) {
 #pragma unroll
@@ -917,7 +939,7 @@ __device__ __forceinline__ void z_c2r_body(Src& src, int nin, const Dims& dims, 
 #pragma unroll 1
             for (int c = 0; c < NMAX; c++) {
                 C v[8];
-                src.row(c, row, ok, t, buf, addr, tw, wk, v);
+                src.template row<WS>(c, row, ok, t, buf, addr, tw, wk, v);
                 const T fc = (T)select6(e.factor, c) * sc;
 #pragma unroll
                 for (int i = 0; i < 8; i++) {

@@ -378,7 +378,10 @@ template <typename T, int M, int ROWS, int S> struct TmaRows {
             for (int u = 0; u < S; u++) issue(u);
     }
 
-    // Same result as row_c2r, the row read from the stage instead of global memory.
+    // Same result as row_c2r, the row read from the stage instead of global memory.  The barrier before
+    // the stage is re-armed stays the block's (every row of the tile reads the stage); WS: the row's
+    // transform exchanges synchronise per warp.
+    template <bool WS>
     __device__ __forceinline__ void row(int, int64_t, bool, int t, C* buf, const RowAddr& addr, const C* tw,
                                         const C* wk, C (&v)[8]) {
         constexpr int TL = M / 8;
@@ -403,8 +406,8 @@ template <typename T, int M, int ROWS, int S> struct TmaRows {
             issue(next + S);
         }
         next++;
-        if constexpr (PRC_C2R_PP) fft_regs_pp<C, M, +1>(v, t, buf, buf2 + (buf - buf1), addr, tw);
-        else fft_regs<C, M, +1>(v, t, buf, addr, tw);
+        if constexpr (PRC_C2R_PP) fft_regs_pp<C, M, +1, WS>(v, t, buf, buf2 + (buf - buf1), addr, tw);
+        else fft_regs<C, M, +1, WS>(v, t, buf, addr, tw);
     }
 
     // End of a tile: if any thread's wait ran out, thread 0 waits (bounded) for the copies it issued

@@ -214,11 +214,12 @@ def _fft_outputs(path, nmesh, dtype):
     np.savez(path, spec=spec.cpu().numpy(), back=back.cpu().numpy())
 
 
-@pytest.mark.parametrize('variant', ['nopp'])
+@pytest.mark.parametrize('variant', ['nopp', 'rowblock'])
 def test_library_variant_same_bits(variant, tmp_path):
-    """The library built with the ping-pong exchanges switched off (two barriers per exchange) gives the
-    same bits as the default build on the nmesh-256 iterative pipeline and a 512^3 FFT round trip: the
-    exchanges change only which shared-memory buffer a pass reads."""
+    """The library built with the ping-pong exchanges switched off (two barriers per exchange), or with the
+    z passes' row exchanges synchronised per block instead of per warp, gives the same bits as the default
+    build on the nmesh-256 iterative pipeline and a 512^3 FFT round trip: the exchanges change only which
+    shared-memory buffer a pass reads and which threads wait for it."""
     from pyrecon_b200 import build
     assert os.path.isfile(build.library_path(variant)), 'variant {} not built'.format(variant)
     for kind, args in [('pipeline', ('iterative_fft', 256, 'f4')), ('fft', ((512, 512, 512), 'f4'))]:
