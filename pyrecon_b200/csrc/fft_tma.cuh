@@ -337,6 +337,11 @@ __global__ void __launch_bounds__(N / 8 * B, (LEAN ? MinBlocks<T, N / 8 * B, 2>:
 // each tile, tiles blockIdx.x, blockIdx.x + gridDim.x, ...
 // PRC_C2R_PP: the row transforms exchange through two row buffers in turn (fft_regs_pp); the barrier
 // before a stage is re-armed also orders each row's first exchange after the previous row's reads.
+// Rows in whole warps (RowWarp): no block barrier per unit.  Each warp releases a stage once it has read
+// its rows (one arrival on the stage's `empty` barrier, which counts the warps), and thread 0 re-arms the
+// stage of the previous unit once every warp has released it (a bounded wait that normally finds it
+// done): S - 1 units stay in flight ahead of the one being read, and the warps of a block drift apart
+// instead of meeting at every row transform.
 #ifndef PRC_C2R_PP
 #define PRC_C2R_PP 1
 #endif
@@ -346,10 +351,12 @@ template <typename T, int M, int ROWS, int S> struct TmaRows {
     static constexpr int PS = (M + 1 + Q - 1) / Q * Q;
     static constexpr int STAGE = ROWS * PS;
     static constexpr bool PP = PRC_C2R_PP;   // the row transforms alternate between buf1 and buf2
+    static constexpr bool WR = RowWarp<M, ROWS>::value;   // stages released per warp
     C* stages;
     C* buf1 = nullptr;       // PRC_C2R_PP: the row buffer the caller passes, and the second one
     C* buf2 = nullptr;       // (same layout, so a row's offset in buf1 is its offset in buf2)
     uint64_t* bars;
+    uint64_t* empty = nullptr;   // WR: per stage, the warps that have read its unit
     const Specs<C>& in;
     int nin;
     int64_t rows, ntiles;
@@ -400,10 +407,25 @@ template <typename T, int M, int ROWS, int S> struct TmaRows {
             const C od = cmul(cconj(wk[k]), csub(xk, xc));
             v[i] = cadd(ev, cmul_i(od, +1));
         }
-        __syncthreads();
-        if (threadIdx.x == 0 && !failed) {
-            prc::tma::fence_proxy_async();
-            issue(next + S);
+        if constexpr (WR) {
+            __syncwarp();
+            if ((threadIdx.x & 31) == 0) prc::tma::arrive(&empty[st]);
+            if (threadIdx.x == 0 && !failed && next >= 1) {
+                const int64_t u = next - 1;
+                if (prc::tma::wait(&empty[u % S], (uint32_t)((u / S) & 1))) {
+                    prc::tma::fence_proxy_async();
+                    issue(u + S);
+                } else {
+                    if (first_fail < 0) first_fail = next;
+                    failed = true;
+                }
+            }
+        } else {
+            __syncthreads();
+            if (threadIdx.x == 0 && !failed) {
+                prc::tma::fence_proxy_async();
+                issue(next + S);
+            }
         }
         next++;
         if constexpr (PRC_C2R_PP) fft_regs_pp<C, M, +1, WS>(v, t, buf, buf2 + (buf - buf1), addr, tw);
@@ -428,7 +450,7 @@ template <typename T, int M, int ROWS, int S> struct C2RTmaSmem {
     static constexpr size_t STAGES = (size_t)S * TmaRows<T, M, ROWS, S>::STAGE * sizeof(C);
     static constexpr size_t BUF = (size_t)ROWS * row_stride(M) * sizeof(C);
     static constexpr size_t BYTES =
-        STAGES + (PRC_C2R_PP ? 2 : 1) * BUF + (size_t)(2 * M + 1) * sizeof(C) + 8 + S * sizeof(uint64_t);
+        STAGES + (PRC_C2R_PP ? 2 : 1) * BUF + (size_t)(2 * M + 1) * sizeof(C) + 8 + 2 * S * sizeof(uint64_t);
 };
 
 template <typename T, int M, int ROWS, int ET, int S>
@@ -443,8 +465,11 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
     C* tw = buf2 + (PRC_C2R_PP ? ROWS * row_stride(M) : 0);
     C* wk = tw + M;
     uint64_t* bars = (uint64_t*)(((uintptr_t)(wk + M + 1) + 7) & ~(uintptr_t)7);
+    uint64_t* empty = bars + S;
     if (threadIdx.x == 0) {
         for (int i = 0; i < S; i++) prc::tma::barrier_init(&bars[i], 1);
+        if constexpr (Rows::WR)
+            for (int i = 0; i < S; i++) prc::tma::barrier_init(&empty[i], blockDim.x / 32);
         prc::tma::fence_barrier_init();
     }
     fill_pass_twiddles<C, M>(tw);
@@ -457,6 +482,7 @@ __global__ void __launch_bounds__(M / 8 * ROWS, (MinBlocks<T, M / 8 * ROWS, PRC_
     Rows src(stages, bars, in, nin, (int64_t)dims.n[0] * dims.n[1]);
     src.buf1 = buf;
     src.buf2 = buf2;
+    src.empty = empty;
     src.start();
     z_c2r_body<T, M, ROWS, ET>(src, nin, dims, e, tw, wk, buf);
 }
