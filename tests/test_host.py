@@ -212,6 +212,29 @@ def test_serving_admission_counts_resident_slot_memory():
     assert ReconstructionServer._pick_slot(srv, 20.) == (2, 10.)      # slot 2 holds 30: nothing added
 
 
+def test_serving_batch_keys():
+    """Queued multigrid and plane-parallel requests of the same mesh and settings share a batch key (one
+    batched run); another mesh, other settings, catalogue-derived geometry or another algorithm do not."""
+    from pyrecon_b200.serving import ReconstructionRequest, batch_key
+    cat = np.zeros((10, 3))
+    box = dict(f=0.8, bias=2., los='z', boxsize=1000., boxcenter=500., wrap=True, dtype='f4',
+               density_kwargs=dict(smoothing_radius=15.))
+
+    def req(algo, **kw):
+        args = dict(box, **kw)
+        return ReconstructionRequest(algo, data=cat, **args)
+
+    for algo in ['MultiGridReconstruction', 'PlaneParallelFFTReconstruction']:
+        a, b = req(algo, nmesh=64), req(algo, nmesh=64)
+        assert batch_key(a) is not None and batch_key(a) == batch_key(b)
+        assert batch_key(req(algo, nmesh=128)) != batch_key(a)
+        assert batch_key(req(algo, nmesh=64, f=0.7)) != batch_key(a)
+        assert batch_key(ReconstructionRequest(algo, data=cat, positions=cat, **box)) is None
+    assert batch_key(req('MultiGridReconstruction', nmesh=64)) != batch_key(req('PlaneParallelFFTReconstruction',
+                                                                               nmesh=64))
+    assert batch_key(req('IterativeFFTReconstruction', nmesh=64)) is None
+
+
 def test_flag_words_map_to_mesh_errors():
     """Every PRC_FLAG_* bit the kernels can raise (box, NaN/inf, a bounded device wait that gave up) turns
     into MeshError on the host; the header and the binding agree on the values."""
