@@ -41,12 +41,12 @@ sys.path.insert(0, ROOT)
 METRIC = 'recons/s + p50/p99 latency vs plain GPU path, nmesh 512, shift err<1e-3 Mpc/h'
 
 WORKLOADS = {
-    # BASELINE config: IterativeFFTReconstruction nmesh=512, boxsize=2000, niterations=3, f=0.8, bias=2, local los,
+    # the metric's workload: IterativeFFTReconstruction nmesh=512, boxsize=2000, niterations=3, f=0.8, bias=2, local los,
     # smoothing_radius=15, 5M lognormal data, 20M uniform randoms, float32 positions
     'iterative_fft_512': dict(algorithm='IterativeFFTReconstruction', nmesh=512, boxsize=2000., boxcenter=2000.,
                               los=None, ndata=5_000_000, nrandoms=20_000_000, pos_dtype='f4', dtype='f4',
                               weights=None, run_kwargs=dict(niterations=3)),
-    # BASELINE config: MultiGridReconstruction nmesh=256, boxsize=2000, local los, 2M data, 10M randoms,
+    # multigrid workload: MultiGridReconstruction nmesh=256, boxsize=2000, local los, 2M data, 10M randoms,
     # weights uniform in [0.5, 1.5]; FP32 stencils with FP64 residual refinement
     'multigrid_256': dict(algorithm='MultiGridReconstruction', nmesh=256, boxsize=2000., boxcenter=2000., los=None,
                           ndata=2_000_000, nrandoms=10_000_000, pos_dtype='f8', dtype='f4', weights=(0.5, 1.5),
@@ -76,13 +76,13 @@ DEFAULT_WORKLOAD = 'iterative_fft_512'
 # Many requests at once through the request loop (pyrecon_b200.serving), against the same requests run one
 # after the other on one stream (the plain path).  A step is the whole set of requests.
 MULTI_WORKLOADS = {
-    # BASELINE config: 64 periodic-box mocks, plane-parallel and multigrid mixed, los='z', nmesh in
+    # batched mocks: 64 periodic-box mocks, plane-parallel and multigrid mixed, los='z', nmesh in
     # {128, 192, 256}, boxsize 1000, 0.3M-2M lognormal data each, no randoms
     'batched_mocks': dict(kind='batched', nrequests=64, algorithms=['PlaneParallelFFTReconstruction',
                                                                     'MultiGridReconstruction'],
                           nmesh=[128, 192, 256], ndata=(300_000, 2_000_000), randoms_factor=0, boxsize=1000.,
                           boxcenter=500., los='z', wrap=True, dtype='f4', slots=2, max_batch=8, passes=5),
-    # BASELINE config: 500 requests with Poisson arrivals at 20 req/s, the three algorithms, nmesh in
+    # serving: 500 requests with Poisson arrivals at 20 req/s, the three algorithms, nmesh in
     # {128, 256, 384, 512}, 0.5M-8M data with 4x randoms, 150 GB admission budget.  Two slots: measured
     # p50 / p99 19.5-19.9 / 162-171 ms with 2, 21.3 / 174 with 1, 20.1 / 201 with 4 (the device is ~43 %
     # busy at this rate; more concurrent requests stretch the long ones)
