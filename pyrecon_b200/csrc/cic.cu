@@ -897,17 +897,48 @@ __device__ __forceinline__ void cic_read3(const typename vec4_of<F>::type* __res
 template <typename F>
 __device__ __forceinline__ void fd_read(const F* __restrict__ m, const Cic<F>& c, const int n[3], const F twocell[3],
                                         F out[3]) {
+    // Along each axis the eight corners and their +-1 neighbours span four nodes, lo - 1, lo, hi, hi + 1
+    // (periodic), indexed 0..3: corner c (0 or 1) sits at index c + 1, its neighbours at c and c + 2.  The
+    // 32 distinct values are loaded once from precomputed plane, row and cell offsets; the arithmetic and
+    // its order are those of the corner loop of src/mesh.c:187-266.
+    const int64_t sx = (int64_t)n[1] * n[2];
+    const int64_t X[4] = {wrap_dn(c.lo[0], n[0]) * sx, c.lo[0] * sx, c.hi[0] * sx, wrap_up(c.hi[0], n[0]) * sx};
+    const int64_t Y[4] = {(int64_t)wrap_dn(c.lo[1], n[1]) * n[2], (int64_t)c.lo[1] * n[2], (int64_t)c.hi[1] * n[2],
+                          (int64_t)wrap_up(c.hi[1], n[1]) * n[2]};
+    const int Z[4] = {wrap_dn(c.lo[2], n[2]), c.lo[2], c.hi[2], wrap_up(c.hi[2], n[2])};
+    F xv[4][2][2], yv[2][4][2], zv[2][2][4];   // [axis index 0..3 along the derivative's axis][corner][corner]
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const bool core = e == 1 || e == 2;
+                xv[e][a][b] = __ldg(m + X[e] + Y[a + 1] + Z[b + 1]);
+                yv[a][e][b] = core ? F(0) : __ldg(m + X[a + 1] + Y[e] + Z[b + 1]);
+                zv[a][b][e] = core ? F(0) : __ldg(m + X[a + 1] + Y[b + 1] + Z[e]);
+            }
+        }
+    // core nodes (indices 1, 2 on every axis) come from the x table
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int e = 1; e < 3; e++) {
+                yv[a][e][b] = xv[a + 1][e - 1][b];
+                zv[a][b][e] = xv[a + 1][b][e - 1];
+            }
     const int order[8] = {0, 4, 2, 1, 6, 5, 3, 7};   // (cx<<2 | cy<<1 | cz)
     F g[3] = {0, 0, 0};
 #pragma unroll
     for (int kk = 0; kk < 8; kk++) {
         const int k = order[kk];
         const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
-        const int x = cx ? c.hi[0] : c.lo[0], y = cy ? c.hi[1] : c.lo[1], z = cz ? c.hi[2] : c.lo[2];
         const F wt = rn_mul(rn_mul(c.w[0][cx], c.w[1][cy]), c.w[2][cz]);
-        const F gx = rn_mul(rn_sub(__ldg(m + at3(n, wrap_up(x, n[0]), y, z)), __ldg(m + at3(n, wrap_dn(x, n[0]), y, z))), wt);
-        const F gy = rn_mul(rn_sub(__ldg(m + at3(n, x, wrap_up(y, n[1]), z)), __ldg(m + at3(n, x, wrap_dn(y, n[1]), z))), wt);
-        const F gz = rn_mul(rn_sub(__ldg(m + at3(n, x, y, wrap_up(z, n[2]))), __ldg(m + at3(n, x, y, wrap_dn(z, n[2])))), wt);
+        const F gx = rn_mul(rn_sub(xv[cx + 2][cy][cz], xv[cx][cy][cz]), wt);
+        const F gy = rn_mul(rn_sub(yv[cx][cy + 2][cz], yv[cx][cy][cz]), wt);
+        const F gz = rn_mul(rn_sub(zv[cx][cy][cz + 2], zv[cx][cy][cz]), wt);
         if (kk == 0) {
             g[0] = gx; g[1] = gy; g[2] = gz;
         } else {
